@@ -1,0 +1,167 @@
+/* nrg_b200.h -- C-ABI of the B200 (sm_100a) NRG step core.
+ *
+ * Drop-in boundary for the data-parallel hot path of one NRG iteration of NRG Ljubljana:
+ * the diagonalisation of every symmetry-subspace block, the recalculation of irreducible
+ * matrix elements (U^T O U contractions), the density-matrix rotations and the DM-NRG /
+ * FDM spectral-weight accumulation into log-spaced bins. All arithmetic is FP64.
+ *
+ * Conventions (those of the reference):
+ *   - matrices are dense ROW-major with an explicit leading dimension (elements between
+ *     rows); strided views such as the ancestor blocks U(i) of recalc.hpp are expressed
+ *     by a pointer to their first element plus the leading dimension of the parent;
+ *   - a diagonalised block returns its eigenvalues ascending and its eigenvectors as ROWS
+ *     (vec(r, j) = component j of eigenvector r), c++/diag.hpp:41-48;
+ *   - entry points without the _host suffix take DEVICE pointers and are asynchronous on
+ *     `stream` (a cudaStream_t, NULL = legacy default stream); the _host variants take
+ *     HOST pointers, copy in, compute and copy out, and return when the results are in
+ *     host memory.
+ * Return codes: NRG_OK, a negative NRG_ERR_* code, or (diagonalisation) the number of
+ * blocks whose per-block status word is non-zero. nrg_last_error() gives the message of
+ * the last failure on the calling thread. No entry point falls back to the CPU.
+ */
+#ifndef NRG_B200_H
+#define NRG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NRG_B200_VERSION 1
+
+#define NRG_OK 0
+#define NRG_ERR_ARG (-1)    /* invalid argument (sizes, null pointers, shapes) */
+#define NRG_ERR_CUDA (-2)   /* a CUDA runtime call or a kernel launch failed */
+#define NRG_ERR_OOM (-3)    /* device workspace could not be allocated within the budget */
+#define NRG_ERR_NODEV (-4)  /* no usable sm_100 device */
+
+#if defined(__GNUC__)
+#define NRG_API __attribute__((visibility("default")))
+#else
+#define NRG_API
+#endif
+
+typedef struct nrg_ctx nrg_ctx;
+
+NRG_API int nrg_version(void);
+NRG_API const char* nrg_last_error(void);
+
+/* Per-run context: device, device workspace (grown on demand up to workspace_limit bytes,
+ * 0 = 90% of the free device memory at creation), descriptor staging. One context may
+ * be used from one host thread at a time. */
+NRG_API int nrg_create(nrg_ctx** ctx, int device, size_t workspace_limit);
+NRG_API int nrg_destroy(nrg_ctx* ctx);
+
+/* ------------------------------------------------------------------ diagonalisation
+ * Replaces diagonalise() (c++/diag.hpp:261-292) with diag=dsyev|dsyevd|default for real
+ * matrices, and the per-step batch loop diagonalisations() / diagonalisations_OpenMP()
+ * (c++/core.hpp:90-120): all nblk blocks of a step in one call.
+ *   n[b]       order of block b (host array), 1 <= n[b] <= NRG_DIAG_MAX_N
+ *   H[b]       n x n row-major, upper triangle read (lower ignored); CONSUMED (overwritten),
+ *              as the reference consumes its argument (c++/diag.hpp:259-260)
+ *   evals[b]   n doubles, ascending
+ *   evecs[b]   n x n row-major, row r = eigenvector of evals[b][r]
+ *   info       host array of nblk status words: 0 ok; -2 non-finite input; > 0 the
+ *              tridiagonal iteration did not converge (the reference's INFO != 0)
+ * H, evals, evecs are host arrays of device pointers; evecs[b] must not alias H[b]. */
+#define NRG_DIAG_MAX_N 4096
+NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* H, double* const* evals,
+                   double* const* evecs, int* info, void* stream);
+
+/* Same with host pointers for H[b], evals[b], evecs[b] (the call the reference's
+ * diagonalise() makes with its ublas matrix); H[b] is left unchanged. */
+NRG_API int nrg_diag_batch_host(nrg_ctx* ctx, int nblk, const int* n, const double* const* H, double* const* evals,
+                        double* const* evecs, int* info, void* stream);
+
+/* ------------------------------------------------------------------ GEMM leaves
+ * One term M += factor * op(A) * O * op(B), grouped by M. Expresses
+ *   product   (c++/numerics_ublas.hpp:108-116): M += f A B^T         O = NULL, transB = 1
+ *   transform (c++/numerics_ublas.hpp:119-128): M += f A O B^T       transB = 1
+ *   rotate    (c++/numerics_ublas.hpp:130-140): M += f U^T O U       A = U, transA = 1, B = U
+ * as used by recalc_general / recalc_f / recalc1_global (c++/recalc.hpp:52-122) and
+ * cdmI (c++/dmnrg.hpp:55-80). op(A) is rows x ka, O is ka x kb (NULL means the identity,
+ * ka == kb), op(B) is kb x cols. The product O op(B) is formed first, as in the
+ * reference. Terms with the same M are summed in the order given; distinct M regions must
+ * not overlap. A term with rows, cols, ka or kb zero is skipped (finite_size checks of the
+ * reference). Pointers are device pointers. */
+typedef struct nrg_gemm3 {
+  double* M;
+  int64_t ldm;
+  const double* A;
+  int64_t lda;
+  const double* O;
+  int64_t ldo;
+  const double* B;
+  int64_t ldb;
+  int rows, cols, ka, kb;
+  int transA, transB;
+  double factor;
+} nrg_gemm3;
+
+NRG_API int nrg_gemm3_batch(nrg_ctx* ctx, int nterm, const nrg_gemm3* terms, void* stream);
+NRG_API int nrg_gemm3_batch_host(nrg_ctx* ctx, int nterm, const nrg_gemm3* terms, void* stream);
+
+/* ------------------------------------------------------------------ spectral accumulation
+ * Replaces the per-pair calc() of Algo_DMNRG (c++/algo_DMNRG.hpp:29-52), Algo_FDMgt
+ * (c++/algo_FDM.hpp:84-114) and Algo_FDMls (c++/algo_FDM.hpp:30-60), driven over all
+ * subspace pairs of one step as BaseSpectrum::calc does (c++/algo.hpp:55-67), binned by
+ * ChainBinning/Bins (c++/spectrum.hpp:19-28, c++/bins.hpp:95-132) on the standard log
+ * grid. Weights are real (S = double). One pair (Ii, Ij) has
+ *   op1, op2   dim_j x dim_i, row-major (rows: states of Ij, columns: states of Ii)
+ *   Ei, Ej     energies (abs_zero for DMNRG, abs_G for FDM), ni and nj entries
+ *   ki, kj     kept states (DMNRG: the loop ranges; FDM: K ranges, the rest is D)
+ *   rho_i      DMNRG: rho(Ii) (ki x ki); FDM-gt: rhoFDM(Ii) (rdi x rdi); else unused
+ *   rho_j      DMNRG: rho(Ij) (kj x kj); FDM-ls: rhoFDM(Ij) (rdj x rdj); else unused
+ *   factor     ff(Ii, Ij)
+ * algo: NRG_SPEC_DMNRG, NRG_SPEC_FDMGT, NRG_SPEC_FDMLS. pos/neg: device arrays of
+ * bins.nbins doubles per sign half, ACCUMULATED (+=). */
+#define NRG_SPEC_DMNRG 0
+#define NRG_SPEC_FDMGT 1
+#define NRG_SPEC_FDMLS 2
+
+typedef struct nrg_spec_pair {
+  const double* Ei;
+  const double* Ej;
+  const double* op1;
+  int64_t ld1;
+  const double* op2;
+  int64_t ld2;
+  const double* rho_i;
+  int64_t ldri;
+  const double* rho_j;
+  int64_t ldrj;
+  int ni, ki, nj, kj;
+  int rdi, rdj;
+  double factor;
+} nrg_spec_pair;
+
+typedef struct nrg_spec_params {
+  int algo;
+  int sign;      /* 1 bosonic, -1 fermionic (gf_sign) */
+  double T;      /* temperature (FDM) */
+  double wnf;    /* stats.wnfactor[step.ndx()] (FDM) */
+  double Emin;   /* DMNRG window: step.scale() * P.getEmin() */
+  double Emax;   /* DMNRG window: step.scale() * P.getEmax() */
+} nrg_spec_params;
+
+typedef struct nrg_bins {
+  double log10emin;            /* floor(log10(emin)), c++/bins.hpp:67 */
+  double log10emax;            /* ceil(log10(emax)),  c++/bins.hpp:68 */
+  int bins;                    /* bins per decade (P.bins) */
+  int nbins;                   /* (int)((log10emax - log10emin) * bins + 1), c++/bins.hpp:97 */
+  double discard_immediately;  /* P.discard_immediately, c++/bins.hpp:105 */
+} nrg_bins;
+
+NRG_API int nrg_spec_accumulate(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* params,
+                        const nrg_bins* bins, double* pos, double* neg, void* stream);
+
+/* Energies of the log grid (c++/bins.hpp:95-100) for one sign half; returns nbins. */
+NRG_API int nrg_bins_grid(const nrg_bins* bins, double* energies_host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NRG_B200_H */

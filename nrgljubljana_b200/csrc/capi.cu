@@ -1,0 +1,537 @@
+// capi.cu -- the C-ABI of the NRG step core (include/nrg_b200.h): context, device
+// workspace, descriptor staging and the host-side planning of every batched launch.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/nrg_b200.h"
+#include "ctx.h"
+#include "eig_large.h"
+#include "kernels.h"
+#include "spec.h"
+
+namespace nrg {
+
+namespace {
+thread_local std::string g_err;
+}
+
+const char* last_error_text() { return g_err.c_str(); }
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int ensure_ws(nrg_ctx* c, size_t bytes) {
+  if (bytes <= c->ws_size) return NRG_OK;
+  if (bytes > c->ws_limit)
+    return fail(NRG_ERR_OOM, "workspace of %zu bytes exceeds the context limit of %zu bytes", bytes, c->ws_limit);
+  if (c->ws) {
+    NRG_CK(cudaDeviceSynchronize());
+    NRG_CK(cudaFree(c->ws));
+    c->ws = nullptr;
+    c->ws_size = 0;
+  }
+  const size_t sz = std::max(bytes, std::min(c->ws_limit, align_up(bytes + bytes / 4, 1 << 20)));
+  if (cudaMalloc(&c->ws, sz) != cudaSuccess) {
+    cudaGetLastError();
+    if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      c->ws = nullptr;
+      return fail(NRG_ERR_OOM, "cudaMalloc of %zu bytes of workspace failed", bytes);
+    }
+    c->ws_size = bytes;
+  } else {
+    c->ws_size = sz;
+  }
+  return NRG_OK;
+}
+
+// The host image is pageable, so the copy has left it when cudaMemcpyAsync returns.
+int stage_desc(nrg_ctx* c, const std::vector<char>& img, cudaStream_t s) {
+  if (img.empty()) return NRG_OK;
+  if (img.size() > c->desc_size) {
+    if (c->desc) {
+      NRG_CK(cudaDeviceSynchronize());
+      NRG_CK(cudaFree(c->desc));
+      c->desc = nullptr;
+    }
+    const size_t sz = align_up(img.size() * 2, 1 << 16);
+    NRG_CK(cudaMalloc(&c->desc, sz));
+    c->desc_size = sz;
+  }
+  NRG_CK(cudaMemcpyAsync(c->desc, img.data(), img.size(), cudaMemcpyHostToDevice, s));
+  return NRG_OK;
+}
+
+void GemmPlan::add_out(double* C, int64_t ldc, int M, int N, double beta) {
+  GemmOut o{};
+  o.C = C;
+  o.ldc = ldc;
+  o.M = M;
+  o.N = N;
+  o.seg0 = (int)segs.size();
+  o.nseg = 0;
+  o.tile0 = tiles;
+  o.beta = beta;
+  tiles += ((M + kGemmBM - 1) / kGemmBM) * ((N + kGemmBN - 1) / kGemmBN);
+  outs.push_back(o);
+}
+
+void GemmPlan::add_seg(const double* A, int64_t lda, int transA, const double* B, int64_t ldb, int transB, int K,
+                       double alpha) {
+  GemmSeg g{};
+  g.A = A;
+  g.B = B;
+  g.lda = lda;
+  g.ldb = ldb;
+  g.K = K;
+  g.transA = transA;
+  g.transB = transB;
+  g.alpha = alpha;
+  segs.push_back(g);
+  outs.back().nseg++;
+}
+
+StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p) {
+  StagedGemm g;
+  g.outs_off = push(img, p.outs);
+  g.segs_off = push(img, p.segs);
+  g.nout = (int)p.outs.size();
+  g.tiles = p.tiles;
+  return g;
+}
+
+int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s) {
+  if (g.nout == 0 || g.tiles == 0) return NRG_OK;
+  const char* base = static_cast<const char*>(c->desc);
+  NRG_CK(gemm_batch_launch(reinterpret_cast<const GemmOut*>(base + g.outs_off),
+                           reinterpret_cast<const GemmSeg*>(base + g.segs_off), g.nout, g.tiles, s));
+  return NRG_OK;
+}
+
+int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s) {
+  if (p.outs.empty() || p.tiles == 0) return NRG_OK;
+  std::vector<char> img;
+  const StagedGemm g = stage_gemm(img, p);
+  int rc = stage_desc(c, img, s);
+  if (rc) return rc;
+  return launch_staged_gemm(c, g, s);
+}
+
+}  // namespace nrg
+
+namespace {
+using nrg::fail;
+using nrg::ensure_ws;
+using nrg::stage_desc;
+using nrg::push;
+using nrg::GemmPlan;
+using nrg::run_gemm_plan;
+#define CK NRG_CK
+
+int check_ctx(nrg_ctx* c) {
+  if (!c) return fail(NRG_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  return NRG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int nrg_version(void) { return NRG_B200_VERSION; }
+
+const char* nrg_last_error(void) { return nrg::last_error_text(); }
+
+int nrg_create(nrg_ctx** out, int device, size_t workspace_limit) {
+  if (!out) return fail(NRG_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(NRG_ERR_NODEV, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return fail(NRG_ERR_ARG, "device %d out of range [0,%d)", device, ndev);
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return fail(NRG_ERR_NODEV, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                                    prop.major, prop.minor);
+  CK(cudaSetDevice(device));
+  auto* c = new nrg_ctx();
+  c->device = device;
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  c->ws_limit = workspace_limit ? workspace_limit : (size_t)(0.9 * (double)fr);
+  *out = c;
+  return NRG_OK;
+}
+
+int nrg_destroy(nrg_ctx* c) {
+  if (!c) return NRG_OK;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  if (c->ws) cudaFree(c->ws);
+  if (c->desc) cudaFree(c->desc);
+  if (c->info_dev) cudaFree(c->info_dev);
+  delete c;
+  return NRG_OK;
+}
+
+// ---------------------------------------------------------------- diagonalisation
+int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double* const* evals, double* const* evecs,
+                   int* info, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nblk < 0 || (nblk > 0 && (!n || !H || !evals || !evecs || !info))) return fail(NRG_ERR_ARG, "bad arguments");
+  if (nblk == 0) return NRG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  for (int b = 0; b < nblk; b++) {
+    if (n[b] < 1 || n[b] > NRG_DIAG_MAX_N) return fail(NRG_ERR_ARG, "block %d: order %d out of range", b, n[b]);
+    if (!H[b] || !evals[b] || !evecs[b]) return fail(NRG_ERR_ARG, "block %d: null pointer", b);
+    if (H[b] == evecs[b]) return fail(NRG_ERR_ARG, "block %d: evecs aliases H", b);
+  }
+  if ((size_t)nblk > c->info_cap) {
+    if (c->info_dev) CK(cudaFree(c->info_dev));
+    CK(cudaMalloc(&c->info_dev, sizeof(int) * (size_t)nblk));
+    c->info_cap = nblk;
+  }
+  CK(cudaMemsetAsync(c->info_dev, 0, sizeof(int) * (size_t)nblk, s));
+
+  std::vector<int> small, large;
+  for (int b = 0; b < nblk; b++) (n[b] <= nrg::kSmallMaxN ? small : large).push_back(b);
+
+  if (!small.empty()) {
+    // Largest first, so that the long CTAs start early.
+    std::stable_sort(small.begin(), small.end(), [n](int a, int b) { return n[a] > n[b]; });
+    std::vector<nrg::EigBlock> blk(small.size());
+    for (size_t t = 0; t < small.size(); t++) {
+      const int b = small[t];
+      nrg::EigBlock& e = blk[t];
+      std::memset(&e, 0, sizeof e);
+      e.H = H[b];
+      e.evals = evals[b];
+      e.evecs = evecs[b];
+      e.info = c->info_dev + b;
+      e.n = n[b];
+    }
+    std::vector<char> img;
+    const size_t off = push(img, blk);
+    rc = stage_desc(c, img, s);
+    if (rc) return rc;
+    CK(nrg::eig_small_launch(reinterpret_cast<const nrg::EigBlock*>(static_cast<char*>(c->desc) + off),
+                             (int)small.size(), n[small[0]], s));
+  }
+  if (!large.empty()) {
+    rc = nrg::eig_large_run(c, large, n, H, evals, evecs, c->info_dev, s);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(info, c->info_dev, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  int bad = 0;
+  for (int b = 0; b < nblk; b++) bad += info[b] != 0;
+  if (bad) fail(bad, "%d of %d blocks returned a non-zero status", bad, nblk);
+  return bad;
+}
+
+int nrg_diag_batch_host(nrg_ctx* c, int nblk, const int* n, const double* const* H, double* const* evals,
+                        double* const* evecs, int* info, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nblk < 0 || (nblk > 0 && (!n || !H || !evals || !evecs || !info))) return fail(NRG_ERR_ARG, "bad arguments");
+  if (nblk == 0) return NRG_OK;
+  auto s = static_cast<cudaStream_t>(stream);
+  size_t mat = 0, val = 0;
+  for (int b = 0; b < nblk; b++) {
+    if (n[b] < 1 || n[b] > NRG_DIAG_MAX_N) return fail(NRG_ERR_ARG, "block %d: order %d out of range", b, n[b]);
+    mat += (size_t)n[b] * n[b];
+    val += n[b];
+  }
+  // Device copies: H, evecs (n^2 each) and evals; the large path needs its own workspace
+  // on top, so the host variant allocates these buffers separately from the arena.
+  double *dH = nullptr, *dV = nullptr, *dE = nullptr;
+  CK(cudaMalloc(&dH, sizeof(double) * mat));
+  if (cudaMalloc(&dV, sizeof(double) * mat) != cudaSuccess || cudaMalloc(&dE, sizeof(double) * val) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(dH);
+    if (dV) cudaFree(dV);
+    return fail(NRG_ERR_OOM, "device buffers for %zu matrix elements", mat);
+  }
+  std::vector<double*> pH(nblk), pV(nblk), pE(nblk);
+  size_t mo = 0, vo = 0;
+  for (int b = 0; b < nblk; b++) {
+    pH[b] = dH + mo;
+    pV[b] = dV + mo;
+    pE[b] = dE + vo;
+    cudaMemcpyAsync(pH[b], H[b], sizeof(double) * n[b] * n[b], cudaMemcpyHostToDevice, s);
+    mo += (size_t)n[b] * n[b];
+    vo += n[b];
+  }
+  rc = nrg_diag_batch(c, nblk, n, pH.data(), pE.data(), pV.data(), info, stream);
+  if (rc >= 0) {
+    for (int b = 0; b < nblk; b++) {
+      cudaMemcpyAsync(evals[b], pE[b], sizeof(double) * n[b], cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(evecs[b], pV[b], sizeof(double) * n[b] * n[b], cudaMemcpyDeviceToHost, s);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = fail(NRG_ERR_CUDA, "copy-out failed");
+  }
+  cudaFree(dH);
+  cudaFree(dV);
+  cudaFree(dE);
+  return rc;
+}
+
+// ---------------------------------------------------------------- GEMM leaves
+int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nterm < 0 || (nterm > 0 && !terms)) return fail(NRG_ERR_ARG, "bad arguments");
+  auto s = static_cast<cudaStream_t>(stream);
+  // Group by output pointer, keeping the given order inside a group.
+  std::vector<int> live;
+  for (int t = 0; t < nterm; t++) {
+    const nrg_gemm3& g = terms[t];
+    if (g.rows < 0 || g.cols < 0 || g.ka < 0 || g.kb < 0) return fail(NRG_ERR_ARG, "term %d: negative size", t);
+    if (g.rows == 0 || g.cols == 0 || g.ka == 0 || g.kb == 0) continue;
+    if (!g.M || !g.A || !g.B) return fail(NRG_ERR_ARG, "term %d: null pointer", t);
+    if (!g.O && g.ka != g.kb) return fail(NRG_ERR_ARG, "term %d: O = NULL needs ka == kb", t);
+    if (!(g.factor == g.factor) || g.factor - g.factor != 0.0)
+      return fail(NRG_ERR_ARG, "term %d: non-finite factor", t);  // my_assert(my_isfinite(factor))
+    live.push_back(t);
+  }
+  if (live.empty()) return NRG_OK;
+  std::map<double*, std::vector<int>> groups;
+  std::vector<double*> order;
+  for (int t : live) {
+    auto& v = groups[terms[t].M];
+    if (v.empty()) order.push_back(terms[t].M);
+    else {
+      const nrg_gemm3& f = terms[v[0]];
+      if (f.rows != terms[t].rows || f.cols != terms[t].cols || f.ldm != terms[t].ldm)
+        return fail(NRG_ERR_ARG, "term %d: shape of M differs from term %d with the same M", t, v[0]);
+    }
+    v.push_back(t);
+  }
+  // Phase 1: T_t = O_t op(B_t) (ka x cols) for terms with an explicit O.
+  std::vector<size_t> toff(nterm, 0);
+  size_t need = 0;
+  for (int t : live)
+    if (terms[t].O) {
+      toff[t] = need;
+      need += (size_t)terms[t].ka * terms[t].cols;
+    }
+  rc = ensure_ws(c, sizeof(double) * std::max<size_t>(need, 1));
+  if (rc) return rc;
+  double* T = static_cast<double*>(c->ws);
+  GemmPlan p1, p2;
+  for (int t : live) {
+    const nrg_gemm3& g = terms[t];
+    if (!g.O) continue;
+    p1.add_out(T + toff[t], g.cols, g.ka, g.cols, 0.0);
+    p1.add_seg(g.O, g.ldo, 0, g.B, g.ldb, g.transB, g.kb, 1.0);
+  }
+  // Phase 2: M += sum_t factor_t op(A_t) T_t.
+  for (double* M : order) {
+    const auto& v = groups[M];
+    const nrg_gemm3& f = terms[v[0]];
+    p2.add_out(M, f.ldm, f.rows, f.cols, 1.0);
+    for (int t : v) {
+      const nrg_gemm3& g = terms[t];
+      if (g.O) p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
+      else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
+    }
+  }
+  rc = run_gemm_plan(c, p1, s);
+  if (rc) return rc;
+  return run_gemm_plan(c, p2, s);
+}
+
+int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nterm < 0 || (nterm > 0 && !terms)) return fail(NRG_ERR_ARG, "bad arguments");
+  auto s = static_cast<cudaStream_t>(stream);
+  // Copy every referenced host span once (by pointer), compute, copy M spans back.
+  struct Span { size_t bytes; double* dev; };
+  std::map<const double*, Span> spans;
+  auto span_of = [](const double* p, int r, int cc, int64_t ld) -> size_t {
+    return (r == 0 || cc == 0) ? 0 : sizeof(double) * ((size_t)(r - 1) * ld + cc);
+  };
+  auto note = [&](const double* p, size_t bytes) {
+    if (!p || !bytes) return;
+    auto it = spans.find(p);
+    if (it == spans.end()) spans[p] = Span{bytes, nullptr};
+    else it->second.bytes = std::max(it->second.bytes, bytes);
+  };
+  for (int t = 0; t < nterm; t++) {
+    const nrg_gemm3& g = terms[t];
+    if (g.rows <= 0 || g.cols <= 0 || g.ka <= 0 || g.kb <= 0) continue;
+    note(g.M, span_of(g.M, g.rows, g.cols, g.ldm));
+    note(g.A, g.transA ? span_of(g.A, g.ka, g.rows, g.lda) : span_of(g.A, g.rows, g.ka, g.lda));
+    if (g.O) note(g.O, span_of(g.O, g.ka, g.kb, g.ldo));
+    note(g.B, g.transB ? span_of(g.B, g.cols, g.kb, g.ldb) : span_of(g.B, g.kb, g.cols, g.ldb));
+  }
+  std::vector<double*> allocs;
+  auto cleanup = [&]() { for (double* p : allocs) cudaFree(p); };
+  for (auto& kv : spans) {
+    double* d = nullptr;
+    if (cudaMalloc(&d, kv.second.bytes) != cudaSuccess) {
+      cudaGetLastError();
+      cleanup();
+      return fail(NRG_ERR_OOM, "device copy of %zu bytes", kv.second.bytes);
+    }
+    allocs.push_back(d);
+    kv.second.dev = d;
+    cudaMemcpyAsync(d, kv.first, kv.second.bytes, cudaMemcpyHostToDevice, s);
+  }
+  std::vector<nrg_gemm3> dt(terms, terms + nterm);
+  auto dev = [&](const double* p) -> double* { return p ? spans.at(p).dev : nullptr; };
+  for (auto& g : dt) {
+    if (g.rows <= 0 || g.cols <= 0 || g.ka <= 0 || g.kb <= 0) continue;
+    g.M = dev(g.M);
+    g.A = dev(g.A);
+    g.O = dev(g.O);
+    g.B = dev(g.B);
+  }
+  rc = nrg_gemm3_batch(c, nterm, dt.data(), stream);
+  if (rc == NRG_OK) {
+    for (int t = 0; t < nterm; t++) {
+      const nrg_gemm3& g = terms[t];
+      if (g.rows <= 0 || g.cols <= 0 || g.ka <= 0 || g.kb <= 0) continue;
+      const Span& sp = spans.at(g.M);
+      cudaMemcpyAsync(g.M, sp.dev, sp.bytes, cudaMemcpyDeviceToHost, s);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = fail(NRG_ERR_CUDA, "copy-out failed");
+  }
+  cleanup();
+  return rc;
+}
+
+// ---------------------------------------------------------------- spectral accumulation
+int nrg_bins_grid(const nrg_bins* b, double* energies) {
+  if (!b || b->bins <= 0) return fail(NRG_ERR_ARG, "bad bins");
+  const int nr = (int)((b->log10emax - b->log10emin) * b->bins + 1.0);
+  if (energies)
+    for (int i = 0; i < nr; i++) energies[i] = std::pow(10.0, b->log10emin + (double)i / b->bins);
+  return nr;
+}
+
+int nrg_spec_accumulate(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* prm,
+                        const nrg_bins* bins, double* pos, double* neg, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (npair < 0 || (npair > 0 && (!pairs || !prm || !bins || !pos || !neg))) return fail(NRG_ERR_ARG, "bad arguments");
+  if (npair == 0) return NRG_OK;
+  if (bins->nbins < 2 || bins->bins <= 0) return fail(NRG_ERR_ARG, "bad bins");
+  if (prm->algo < NRG_SPEC_DMNRG || prm->algo > NRG_SPEC_FDMLS) return fail(NRG_ERR_ARG, "bad algo %d", prm->algo);
+  auto s = static_cast<cudaStream_t>(stream);
+
+  // GEMM-derived matrices in workspace.
+  std::vector<size_t> xo(npair, 0), yo(npair, 0);
+  size_t need = 0;
+  for (int p = 0; p < npair; p++) {
+    const nrg_spec_pair& q = pairs[p];
+    if (q.ni < 0 || q.nj < 0 || q.ki < 0 || q.kj < 0 || q.ki > q.ni || q.kj > q.nj)
+      return fail(NRG_ERR_ARG, "pair %d: bad ranges", p);
+    if (prm->algo == NRG_SPEC_DMNRG) {
+      xo[p] = need; need += (size_t)q.kj * q.ki;
+      yo[p] = need; need += (size_t)q.kj * q.ki;
+    } else if (prm->algo == NRG_SPEC_FDMGT) {
+      if (q.ki > q.rdi) return fail(NRG_ERR_ARG, "pair %d: rdi < ki", p);
+      xo[p] = need; need += (size_t)q.nj * q.rdi;
+    } else {
+      if (q.kj > q.rdj) return fail(NRG_ERR_ARG, "pair %d: rdj < kj", p);
+      xo[p] = need; need += (size_t)q.rdj * q.ni;
+    }
+  }
+  rc = ensure_ws(c, sizeof(double) * std::max<size_t>(need, 1));
+  if (rc) return rc;
+  double* W = static_cast<double*>(c->ws);
+  GemmPlan gp;
+  std::vector<nrg::SpecRegion> regs;
+  auto region = [&](const nrg_spec_pair& q, int kind, int i0, int i1, int j0, int j1, const double* X, int64_t ldx,
+                    const double* Y, int64_t ldy, double coef) {
+    if (i1 <= i0 || j1 <= j0) return;
+    nrg::SpecRegion r{};
+    r.Ei = q.Ei; r.Ej = q.Ej; r.op1 = q.op1; r.op2 = q.op2; r.X = X; r.Y = Y;
+    r.ld1 = q.ld1; r.ld2 = q.ld2; r.ldx = ldx; r.ldy = ldy;
+    r.i0 = i0; r.i1 = i1; r.j0 = j0; r.j1 = j1;
+    r.kind = kind; r.sign = prm->sign; r.coef = coef; r.factor = q.factor; r.T = prm->T;
+    r.Emin = prm->Emin; r.Emax = prm->Emax;
+    regs.push_back(r);
+  };
+  for (int p = 0; p < npair; p++) {
+    const nrg_spec_pair& q = pairs[p];
+    if (prm->algo == NRG_SPEC_DMNRG) {
+      if (q.ki == 0 || q.kj == 0) continue;
+      double* X = W + xo[p];
+      double* Y = W + yo[p];
+      // X(rj, rm) = sum_ri op2(rj, ri) rho_i(rm, ri)   (algo_DMNRG.hpp:38)
+      gp.add_out(X, q.ki, q.kj, q.ki, 0.0);
+      gp.add_seg(q.op2, q.ld2, 0, q.rho_i, q.ldri, 1, q.ki, 1.0);
+      // Y(rj, rm) = sum_ri rho_j(rj, ri) op1(ri, rm)   (algo_DMNRG.hpp:41)
+      gp.add_out(Y, q.ki, q.kj, q.ki, 0.0);
+      gp.add_seg(q.rho_j, q.ldrj, 0, q.op1, q.ld1, 0, q.kj, 1.0);
+      region(q, nrg::kSpecDMNRG, 0, q.ki, 0, q.kj, X, q.ki, Y, q.ki, 0.0);
+    } else if (prm->algo == NRG_SPEC_FDMGT) {
+      // op2_rho = prod_fit(op2, rhoFDM(Ii)) (algo_FDM.hpp:89, numerics.hpp:283-306)
+      double* X = W + xo[p];
+      if (q.rdi > 0 && q.nj > 0) {
+        gp.add_out(X, q.rdi, q.nj, q.rdi, 0.0);
+        gp.add_seg(q.op2, q.ld2, 0, q.rho_i, q.ldri, 0, std::min(q.rdi, q.ni), 1.0);
+      }
+      region(q, nrg::kSpecExpI, q.ki, q.ni, 0, q.nj, nullptr, 0, nullptr, 0, prm->wnf);   // D x (D + K)
+      region(q, nrg::kSpecGemmX, 0, q.ki, q.kj, q.nj, X, q.rdi, nullptr, 0, 1.0);         // K x D
+    } else {
+      // rho_op2 = prod_fit(rhoFDM(Ij), op2) (algo_FDM.hpp:35)
+      double* X = W + xo[p];
+      if (q.rdj > 0 && q.ni > 0) {
+        gp.add_out(X, q.ni, q.rdj, q.ni, 0.0);
+        gp.add_seg(q.rho_j, q.ldrj, 0, q.op2, q.ld2, 0, std::min(q.rdj, q.nj), 1.0);
+      }
+      const double ms = (double)(-prm->sign);
+      region(q, nrg::kSpecExpJ, 0, q.ni, q.kj, q.nj, nullptr, 0, nullptr, 0, ms * prm->wnf);  // (D + K) x D
+      region(q, nrg::kSpecGemmX, q.ki, q.ni, 0, q.kj, X, q.ni, nullptr, 0, ms);                // D x K
+    }
+  }
+  rc = run_gemm_plan(c, gp, s);
+  if (rc) return rc;
+  if (regs.empty()) return NRG_OK;
+  std::vector<nrg::SpecTask> tasks;
+  const int64_t chunk = 8192;
+  for (size_t r = 0; r < regs.size(); r++) {
+    const int64_t nt = (int64_t)(regs[r].i1 - regs[r].i0) * (regs[r].j1 - regs[r].j0);
+    for (int64_t t0 = 0; t0 < nt; t0 += chunk) {
+      nrg::SpecTask k{};
+      k.t0 = t0;
+      k.t1 = std::min(nt, t0 + chunk);
+      k.region = (int)r;
+      tasks.push_back(k);
+    }
+  }
+  std::vector<char> img;
+  const size_t ro = push(img, regs), to = push(img, tasks);
+  rc = stage_desc(c, img, s);
+  if (rc) return rc;
+  nrg::BinParams bp{};
+  bp.log10emin = bins->log10emin;
+  bp.discard_immediately = bins->discard_immediately;
+  bp.bins = bins->bins;
+  bp.nbins = bins->nbins;
+  const char* base = static_cast<const char*>(c->desc);
+  CK(nrg::spec_bin_launch(reinterpret_cast<const nrg::SpecTask*>(base + to), (int)tasks.size(),
+                          reinterpret_cast<const nrg::SpecRegion*>(base + ro), bp, pos, neg, s));
+  return NRG_OK;
+}
+
+}  // extern "C"

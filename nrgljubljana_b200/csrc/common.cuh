@@ -1,0 +1,64 @@
+// common.cuh -- shared device helpers for the NRG step core kernels (sm_100a, FP64).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define NRG_DEV __device__ __forceinline__
+
+namespace nrg {
+
+constexpr double kEps = 1.1102230246251565e-16;   // 2^-53, unit round-off of IEEE double
+constexpr double kSafeMin = 2.2250738585072014e-308;
+
+NRG_DEV double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+NRG_DEV double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide sum; `red` must hold one double per warp. Every thread gets the result.
+NRG_DEV double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
+  if (wid == 0) t = warp_sum(t);
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+NRG_DEV double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
+  if (wid == 0) t = warp_max(t);
+  if (threadIdx.x == 0) red[0] = t;
+  __syncthreads();
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// FP64 tensor-core MMA: D(8x8) += A(8x4) * B(4x8). Fragment layout (per lane l):
+// a = A[l/4][l%4], b = B[l%4][l/4], d = {D[l/4][2*(l%4)], D[l/4][2*(l%4)+1]}.
+NRG_DEV void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+}  // namespace nrg

@@ -1,0 +1,69 @@
+// ctx.h -- internal: the context object behind nrg_ctx* and the host helpers shared by
+// the C-ABI layer and the launch planners (workspace arena, descriptor staging, GEMM plans).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nrg_b200.h"
+#include "kernels.h"
+
+struct nrg_ctx {
+  int device = 0;
+  size_t ws_limit = 0;
+  void* ws = nullptr;  // device workspace arena (grow-only)
+  size_t ws_size = 0;
+  void* desc = nullptr;  // device copy of launch descriptors
+  size_t desc_size = 0;
+  int* info_dev = nullptr;
+  size_t info_cap = 0;
+};
+
+namespace nrg {
+
+int fail(int code, const char* fmt, ...);
+const char* last_error_text();
+int ensure_ws(nrg_ctx* c, size_t bytes);
+// Copies a host byte image to c->desc (stream-ordered); returns the device base pointer.
+int stage_desc(nrg_ctx* c, const std::vector<char>& img, cudaStream_t s);
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <typename T>
+size_t push(std::vector<char>& img, const std::vector<T>& v) {
+  const size_t off = align_up(img.size(), 256);
+  img.resize(off + sizeof(T) * v.size());
+  if (!v.empty()) std::memcpy(img.data() + off, v.data(), sizeof(T) * v.size());
+  return off;
+}
+
+struct GemmPlan {
+  std::vector<GemmOut> outs;
+  std::vector<GemmSeg> segs;
+  int tiles = 0;
+  void add_out(double* C, int64_t ldc, int M, int N, double beta);
+  void add_seg(const double* A, int64_t lda, int transA, const double* B, int64_t ldb, int transB, int K,
+               double alpha);
+};
+
+// Stage the plan's descriptors into `img` (offsets returned) -- used when several plans
+// and other descriptors share one staging copy.
+struct StagedGemm {
+  size_t outs_off = 0, segs_off = 0;
+  int nout = 0, tiles = 0;
+};
+StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p);
+int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s);
+
+int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s);
+
+}  // namespace nrg
+
+#define NRG_CK(call)                                                                                      \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return ::nrg::fail(NRG_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)

@@ -1,0 +1,996 @@
+// eig_large.cu -- batched FP64 symmetric eigensolver for blocks larger than kSmallMaxN.
+//
+// Replaces LAPACK dsyev/dsyevd as called by diagonalise() (c++/diag.hpp:62-115, 261-292
+// of the reference) for the large symmetry blocks of an NRG step, with the output layout
+// of copy_results (ascending eigenvalues, eigenvectors as rows, c++/diag.hpp:41-58).
+//
+// Pipeline per chunk of blocks (all blocks of the chunk advance together):
+//   1. tridiag_kernel     one CTA per block: blocked Householder reduction A = Q T Q^T
+//                         (panel width NB); the symmetric matrix-vector product streams
+//                         the lower triangle from HBM once per column, the panel update
+//                         is a rank-2NB update of the trailing lower triangle.
+//   2. divide and conquer on T: leaves (<= kLeaf) by implicit QL in shared memory, merges
+//      by rank-one tearing (Cuppen), deflation (small z and close poles with Givens
+//      rotations), secular-equation roots with a two-pole rational model safeguarded by
+//      bisection, Gu-Eisenstat recomputation of z for orthogonal vectors, and the merge
+//      products as FP64 tensor-core GEMMs that skip the zero blocks of the children.
+//   3. sort of the eigenvalues and row permutation of the eigenvectors.
+//   4. back-transform with the compact-WY form of Q, panels of NBT reflectors, as GEMMs.
+// Eigenvectors are kept as ROWS throughout (Zt = Z^T), the layout of the output.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <vector>
+
+#include "common.cuh"
+#include "eig_large.h"
+#include "eig_small.cuh"
+
+namespace nrg {
+namespace {
+
+constexpr int kTriThreads = 256;
+constexpr int NB = 16;     // tridiagonalisation panel width
+constexpr int NBT = 64;    // back-transform panel width
+constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
+constexpr int kMaxLargeN = 4096;
+
+struct LargeBlock {
+  double* H;      // input (consumed): Householder vectors end up in its rows
+  double* evals;
+  double* evecs;  // output; scratch for the merge matrices during divide and conquer
+  double* W1;     // n x n: eigenvector rows of T under construction; VT factors later
+  double* W2;     // n x n: panel W of the reduction; grouped rows of a merge; back-transform W
+  double* d;
+  double* e;
+  double* tau;
+  double* lam;    // eigenvalues of the current divide-and-conquer nodes
+  double* dsort;  // per node: non-deflated poles, ascending
+  double* dgrp;   // per node: non-deflated poles, grouped order
+  double* zgrp;   // per node: z in grouped order
+  double* GT;     // per back-transform panel: Gram matrix V^T V (NBT^2) then T (NBT^2)
+  int* rank;      // per node: sorted position of grouped entry
+  int* perm;      // final eigenvalue order
+  int* info;
+  int n, npanel;
+};
+
+struct DcLeaf {
+  int blk, a0, a1, pad;
+};
+
+struct DcNode {
+  int blk, a, m, b;
+  int gout;  // index of the first of its two GEMM outputs in the level's GEMM arrays
+  int pad;
+};
+
+struct DcState {
+  int K, k1, k2, k3;
+  double rho;
+};
+
+// ---------------------------------------------------------------- tridiagonalisation
+
+// Transpose-reduction across a warp: lane c returns sum over lanes of x[c].
+NRG_DEV double transpose_reduce32(double (&x)[32], int lane) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool up = (lane & s) != 0;
+#pragma unroll
+    for (int q = 0; q < s; q++) {
+      const double send = up ? x[q] : x[q + s];
+      const double keep = up ? x[q + s] : x[q];
+      x[q] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return x[0];
+}
+
+// y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n, A symmetric with its lower triangle
+// stored as A(i, j) = H[j*n + i] (i >= j). Warps own 32-row tile rows; row sums stay in
+// registers, column sums are transposed across the warp and added to y in shared memory.
+NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const double* v, double* y) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
+  const bool full_last = (n & 31) == 0;
+  for (int I = Tn - warp; I >= T0; I -= nwarps) {
+    const int i = (I << 5) + lane;
+    const bool iv = (i >= s0) && (i < n);
+    const double vi = iv ? v[i] : 0.0;
+    double racc = 0.0;
+    for (int J = T0; J <= I; J++) {
+      const int j0 = J << 5;
+      double cp[32];
+      const bool interior = (J > T0) && (J < I) && (I < Tn || full_last);
+      if (interior) {
+        const double* col = H + (size_t)j0 * n + i;
+        double a[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) a[c] = col[(size_t)c * n];
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+          racc = fma(a[c], v[j0 + c], racc);
+          cp[c] = a[c] * vi;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+          const int jj = j0 + c;
+          const bool ok = iv && jj >= s0 && jj < n && i >= jj;
+          const double a = ok ? H[(size_t)jj * n + i] : 0.0;
+          const double vj = (jj < n) ? v[jj] : 0.0;
+          racc = fma(a, vj, racc);
+          cp[c] = (i > jj) ? a * vi : 0.0;
+        }
+      }
+      const double cs = transpose_reduce32(cp, lane);
+      const int jc = j0 + lane;
+      if (jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
+    }
+    if (iv) atomicAdd(&y[i], racc);
+  }
+}
+
+// A(i, j) -= sum_{q < nbp} V(i,q) W(j,q) + W(i,q) V(j,q) for s0 <= j <= i < n, with
+// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i].
+NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
+  for (int I = Tn - warp; I >= T0; I -= nwarps) {
+    const int i = (I << 5) + lane;
+    const bool iv = (i >= s0) && (i < n);
+    double Vi[NB], Wi[NB];
+#pragma unroll
+    for (int q = 0; q < NB; q++) {
+      const bool ok = iv && q < nbp;
+      Vi[q] = ok ? H[(size_t)(p0 + q) * n + i] : 0.0;
+      Wi[q] = ok ? W[(size_t)q * n + i] : 0.0;
+    }
+    for (int J = T0; J <= I; J++) {
+      const int jl = (J << 5) + lane;
+      const bool jv = (jl >= s0) && (jl < n);
+      double Vj[NB], Wj[NB];
+#pragma unroll
+      for (int q = 0; q < NB; q++) {
+        const bool ok = jv && q < nbp;
+        Vj[q] = ok ? H[(size_t)(p0 + q) * n + jl] : 0.0;
+        Wj[q] = ok ? W[(size_t)q * n + jl] : 0.0;
+      }
+      double* col = H + (size_t)(J << 5) * n + i;
+#pragma unroll 4
+      for (int c = 0; c < 32; c++) {
+        const int jj = (J << 5) + c;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          s = fma(Vi[q], __shfl_sync(0xffffffffu, Wj[q], c), s);
+          s = fma(Wi[q], __shfl_sync(0xffffffffu, Vj[q], c), s);
+        }
+        if (iv && jj >= s0 && jj < n && i >= jj) col[(size_t)c * n] -= s;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBlock* __restrict__ blocks) {
+  extern __shared__ __align__(16) double sm[];
+  const LargeBlock B = blocks[blockIdx.x];
+  const int n = B.n, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  double* H = B.H;
+  double* W = B.W2;
+  double* v = sm;
+  double* y = v + n;
+  double* part = y + n;                 // nwarps * 2NB
+  double* cwv = part + nwarps * 2 * NB;  // 2NB
+  double* red = cwv + 2 * NB;            // 32
+
+  for (int p0 = 0; p0 < n - 2; p0 += NB) {
+    const int pe = min(p0 + NB, n - 2);
+    for (int k = p0; k < pe; k++) {
+      const int j = k - p0;
+      // (1) current column k (rows k..n-1) = stored column minus the pending panel terms
+      for (int i = k + tid; i < n; i += nt) {
+        double a = H[(size_t)k * n + i];
+        for (int q = 0; q < j; q++) {
+          const double* Vq = H + (size_t)(p0 + q) * n;
+          const double* Wq = W + (size_t)q * n;
+          a -= Vq[i] * Wq[k] + Wq[i] * Vq[k];
+        }
+        v[i] = a;
+      }
+      __syncthreads();
+      // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
+      double ps = 0.0;
+      for (int i = k + 2 + tid; i < n; i += nt) ps += v[i] * v[i];
+      const double sigma = block_sum(ps, red);
+      const double alpha = v[k + 1];
+      double tau = 0.0, beta = alpha, scale = 1.0;
+      if (sigma > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+        tau = (beta - alpha) / beta;
+        scale = 1.0 / (alpha - beta);
+      }
+      if (tid == 0) {
+        B.d[k] = v[k];
+        B.e[k] = beta;
+        B.tau[k] = tau;
+      }
+      for (int i = k + 2 + tid; i < n; i += nt) {
+        const double vi = v[i] * scale;
+        v[i] = vi;
+        H[(size_t)k * n + i] = vi;
+      }
+      // row k of H now holds v_k from column k+1 on; clear its prefix inside the
+      // back-transform panel so that the panel's V block is exactly unit lower trapezoidal
+      const int kb0 = (k / NBT) * NBT;
+      for (int i = kb0 + 1 + tid; i <= k; i += nt) H[(size_t)k * n + i] = 0.0;
+      if (tid == 0) {
+        v[k + 1] = 1.0;
+        H[(size_t)k * n + k + 1] = 1.0;
+      }
+      __syncthreads();
+      if (tau != 0.0) {
+        // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
+        for (int i = k + 1 + tid; i < n; i += nt) y[i] = 0.0;
+        __syncthreads();
+        symv_lower(H, n, k + 1, v, y);
+        if (j > 0) {
+          double pw[NB], pv[NB];
+#pragma unroll
+          for (int q = 0; q < NB; q++) pw[q] = pv[q] = 0.0;
+          for (int i = k + 1 + tid; i < n; i += nt) {
+            const double vi = v[i];
+#pragma unroll
+            for (int q = 0; q < NB; q++)
+              if (q < j) {
+                pw[q] = fma(W[(size_t)q * n + i], vi, pw[q]);
+                pv[q] = fma(H[(size_t)(p0 + q) * n + i], vi, pv[q]);
+              }
+          }
+#pragma unroll
+          for (int q = 0; q < NB; q++) {
+            if (q < j) {
+              const double a = warp_sum(pw[q]);
+              const double b = warp_sum(pv[q]);
+              if (lane == 0) {
+                part[warp * 2 * NB + q] = a;
+                part[warp * 2 * NB + NB + q] = b;
+              }
+            }
+          }
+          __syncthreads();
+          if (tid < 2 * NB) {
+            double s = 0.0;
+            for (int w = 0; w < nwarps; w++) s += part[w * 2 * NB + tid];
+            cwv[tid] = s;
+          }
+        }
+        __syncthreads();
+        double pp = 0.0;
+        for (int i = k + 1 + tid; i < n; i += nt) {
+          double yi = y[i];
+          for (int q = 0; q < j; q++) yi -= H[(size_t)(p0 + q) * n + i] * cwv[q] + W[(size_t)q * n + i] * cwv[NB + q];
+          yi *= tau;
+          y[i] = yi;
+          pp = fma(yi, v[i], pp);
+        }
+        const double Kc = 0.5 * tau * block_sum(pp, red);
+        for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = y[i] - Kc * v[i];
+      } else {
+        for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = 0.0;
+      }
+      __syncthreads();
+    }
+    panel_update(H, W, n, p0, pe - p0, pe);
+    __syncthreads();
+  }
+  if (tid == 0) {
+    B.d[n - 2] = H[(size_t)(n - 2) * n + n - 2];
+    B.e[n - 2] = H[(size_t)(n - 2) * n + n - 1];
+    B.d[n - 1] = H[(size_t)(n - 1) * n + n - 1];
+    B.e[n - 1] = 0.0;
+    B.tau[n - 2] = 0.0;
+    B.tau[n - 1] = 0.0;
+  }
+  __syncthreads();
+  int bad = 0;
+  for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
+  if (__syncthreads_or(bad) && tid == 0) *B.info = -2;
+}
+
+// ---------------------------------------------------------------- divide and conquer: leaves
+__global__ void __launch_bounds__(128) dc_leaf_kernel(const LargeBlock* __restrict__ blocks,
+                                                      const DcLeaf* __restrict__ leaves) {
+  __shared__ double Z[kLeaf * (kLeaf + 1)];
+  __shared__ double d[kLeaf], e[kLeaf], C[kLeaf], S[kLeaf];
+  __shared__ int ctl[4];
+  const DcLeaf L = leaves[blockIdx.x];
+  const LargeBlock B = blocks[L.blk];
+  const int n = B.n, a0 = L.a0, nl = L.a1 - L.a0, ld = kLeaf + 1, tid = threadIdx.x;
+  for (int i = tid; i < nl; i += blockDim.x) {
+    double di = B.d[a0 + i];
+    if (i == 0 && a0 > 0) di -= fabs(B.e[a0 - 1]);             // rank-one tearing at the left cut
+    if (i == nl - 1 && L.a1 < n) di -= fabs(B.e[L.a1 - 1]);    // and at the right cut
+    d[i] = di;
+    e[i] = (i < nl - 1) ? B.e[a0 + i] : 0.0;
+  }
+  for (int idx = tid; idx < nl * nl; idx += blockDim.x) {
+    const int r = idx / nl, c = idx % nl;
+    Z[r * ld + c] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int st = smem_ql(d, e, nl, Z, ld, nl, C, S, ctl);
+  if (st && tid == 0) atomicMax(B.info, st);
+  for (int r = tid; r < nl; r += blockDim.x) B.lam[a0 + r] = d[r];
+  for (int idx = tid; idx < nl * nl; idx += blockDim.x) {
+    const int r = idx / nl, c = idx % nl;  // row r of Zt = column r of Z
+    B.W1[(size_t)(a0 + r) * n + a0 + c] = Z[c * ld + r];
+  }
+}
+
+// ---------------------------------------------------------------- divide and conquer: merge prep
+// Shared-memory layout for a node of order N (P = next power of two >= N).
+struct PrepLayout {
+  size_t key, sidx, zs, lst, rcs, rpos, fl, total;
+};
+
+__host__ __device__ inline size_t r16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline PrepLayout prep_layout(int N) {
+  int P = 1;
+  while (P < N) P <<= 1;
+  PrepLayout L;
+  size_t o = 0;
+  L.key = o;  o += r16(sizeof(double) * (size_t)P);   // pole values, sorted
+  L.sidx = o; o += r16(sizeof(int) * (size_t)P);      // original position
+  L.zs = o;   o += r16(sizeof(double) * (size_t)N);   // z in sorted order
+  L.lst = o;  o += r16(sizeof(int) * (size_t)N);      // non-deflated from the front, deflated from the back
+  L.rcs = o;  o += r16(sizeof(double2) * (size_t)N);  // rotation (c, s)
+  L.rpos = o; o += r16(sizeof(int2) * (size_t)N);     // rotation (pos_p, pos_j), later: grouped slot
+  L.fl = o;   o += r16((size_t)N);                    // support flags per sorted position
+  L.total = o;
+  return L;
+}
+
+__global__ void __launch_bounds__(512) dc_prep_kernel(const LargeBlock* __restrict__ blocks,
+                                                      const DcNode* __restrict__ nodes, DcState* __restrict__ states,
+                                                      GemmOut* __restrict__ gouts, GemmSeg* __restrict__ gsegs) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ double red[32];
+  __shared__ int cnt[8];
+  const DcNode nd = nodes[blockIdx.x];
+  const LargeBlock B = blocks[nd.blk];
+  const int n = B.n, a = nd.a, m = nd.m, b = nd.b, N = b - a;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int P = 1;
+  while (P < N) P <<= 1;
+  const PrepLayout PL = prep_layout(N);
+  char* smc = reinterpret_cast<char*>(sm);
+  double* key = reinterpret_cast<double*>(smc + PL.key);
+  int* sidx = reinterpret_cast<int*>(smc + PL.sidx);
+  double* zs = reinterpret_cast<double*>(smc + PL.zs);
+  int* lst = reinterpret_cast<int*>(smc + PL.lst);
+  double2* rcs = reinterpret_cast<double2*>(smc + PL.rcs);
+  int2* rpos = reinterpret_cast<int2*>(smc + PL.rpos);
+  unsigned char* fl = reinterpret_cast<unsigned char*>(smc + PL.fl);
+  double* Z = B.W1;
+  double* G = B.W2;
+
+  // 1. clear the off-diagonal child blocks of the node
+  const int n1 = m - a, n2 = b - m;
+  for (int idx = tid; idx < n1 * n2; idx += nt) {
+    const int r = idx / n2, c = idx % n2;
+    Z[(size_t)(a + r) * n + m + c] = 0.0;
+    const int r2 = idx / n1, c2 = idx % n1;
+    Z[(size_t)(m + r2) * n + a + c2] = 0.0;
+  }
+  // 2. poles and the rank-one vector z = [last row of child 1; sign(beta) first row of child 2] / sqrt(2)
+  const double beta = B.e[m - 1];
+  const double rho = 2.0 * fabs(beta);
+  const double sg = beta >= 0.0 ? 1.0 : -1.0;
+  for (int s = tid; s < P; s += nt) {
+    key[s] = (s < N) ? B.lam[a + s] : INFINITY;
+    sidx[s] = s;
+  }
+  __syncthreads();
+  // 3. bitonic sort (key, sidx) ascending
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int jb = k >> 1; jb > 0; jb >>= 1) {
+      for (int i = tid; i < P; i += nt) {
+        const int ixj = i ^ jb;
+        if (ixj > i) {
+          const bool asc = (i & k) == 0;
+          const double ki = key[i], kj = key[ixj];
+          const bool sw = asc ? (ki > kj || (ki == kj && sidx[i] > sidx[ixj])) : (ki < kj || (ki == kj && sidx[i] < sidx[ixj]));
+          if (sw) {
+            key[i] = kj;
+            key[ixj] = ki;
+            const int t = sidx[i];
+            sidx[i] = sidx[ixj];
+            sidx[ixj] = t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // A non-finite pole (the block was already flagged) could move a padding slot forward:
+  // leave such a node untouched rather than index outside it.
+  int badidx = 0;
+  for (int s = tid; s < N; s += nt) badidx |= (sidx[s] >= N);
+  if (__syncthreads_or(badidx)) {
+    if (tid == 0) atomicMin(B.info, -3);
+    return;
+  }
+  double dmx = 0.0, zmx = 0.0;
+  for (int s = tid; s < N; s += nt) {
+    const int c = a + sidx[s];
+    const double z = (c < m ? Z[(size_t)c * n + (m - 1)] : sg * Z[(size_t)c * n + m]) * 0.70710678118654752440;
+    zs[s] = z;
+    fl[s] = (c < m) ? 1 : 2;
+    dmx = fmax(dmx, fabs(key[s]));
+    zmx = fmax(zmx, fabs(z));
+  }
+  dmx = block_max(dmx, red);
+  zmx = block_max(zmx, red);
+  // 4. deflation scan (serial)
+  if (tid == 0) {
+    const double tol = 8.0 * kEps * fmax(dmx, zmx);
+    int K = 0, nd_ = 0, nrot = 0;
+    if (rho * zmx <= tol) {
+      for (int s = 0; s < N; s++) lst[N - 1 - (nd_++)] = s;
+    } else {
+      int p = -1;
+      for (int s = 0; s < N; s++) {
+        if (rho * fabs(zs[s]) <= tol) {
+          lst[N - 1 - (nd_++)] = s;
+          continue;
+        }
+        if (p < 0) {
+          p = s;
+          continue;
+        }
+        const double zp = zs[p], zj = zs[s];
+        const double t = hypot(zp, zj);
+        const double c = zj / t, sn = zp / t;
+        if (fabs((key[s] - key[p]) * c * sn) <= tol) {
+          // rotate rows (p, s): z_p -> 0, z_s -> t; p deflates
+          rcs[nrot] = make_double2(c, sn);
+          rpos[nrot] = make_int2(p, s);
+          nrot++;
+          const double dp = key[p], ds = key[s];
+          key[p] = c * c * dp + sn * sn * ds;
+          key[s] = sn * sn * dp + c * c * ds;
+          zs[s] = t;
+          zs[p] = 0.0;
+          fl[s] |= fl[p];
+          fl[p] |= fl[s];
+          lst[N - 1 - (nd_++)] = p;
+          p = s;
+        } else {
+          lst[K++] = p;
+          p = s;
+        }
+      }
+      if (p >= 0) lst[K++] = p;
+    }
+    cnt[0] = K;
+    cnt[1] = nd_;
+    cnt[2] = nrot;
+  }
+  __syncthreads();
+  const int K = cnt[0], ndefl = cnt[1], nrot = cnt[2];
+  // 5. apply the deflation rotations to the eigenvector rows, in order
+  for (int r = 0; r < nrot; r++) {
+    const double c = rcs[r].x, sn = rcs[r].y;
+    const size_t rp = (size_t)(a + sidx[rpos[r].x]) * n, rj = (size_t)(a + sidx[rpos[r].y]) * n;
+    for (int col = a + tid; col < b; col += nt) {
+      const double zp = Z[rp + col], zj = Z[rj + col];
+      Z[rp + col] = c * zp - sn * zj;
+      Z[rj + col] = sn * zp + c * zj;
+    }
+    __syncthreads();
+  }
+  // 6. group the non-deflated entries by support: child 1 only, both, child 2 only
+  if (tid == 0) {
+    int k1 = 0, k2 = 0, k3 = 0;
+    for (int t = 0; t < K; t++) {
+      const int f = fl[lst[t]];
+      if (f == 1) k1++;
+      else if (f == 3) k2++;
+      else k3++;
+    }
+    int g1 = 0, g2 = k1, g3 = k1 + k2;
+    for (int t = 0; t < K; t++) {
+      const int s = lst[t];
+      const int f = fl[s];
+      const int g = (f == 1) ? g1++ : (f == 3) ? g2++ : g3++;
+      B.rank[a + g] = t;
+      B.dgrp[a + g] = key[s];
+      B.zgrp[a + g] = zs[s];
+      B.dsort[a + t] = key[s];
+      // remember where the row goes: reuse rpos.x as the grouped slot of sorted position s
+      rpos[s].x = g;
+    }
+    for (int q = 0; q < ndefl; q++) {
+      const int s = lst[N - 1 - q];
+      B.lam[a + K + q] = key[s];
+      rpos[s].x = K + q;
+    }
+    cnt[3] = k1;
+    cnt[4] = k2;
+    cnt[5] = k3;
+    DcState st;
+    st.K = K;
+    st.k1 = k1;
+    st.k2 = k2;
+    st.k3 = k3;
+    st.rho = rho;
+    states[blockIdx.x] = st;
+    // the two merge GEMMs: rows of child-1 columns from types 1+2, child-2 columns from 2+3
+    gouts[nd.gout].M = K;
+    gouts[nd.gout + 1].M = K;
+    gsegs[nd.gout].K = k1 + k2;
+    gsegs[nd.gout + 1].K = k2 + k3;
+    gsegs[nd.gout + 1].A = B.evecs + (size_t)a * n + a + k1;
+    gsegs[nd.gout + 1].B = B.W2 + (size_t)(a + k1) * n + m;
+  }
+  __syncthreads();
+  // 7. copy the rows into grouped order in G (non-deflated first, then deflated)
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  for (int s = warp; s < N; s += nwarps) {
+    const size_t src = (size_t)(a + sidx[s]) * n, dst = (size_t)(a + rpos[s].x) * n;
+    for (int col = a + lane; col < b; col += 32) G[dst + col] = Z[src + col];
+  }
+}
+
+// ---------------------------------------------------------------- divide and conquer: secular equation
+// Root j of 1 + rho sum_i z_i^2 / (d_i - lambda) = 0 with poles d ascending. One warp per
+// root, lanes over i. On exit Dt[j][g] = d_g - lambda_j for every grouped entry g.
+__global__ void __launch_bounds__(256) dc_secular_kernel(const LargeBlock* __restrict__ blocks,
+                                                         const DcNode* __restrict__ nodes,
+                                                         const DcState* __restrict__ states) {
+  const DcNode nd = nodes[blockIdx.x];
+  const DcState st = states[blockIdx.x];
+  const LargeBlock B = blocks[nd.blk];
+  const int K = st.K;
+  if (K == 0) return;
+  const int n = B.n, a = nd.a;
+  const double rho = st.rho;
+  const int lane = threadIdx.x & 31;
+  const int wg = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int wstride = gridDim.y * (blockDim.x >> 5);
+  const double* ds = B.dsort + a;
+  const double* dg = B.dgrp + a;
+  const double* zg = B.zgrp + a;
+  const int* rk = B.rank + a;
+  double* Dt = B.evecs + (size_t)a * n + a;
+  for (int j = wg; j < K; j += wstride) {
+    double dorg, lo, hi, tau;
+    int p1, p2;
+    if (K == 1) {
+      const double z = zg[0];
+      if (lane == 0) {
+        Dt[0] = -rho * z * z;
+        B.lam[a] = ds[0] + rho * z * z;
+      }
+      continue;
+    }
+    if (j < K - 1) {
+      const double dj = ds[j], mid = 0.5 * (ds[j + 1] - dj);
+      double s = 0.0;
+      for (int i = lane; i < K; i += 32) {
+        const double z = zg[i];
+        s += z * z / ((dg[i] - dj) - mid);
+      }
+      const double f = 1.0 + rho * warp_sum(s);
+      if (f >= 0.0) {
+        dorg = dj;
+        lo = 0.0;
+        hi = mid;
+      } else {
+        dorg = ds[j + 1];
+        lo = -mid;
+        hi = 0.0;
+      }
+      p1 = j;
+      p2 = j + 1;
+    } else {
+      double s = 0.0;
+      for (int i = lane; i < K; i += 32) s += zg[i] * zg[i];
+      dorg = ds[K - 1];
+      lo = 0.0;
+      hi = rho * warp_sum(s);
+      p1 = K - 2;
+      p2 = K - 1;
+    }
+    tau = 0.5 * (lo + hi);
+    const double d1 = ds[p1] - dorg, d2 = ds[p2] - dorg;
+    for (int it = 0; it < 100; it++) {
+      double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
+      for (int i = lane; i < K; i += 32) {
+        const double del = (dg[i] - dorg) - tau;
+        const double t = zg[i] / del;
+        if (rk[i] <= p1) {
+          psi = fma(zg[i], t, psi);
+          dpsi = fma(t, t, dpsi);
+        } else {
+          phi = fma(zg[i], t, phi);
+          dphi = fma(t, t, dphi);
+        }
+      }
+      psi = rho * warp_sum(psi);
+      dpsi = rho * warp_sum(dpsi);
+      phi = rho * warp_sum(phi);
+      dphi = rho * warp_sum(dphi);
+      const double f = 1.0 + psi + phi;
+      const double err = 8.0 * (fabs(psi) + fabs(phi)) + 2.0 + 3.0 * fabs(tau) * (dpsi + dphi);
+      if (fabs(f) <= kEps * err) break;
+      if (f < 0.0) lo = tau; else hi = tau;
+      // two-pole rational model through poles p1, p2 matching f and f'
+      const double del1 = d1 - tau, del2 = d2 - tau;
+      const double cc = f - del1 * dpsi - del2 * dphi;
+      const double s1 = del1 * del1 * dpsi, s2 = del2 * del2 * dphi;
+      const double A1 = cc * (del1 + del2) + s1 + s2;
+      const double A0 = cc * del1 * del2 + s1 * del2 + s2 * del1;
+      double eta;
+      if (cc == 0.0) {
+        eta = A0 / A1;
+      } else {
+        const double disc = sqrt(fabs(A1 * A1 - 4.0 * cc * A0));
+        eta = (A1 <= 0.0) ? (A1 - disc) / (2.0 * cc) : 2.0 * A0 / (A1 + disc);
+      }
+      double tn = tau + eta;
+      if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+      if (tn == tau) break;
+      tau = tn;
+    }
+    for (int i = lane; i < K; i += 32) Dt[(size_t)j * n + i] = (dg[i] - dorg) - tau;
+    if (lane == 0) B.lam[a + j] = dorg + tau;
+  }
+}
+
+// ---------------------------------------------------------------- divide and conquer: vectors
+// z-hat by the Gu-Eisenstat product formula, then u_j(g) = zhat_g / (d_g - lambda_j),
+// normalised, written over Dt in place (same grouped column order).
+__global__ void __launch_bounds__(512) dc_vectors_kernel(const LargeBlock* __restrict__ blocks,
+                                                         const DcNode* __restrict__ nodes,
+                                                         const DcState* __restrict__ states) {
+  extern __shared__ __align__(16) double zh[];
+  const DcNode nd = nodes[blockIdx.x];
+  const DcState st = states[blockIdx.x];
+  const LargeBlock B = blocks[nd.blk];
+  const int K = st.K;
+  const int n = B.n, a = nd.a, tid = threadIdx.x, nt = blockDim.x;
+  {  // deflated rows are final: grouped copy (W2) back to the node's rows a+K.. (W1)
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int r = a + K + warp; r < nd.b; r += nwarps)
+      for (int col = a + lane; col < nd.b; col += 32) B.W1[(size_t)r * n + col] = B.W2[(size_t)r * n + col];
+  }
+  if (K == 0) return;
+  const double* ds = B.dsort + a;
+  const double* zg = B.zgrp + a;
+  const int* rk = B.rank + a;
+  double* Dt = B.evecs + (size_t)a * n + a;
+  const double rho = st.rho;
+  for (int g = tid; g < K; g += nt) {
+    const int i = rk[g];
+    const double di = ds[i];
+    double prod = -Dt[(size_t)(K - 1) * n + g] / rho;
+    for (int j = 0; j < i; j++) prod *= -Dt[(size_t)j * n + g] / (ds[j] - di);
+    for (int j = i; j < K - 1; j++) prod *= -Dt[(size_t)j * n + g] / (ds[j + 1] - di);
+    zh[g] = copysign(sqrt(fabs(prod)), zg[g]);
+  }
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  for (int j = warp; j < K; j += nwarps) {
+    double* row = Dt + (size_t)j * n;
+    double ss = 0.0;
+    for (int g = lane; g < K; g += 32) {
+      const double u = zh[g] / row[g];
+      ss = fma(u, u, ss);
+    }
+    const double inv = 1.0 / sqrt(warp_sum(ss));
+    for (int g = lane; g < K; g += 32) row[g] = zh[g] / row[g] * inv;
+  }
+}
+
+// ---------------------------------------------------------------- final order
+__global__ void __launch_bounds__(1024) sort_final_kernel(const LargeBlock* __restrict__ blocks) {
+  extern __shared__ __align__(16) double key[];
+  const LargeBlock B = blocks[blockIdx.x];
+  const int n = B.n, tid = threadIdx.x, nt = blockDim.x;
+  int P = 1;
+  while (P < n) P <<= 1;
+  int* idx = reinterpret_cast<int*>(key + P);
+  for (int s = tid; s < P; s += nt) {
+    key[s] = (s < n) ? B.lam[s] : INFINITY;
+    idx[s] = s;
+  }
+  __syncthreads();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int jb = k >> 1; jb > 0; jb >>= 1) {
+      for (int i = tid; i < P; i += nt) {
+        const int ixj = i ^ jb;
+        if (ixj > i) {
+          const bool asc = (i & k) == 0;
+          const double ki = key[i], kj = key[ixj];
+          const bool sw = asc ? (ki > kj || (ki == kj && idx[i] > idx[ixj])) : (ki < kj || (ki == kj && idx[i] < idx[ixj]));
+          if (sw) {
+            key[i] = kj;
+            key[ixj] = ki;
+            const int t = idx[i];
+            idx[i] = idx[ixj];
+            idx[ixj] = t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int s = tid; s < n; s += nt) {
+    B.evals[s] = key[s];
+    B.perm[s] = idx[s];
+  }
+}
+
+// evecs[r][:] = W1[perm[r]][:]; grid (rows / 8, blocks)
+__global__ void __launch_bounds__(256) permute_rows_kernel(const LargeBlock* __restrict__ blocks) {
+  const LargeBlock B = blocks[blockIdx.y];
+  const int n = B.n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r = blockIdx.x * 8 + warp;
+  if (r >= n) return;
+  int pr = B.perm[r];
+  if (pr < 0 || pr >= n) pr = r;  // only after a flagged non-finite block
+  const double* src = B.W1 + (size_t)pr * n;
+  double* dst = B.evecs + (size_t)r * n;
+  for (int c = lane; c < n; c += 32) dst[c] = src[c];
+}
+
+// ---------------------------------------------------------------- back-transform factors
+// T of the compact-WY form H_k0 ... H_k0+nb-1 = I - V T V^T (forward, columnwise), from
+// the Gram matrix G = V^T V already in GT[p] (first NBT^2), written to GT[p] + NBT^2.
+struct PanelRef {
+  int blk, k0, nb, pad;
+};
+
+__global__ void __launch_bounds__(NBT) tfactor_kernel(const LargeBlock* __restrict__ blocks,
+                                                      const PanelRef* __restrict__ panels) {
+  __shared__ double Ts[NBT][NBT + 1];
+  __shared__ double w[NBT];
+  const PanelRef P = panels[blockIdx.x];
+  const LargeBlock B = blocks[P.blk];
+  const int p = P.k0 / NBT, nb = P.nb, t = threadIdx.x;
+  const double* G = B.GT + (size_t)p * 2 * NBT * NBT;
+  double* T = B.GT + (size_t)p * 2 * NBT * NBT + NBT * NBT;
+  for (int r = 0; r < NBT; r++) Ts[r][t] = 0.0;
+  __syncthreads();
+  for (int q = 0; q < nb; q++) {
+    const double tq = B.tau[P.k0 + q];
+    // w = -tau_q G[0:q, q]; T[0:q, q] = T[0:q, 0:q] w
+    if (t < q) w[t] = -tq * G[t * NBT + q];
+    __syncthreads();
+    if (t < q) {
+      double s = 0.0;
+      for (int r = t; r < q; r++) s += Ts[t][r] * w[r];
+      Ts[t][q] = s;
+    }
+    if (t == q) Ts[q][q] = tq;
+    __syncthreads();
+  }
+  for (int r = 0; r < NBT; r++) T[r * NBT + t] = Ts[r][t];
+}
+
+size_t large_block_doubles(int n) {
+  const int npanel = (n - 2 + NBT - 1) / NBT;
+  return 2 * (size_t)n * n + 8 * (size_t)n + (size_t)npanel * 2 * NBT * NBT + 2 * (size_t)n;  // last: ints
+}
+
+}  // namespace
+
+int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, double* const* H, double* const* evals,
+                  double* const* evecs, int* info_dev, cudaStream_t s) {
+  std::vector<int> ord(which);
+  std::stable_sort(ord.begin(), ord.end(), [n](int x, int y) { return n[x] > n[y]; });
+  for (int b : ord)
+    if (n[b] > kMaxLargeN)
+      return fail(NRG_ERR_ARG, "block %d: order %d exceeds the supported maximum %d", b, n[b], kMaxLargeN);
+  // Chunk the blocks so that their workspaces fit in the context limit.
+  size_t limit = c->ws_limit;
+  size_t pos = 0;
+  while (pos < ord.size()) {
+    size_t bytes = 0, end = pos;
+    while (end < ord.size()) {
+      const size_t bb = align_up(sizeof(double) * large_block_doubles(n[ord[end]]), 256);
+      if (end > pos && bytes + bb > limit) break;
+      bytes += bb;
+      end++;
+    }
+    int rc = ensure_ws(c, bytes);
+    if (rc) return rc;
+    // ---- per-block descriptors
+    std::vector<LargeBlock> blk;
+    char* base = static_cast<char*>(c->ws);
+    size_t off = 0;
+    int maxn = 0, maxpanel = 0;
+    for (size_t t = pos; t < end; t++) {
+      const int b = ord[t], nb_ = n[b];
+      LargeBlock L{};
+      auto take = [&](size_t nd) {
+        double* p = reinterpret_cast<double*>(base + off);
+        off += align_up(sizeof(double) * nd, 256);
+        return p;
+      };
+      L.H = H[b];
+      L.evals = evals[b];
+      L.evecs = evecs[b];
+      L.W1 = take((size_t)nb_ * nb_);
+      L.W2 = take((size_t)nb_ * nb_);
+      L.d = take(nb_);
+      L.e = take(nb_);
+      L.tau = take(nb_);
+      L.lam = take(nb_);
+      L.dsort = take(nb_);
+      L.dgrp = take(nb_);
+      L.zgrp = take(nb_);
+      L.npanel = (nb_ - 2 + NBT - 1) / NBT;
+      L.GT = take((size_t)L.npanel * 2 * NBT * NBT);
+      int* ip = reinterpret_cast<int*>(take(nb_));
+      L.rank = ip;
+      L.perm = ip + nb_;
+      L.info = info_dev + b;
+      L.n = nb_;
+      blk.push_back(L);
+      maxn = std::max(maxn, nb_);
+      maxpanel = std::max(maxpanel, L.npanel);
+    }
+    const int nb = (int)blk.size();
+    // ---- divide-and-conquer tree (leaves and merge levels by height)
+    std::vector<DcLeaf> leaves;
+    std::vector<std::vector<DcNode>> levels;
+    std::function<int(int, int, int)> build = [&](int bi, int lo, int hi) -> int {
+      if (hi - lo <= kLeaf) {
+        leaves.push_back(DcLeaf{bi, lo, hi, 0});
+        return 0;
+      }
+      const int mid = lo + (hi - lo) / 2;
+      const int h = 1 + std::max(build(bi, lo, mid), build(bi, mid, hi));
+      if ((int)levels.size() < h) levels.resize(h);
+      DcNode nd{};
+      nd.blk = bi;
+      nd.a = lo;
+      nd.m = mid;
+      nd.b = hi;
+      levels[h - 1].push_back(nd);
+      return h;
+    };
+    for (int bi = 0; bi < nb; bi++) build(bi, 0, blk[bi].n);
+    // ---- one staging image for the whole chunk
+    std::vector<char> img;
+    const size_t blk_off = push(img, blk);
+    const size_t leaf_off = push(img, leaves);
+    std::vector<size_t> node_off(levels.size()), st_off(levels.size());
+    std::vector<StagedGemm> lvl_gemm(levels.size());
+    for (size_t h = 0; h < levels.size(); h++) {
+      GemmPlan gp;
+      for (auto& nd : levels[h]) {
+        const LargeBlock& L = blk[nd.blk];
+        const int N = nd.b - nd.a, nn = L.n;
+        nd.gout = (int)gp.outs.size();
+        // child-1 columns: C = Zt[a:a+K, a:m] = U[:, 0:k1+k2] * G[a:a+k1+k2, a:m]
+        gp.add_out(L.W1 + (size_t)nd.a * nn + nd.a, nn, N, nd.m - nd.a, 0.0);
+        gp.add_seg(L.evecs + (size_t)nd.a * nn + nd.a, nn, 0, L.W2 + (size_t)nd.a * nn + nd.a, nn, 0, N, 1.0);
+        // child-2 columns: C = Zt[a:a+K, m:b] = U[:, k1:K] * G[a+k1:a+K, m:b] (pointers set on device)
+        gp.add_out(L.W1 + (size_t)nd.a * nn + nd.m, nn, N, nd.b - nd.m, 0.0);
+        gp.add_seg(L.evecs + (size_t)nd.a * nn + nd.a, nn, 0, L.W2 + (size_t)nd.a * nn + nd.m, nn, 0, N, 1.0);
+      }
+      node_off[h] = push(img, levels[h]);
+      st_off[h] = push(img, std::vector<DcState>(levels[h].size()));
+      lvl_gemm[h] = stage_gemm(img, gp);
+    }
+    // back-transform: Gram, T, VT, then per panel step two GEMMs
+    std::vector<PanelRef> panels;
+    GemmPlan gram, vt;
+    std::vector<GemmPlan> bsteps(maxpanel * 2);
+    for (int bi = 0; bi < nb; bi++) {
+      const LargeBlock& L = blk[bi];
+      const int nn = L.n;
+      size_t vt_off = 0;
+      for (int p = 0; p < L.npanel; p++) {
+        const int k0 = p * NBT, pnb = std::min(NBT, (nn - 2) - k0), K = nn - k0 - 1;
+        panels.push_back(PanelRef{bi, k0, pnb, 0});
+        double* Gp = L.GT + (size_t)p * 2 * NBT * NBT;
+        const double* Vrows = L.H + (size_t)k0 * nn + k0 + 1;  // pnb x K, row q = v_{k0+q}
+        gram.add_out(Gp, NBT, pnb, pnb, 0.0);
+        gram.add_seg(Vrows, nn, 0, Vrows, nn, 1, K, 1.0);
+        double* VTp = L.W1 + vt_off;  // K x pnb
+        vt_off += (size_t)K * NBT;
+        if (vt_off > (size_t)nn * nn) return fail(NRG_ERR_ARG, "internal: VT factors exceed W1 for n=%d", nn);
+        vt.add_out(VTp, NBT, K, pnb, 0.0);
+        vt.add_seg(Vrows, nn, 1, Gp + NBT * NBT, NBT, 0, pnb, 1.0);
+        // step index counts from the last panel of each block
+        const int stp = L.npanel - 1 - p;
+        GemmPlan& g1 = bsteps[2 * stp];
+        GemmPlan& g2 = bsteps[2 * stp + 1];
+        double* Wb = L.W2;  // n x NBT
+        g1.add_out(Wb, NBT, nn, pnb, 0.0);
+        g1.add_seg(L.evecs + k0 + 1, nn, 0, Vrows, nn, 1, K, 1.0);
+        g2.add_out(L.evecs + k0 + 1, nn, nn, K, 1.0);
+        g2.add_seg(Wb, NBT, 0, VTp, NBT, 1, pnb, -1.0);
+      }
+    }
+    const size_t pan_off = push(img, panels);
+    const StagedGemm gram_g = stage_gemm(img, gram), vt_g = stage_gemm(img, vt);
+    std::vector<StagedGemm> bs_g(bsteps.size());
+    for (size_t t = 0; t < bsteps.size(); t++) bs_g[t] = stage_gemm(img, bsteps[t]);
+    rc = stage_desc(c, img, s);
+    if (rc) return rc;
+    char* dbase = static_cast<char*>(c->desc);
+    const LargeBlock* dblk = reinterpret_cast<const LargeBlock*>(dbase + blk_off);
+
+    // ---- 1. tridiagonalisation
+    {
+      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 32);
+      NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
+      NRG_CK(cudaGetLastError());
+    }
+    // ---- 2. divide and conquer
+    dc_leaf_kernel<<<(int)leaves.size(), 128, 0, s>>>(dblk, reinterpret_cast<const DcLeaf*>(dbase + leaf_off));
+    NRG_CK(cudaGetLastError());
+    for (size_t h = 0; h < levels.size(); h++) {
+      int maxN = 0;
+      for (auto& nd : levels[h]) maxN = std::max(maxN, nd.b - nd.a);
+      const int nn = (int)levels[h].size();
+      const DcNode* dn = reinterpret_cast<const DcNode*>(dbase + node_off[h]);
+      DcState* dst = reinterpret_cast<DcState*>(dbase + st_off[h]);
+      GemmOut* go = reinterpret_cast<GemmOut*>(dbase + lvl_gemm[h].outs_off);
+      GemmSeg* gs = reinterpret_cast<GemmSeg*>(dbase + lvl_gemm[h].segs_off);
+      const size_t ps = prep_layout(maxN).total;
+      NRG_CK(cudaFuncSetAttribute(dc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+      dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs);
+      NRG_CK(cudaGetLastError());
+      const int ysplit = std::max(1, std::min(16, maxN / 256));
+      dc_secular_kernel<<<dim3(nn, ysplit), 256, 0, s>>>(dblk, dn, dst);
+      NRG_CK(cudaGetLastError());
+      const size_t vs = sizeof(double) * (size_t)maxN;
+      NRG_CK(cudaFuncSetAttribute(dc_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vs));
+      dc_vectors_kernel<<<nn, 512, vs, s>>>(dblk, dn, dst);
+      NRG_CK(cudaGetLastError());
+      rc = launch_staged_gemm(c, lvl_gemm[h], s);
+      if (rc) return rc;
+    }
+    // ---- 3. order
+    {
+      int P = 1;
+      while (P < maxn) P <<= 1;
+      const size_t ss = (sizeof(double) + sizeof(int)) * (size_t)P;
+      NRG_CK(cudaFuncSetAttribute(sort_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+      sort_final_kernel<<<nb, 1024, ss, s>>>(dblk);
+      NRG_CK(cudaGetLastError());
+      permute_rows_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
+      NRG_CK(cudaGetLastError());
+    }
+    // ---- 4. back-transform
+    rc = launch_staged_gemm(c, gram_g, s);
+    if (rc) return rc;
+    if (!panels.empty()) {
+      tfactor_kernel<<<(int)panels.size(), NBT, 0, s>>>(dblk, reinterpret_cast<const PanelRef*>(dbase + pan_off));
+      NRG_CK(cudaGetLastError());
+    }
+    rc = launch_staged_gemm(c, vt_g, s);
+    if (rc) return rc;
+    for (size_t t = 0; t < bs_g.size(); t++) {
+      rc = launch_staged_gemm(c, bs_g[t], s);
+      if (rc) return rc;
+    }
+    pos = end;
+    if (pos < ord.size()) NRG_CK(cudaStreamSynchronize(s));  // the next chunk reuses the workspace
+  }
+  return NRG_OK;
+}
+
+}  // namespace nrg

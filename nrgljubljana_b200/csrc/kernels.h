@@ -1,0 +1,58 @@
+// kernels.h -- internal host-side launch interface between the C-ABI layer and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nrg {
+
+// ---------------------------------------------------------------- batched FP64 GEMM
+// One K-segment of an output: alpha * op(A) * op(B), op(A) is M x K, op(B) is K x N.
+// transA: A is stored K x M row-major (op(A) = A^T); transB: B is stored N x K (op(B) = B^T).
+struct GemmSeg {
+  const double* A;
+  const double* B;
+  int64_t lda, ldb;
+  int K, transA, transB, pad_;
+  double alpha;
+};
+
+// One output C (M x N, row-major, ldc): C = beta*C + sum over its segments. Tiles of
+// 64 x 64 are numbered from tile0 in row-major tile order.
+struct GemmOut {
+  double* C;
+  int64_t ldc;
+  int M, N;
+  int seg0, nseg;
+  int tile0, pad_;
+  double beta;
+};
+
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16, kGemmThreads = 128;
+
+// Launch over nout outputs whose descriptors already live in device memory.
+cudaError_t gemm_batch_launch(const GemmOut* d_outs, const GemmSeg* d_segs, int nout, int ntiles,
+                              cudaStream_t stream);
+
+// ---------------------------------------------------------------- eigensolver
+// Per-block descriptor of the batched symmetric eigensolver. H is n x n row-major with the
+// upper triangle set (it is overwritten); evals n doubles; evecs n x n row-major, row r =
+// eigenvector r. W1/W2 are n x n workspaces (large path only); d, e, tau are n-vectors.
+struct EigBlock {
+  double* H;
+  double* evals;
+  double* evecs;
+  double* W1;
+  double* W2;
+  double* d;
+  double* e;
+  double* tau;
+  int* iwork;     // 4n ints (large path)
+  int* info;      // per-block status word (0 ok, >0 not converged, <0 invalid)
+  int n, pad_;
+};
+
+constexpr int kSmallMaxN = 64;   // blocks up to this size are solved entirely in shared memory
+
+cudaError_t eig_small_launch(const EigBlock* d_blocks, int nblk, int maxn, cudaStream_t stream);
+
+}  // namespace nrg

@@ -1,0 +1,47 @@
+// spec.h -- internal descriptors of the spectral-weight binning kernel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nrg {
+
+enum SpecKind : int {
+  kSpecDMNRG = 0,  // w = X(j,i) op1(j,i) - sign Y(j,i) op2(j,i), energy window [Emin, Emax]
+  kSpecExpI = 1,   // w = coef op1(j,i) op2(j,i) exp(-Ei/T)
+  kSpecExpJ = 2,   // w = coef op1(j,i) op2(j,i) exp(-Ej/T)
+  kSpecGemmX = 3,  // w = coef op1(j,i) X(j,i)
+};
+
+// One rectangle of (i, j) index pairs of one subspace pair with one weight formula.
+// The energy of a term is Ej[j] - Ei[i]; every weight is multiplied by `factor`.
+struct SpecRegion {
+  const double* Ei;
+  const double* Ej;
+  const double* op1;
+  const double* op2;
+  const double* X;
+  const double* Y;
+  int64_t ld1, ld2, ldx, ldy;
+  int i0, i1, j0, j1;
+  int kind, sign;
+  double coef, factor, T, Emin, Emax;
+};
+
+struct SpecTask {  // a contiguous range [t0, t1) of the terms of one region (t = (j-j0)*(i1-i0) + (i-i0))
+  int64_t t0, t1;
+  int region, pad_;
+};
+
+struct BinParams {
+  double log10emin;
+  double discard_immediately;
+  int bins;   // bins per decade
+  int nbins;  // points per sign half
+};
+
+constexpr size_t kSpecSmemMax = 96 * 1024;  // private histograms up to 6144 bins per half
+
+cudaError_t spec_bin_launch(const SpecTask* d_tasks, int ntask, const SpecRegion* d_regs, const BinParams& bp,
+                            double* pos, double* neg, cudaStream_t stream);
+
+}  // namespace nrg

@@ -1,0 +1,163 @@
+"""Parity of the batched GPU eigensolver (C-ABI nrg_diag_batch[_host]) with the oracle's
+LAPACK dsyev (c++/diag.hpp:62-82), through sign/degeneracy-invariant checks."""
+import math
+
+import numpy as np
+import pytest
+
+from eigcheck import check_eig, full_from_upper
+
+pytestmark = pytest.mark.gpu
+
+SQ2 = 1.0 / math.sqrt(2.0)
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import nrgljubljana_b200 as m
+    m.context()
+    return m
+
+
+def rand_upper(rng, n, scale=1.0):
+    a = rng.standard_normal((n, n)) * scale
+    return np.triu(a + a.T)
+
+
+def graded_block(rng, n):
+    """Diagonal 2^{-k/2} plus symmetric N(0, 0.1^2) couplings (the synthetic NRG-like blocks)."""
+    h = np.triu(rng.standard_normal((n, n)) * 0.1, 1)
+    h[np.diag_indices(n)] = 2.0 ** (-np.arange(n) / 2.0)
+    return h
+
+
+def test_pauli_kats(nb):
+    # test/unit/diag_test/diag_test.cpp:83-112 through the C-ABI
+    r = nb.diagonalise(np.array([[-1.0, 0.0], [0.0, 1.0]]))
+    assert r.val[0] == -1.0 and r.val[1] == 1.0
+    assert abs(abs(r.vec[0, 0]) - 1) < 1e-15 and r.vec[0, 1] == 0.0 and r.vec[1, 0] == 0.0
+    r = nb.diagonalise(np.array([[0.0, 1.0], [0.0, 0.0]]))
+    assert abs(r.val[0] + 1) < 4e-16 and abs(r.val[1] - 1) < 4e-16
+    for k in range(2):
+        assert abs(abs(r.vec[k, 0]) - SQ2) < 4e-16 and abs(abs(r.vec[k, 1]) - SQ2) < 4e-16
+    assert abs(r.vec[0, 0] * r.vec[0, 1] + 0.5) < 4e-16
+    assert abs(r.vec[1, 0] * r.vec[1, 1] - 0.5) < 4e-16
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 16, 31, 32, 33, 47, 63, 64])
+def test_small_path_random(nb, oracle, n):
+    rng = np.random.default_rng(100 + n)
+    blocks = [rand_upper(rng, n) for _ in range(3)]
+    got = nb.diagonalisations(blocks)
+    for h, g in zip(blocks, got):
+        w, v = oracle.diagonalise(h)
+        check_eig(h, g.val, g.vec, w, v, oracle)
+
+
+@pytest.mark.parametrize("n", [65, 66, 96, 100, 127, 128, 129, 200, 256, 300, 511, 512, 777])
+def test_large_path_random(nb, oracle, n):
+    rng = np.random.default_rng(200 + n)
+    h = rand_upper(rng, n)
+    g = nb.diagonalisations([h])[0]
+    w, v = oracle.diagonalise(h)
+    check_eig(h, g.val, g.vec, w, v, oracle)
+
+
+@pytest.mark.parametrize("n", [40, 70, 150, 300, 600])
+def test_graded_blocks(nb, oracle, n):
+    rng = np.random.default_rng(300 + n)
+    h = graded_block(rng, n)
+    g = nb.diagonalisations([h])[0]
+    w, v = oracle.diagonalise(h)
+    check_eig(h, g.val, g.vec, w, v, oracle)
+
+
+@pytest.mark.parametrize("n", [10, 80, 200])
+def test_degenerate_spectrum(nb, oracle, n):
+    # Exactly repeated eigenvalues (a rotated matrix with a 3-fold and a 5-fold level) and
+    # a diagonal matrix: exercises deflation by small z and by close poles.
+    rng = np.random.default_rng(400 + n)
+    lam = np.sort(rng.standard_normal(n))
+    lam[1:4] = lam[1]
+    lam[n // 2:n // 2 + 5] = lam[n // 2]
+    q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    H = (q * lam) @ q.T
+    h = np.triu(H)
+    g = nb.diagonalisations([h])[0]
+    w, v = oracle.diagonalise(h)
+    check_eig(h, g.val, g.vec, w, v, oracle)
+    d = np.triu(np.diag(rng.standard_normal(n)))
+    g = nb.diagonalisations([d])[0]
+    w, v = oracle.diagonalise(d)
+    check_eig(d, g.val, g.vec, w, v, oracle)
+
+
+def test_block_diagonal_and_tridiagonal(nb, oracle):
+    rng = np.random.default_rng(5)
+    n = 160
+    h = np.zeros((n, n))
+    h[:80, :80] = rand_upper(rng, 80)
+    h[80:, 80:] = rand_upper(rng, 80)  # decoupled halves: beta = 0 at the top split
+    h = np.triu(h)
+    g = nb.diagonalisations([h])[0]
+    w, v = oracle.diagonalise(h)
+    check_eig(h, g.val, g.vec, w, v, oracle)
+    t = np.diag(rng.standard_normal(n)) + np.diag(rng.standard_normal(n - 1), 1)
+    g = nb.diagonalisations([t])[0]
+    w, v = oracle.diagonalise(t)
+    check_eig(t, g.val, g.vec, w, v, oracle)
+
+
+def test_mixed_batch(nb, oracle):
+    rng = np.random.default_rng(11)
+    sizes = [3, 150, 64, 65, 17, 400, 1, 90]
+    blocks = [rand_upper(rng, n) if i % 2 else graded_block(rng, n) for i, n in enumerate(sizes)]
+    got = nb.diagonalisations(blocks)
+    for h, g in zip(blocks, got):
+        w, v = oracle.diagonalise(h)
+        check_eig(h, g.val, g.vec, w, v, oracle)
+
+
+def test_device_api_consumes_input(nb, oracle):
+    import torch
+    rng = np.random.default_rng(12)
+    hs = [rand_upper(rng, n) for n in (20, 130)]
+    H = [torch.tensor(h, device="cuda") for h in hs]
+    E = [torch.empty(h.shape[0], dtype=torch.float64, device="cuda") for h in hs]
+    V = [torch.empty_like(x) for x in H]
+    info = nb.diag_batch_device(H, E, V)
+    torch.cuda.synchronize()
+    assert (info == 0).all()
+    for h, e, v in zip(hs, E, V):
+        w, z = oracle.diagonalise(h)
+        check_eig(h, e.cpu().numpy(), v.cpu().numpy(), w, z, oracle)
+
+
+def test_nonfinite_input_is_reported(nb):
+    h = np.eye(5)
+    h[0, 3] = np.nan
+    with pytest.raises(RuntimeError, match="INFO"):
+        nb.diagonalisations([h])
+    h = np.triu(np.ones((70, 70)))
+    h[10, 20] = np.inf
+    with pytest.raises(RuntimeError, match="INFO"):
+        nb.diagonalisations([h])
+
+
+def test_lower_triangle_is_ignored_and_checked(nb):
+    rng = np.random.default_rng(13)
+    h = rand_upper(rng, 9)
+    with pytest.raises(AssertionError):
+        nb.diagonalisations([h + np.tril(np.ones((9, 9)), -1)])
+    a = nb.diagonalisations([h + np.tril(np.ones((9, 9)), -1)], check_upper=False)[0]
+    b = nb.diagonalisations([h])[0]
+    assert np.array_equal(a.val, b.val)
+
+
+def test_dsyevr_ratio(nb, oracle):
+    rng = np.random.default_rng(14)
+    h = rand_upper(rng, 30)
+    r = nb.diagonalise(h, "dsyevr", 0.5)
+    w, v = oracle.diagonalise(h, "dsyevr", 0.5)
+    assert len(r.val) == len(w) == 15
+    assert np.abs(r.val - w).max() < 1e-12 * np.linalg.norm(full_from_upper(h), 2)
