@@ -1,0 +1,364 @@
+"""Benchmark of the B200 NRG step core on the synthetic batched-eigensolve workload.
+
+Workload (one "step"): 10,000 real symmetric FP64 blocks with orders drawn log-uniform in
+[8, 2048] (numpy PCG64, seed 20261203); block b is diag(2^{-k/2}, k = 0..n-1) plus
+symmetric Gaussian couplings N(0, 0.1^2) (torch CUDA generator seeded 20261203 * 100003
++ b), the shape of an NRG step's symmetry blocks. All blocks are diagonalised in one
+batched call (nrg_diag_batch). Metric: FP64 eigensolve GFLOP/s counted as
+F_eig(n) = (10/3) n^3 per block (tridiagonal reduction 4/3 n^3 + back-transform 2 n^3).
+
+Arms:
+  default           the library, inputs resident in HBM (a device-to-device refresh of the
+                    consumed inputs is inside each timed step); e2e through the host-pointer
+                    entry point nrg_diag_batch_host from pinned host memory.
+  --impl reference  the reference's CPU path (the oracle restatement of diagonalise() with
+                    LAPACK dsyev, OpenMP over blocks as diagonalisations_OpenMP) on all host
+                    cores, on a stratified sample of the same blocks.
+Multi-GPU (--gpus N under torchrun): independent replicas, one batch per GPU, no collective
+on the data path; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 20261203
+NMIN, NMAX = 8, 2048
+METRIC = "fp64_eig_gflops"
+UNIT = "GFLOP/s"
+WORKLOAD = ("synthetic batched eigensolve: {nblk} real symmetric FP64 blocks, n log-uniform in [8, 2048] "
+            "(PCG64 seed 20261203), H = diag(2^-k/2) + symmetric N(0, 0.1^2) couplings")
+
+
+def block_sizes(nblk: int) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    u = rng.uniform(math.log(NMIN), math.log(NMAX), nblk)
+    return np.clip(np.rint(np.exp(u)), NMIN, NMAX).astype(np.int64)
+
+
+def f_eig(n) -> float:
+    n = np.asarray(n, dtype=np.float64)
+    return float(np.sum(10.0 / 3.0 * n ** 3))
+
+
+def tridiag_bytes(n: int, nb: int = 16) -> float:
+    """Algorithmic HBM bytes of the one-stage blocked reduction of an n x n block: each column's
+    symmetric matrix-vector product reads the trailing lower triangle once, and each panel of nb
+    columns reads and writes the trailing lower triangle once in its rank-2nb update."""
+    m = np.arange(1, n - 1, dtype=np.float64)  # trailing orders n-k-1 for k = 0..n-3
+    symv = 8.0 * np.sum(m * (m + 1) / 2)
+    pe = np.minimum(np.arange(nb, n - 2 + nb, nb), n - 2).astype(np.float64)
+    t = n - pe
+    upd = 16.0 * np.sum(t * (t + 1) / 2)
+    return symv + upd
+
+
+def make_block(torch, b: int, n: int, device):
+    g = torch.Generator(device=device)
+    g.manual_seed(SEED * 100003 + b)
+    h = torch.randn((n, n), generator=g, dtype=torch.float64, device=device).mul_(0.1).triu_(1)
+    h.diagonal().copy_(torch.pow(2.0, -torch.arange(n, dtype=torch.float64, device=device) / 2.0))
+    return h
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.p, self.lines = gpu, None, []
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        busy = [x for x in sm if mx and x > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(busy)) if busy else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(p))
+    except OSError:
+        return {}
+
+
+def cpu_sample(sizes: np.ndarray, target_s: float, threads: int):
+    """Stratified sample (every s-th block in size order) whose dsyev time on `threads`
+    cores is about target_s, calibrated with a short dsyev timing."""
+    from oracle import oracle
+    rng = np.random.default_rng(0)
+    cal = [np.triu(rng.standard_normal((384, 384))) for _ in range(max(1, threads))]
+    oracle.blas_threads(1)
+    t0 = time.perf_counter()
+    oracle.diag_batch(cal, nthreads=threads)
+    dt = time.perf_counter() - t0
+    per_n3 = dt * threads / (len(cal) * 384.0 ** 3)  # core-seconds per n^3
+    total = per_n3 * float(np.sum(sizes.astype(np.float64) ** 3)) / threads
+    stride = max(1, int(math.ceil(total / target_s)))
+    order = np.argsort(sizes, kind="stable")
+    return order[stride // 2::stride], stride
+
+
+def run_cpu(blocks, threads: int):
+    from oracle import oracle
+    oracle.blas_threads(1)
+    n = np.array([b.shape[0] for b in blocks], dtype=np.int32)
+    moff = np.zeros(len(n), dtype=np.int64)
+    voff = np.zeros(len(n), dtype=np.int64)
+    moff[1:] = np.cumsum(n.astype(np.int64) ** 2)[:-1]
+    voff[1:] = np.cumsum(n.astype(np.int64))[:-1]
+    H0 = np.concatenate([b.ravel() for b in blocks])
+    V = np.zeros(int(n.sum()))
+    Z = np.zeros_like(H0)
+    H = H0.copy()
+    t0 = time.perf_counter()
+    bad = oracle.diag_batch_packed(n, moff, voff, H, V, Z, threads)
+    dt = time.perf_counter() - t0
+    if bad:
+        raise RuntimeError(f"{bad} blocks failed in dsyev")
+    return dt
+
+
+def sample_blocks_host(torch, sizes, idx, device):
+    out = []
+    for b in idx:
+        out.append(make_block(torch, int(b), int(sizes[b]), device).cpu().numpy())
+    return out
+
+
+def reference_arm(args, rank: int) -> None:
+    import torch
+    if rank != 0:
+        return
+    sizes = block_sizes(args.nblk)
+    threads = os.cpu_count() or 1
+    idx, stride = cpu_sample(sizes, args.cpu_seconds, threads)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    blocks = sample_blocks_host(torch, sizes, idx, dev)
+    flop = f_eig(sizes[idx])
+    for _ in range(args.warmup):
+        run_cpu(blocks, threads)
+    times = [run_cpu(blocks, threads) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    value = flop / t / 1e9
+    sample = (f"{len(idx)} of {args.nblk} blocks (every {stride}th in size order, sum n^3 = "
+              f"{float(np.sum(sizes[idx].astype(float) ** 3)):.3e}); LAPACK dsyev, OpenMP over blocks, 1 BLAS thread each")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.format(nblk=args.nblk), "nblk": args.nblk, "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nblk", type=int, default=10000)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import nrgljubljana_b200 as nb
+    ctx = nb.context(local)
+
+    sizes = block_sizes(args.nblk)
+    offs = np.zeros(args.nblk + 1, dtype=np.int64)
+    offs[1:] = np.cumsum(sizes.astype(np.int64) ** 2)
+    voffs = np.zeros(args.nblk + 1, dtype=np.int64)
+    voffs[1:] = np.cumsum(sizes)
+    total = int(offs[-1])
+    dev = torch.device("cuda", local)
+    pristine = torch.empty(total, dtype=torch.float64, device=dev)
+    for b in range(args.nblk):
+        n = int(sizes[b])
+        pristine[offs[b]:offs[b + 1]].view(n, n).copy_(make_block(torch, b, n, dev))
+    work = torch.empty_like(pristine)
+    evecs = torch.empty_like(pristine)
+    evals = torch.empty(int(voffs[-1]), dtype=torch.float64, device=dev)
+    import ctypes as C
+    nbk = args.nblk
+    n_c = (C.c_int * nbk)(*[int(x) for x in sizes])
+    Hp = (C.c_void_p * nbk)(*[work.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+    Vp = (C.c_void_p * nbk)(*[evecs.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+    Ep = (C.c_void_p * nbk)(*[evals.data_ptr() + 8 * int(voffs[b]) for b in range(nbk)])
+    info = (C.c_int * nbk)()
+
+    def step():
+        work.copy_(pristine)
+        rc = ctx.lib.nrg_diag_batch(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)
+        if rc != 0:
+            raise RuntimeError(f"nrg_diag_batch returned {rc}: {nb.load_library().nrg_last_error().decode()}")
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    phases = ctx.profile_read()
+    ctx.profile(False)
+    if dist:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    flop_step = f_eig(sizes)
+    value = world * args.steps * flop_step / elapsed / 1e9
+    launches = int(sum(v[1] for v in phases.values()))
+
+    # roofline of the dominant kernel
+    peaks = measured_peaks()
+    top = max(phases.items(), key=lambda kv: kv[1][0])
+    roof = None
+    if top[0] == "tridiag":
+        per_launch_bytes = args.steps * sum(tridiag_bytes(int(n)) for n in sizes if n > 64) / top[1][1]
+        avg = top[1][0] / 1e3 / top[1][1]
+        ach = per_launch_bytes / avg / 1e9
+        pk = peaks.get("hbm_gbs", 6650.0)
+        roof = {"kernel": "tridiag_kernel", "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
+                "frac": ach / pk, "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg * 1e3}
+    else:
+        roof = {"kernel": top[0], "bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s",
+                "frac": None, "traffic": None}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.format(nblk=nbk), "nblk": nbk, "sum_n3": float(np.sum(sizes.astype(float) ** 3)),
+                       "flop_per_step": flop_step, "input_bytes": 8 * total,
+                       "l2": "inputs larger than L2 (30 GB vs 126 MB); consumed inputs refreshed by a D2D copy inside each step",
+                       "parallelism": f"replicas x{world}"},
+            "steps_per_s": world * args.steps / elapsed, "gpu_launches": launches, "roofline": roof,
+            "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
+            "clocks": clk.summary()}
+
+    del work, evecs, evals
+    torch.cuda.empty_cache()
+    if not args.no_e2e and rank == 0 and world == 1:
+        try:
+            line["e2e"] = e2e_arm(torch, ctx, nb, pristine, sizes, offs, voffs, args)
+        except (RuntimeError, MemoryError) as err:
+            line["e2e"] = {"value": None, "unit": UNIT, "error": str(err)[:300]}
+    if not args.no_cpu and rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        idx, stride = cpu_sample(sizes, args.cpu_seconds, threads)
+        blocks = [pristine[offs[b]:offs[b + 1]].view(int(sizes[b]), int(sizes[b])).cpu().numpy() for b in idx]
+        t = run_cpu(blocks, threads)
+        cpu_v = f_eig(sizes[idx]) / t / 1e9
+        line["cpu_baseline"] = {"value": cpu_v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{len(idx)} of {nbk} blocks (every {stride}th in size order), {t:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def e2e_arm(torch, ctx, nb, pristine, sizes, offs, voffs, args) -> dict:
+    """Same metric through the host-pointer entry point, from pinned host memory."""
+    import ctypes as C
+    nbk = len(sizes)
+    hostH = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+    hostH.copy_(pristine)
+    hostV = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+    hostE = torch.empty(int(voffs[-1]), dtype=torch.float64, pin_memory=True)
+    n_c = (C.c_int * nbk)(*[int(x) for x in sizes])
+    Hp = (C.c_void_p * nbk)(*[hostH.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+    Vp = (C.c_void_p * nbk)(*[hostV.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+    Ep = (C.c_void_p * nbk)(*[hostE.data_ptr() + 8 * int(voffs[b]) for b in range(nbk)])
+    info = (C.c_int * nbk)()
+    rc = ctx.lib.nrg_diag_batch_host(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)  # warm-up
+    if rc != 0:
+        raise RuntimeError(f"nrg_diag_batch_host returned {rc}")
+    k = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        rc = ctx.lib.nrg_diag_batch_host(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)
+        if rc != 0:
+            raise RuntimeError(f"nrg_diag_batch_host returned {rc}")
+    dt = (time.perf_counter() - t0) / k
+    return {"value": f_eig(sizes) / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(8 * offs[-1]),
+            "d2h_bytes_per_step": int(8 * (offs[-1] + voffs[-1])), "steps": k, "ms_per_step": dt * 1e3}
+
+
+if __name__ == "__main__":
+    main()

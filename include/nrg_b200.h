@@ -157,6 +157,21 @@ typedef struct nrg_bins {
 NRG_API int nrg_spec_accumulate(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* params,
                         const nrg_bins* bins, double* pos, double* neg, void* stream);
 
+/* ------------------------------------------------------------------ timing
+ * Per-phase device timing in the spirit of the reference's MemTime::time_it sections
+ * (c++/time_mem.hpp:97-115): nrg_profile(ctx, 1) resets the counters and brackets every
+ * later launch group with CUDA events on its stream; nrg_profile_read synchronises on
+ * those events and returns one entry per phase that launched (name, total ms, number of
+ * kernel launches). Launch counts are kept even when timing is off. */
+typedef struct nrg_phase_stat {
+  char name[24];
+  double ms;
+  long long launches;
+} nrg_phase_stat;
+
+NRG_API int nrg_profile(nrg_ctx* ctx, int enable);
+NRG_API int nrg_profile_read(nrg_ctx* ctx, nrg_phase_stat* out, int max);
+
 /* Energies of the log grid (c++/bins.hpp:95-100) for one sign half; returns nbins. */
 NRG_API int nrg_bins_grid(const nrg_bins* bins, double* energies_host);
 

@@ -38,6 +38,16 @@ class Context:
         check(self.lib.nrg_create(C.byref(self.ptr), device, workspace_limit), "nrg_create")
         self.device = device
 
+    def profile(self, enable: bool = True) -> None:
+        """Start (reset) or stop per-phase CUDA-event timing (nrg_profile)."""
+        check(self.lib.nrg_profile(self.ptr, int(enable)), "nrg_profile")
+
+    def profile_read(self) -> dict:
+        """{phase: (ms, launches)} since the last profile(True) (nrg_profile_read)."""
+        arr = (_lib.PhaseStat * 32)()
+        k = check(self.lib.nrg_profile_read(self.ptr, arr, 32), "nrg_profile_read")
+        return {arr[i].name.decode(): (arr[i].ms, int(arr[i].launches)) for i in range(k)}
+
     def close(self):
         if self.ptr:
             self.lib.nrg_destroy(self.ptr)

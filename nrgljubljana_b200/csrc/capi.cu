@@ -113,21 +113,52 @@ StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p) {
   return g;
 }
 
-int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s) {
+const char* phase_name(int p) {
+  static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
+                                        "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
+                                        "gemm3", "spec_gemm", "spec_bin"};
+  return (p >= 0 && p < kPhCount) ? names[p] : "?";
+}
+
+static cudaEvent_t take_event(nrg_ctx* c) {
+  if (c->ev_used == c->ev_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    c->ev_pool.push_back(e);
+  }
+  return c->ev_pool[c->ev_used++];
+}
+
+PhaseScope::PhaseScope(nrg_ctx* c_, int phase, cudaStream_t s_, int nlaunch) : c(c_), s(s_) {
+  c->launches[phase] += nlaunch;
+  if (!c->prof) return;
+  cudaEvent_t b = take_event(c), e = take_event(c);
+  if (!b || !e) return;
+  cudaEventRecord(b, s);
+  mark = (int)c->marks.size();
+  c->marks.push_back(nrg_ctx::Mark{phase, (int)c->ev_used - 2, (int)c->ev_used - 1});
+}
+
+PhaseScope::~PhaseScope() {
+  if (mark >= 0) cudaEventRecord(c->ev_pool[c->marks[mark].e], s);
+}
+
+int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s, int phase) {
   if (g.nout == 0 || g.tiles == 0) return NRG_OK;
+  PhaseScope ps(c, phase, s);
   const char* base = static_cast<const char*>(c->desc);
   NRG_CK(gemm_batch_launch(reinterpret_cast<const GemmOut*>(base + g.outs_off),
                            reinterpret_cast<const GemmSeg*>(base + g.segs_off), g.nout, g.tiles, s));
   return NRG_OK;
 }
 
-int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s) {
+int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s, int phase) {
   if (p.outs.empty() || p.tiles == 0) return NRG_OK;
   std::vector<char> img;
   const StagedGemm g = stage_gemm(img, p);
   int rc = stage_desc(c, img, s);
   if (rc) return rc;
-  return launch_staged_gemm(c, g, s);
+  return launch_staged_gemm(c, g, s, phase);
 }
 
 }  // namespace nrg
@@ -177,10 +208,45 @@ int nrg_create(nrg_ctx** out, int device, size_t workspace_limit) {
   return NRG_OK;
 }
 
+int nrg_profile(nrg_ctx* c, int enable) {
+  if (!c) return fail(NRG_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  if (enable) {
+    CK(cudaDeviceSynchronize());
+    c->marks.clear();
+    c->ev_used = 0;
+    for (auto& l : c->launches) l = 0;
+  }
+  c->prof = enable != 0;
+  return NRG_OK;
+}
+
+int nrg_profile_read(nrg_ctx* c, nrg_phase_stat* out, int max) {
+  if (!c || (max > 0 && !out)) return fail(NRG_ERR_ARG, "bad arguments");
+  CK(cudaSetDevice(c->device));
+  double ms[nrg::kPhCount] = {};
+  for (const auto& m : c->marks) {
+    CK(cudaEventSynchronize(c->ev_pool[m.e]));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->ev_pool[m.b], c->ev_pool[m.e]));
+    ms[m.phase] += t;
+  }
+  int k = 0;
+  for (int p = 0; p < nrg::kPhCount && k < max; p++) {
+    if (c->launches[p] == 0) continue;
+    std::snprintf(out[k].name, sizeof out[k].name, "%s", nrg::phase_name(p));
+    out[k].ms = ms[p];
+    out[k].launches = c->launches[p];
+    k++;
+  }
+  return k;
+}
+
 int nrg_destroy(nrg_ctx* c) {
   if (!c) return NRG_OK;
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
   if (c->ws) cudaFree(c->ws);
   if (c->desc) cudaFree(c->desc);
   if (c->info_dev) cudaFree(c->info_dev);
@@ -229,6 +295,7 @@ int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double*
     const size_t off = push(img, blk);
     rc = stage_desc(c, img, s);
     if (rc) return rc;
+    nrg::PhaseScope ps(c, nrg::kPhEigSmall, s);
     CK(nrg::eig_small_launch(reinterpret_cast<const nrg::EigBlock*>(static_cast<char*>(c->desc) + off),
                              (int)small.size(), n[small[0]], s));
   }
@@ -351,9 +418,9 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
       else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
     }
   }
-  rc = run_gemm_plan(c, p1, s);
+  rc = run_gemm_plan(c, p1, s, nrg::kPhGemm3);
   if (rc) return rc;
-  return run_gemm_plan(c, p2, s);
+  return run_gemm_plan(c, p2, s, nrg::kPhGemm3);
 }
 
 int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream) {
@@ -504,7 +571,7 @@ int nrg_spec_accumulate(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const
       region(q, nrg::kSpecGemmX, q.ki, q.ni, 0, q.kj, X, q.ni, nullptr, 0, ms);                // D x K
     }
   }
-  rc = run_gemm_plan(c, gp, s);
+  rc = run_gemm_plan(c, gp, s, nrg::kPhSpecGemm);
   if (rc) return rc;
   if (regs.empty()) return NRG_OK;
   std::vector<nrg::SpecTask> tasks;
@@ -529,6 +596,7 @@ int nrg_spec_accumulate(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const
   bp.bins = bins->bins;
   bp.nbins = bins->nbins;
   const char* base = static_cast<const char*>(c->desc);
+  nrg::PhaseScope ps(c, nrg::kPhSpecBin, s);
   CK(nrg::spec_bin_launch(reinterpret_cast<const nrg::SpecTask*>(base + to), (int)tasks.size(),
                           reinterpret_cast<const nrg::SpecRegion*>(base + ro), bp, pos, neg, s));
   return NRG_OK;

@@ -10,8 +10,24 @@
 #include "../../include/nrg_b200.h"
 #include "kernels.h"
 
+namespace nrg {
+// Launch groups timed by nrg_profile (names in phase_name()).
+enum Phase : int {
+  kPhEigSmall, kPhTridiag, kPhDcLeaf, kPhDcPrep, kPhDcSecular, kPhDcVectors, kPhDcGemm, kPhSort, kPhBtGemm,
+  kPhBtTfactor, kPhGemm3, kPhSpecGemm, kPhSpecBin, kPhCount
+};
+const char* phase_name(int p);
+}  // namespace nrg
+
 struct nrg_ctx {
   int device = 0;
+  // profiling: launch counts per phase (always), CUDA-event intervals (when enabled)
+  bool prof = false;
+  long long launches[nrg::kPhCount] = {};
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct Mark { int phase, b, e; };
+  std::vector<Mark> marks;
   size_t ws_limit = 0;
   void* ws = nullptr;  // device workspace arena (grow-only)
   size_t ws_size = 0;
@@ -55,9 +71,19 @@ struct StagedGemm {
   int nout = 0, tiles = 0;
 };
 StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p);
-int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s);
+int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s, int phase);
 
-int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s);
+int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s, int phase);
+
+// Counts `nlaunch` kernel launches of `phase` and, when profiling, brackets them with
+// CUDA events recorded on stream s.
+struct PhaseScope {
+  nrg_ctx* c;
+  cudaStream_t s;
+  int mark = -1;
+  PhaseScope(nrg_ctx* c, int phase, cudaStream_t s, int nlaunch = 1);
+  ~PhaseScope();
+};
 
 }  // namespace nrg
 

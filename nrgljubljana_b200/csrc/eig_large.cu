@@ -935,12 +935,16 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     {
       const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 32);
       NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PhaseScope ps(c, kPhTridiag, s);
       tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
       NRG_CK(cudaGetLastError());
     }
     // ---- 2. divide and conquer
-    dc_leaf_kernel<<<(int)leaves.size(), 128, 0, s>>>(dblk, reinterpret_cast<const DcLeaf*>(dbase + leaf_off));
-    NRG_CK(cudaGetLastError());
+    {
+      PhaseScope ps(c, kPhDcLeaf, s);
+      dc_leaf_kernel<<<(int)leaves.size(), 128, 0, s>>>(dblk, reinterpret_cast<const DcLeaf*>(dbase + leaf_off));
+      NRG_CK(cudaGetLastError());
+    }
     for (size_t h = 0; h < levels.size(); h++) {
       int maxN = 0;
       for (auto& nd : levels[h]) maxN = std::max(maxN, nd.b - nd.a);
@@ -951,16 +955,25 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       GemmSeg* gs = reinterpret_cast<GemmSeg*>(dbase + lvl_gemm[h].segs_off);
       const size_t ps = prep_layout(maxN).total;
       NRG_CK(cudaFuncSetAttribute(dc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-      dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs);
-      NRG_CK(cudaGetLastError());
+      {
+        PhaseScope sc(c, kPhDcPrep, s);
+        dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs);
+        NRG_CK(cudaGetLastError());
+      }
       const int ysplit = std::max(1, std::min(16, maxN / 256));
-      dc_secular_kernel<<<dim3(nn, ysplit), 256, 0, s>>>(dblk, dn, dst);
-      NRG_CK(cudaGetLastError());
+      {
+        PhaseScope sc(c, kPhDcSecular, s);
+        dc_secular_kernel<<<dim3(nn, ysplit), 256, 0, s>>>(dblk, dn, dst);
+        NRG_CK(cudaGetLastError());
+      }
       const size_t vs = sizeof(double) * (size_t)maxN;
       NRG_CK(cudaFuncSetAttribute(dc_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vs));
-      dc_vectors_kernel<<<nn, 512, vs, s>>>(dblk, dn, dst);
-      NRG_CK(cudaGetLastError());
-      rc = launch_staged_gemm(c, lvl_gemm[h], s);
+      {
+        PhaseScope sc(c, kPhDcVectors, s);
+        dc_vectors_kernel<<<nn, 512, vs, s>>>(dblk, dn, dst);
+        NRG_CK(cudaGetLastError());
+      }
+      rc = launch_staged_gemm(c, lvl_gemm[h], s, kPhDcGemm);
       if (rc) return rc;
     }
     // ---- 3. order
@@ -969,22 +982,24 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       while (P < maxn) P <<= 1;
       const size_t ss = (sizeof(double) + sizeof(int)) * (size_t)P;
       NRG_CK(cudaFuncSetAttribute(sort_final_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+      PhaseScope sc(c, kPhSort, s, 2);
       sort_final_kernel<<<nb, 1024, ss, s>>>(dblk);
       NRG_CK(cudaGetLastError());
       permute_rows_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
       NRG_CK(cudaGetLastError());
     }
     // ---- 4. back-transform
-    rc = launch_staged_gemm(c, gram_g, s);
+    rc = launch_staged_gemm(c, gram_g, s, kPhBtGemm);
     if (rc) return rc;
     if (!panels.empty()) {
+      PhaseScope sc(c, kPhBtTfactor, s);
       tfactor_kernel<<<(int)panels.size(), NBT, 0, s>>>(dblk, reinterpret_cast<const PanelRef*>(dbase + pan_off));
       NRG_CK(cudaGetLastError());
     }
-    rc = launch_staged_gemm(c, vt_g, s);
+    rc = launch_staged_gemm(c, vt_g, s, kPhBtGemm);
     if (rc) return rc;
     for (size_t t = 0; t < bs_g.size(); t++) {
-      rc = launch_staged_gemm(c, bs_g[t], s);
+      rc = launch_staged_gemm(c, bs_g[t], s, kPhBtGemm);
       if (rc) return rc;
     }
     pos = end;
