@@ -29,7 +29,7 @@
 namespace nrg {
 namespace {
 
-constexpr int kTriThreads = 256;
+constexpr int kTriThreads = 512;
 constexpr int NB = 16;     // tridiagonalisation panel width
 constexpr int NBT = 64;    // back-transform panel width
 constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
@@ -72,71 +72,95 @@ struct DcState {
 
 // ---------------------------------------------------------------- tridiagonalisation
 
-// Transpose-reduction across a warp: lane c returns sum over lanes of x[c].
-NRG_DEV double transpose_reduce32(double (&x)[32], int lane) {
+// Column sums of an 8-column slab: lane l holds x[c] = A(i_l, j0+c) * v[i_l]; returns, in
+// every lane, the sum over all 32 lanes of x[c] for c = (l >> 2) & 7 (9 shuffles).
+NRG_DEV double slab_colsum8(double (&x)[8], int lane) {
+  {
+    const bool up = (lane & 16) != 0;
 #pragma unroll
-  for (int s = 16; s >= 1; s >>= 1) {
-    const bool up = (lane & s) != 0;
-#pragma unroll
-    for (int q = 0; q < s; q++) {
-      const double send = up ? x[q] : x[q + s];
-      const double keep = up ? x[q + s] : x[q];
-      x[q] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    for (int q = 0; q < 4; q++) {
+      const double send = up ? x[q] : x[q + 4];
+      const double keep = up ? x[q + 4] : x[q];
+      x[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
     }
   }
+  {
+    const bool up = (lane & 8) != 0;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const double send = up ? x[q] : x[q + 2];
+      const double keep = up ? x[q + 2] : x[q];
+      x[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+  }
+  {
+    const bool up = (lane & 4) != 0;
+    const double send = up ? x[0] : x[1];
+    const double keep = up ? x[1] : x[0];
+    x[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  x[0] += __shfl_xor_sync(0xffffffffu, x[0], 2);
+  x[0] += __shfl_xor_sync(0xffffffffu, x[0], 1);
   return x[0];
 }
 
 // y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n, A symmetric with its lower triangle
-// stored as A(i, j) = H[j*n + i] (i >= j). Warps own 32-row tile rows; row sums stay in
-// registers, column sums are transposed across the warp and added to y in shared memory.
+// stored as A(i, j) = H[j*n + i] (i >= j). Warps own 32-row tile rows and walk them in
+// 8-column slabs (one coalesced 256-byte load per column), prefetching the next slab; row
+// sums stay in registers, column sums are transposed across the warp and added to y
+// (shared memory) once per slab column.
 NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const double* v, double* y) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
-  const bool full_last = (n & 31) == 0;
+  const int sl0 = s0 >> 3;  // first slab touching column s0
   for (int I = Tn - warp; I >= T0; I -= nwarps) {
     const int i = (I << 5) + lane;
     const bool iv = (i >= s0) && (i < n);
     const double vi = iv ? v[i] : 0.0;
+    const int sl1 = min((I << 2) + 3, (n - 1) >> 3);  // last slab of this tile row
     double racc = 0.0;
-    for (int J = T0; J <= I; J++) {
-      const int j0 = J << 5;
-      double cp[32];
-      const bool interior = (J > T0) && (J < I) && (I < Tn || full_last);
-      if (interior) {
-        const double* col = H + (size_t)j0 * n + i;
-        double a[32];
+    double cur[8], nxt[8];
+    auto load = [&](int sl, double (&dst)[8]) {
+      const int j0 = sl << 3;
 #pragma unroll
-        for (int c = 0; c < 32; c++) a[c] = col[(size_t)c * n];
-#pragma unroll
-        for (int c = 0; c < 32; c++) {
-          racc = fma(a[c], v[j0 + c], racc);
-          cp[c] = a[c] * vi;
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < 32; c++) {
-          const int jj = j0 + c;
-          const bool ok = iv && jj >= s0 && jj < n && i >= jj;
-          const double a = ok ? H[(size_t)jj * n + i] : 0.0;
-          const double vj = (jj < n) ? v[jj] : 0.0;
-          racc = fma(a, vj, racc);
-          cp[c] = (i > jj) ? a * vi : 0.0;
-        }
+      for (int c = 0; c < 8; c++) {
+        const int jj = j0 + c;
+        const bool ok = iv && jj >= s0 && jj <= i;
+        dst[c] = ok ? H[(size_t)jj * n + i] : 0.0;
       }
-      const double cs = transpose_reduce32(cp, lane);
-      const int jc = j0 + lane;
-      if (jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
+    };
+    load(sl0, cur);
+    for (int sl = sl0; sl <= sl1; sl++) {
+      if (sl < sl1) load(sl + 1, nxt);
+      const int j0 = sl << 3;
+      double cp[8];
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int jj = j0 + c;
+        const double vj = (jj < n) ? v[jj] : 0.0;
+        racc = fma(cur[c], vj, racc);
+        cp[c] = (jj < i) ? cur[c] * vi : 0.0;  // the diagonal enters the row sum only
+      }
+      const double cs = slab_colsum8(cp, lane);
+      const int jc = j0 + ((lane >> 2) & 7);
+      if ((lane & 3) == 0 && jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
+#pragma unroll
+      for (int c = 0; c < 8; c++) cur[c] = nxt[c];
     }
     if (iv) atomicAdd(&y[i], racc);
   }
 }
 
 // A(i, j) -= sum_{q < nbp} V(i,q) W(j,q) + W(i,q) V(j,q) for s0 <= j <= i < n, with
-// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i].
-NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0) {
+// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i]. A lane keeps its row's V and W in
+// registers; the 32 columns of a tile are staged per warp in shared memory (stage: 2 * 32 *
+// (NB+1) doubles per warp) and read as broadcasts.
+NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0,
+                          double* stage) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
+  double* Vs = stage + (size_t)warp * 2 * 32 * (NB + 1);
+  double* Ws = Vs + 32 * (NB + 1);
   for (int I = Tn - warp; I >= T0; I -= nwarps) {
     const int i = (I << 5) + lane;
     const bool iv = (i >= s0) && (i < n);
@@ -150,24 +174,25 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
     for (int J = T0; J <= I; J++) {
       const int jl = (J << 5) + lane;
       const bool jv = (jl >= s0) && (jl < n);
-      double Vj[NB], Wj[NB];
+      __syncwarp();
 #pragma unroll
       for (int q = 0; q < NB; q++) {
         const bool ok = jv && q < nbp;
-        Vj[q] = ok ? H[(size_t)(p0 + q) * n + jl] : 0.0;
-        Wj[q] = ok ? W[(size_t)q * n + jl] : 0.0;
+        Vs[lane * (NB + 1) + q] = ok ? H[(size_t)(p0 + q) * n + jl] : 0.0;
+        Ws[lane * (NB + 1) + q] = ok ? W[(size_t)q * n + jl] : 0.0;
       }
+      __syncwarp();
       double* col = H + (size_t)(J << 5) * n + i;
-#pragma unroll 4
-      for (int c = 0; c < 32; c++) {
+      const int cmax = min(32, n - (J << 5));
+      for (int c = 0; c < cmax; c++) {
         const int jj = (J << 5) + c;
-        double s = 0.0;
+        double sacc = 0.0;
 #pragma unroll
         for (int q = 0; q < NB; q++) {
-          s = fma(Vi[q], __shfl_sync(0xffffffffu, Wj[q], c), s);
-          s = fma(Wi[q], __shfl_sync(0xffffffffu, Vj[q], c), s);
+          sacc = fma(Vi[q], Ws[c * (NB + 1) + q], sacc);
+          sacc = fma(Wi[q], Vs[c * (NB + 1) + q], sacc);
         }
-        if (iv && jj >= s0 && jj < n && i >= jj) col[(size_t)c * n] -= s;
+        if (iv && jj >= s0 && i >= jj) col[(size_t)c * n] -= sacc;
       }
     }
   }
@@ -185,6 +210,7 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
   double* part = y + n;                 // nwarps * 2NB
   double* cwv = part + nwarps * 2 * NB;  // 2NB
   double* red = cwv + 2 * NB;            // 32
+  double* stage = red + 32;              // nwarps * 2 * 32 * (NB+1), panel update
 
   for (int p0 = 0; p0 < n - 2; p0 += NB) {
     const int pe = min(p0 + NB, n - 2);
@@ -283,7 +309,7 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
       }
       __syncthreads();
     }
-    panel_update(H, W, n, p0, pe - p0, pe);
+    panel_update(H, W, n, p0, pe - p0, pe, stage);
     __syncthreads();
   }
   if (tid == 0) {
@@ -933,7 +959,8 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
 
     // ---- 1. tridiagonalisation
     {
-      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 32);
+      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 32 +
+                                            (kTriThreads / 32) * 2 * 32 * (NB + 1));
       NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       PhaseScope ps(c, kPhTridiag, s);
       tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
