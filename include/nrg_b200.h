@@ -103,6 +103,23 @@ typedef struct nrg_gemm3 {
 NRG_API int nrg_gemm3_batch(nrg_ctx* ctx, int nterm, const nrg_gemm3* terms, void* stream);
 NRG_API int nrg_gemm3_batch_host(nrg_ctx* ctx, int nterm, const nrg_gemm3* terms, void* stream);
 
+/* One transform term, M (rows x cols) += factor * A (rows x ka) * O (ka x kb) * B^T
+ * (B is cols x kb; O = NULL means the identity, ka == kb), that allocates nothing.
+ * This entry point has no counterpart in the reference. It is for callers that cannot call
+ * cudaMalloc: a host thread that must not stall the device (cudaMalloc/cudaFree may
+ * synchronise it), a plugin in a process whose device memory is already reserved by
+ * another allocator, or code that may not own device memory. It needs no context: the
+ * intermediate O * B^T is kept in a fixed device array of NRG_NOALLOC_SCRATCH_DOUBLES
+ * doubles (8 MiB) that every GPU loading this library holds until the process exits, and
+ * ka * cols beyond that limit is rejected with NRG_ERR_ARG. Pointers are device pointers on
+ * the current device. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU (other streams, other host threads) race. */
+#define NRG_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+NRG_API int nrg_transform_noalloc(double* M, int64_t ldm, const double* A, int64_t lda, const double* O,
+                                  int64_t ldo, const double* B, int64_t ldb, int rows, int cols, int ka, int kb,
+                                  double factor, void* stream);
+
 /* ------------------------------------------------------------------ spectral accumulation
  * Replaces the per-pair calc() of Algo_DMNRG (c++/algo_DMNRG.hpp:29-52), Algo_FDMgt
  * (c++/algo_FDM.hpp:84-114) and Algo_FDMls (c++/algo_FDM.hpp:30-60), driven over all

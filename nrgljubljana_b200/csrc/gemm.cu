@@ -67,21 +67,12 @@ __device__ __forceinline__ void store_stage(const Stage& s, const GemmSeg& g, do
   }
 }
 
-__global__ void __launch_bounds__(NT) gemm_batch_kernel(const GemmOut* __restrict__ outs,
-                                                         const GemmSeg* __restrict__ segs, int nout) {
+// One 64 x 64 output tile `tt` (row-major tile order) of output o, whose segments are
+// segs[o.seg0 .. o.seg0 + o.nseg).
+__device__ __forceinline__ void gemm_tile(const GemmOut& o, const GemmSeg* __restrict__ segs, int tt) {
   __shared__ __align__(16) double As[2][BK * LDS];
   __shared__ __align__(16) double Bs[2][BK * LDS];
-
-  // Locate the output that owns this tile (binary search over tile0).
-  const int t = blockIdx.x;
-  int lo = 0, hi = nout - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (outs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const GemmOut o = outs[lo];
   const int tiles_n = (o.N + BN - 1) / BN;
-  const int tt = t - o.tile0;
   const int m0 = (tt / tiles_n) * BM, n0 = (tt % tiles_n) * BN;
   if (m0 >= o.M) return;  // outputs whose row count is set on the device may shrink
 
@@ -166,7 +157,37 @@ __global__ void __launch_bounds__(NT) gemm_batch_kernel(const GemmOut* __restric
   }
 }
 
+__global__ void __launch_bounds__(NT) gemm_batch_kernel(const GemmOut* __restrict__ outs,
+                                                         const GemmSeg* __restrict__ segs, int nout) {
+  // Locate the output that owns this tile (binary search over tile0).
+  const int t = blockIdx.x;
+  int lo = 0, hi = nout - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (outs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+  }
+  const GemmOut o = outs[lo];
+  gemm_tile(o, segs, t - o.tile0);
+}
+
+// Single output with a single segment, both passed by value (no descriptor memory).
+__global__ void __launch_bounds__(NT) gemm_one_kernel(const __grid_constant__ GemmOut o,
+                                                       const __grid_constant__ GemmSeg g) {
+  gemm_tile(o, &g, blockIdx.x);
+}
+
 }  // namespace
+
+cudaError_t gemm_one_launch(const GemmOut& o, const GemmSeg& g, cudaStream_t stream) {
+  const int tiles = ((o.M + BM - 1) / BM) * ((o.N + BN - 1) / BN);
+  if (tiles <= 0) return cudaSuccess;
+  GemmOut oo = o;
+  oo.seg0 = 0;
+  oo.nseg = 1;
+  oo.tile0 = 0;
+  gemm_one_kernel<<<tiles, NT, 0, stream>>>(oo, g);
+  return cudaGetLastError();
+}
 
 cudaError_t gemm_batch_launch(const GemmOut* d_outs, const GemmSeg* d_segs, int nout, int ntiles,
                               cudaStream_t stream) {

@@ -32,6 +32,8 @@ constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16, kGemmThreads = 128;
 // Launch over nout outputs whose descriptors already live in device memory.
 cudaError_t gemm_batch_launch(const GemmOut* d_outs, const GemmSeg* d_segs, int nout, int ntiles,
                               cudaStream_t stream);
+// One output C = beta*C + alpha op(A) op(B) with descriptors passed as kernel parameters.
+cudaError_t gemm_one_launch(const GemmOut& o, const GemmSeg& g, cudaStream_t stream);
 
 // ---------------------------------------------------------------- eigensolver
 // Per-block descriptor of the batched symmetric eigensolver. H is n x n row-major with the

@@ -1,0 +1,71 @@
+"""The allocation-free transform entry point (nrg_transform_noalloc), called through the
+C-ABI and checked against the batched entry point nrg_gemm3_batch on the same inputs.
+
+This file is collected last, so that a run stopping at the first failure has run every
+other test before it. It must pass alone in a fresh process as well."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-13  # the tolerance of the GEMM-leaf parity tests
+
+
+def _view(torch, rng, rows, cols, pad):
+    """A strided view (leading dimension cols + 2 * pad) such as a U(i) block of recalc.hpp."""
+    wide = torch.tensor(rng.standard_normal((rows, cols + 2 * pad)), device="cuda")
+    return wide[:, pad:pad + cols]
+
+
+def test_noalloc_matches_batched_entry_point_twice():
+    import torch
+
+    import nrgljubljana_b200 as nb
+    lib = nb.load_library()
+    nb.context()
+    rng = np.random.default_rng(2027)
+    # two calls in a row with different shapes: the shared scratch keeps the first call's
+    # contents, which the second call must not depend on
+    for rows, cols, ka, kb, f in ((70, 90, 40, 33, 0.75), (33, 129, 64, 17, -1.5)):
+        A = _view(torch, rng, rows, ka, 3)
+        B = _view(torch, rng, cols, kb, 2)
+        O = torch.tensor(rng.standard_normal((ka, kb)), device="cuda")
+        M0 = torch.tensor(rng.standard_normal((rows, cols)), device="cuda")
+        ref = M0.clone()
+        nb.gemm3_batch([nb.gemm3(ref, f, A, O, B)], host=False)
+        got = M0.clone()
+        rc = lib.nrg_transform_noalloc(got.data_ptr(), got.stride(0), A.data_ptr(), A.stride(0), O.data_ptr(),
+                                       O.stride(0), B.data_ptr(), B.stride(0), rows, cols, ka, kb, f, None)
+        assert rc == 0, nb._lib.last_error()
+        torch.cuda.synchronize()
+        r, g = ref.cpu().numpy(), got.cpu().numpy()
+        assert np.abs(g - r).max() <= REL * max(1.0, np.abs(r).max()) * g.size ** 0.5
+    # identity O (product): no scratch involved
+    A = _view(torch, rng, 20, 16, 1)
+    B = _view(torch, rng, 24, 16, 1)
+    ref = torch.zeros((20, 24), dtype=torch.float64, device="cuda")
+    nb.gemm3_batch([nb.gemm3(ref, 2.0, A, None, B)], host=False)
+    got = torch.zeros_like(ref)
+    assert lib.nrg_transform_noalloc(got.data_ptr(), 24, A.data_ptr(), A.stride(0), None, 0, B.data_ptr(),
+                                     B.stride(0), 20, 24, 16, 16, 2.0, None) == 0
+    torch.cuda.synchronize()
+    assert torch.allclose(got, ref, rtol=REL, atol=REL)
+
+
+def test_noalloc_rejects_sizes_beyond_the_scratch():
+    import torch
+
+    import nrgljubljana_b200 as nb
+    lib = nb.load_library()
+    limit = nb._lib.NRG_NOALLOC_SCRATCH_DOUBLES
+    ka, cols = 1024, limit // 1024 + 1
+    M = torch.zeros((1, cols), dtype=torch.float64, device="cuda")
+    A = torch.zeros((1, ka), dtype=torch.float64, device="cuda")
+    O = torch.zeros((ka, 1), dtype=torch.float64, device="cuda")
+    B = torch.zeros((cols, 1), dtype=torch.float64, device="cuda")
+    rc = lib.nrg_transform_noalloc(M.data_ptr(), cols, A.data_ptr(), ka, O.data_ptr(), 1, B.data_ptr(), 1, 1, cols, ka,
+                                   1, 1.0, None)
+    assert rc == nb._lib.NRG_ERR_ARG
+    assert "static scratch" in nb._lib.last_error()
