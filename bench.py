@@ -37,14 +37,14 @@ SEED = 20261203
 NMIN, NMAX = 8, 2048
 METRIC = "fp64_eig_gflops"
 UNIT = "GFLOP/s"
-WORKLOAD = ("synthetic batched eigensolve: {nblk} real symmetric FP64 blocks, n log-uniform in [8, 2048] "
+WORKLOAD = ("synthetic batched eigensolve: {nblk} real symmetric FP64 blocks, n log-uniform in [{nmin}, {nmax}] "
             "(PCG64 seed 20261203), H = diag(2^-k/2) + symmetric N(0, 0.1^2) couplings")
 
 
-def block_sizes(nblk: int) -> np.ndarray:
+def block_sizes(nblk: int, nmin: int = NMIN, nmax: int = NMAX) -> np.ndarray:
     rng = np.random.Generator(np.random.PCG64(SEED))
-    u = rng.uniform(math.log(NMIN), math.log(NMAX), nblk)
-    return np.clip(np.rint(np.exp(u)), NMIN, NMAX).astype(np.int64)
+    u = rng.uniform(math.log(nmin), math.log(nmax), nblk)
+    return np.clip(np.rint(np.exp(u)), nmin, nmax).astype(np.int64)
 
 
 def f_eig(n) -> float:
@@ -180,7 +180,7 @@ def reference_arm(args, rank: int) -> None:
     import torch
     if rank != 0:
         return
-    sizes = block_sizes(args.nblk)
+    sizes = block_sizes(args.nblk, args.nmin, args.nmax)
     threads = os.cpu_count() or 1
     idx, stride = cpu_sample(sizes, args.cpu_seconds, threads)
     dev = "cuda" if torch.cuda.is_available() else "cpu"
@@ -196,7 +196,7 @@ def reference_arm(args, rank: int) -> None:
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(nblk=args.nblk), "nblk": args.nblk, "parallelism": "replicas"},
+            "config": {"workload": WORKLOAD.format(nblk=args.nblk, nmin=args.nmin, nmax=args.nmax), "nblk": args.nblk, "parallelism": "replicas"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -209,6 +209,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nblk", type=int, default=10000)
+    ap.add_argument("--nmin", type=int, default=NMIN, help="smallest block order (profiling cases)")
+    ap.add_argument("--nmax", type=int, default=NMAX, help="largest block order (profiling cases)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -231,7 +233,7 @@ def main():
     import nrgljubljana_b200 as nb
     ctx = nb.context(local)
 
-    sizes = block_sizes(args.nblk)
+    sizes = block_sizes(args.nblk, args.nmin, args.nmax)
     offs = np.zeros(args.nblk + 1, dtype=np.int64)
     offs[1:] = np.cumsum(sizes.astype(np.int64) ** 2)
     voffs = np.zeros(args.nblk + 1, dtype=np.int64)
@@ -303,7 +305,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(nblk=nbk), "nblk": nbk, "sum_n3": float(np.sum(sizes.astype(float) ** 3)),
+            "config": {"workload": WORKLOAD.format(nblk=nbk, nmin=args.nmin, nmax=args.nmax), "nblk": nbk, "sum_n3": float(np.sum(sizes.astype(float) ** 3)),
                        "flop_per_step": flop_step, "input_bytes": 8 * total,
                        "l2": "inputs larger than L2 (30 GB vs 126 MB); consumed inputs refreshed by a D2D copy inside each step",
                        "parallelism": f"replicas x{world}"},

@@ -29,13 +29,26 @@ NRG_DEV double block_sum(double v, double* red) {
   __syncthreads();
   if (lane == 0) red[wid] = v;
   __syncthreads();
-  double t = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
-  if (wid == 0) t = warp_sum(t);
-  if (threadIdx.x == 0) red[0] = t;
+  double t = 0.0;
+  for (int w = 0; w < nw; w++) t += red[w];
   __syncthreads();
-  const double r = red[0];
+  return t;
+}
+
+// Block-wide sum with one barrier. `red` holds 64 doubles; `phase` is a per-thread counter
+// that every thread of the block passes through the same sequence of calls, so consecutive
+// calls use alternate halves of `red` and never overwrite values a slower thread may still
+// be reading from the previous call.
+NRG_DEV double block_sum_1b(double v, double* red, int& phase) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  double* buf = red + 32 * (phase & 1);
+  phase++;
+  if (lane == 0) buf[wid] = v;
   __syncthreads();
-  return r;
+  double t = 0.0;
+  for (int w = 0; w < nw; w++) t += buf[w];
+  return t;
 }
 
 NRG_DEV double block_max(double v, double* red) {
@@ -44,13 +57,10 @@ NRG_DEV double block_max(double v, double* red) {
   __syncthreads();
   if (lane == 0) red[wid] = v;
   __syncthreads();
-  double t = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
-  if (wid == 0) t = warp_max(t);
-  if (threadIdx.x == 0) red[0] = t;
+  double t = 0.0;
+  for (int w = 0; w < nw; w++) t = fmax(t, red[w]);
   __syncthreads();
-  const double r = red[0];
-  __syncthreads();
-  return r;
+  return t;
 }
 
 // FP64 tensor-core MMA: D(8x8) += A(8x4) * B(4x8). Fragment layout (per lane l):

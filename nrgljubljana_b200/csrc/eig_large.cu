@@ -29,7 +29,7 @@
 namespace nrg {
 namespace {
 
-constexpr int kTriThreads = 512;
+constexpr int kTriThreads = 256;
 constexpr int NB = 16;     // tridiagonalisation panel width
 constexpr int NBT = 64;    // back-transform panel width
 constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
@@ -105,100 +105,170 @@ NRG_DEV double slab_colsum8(double (&x)[8], int lane) {
 }
 
 // y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n, A symmetric with its lower triangle
-// stored as A(i, j) = H[j*n + i] (i >= j). Warps own 32-row tile rows and walk them in
-// 8-column slabs (one coalesced 256-byte load per column), prefetching the next slab; row
-// sums stay in registers, column sums are transposed across the warp and added to y
-// (shared memory) once per slab column.
+// stored as A(i, j) = H[j*n + i] (i >= j). The lower triangle is cut into 32-row x 8-column
+// slabs (one coalesced 256-byte load per column); the slabs, in tile-row order, are split
+// evenly between the warps, and each warp streams its range with two slabs in flight. Row
+// sums stay in registers until the tile row changes; column sums are transposed across the
+// warp; both are added to y (shared memory).
 NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const double* v, double* y) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
-  const int sl0 = s0 >> 3;  // first slab touching column s0
-  for (int I = Tn - warp; I >= T0; I -= nwarps) {
-    const int i = (I << 5) + lane;
+  const int T0 = s0 >> 5, Tn = (n - 1) >> 5, sl0 = s0 >> 3, slmax = (n - 1) >> 3;
+  auto rowlen = [&](int I) { return min(4 * I + 3, slmax) - sl0 + 1; };
+  long long S = 0;
+  for (int I = T0; I <= Tn; I++) S += rowlen(I);
+  const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
+  if (f0 >= f1) return;
+  int I = T0;
+  long long acc = 0;
+  while (acc + rowlen(I) <= f0) {
+    acc += rowlen(I);
+    I++;
+  }
+  int sl = sl0 + (int)(f0 - acc);
+  auto advance = [&](int& I_, int& sl_) {
+    if (sl_ < min(4 * I_ + 3, slmax)) {
+      sl_++;
+    } else {
+      I_++;
+      sl_ = sl0;
+    }
+  };
+#define NRG_SLAB_LOAD(I_, sl_, dst)                                 \
+  do {                                                              \
+    const int li_ = ((I_) << 5) + lane, lj0_ = (sl_) << 3;          \
+    _Pragma("unroll") for (int c_ = 0; c_ < 8; c_++) {              \
+      const int jj_ = lj0_ + c_;                                    \
+      const bool ok_ = li_ < n && jj_ >= s0 && jj_ <= li_;          \
+      dst[c_] = ok_ ? H[(size_t)jj_ * n + li_] : 0.0;               \
+    }                                                               \
+  } while (0)
+  double cur[8], n1[8], n2[8];
+  int cI = I, csl = sl, aI = I, asl = sl, bI, bsl;
+  NRG_SLAB_LOAD(cI, csl, cur);
+  advance(aI, asl);
+  if (f0 + 1 < f1) NRG_SLAB_LOAD(aI, asl, n1);
+  bI = aI;
+  bsl = asl;
+  advance(bI, bsl);
+  if (f0 + 2 < f1) NRG_SLAB_LOAD(bI, bsl, n2);
+  double racc = 0.0;
+  for (long long f = f0; f < f1; f++) {
+    const int i = (cI << 5) + lane, j0 = csl << 3;
     const bool iv = (i >= s0) && (i < n);
     const double vi = iv ? v[i] : 0.0;
-    const int sl1 = min((I << 2) + 3, (n - 1) >> 3);  // last slab of this tile row
-    double racc = 0.0;
-    double cur[8], nxt[8];
-    auto load = [&](int sl, double (&dst)[8]) {
-      const int j0 = sl << 3;
+    double cp[8];
 #pragma unroll
-      for (int c = 0; c < 8; c++) {
-        const int jj = j0 + c;
-        const bool ok = iv && jj >= s0 && jj <= i;
-        dst[c] = ok ? H[(size_t)jj * n + i] : 0.0;
-      }
-    };
-    load(sl0, cur);
-    for (int sl = sl0; sl <= sl1; sl++) {
-      if (sl < sl1) load(sl + 1, nxt);
-      const int j0 = sl << 3;
-      double cp[8];
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        const int jj = j0 + c;
-        const double vj = (jj < n) ? v[jj] : 0.0;
-        racc = fma(cur[c], vj, racc);
-        cp[c] = (jj < i) ? cur[c] * vi : 0.0;  // the diagonal enters the row sum only
-      }
-      const double cs = slab_colsum8(cp, lane);
-      const int jc = j0 + ((lane >> 2) & 7);
-      if ((lane & 3) == 0 && jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
-#pragma unroll
-      for (int c = 0; c < 8; c++) cur[c] = nxt[c];
+    for (int c = 0; c < 8; c++) {
+      const int jj = j0 + c;
+      const double vj = (jj < n) ? v[jj] : 0.0;
+      racc = fma(cur[c], vj, racc);
+      cp[c] = (jj < i) ? cur[c] * vi : 0.0;  // the diagonal enters the row sum only
     }
-    if (iv) atomicAdd(&y[i], racc);
+    const double cs = slab_colsum8(cp, lane);
+    const int jc = j0 + ((lane >> 2) & 7);
+    if ((lane & 3) == 0 && jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
+    if (f + 1 == f1 || aI != cI) {
+      if (iv && racc != 0.0) atomicAdd(&y[i], racc);
+      racc = 0.0;
+    }
+    // shift the pipeline by one slab
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      cur[c] = n1[c];
+      n1[c] = n2[c];
+    }
+    cI = aI;
+    csl = asl;
+    aI = bI;
+    asl = bsl;
+    advance(bI, bsl);
+    if (f + 3 < f1) NRG_SLAB_LOAD(bI, bsl, n2);
   }
+#undef NRG_SLAB_LOAD
 }
 
 // A(i, j) -= sum_{q < nbp} V(i,q) W(j,q) + W(i,q) V(j,q) for s0 <= j <= i < n, with
-// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i]. A lane keeps its row's V and W in
-// registers; the 32 columns of a tile are staged per warp in shared memory (stage: 2 * 32 *
-// (NB+1) doubles per warp) and read as broadcasts.
-NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0,
-                          double* stage) {
+// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i], on the FP64 tensor cores. In the
+// stored orientation C'(j, i) = H[j*n + i] = A(i, j) the update is C' -= X Y^T with
+// X = [W_J | V_J] and Y = [V_I | W_I] (32 x 2NB each): per 32 x 32 tile a warp runs 4 x 4
+// DMMA 8x8x4 tiles over K = 2NB, operands read straight from the panel rows (L1/L2).
+// The tiles of the trailing lower triangle, in tile-row order, are split evenly between warps.
+NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int r = lane >> 2, c4 = lane & 3;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
-  double* Vs = stage + (size_t)warp * 2 * 32 * (NB + 1);
-  double* Ws = Vs + 32 * (NB + 1);
-  for (int I = Tn - warp; I >= T0; I -= nwarps) {
-    const int i = (I << 5) + lane;
-    const bool iv = (i >= s0) && (i < n);
-    double Vi[NB], Wi[NB];
+  const int nt = Tn - T0 + 1;
+  const long long S = (long long)nt * (nt + 1) / 2;
+  const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
+  if (f0 >= f1) return;
+  int I = T0;
+  long long acc0 = 0;
+  while (acc0 + (I - T0 + 1) <= f0) {
+    acc0 += I - T0 + 1;
+    I++;
+  }
+  int J = T0 + (int)(f0 - acc0);
+  for (long long f = f0; f < f1; f++) {
+    const int j0 = J << 5;
+    // two halves of 16 columns i keep the accumulators within the register budget
+#pragma unroll 1
+    for (int half = 0; half < 2; half++) {
+      const int i0 = (I << 5) + 16 * half;
+      double acc[4][2][2];
 #pragma unroll
-    for (int q = 0; q < NB; q++) {
-      const bool ok = iv && q < nbp;
-      Vi[q] = ok ? H[(size_t)(p0 + q) * n + i] : 0.0;
-      Wi[q] = ok ? W[(size_t)q * n + i] : 0.0;
-    }
-    for (int J = T0; J <= I; J++) {
-      const int jl = (J << 5) + lane;
-      const bool jv = (jl >= s0) && (jl < n);
-      __syncwarp();
+      for (int mi = 0; mi < 4; mi++)
 #pragma unroll
-      for (int q = 0; q < NB; q++) {
-        const bool ok = jv && q < nbp;
-        Vs[lane * (NB + 1) + q] = ok ? H[(size_t)(p0 + q) * n + jl] : 0.0;
-        Ws[lane * (NB + 1) + q] = ok ? W[(size_t)q * n + jl] : 0.0;
-      }
-      __syncwarp();
-      double* col = H + (size_t)(J << 5) * n + i;
-      const int cmax = min(32, n - (J << 5));
-      for (int c = 0; c < cmax; c++) {
-        const int jj = (J << 5) + c;
-        double sacc = 0.0;
+        for (int ni = 0; ni < 2; ni++)
 #pragma unroll
-        for (int q = 0; q < NB; q++) {
-          sacc = fma(Vi[q], Ws[c * (NB + 1) + q], sacc);
-          sacc = fma(Wi[q], Vs[c * (NB + 1) + q], sacc);
+          for (int h = 0; h < 2; h++) {
+            const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
+            const bool ok = jj >= s0 && ii < n && ii >= jj;
+            acc[mi][ni][h] = ok ? H[(size_t)jj * n + ii] : 0.0;
+          }
+#pragma unroll 2
+      for (int kk = 0; kk < 2 * NB; kk += 4) {
+        const int q = kk + c4;      // column of X and Y
+        const bool first = q < NB;  // X: W part / Y: V part
+        const int qq = first ? q : q - NB;
+        const bool qok = qq < nbp;
+        const double* xrow = first ? W + (size_t)qq * n : H + (size_t)(p0 + qq) * n;
+        const double* yrow = first ? H + (size_t)(p0 + qq) * n : W + (size_t)qq * n;
+        double a[4], b[2];
+#pragma unroll
+        for (int mi = 0; mi < 4; mi++) {
+          const int jj = j0 + 8 * mi + r;
+          a[mi] = (qok && jj < n) ? -xrow[jj] : 0.0;
         }
-        if (iv && jj >= s0 && i >= jj) col[(size_t)c * n] -= sacc;
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++) {
+          const int ii = i0 + 8 * ni + r;
+          b[ni] = (qok && ii < n) ? yrow[ii] : 0.0;
+        }
+#pragma unroll
+        for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+          for (int ni = 0; ni < 2; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
       }
+#pragma unroll
+      for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+        for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
+            if (jj >= s0 && ii < n && ii >= jj) H[(size_t)jj * n + ii] = acc[mi][ni][h];
+          }
+    }
+    if (J < I) {
+      J++;
+    } else {
+      I++;
+      J = T0;
     }
   }
 }
 
-__global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBlock* __restrict__ blocks) {
+__global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBlock* __restrict__ blocks) {
   extern __shared__ __align__(16) double sm[];
   const LargeBlock B = blocks[blockIdx.x];
   const int n = B.n, tid = threadIdx.x, nt = blockDim.x;
@@ -209,8 +279,8 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
   double* y = v + n;
   double* part = y + n;                 // nwarps * 2NB
   double* cwv = part + nwarps * 2 * NB;  // 2NB
-  double* red = cwv + 2 * NB;            // 32
-  double* stage = red + 32;              // nwarps * 2 * 32 * (NB+1), panel update
+  double* red = cwv + 2 * NB;            // 64 (two halves for block_sum_1b)
+  int phase = 0;
 
   for (int p0 = 0; p0 < n - 2; p0 += NB) {
     const int pe = min(p0 + NB, n - 2);
@@ -225,12 +295,13 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
           a -= Vq[i] * Wq[k] + Wq[i] * Vq[k];
         }
         v[i] = a;
+        y[i] = 0.0;
       }
       __syncthreads();
       // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
       double ps = 0.0;
       for (int i = k + 2 + tid; i < n; i += nt) ps += v[i] * v[i];
-      const double sigma = block_sum(ps, red);
+      const double sigma = block_sum_1b(ps, red, phase);
       const double alpha = v[k + 1];
       double tau = 0.0, beta = alpha, scale = 1.0;
       if (sigma > 0.0) {
@@ -259,8 +330,6 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        for (int i = k + 1 + tid; i < n; i += nt) y[i] = 0.0;
-        __syncthreads();
         symv_lower(H, n, k + 1, v, y);
         if (j > 0) {
           double pw[NB], pv[NB];
@@ -302,14 +371,14 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_kernel(const LargeBloc
           y[i] = yi;
           pp = fma(yi, v[i], pp);
         }
-        const double Kc = 0.5 * tau * block_sum(pp, red);
+        const double Kc = 0.5 * tau * block_sum_1b(pp, red, phase);
         for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = y[i] - Kc * v[i];
       } else {
         for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = 0.0;
       }
       __syncthreads();
     }
-    panel_update(H, W, n, p0, pe - p0, pe, stage);
+    panel_update(H, W, n, p0, pe - p0, pe);
     __syncthreads();
   }
   if (tid == 0) {
@@ -959,8 +1028,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
 
     // ---- 1. tridiagonalisation
     {
-      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 32 +
-                                            (kTriThreads / 32) * 2 * 32 * (NB + 1));
+      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 64);
       NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       PhaseScope ps(c, kPhTridiag, s);
       tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
