@@ -36,10 +36,11 @@ constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
 constexpr int kMaxLargeN = 4096;
 
 struct LargeBlock {
-  double* H;      // input (consumed): Householder vectors end up in its rows
+  double* H;      // input (consumed); then the eigenvector rows of T during divide and
+                  // conquer; then the VT factors of the back-transform
   double* evals;
   double* evecs;  // output; scratch for the merge matrices during divide and conquer
-  double* W1;     // n x n: eigenvector rows of T under construction; VT factors later
+  double* W1;     // n x ldp: packed lower triangle being reduced; Householder vectors after
   double* W2;     // n x n: panel W of the reduction; grouped rows of a merge; back-transform W
   double* d;
   double* e;
@@ -53,6 +54,7 @@ struct LargeBlock {
   int* perm;      // final eigenvalue order
   int* info;
   int n, npanel;
+  int ldp, pad_;  // leading dimension of the packed lower triangle in W1 (multiple of 32)
 };
 
 struct DcLeaf {
@@ -104,13 +106,60 @@ NRG_DEV double slab_colsum8(double (&x)[8], int lane) {
   return x[0];
 }
 
-// y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n, A symmetric with its lower triangle
-// stored as A(i, j) = H[j*n + i] (i >= j). The lower triangle is cut into 32-row x 8-column
-// slabs (one coalesced 256-byte load per column); the slabs, in tile-row order, are split
-// evenly between the warps, and each warp streams its range with two slabs in flight. Row
-// sums stay in registers until the tile row changes; column sums are transposed across the
-// warp; both are added to y (shared memory).
-NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const double* v, double* y) {
+// ---- bulk asynchronous copies (TMA, non-multicast) into the CTA's own shared memory
+NRG_DEV unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+NRG_DEV void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+NRG_DEV void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+NRG_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Orders this thread's earlier generic-proxy global writes before later bulk (async-proxy)
+// reads of the same memory.
+NRG_DEV void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+NRG_DEV void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Bounded wait for phase `parity` of an mbarrier; false if the bound ran out.
+NRG_DEV bool mbar_wait(uint64_t* bar, unsigned parity, int bound = (1 << 26)) {
+  const unsigned a = smem_u32(bar);
+  for (int it = 0; it < bound; it++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kStages = 4;                      // slabs in flight per warp
+constexpr int kSlabBytes = 8 * 32 * 8;          // 8 columns x 32 rows of FP64
+constexpr int kTriWarps = kTriThreads / 32;
+
+// y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n. A is the packed lower triangle:
+// A(i, j) = P[j*ld + i] for i >= j, zero above the diagonal and in the row padding (ld is a
+// multiple of 32). The triangle is cut into 32-row x 8-column slabs; the slabs, in tile-row
+// order, are split evenly between the warps. Each warp streams its slabs through a ring of
+// kStages shared-memory buffers filled by bulk copies (one 256-byte copy per column,
+// completion on an mbarrier per buffer). Row sums stay in registers until the tile row
+// changes; column sums are transposed across the warp; both are added to y (shared memory).
+// `ring` holds kTriWarps * kStages slabs, `bars` kTriWarps * kStages mbarriers, and
+// `parity` the per-warp phase bits of those mbarriers (kept across calls).
+NRG_DEV void symv_lower(const double* __restrict__ P, int n, int ld, int s0, const double* v, double* y, double* ring,
+                        uint64_t* bars, unsigned& parity, int* err) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5, sl0 = s0 >> 3, slmax = (n - 1) >> 3;
   auto rowlen = [&](int I) { return min(4 * I + 3, slmax) - sl0 + 1; };
@@ -118,13 +167,8 @@ NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const doubl
   for (int I = T0; I <= Tn; I++) S += rowlen(I);
   const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
   if (f0 >= f1) return;
-  int I = T0;
-  long long acc = 0;
-  while (acc + rowlen(I) <= f0) {
-    acc += rowlen(I);
-    I++;
-  }
-  int sl = sl0 + (int)(f0 - acc);
+  double* myring = ring + (size_t)warp * kStages * 256;
+  uint64_t* mybar = bars + warp * kStages;
   auto advance = [&](int& I_, int& sl_) {
     if (sl_ < min(4 * I_ + 3, slmax)) {
       sl_++;
@@ -133,67 +177,100 @@ NRG_DEV void symv_lower(const double* __restrict__ H, int n, int s0, const doubl
       sl_ = sl0;
     }
   };
-#define NRG_SLAB_LOAD(I_, sl_, dst)                                 \
-  do {                                                              \
-    const int li_ = ((I_) << 5) + lane, lj0_ = (sl_) << 3;          \
-    _Pragma("unroll") for (int c_ = 0; c_ < 8; c_++) {              \
-      const int jj_ = lj0_ + c_;                                    \
-      const bool ok_ = li_ < n && jj_ >= s0 && jj_ <= li_;          \
-      dst[c_] = ok_ ? H[(size_t)jj_ * n + li_] : 0.0;               \
-    }                                                               \
-  } while (0)
-  double cur[8], n1[8], n2[8];
-  int cI = I, csl = sl, aI = I, asl = sl, bI, bsl;
-  NRG_SLAB_LOAD(cI, csl, cur);
-  advance(aI, asl);
-  if (f0 + 1 < f1) NRG_SLAB_LOAD(aI, asl, n1);
-  bI = aI;
-  bsl = asl;
-  advance(bI, bsl);
-  if (f0 + 2 < f1) NRG_SLAB_LOAD(bI, bsl, n2);
+  // issue slab (I_, sl_) into stage st (lane 0 only)
+  auto issue = [&](int I_, int sl_, int st) {
+    if (lane == 0) {
+      const int j0 = sl_ << 3, i0 = I_ << 5;
+      const int ncol = min(8, n - j0);
+      mbar_expect_tx(mybar + st, (unsigned)(ncol * 256));
+      for (int c = 0; c < ncol; c++)
+        bulk_g2s(myring + st * 256 + c * 32, P + (size_t)(j0 + c) * ld + i0, 256u, mybar + st);
+    }
+  };
+  int I = T0;
+  long long acc = 0;
+  while (acc + rowlen(I) <= f0) {
+    acc += rowlen(I);
+    I++;
+  }
+  int sl = sl0 + (int)(f0 - acc);
+  // prologue: fill the ring
+  int pI = I, psl = sl;
+  const int npre = (int)((f1 - f0) < (long long)kStages ? (f1 - f0) : (long long)kStages);
+  for (int t = 0; t < npre; t++) {
+    issue(pI, psl, t);
+    advance(pI, psl);
+  }
   double racc = 0.0;
+  int cI = I, csl = sl;
   for (long long f = f0; f < f1; f++) {
+    const int st = (int)((f - f0) % kStages);
+    if (!mbar_wait(mybar + st, (parity >> st) & 1u)) {
+      // a copy never completed: flag the block, wait (bounded) for the copies still in
+      // flight so that none lands after this call, and stop streaming
+      if (lane == 0) atomicExch(err, -5);
+      const long long last = (f + kStages < f1) ? f + kStages : f1;
+      for (long long g = f + 1; g < last; g++) {
+        const int sg = (int)((g - f0) % kStages);
+        mbar_wait(mybar + sg, (parity >> sg) & 1u, 1 << 22);
+        parity ^= 1u << sg;
+      }
+      parity ^= 1u << st;
+      return;
+    }
+    parity ^= 1u << st;
+    const double* buf = myring + st * 256;
     const int i = (cI << 5) + lane, j0 = csl << 3;
     const bool iv = (i >= s0) && (i < n);
     const double vi = iv ? v[i] : 0.0;
     double cp[8];
+    const bool interior = j0 >= s0 && j0 + 8 <= (cI << 5) && j0 + 8 <= n;
+    if (interior) {  // strictly below the diagonal tile, fully inside the trailing block
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int jj = j0 + c;
-      const double vj = (jj < n) ? v[jj] : 0.0;
-      racc = fma(cur[c], vj, racc);
-      cp[c] = (jj < i) ? cur[c] * vi : 0.0;  // the diagonal enters the row sum only
+      for (int c = 0; c < 8; c++) {
+        const double a = buf[c * 32 + lane];
+        racc = fma(a, v[j0 + c], racc);
+        cp[c] = a * vi;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int jj = j0 + c;
+        const bool ok = iv && jj >= s0 && jj < n && jj <= i;
+        const double a = ok ? buf[c * 32 + lane] : 0.0;
+        const double vj = (jj < n) ? v[jj] : 0.0;
+        racc = fma(a, vj, racc);
+        cp[c] = (jj < i) ? a * vi : 0.0;  // the diagonal enters the row sum only
+      }
+    }
+    __syncwarp();
+    if (f + kStages < f1) {  // refill this stage with the slab kStages ahead
+      issue(pI, psl, st);
+      advance(pI, psl);
     }
     const double cs = slab_colsum8(cp, lane);
     const int jc = j0 + ((lane >> 2) & 7);
     if ((lane & 3) == 0 && jc >= s0 && jc < n && cs != 0.0) atomicAdd(&y[jc], cs);
-    if (f + 1 == f1 || aI != cI) {
+    int nI = cI, nsl = csl;
+    advance(nI, nsl);
+    if (f + 1 == f1 || nI != cI) {
       if (iv && racc != 0.0) atomicAdd(&y[i], racc);
       racc = 0.0;
     }
-    // shift the pipeline by one slab
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      cur[c] = n1[c];
-      n1[c] = n2[c];
-    }
-    cI = aI;
-    csl = asl;
-    aI = bI;
-    asl = bsl;
-    advance(bI, bsl);
-    if (f + 3 < f1) NRG_SLAB_LOAD(bI, bsl, n2);
+    cI = nI;
+    csl = nsl;
   }
-#undef NRG_SLAB_LOAD
 }
 
 // A(i, j) -= sum_{q < nbp} V(i,q) W(j,q) + W(i,q) V(j,q) for s0 <= j <= i < n, with
-// V(i, q) = H[(p0+q)*n + i] and W(i, q) = W[q*n + i], on the FP64 tensor cores. In the
-// stored orientation C'(j, i) = H[j*n + i] = A(i, j) the update is C' -= X Y^T with
-// X = [W_J | V_J] and Y = [V_I | W_I] (32 x 2NB each): per 32 x 32 tile a warp runs 4 x 4
-// DMMA 8x8x4 tiles over K = 2NB, operands read straight from the panel rows (L1/L2).
-// The tiles of the trailing lower triangle, in tile-row order, are split evenly between warps.
-NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, int n, int p0, int nbp, int s0) {
+// V(i, q) = P[(p0+q)*ld + i] and W(i, q) = W[q*n + i], on the FP64 tensor cores. In the
+// stored orientation C'(j, i) = P[j*ld + i] = A(i, j) the update is C' -= X Y^T with
+// X = [W_J | V_J] and Y = [V_I | W_I] (32 x 2NB each): per 32 x 32 tile a warp runs DMMA
+// 8x8x4 tiles over K = 2NB in two 16-column halves, operands read straight from the panel
+// rows (L1/L2). The tiles of the trailing lower triangle, in tile-row order, are split
+// evenly between the warps.
+NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, int n, int ld, int p0, int nbp,
+                          int s0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int r = lane >> 2, c4 = lane & 3;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
@@ -210,7 +287,6 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
   int J = T0 + (int)(f0 - acc0);
   for (long long f = f0; f < f1; f++) {
     const int j0 = J << 5;
-    // two halves of 16 columns i keep the accumulators within the register budget
 #pragma unroll 1
     for (int half = 0; half < 2; half++) {
       const int i0 = (I << 5) + 16 * half;
@@ -223,7 +299,7 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
           for (int h = 0; h < 2; h++) {
             const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
             const bool ok = jj >= s0 && ii < n && ii >= jj;
-            acc[mi][ni][h] = ok ? H[(size_t)jj * n + ii] : 0.0;
+            acc[mi][ni][h] = ok ? P[(size_t)jj * ld + ii] : 0.0;
           }
 #pragma unroll 2
       for (int kk = 0; kk < 2 * NB; kk += 4) {
@@ -231,8 +307,8 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
         const bool first = q < NB;  // X: W part / Y: V part
         const int qq = first ? q : q - NB;
         const bool qok = qq < nbp;
-        const double* xrow = first ? W + (size_t)qq * n : H + (size_t)(p0 + qq) * n;
-        const double* yrow = first ? H + (size_t)(p0 + qq) * n : W + (size_t)qq * n;
+        const double* xrow = first ? W + (size_t)qq * n : P + (size_t)(p0 + qq) * ld;
+        const double* yrow = first ? P + (size_t)(p0 + qq) * ld : W + (size_t)qq * n;
         double a[4], b[2];
 #pragma unroll
         for (int mi = 0; mi < 4; mi++) {
@@ -256,7 +332,7 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
-            if (jj >= s0 && ii < n && ii >= jj) H[(size_t)jj * n + ii] = acc[mi][ni][h];
+            if (jj >= s0 && ii < n && ii >= jj) P[(size_t)jj * ld + ii] = acc[mi][ni][h];
           }
     }
     if (J < I) {
@@ -268,34 +344,65 @@ NRG_DEV void panel_update(double* __restrict__ H, const double* __restrict__ W, 
   }
 }
 
+// Packs the upper triangle of the row-major input (the lower triangle in column terms)
+// into W1 with leading dimension ldp: W1[j*ldp + i] = H[j*n + i] for i >= j, zero for i < j
+// and in the padding rows n <= i < ldp. Grid (row chunks of 8, blocks).
+__global__ void __launch_bounds__(256) pack_lower_kernel(const LargeBlock* __restrict__ blocks) {
+  const LargeBlock B = blocks[blockIdx.y];
+  const int n = B.n, ld = B.ldp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = blockIdx.x * 8 + warp;
+  if (j >= n) return;
+  const double* src = B.H + (size_t)j * n;
+  double* dst = B.W1 + (size_t)j * ld;
+  for (int i = lane; i < ld; i += 32) dst[i] = (i >= j && i < n) ? src[i] : 0.0;
+}
+
+// One CTA per block: blocked (NB) Householder reduction of the packed lower triangle in W1
+// (leading dimension ldp) to tridiagonal form; d, e, tau out; Householder vector k is left
+// in column k (W1[k*ldp + k+1 ..], with a unit at k+1).
 __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBlock* __restrict__ blocks) {
-  extern __shared__ __align__(16) double sm[];
+  extern __shared__ __align__(128) double sm[];
+  __shared__ __align__(8) uint64_t bars[kTriWarps * kStages];
   const LargeBlock B = blocks[blockIdx.x];
-  const int n = B.n, tid = threadIdx.x, nt = blockDim.x;
+  const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-  double* H = B.H;
+  double* A = B.W1;
   double* W = B.W2;
-  double* v = sm;
-  double* y = v + n;
-  double* part = y + n;                 // nwarps * 2NB
-  double* cwv = part + nwarps * 2 * NB;  // 2NB
-  double* red = cwv + 2 * NB;            // 64 (two halves for block_sum_1b)
+  double* ring = sm;                                   // kTriWarps * kStages * 256
+  double* v = ring + kTriWarps * kStages * 256;        // n
+  double* y = v + n;                                   // n
+  double* part = y + n;                                // nwarps * 2NB
+  double* cwv = part + nwarps * 2 * NB;                // 2NB
+  double* red = cwv + 2 * NB;                          // 64 (two halves for block_sum_1b)
   int phase = 0;
+  unsigned parity = 0;
+  if (lane == 0) {
+    for (int st = 0; st < kStages; st++) mbar_init(bars + warp * kStages + st, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
   for (int p0 = 0; p0 < n - 2; p0 += NB) {
     const int pe = min(p0 + NB, n - 2);
     for (int k = p0; k < pe; k++) {
       const int j = k - p0;
       // (1) current column k (rows k..n-1) = stored column minus the pending panel terms
-      for (int i = k + tid; i < n; i += nt) {
-        double a = H[(size_t)k * n + i];
-        for (int q = 0; q < j; q++) {
-          const double* Vq = H + (size_t)(p0 + q) * n;
-          const double* Wq = W + (size_t)q * n;
-          a -= Vq[i] * Wq[k] + Wq[i] * Vq[k];
+      {
+        double wk[NB], vk[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          wk[q] = (q < j) ? W[(size_t)q * n + k] : 0.0;
+          vk[q] = (q < j) ? A[(size_t)(p0 + q) * ld + k] : 0.0;
         }
-        v[i] = a;
-        y[i] = 0.0;
+        for (int i = k + tid; i < n; i += nt) {
+          double a = A[(size_t)k * ld + i];
+#pragma unroll
+          for (int q = 0; q < NB; q++)
+            if (q < j) a -= A[(size_t)(p0 + q) * ld + i] * wk[q] + W[(size_t)q * n + i] * vk[q];
+          v[i] = a;
+          y[i] = 0.0;
+        }
       }
       __syncthreads();
       // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
@@ -317,20 +424,20 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       for (int i = k + 2 + tid; i < n; i += nt) {
         const double vi = v[i] * scale;
         v[i] = vi;
-        H[(size_t)k * n + i] = vi;
+        A[(size_t)k * ld + i] = vi;
       }
-      // row k of H now holds v_k from column k+1 on; clear its prefix inside the
-      // back-transform panel so that the panel's V block is exactly unit lower trapezoidal
+      // column k of W1 now holds v_k below the diagonal; clear its entries above, inside
+      // the back-transform panel, so that the panel's V block is exactly unit lower trapezoidal
       const int kb0 = (k / NBT) * NBT;
-      for (int i = kb0 + 1 + tid; i <= k; i += nt) H[(size_t)k * n + i] = 0.0;
+      for (int i = kb0 + 1 + tid; i <= k; i += nt) A[(size_t)k * ld + i] = 0.0;
       if (tid == 0) {
         v[k + 1] = 1.0;
-        H[(size_t)k * n + k + 1] = 1.0;
+        A[(size_t)k * ld + k + 1] = 1.0;
       }
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        symv_lower(H, n, k + 1, v, y);
+        symv_lower(A, n, ld, k + 1, v, y, ring, bars, parity, B.info);
         if (j > 0) {
           double pw[NB], pv[NB];
 #pragma unroll
@@ -341,7 +448,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
             for (int q = 0; q < NB; q++)
               if (q < j) {
                 pw[q] = fma(W[(size_t)q * n + i], vi, pw[q]);
-                pv[q] = fma(H[(size_t)(p0 + q) * n + i], vi, pv[q]);
+                pv[q] = fma(A[(size_t)(p0 + q) * ld + i], vi, pv[q]);
               }
           }
 #pragma unroll
@@ -363,10 +470,18 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
           }
         }
         __syncthreads();
+        double cw[NB], cv[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          cw[q] = (q < j) ? cwv[q] : 0.0;
+          cv[q] = (q < j) ? cwv[NB + q] : 0.0;
+        }
         double pp = 0.0;
         for (int i = k + 1 + tid; i < n; i += nt) {
           double yi = y[i];
-          for (int q = 0; q < j; q++) yi -= H[(size_t)(p0 + q) * n + i] * cwv[q] + W[(size_t)q * n + i] * cwv[NB + q];
+#pragma unroll
+          for (int q = 0; q < NB; q++)
+            if (q < j) yi -= A[(size_t)(p0 + q) * ld + i] * cw[q] + W[(size_t)q * n + i] * cv[q];
           yi *= tau;
           y[i] = yi;
           pp = fma(yi, v[i], pp);
@@ -378,13 +493,14 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       }
       __syncthreads();
     }
-    panel_update(H, W, n, p0, pe - p0, pe);
+    panel_update(A, W, n, ld, p0, pe - p0, pe);
+    fence_proxy_async_global();  // the next symv reads the updated trailing block by bulk copies
     __syncthreads();
   }
   if (tid == 0) {
-    B.d[n - 2] = H[(size_t)(n - 2) * n + n - 2];
-    B.e[n - 2] = H[(size_t)(n - 2) * n + n - 1];
-    B.d[n - 1] = H[(size_t)(n - 1) * n + n - 1];
+    B.d[n - 2] = A[(size_t)(n - 2) * ld + n - 2];
+    B.e[n - 2] = A[(size_t)(n - 2) * ld + n - 1];
+    B.d[n - 1] = A[(size_t)(n - 1) * ld + n - 1];
     B.e[n - 1] = 0.0;
     B.tau[n - 2] = 0.0;
     B.tau[n - 1] = 0.0;
@@ -392,7 +508,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
   __syncthreads();
   int bad = 0;
   for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
-  if (__syncthreads_or(bad) && tid == 0) *B.info = -2;
+  if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
 }
 
 // ---------------------------------------------------------------- divide and conquer: leaves
@@ -421,7 +537,7 @@ __global__ void __launch_bounds__(128) dc_leaf_kernel(const LargeBlock* __restri
   for (int r = tid; r < nl; r += blockDim.x) B.lam[a0 + r] = d[r];
   for (int idx = tid; idx < nl * nl; idx += blockDim.x) {
     const int r = idx / nl, c = idx % nl;  // row r of Zt = column r of Z
-    B.W1[(size_t)(a0 + r) * n + a0 + c] = Z[c * ld + r];
+    B.H[(size_t)(a0 + r) * n + a0 + c] = Z[c * ld + r];
   }
 }
 
@@ -470,7 +586,7 @@ __global__ void __launch_bounds__(512) dc_prep_kernel(const LargeBlock* __restri
   double2* rcs = reinterpret_cast<double2*>(smc + PL.rcs);
   int2* rpos = reinterpret_cast<int2*>(smc + PL.rpos);
   unsigned char* fl = reinterpret_cast<unsigned char*>(smc + PL.fl);
-  double* Z = B.W1;
+  double* Z = B.H;
   double* G = B.W2;
 
   // 1. clear the off-diagonal child blocks of the node
@@ -762,7 +878,7 @@ __global__ void __launch_bounds__(512) dc_vectors_kernel(const LargeBlock* __res
   {  // deflated rows are final: grouped copy (W2) back to the node's rows a+K.. (W1)
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     for (int r = a + K + warp; r < nd.b; r += nwarps)
-      for (int col = a + lane; col < nd.b; col += 32) B.W1[(size_t)r * n + col] = B.W2[(size_t)r * n + col];
+      for (int col = a + lane; col < nd.b; col += 32) B.H[(size_t)r * n + col] = B.W2[(size_t)r * n + col];
   }
   if (K == 0) return;
   const double* ds = B.dsort + a;
@@ -840,7 +956,7 @@ __global__ void __launch_bounds__(256) permute_rows_kernel(const LargeBlock* __r
   if (r >= n) return;
   int pr = B.perm[r];
   if (pr < 0 || pr >= n) pr = r;  // only after a flagged non-finite block
-  const double* src = B.W1 + (size_t)pr * n;
+  const double* src = B.H + (size_t)pr * n;
   double* dst = B.evecs + (size_t)r * n;
   for (int c = lane; c < n; c += 32) dst[c] = src[c];
 }
@@ -881,7 +997,8 @@ __global__ void __launch_bounds__(NBT) tfactor_kernel(const LargeBlock* __restri
 
 size_t large_block_doubles(int n) {
   const int npanel = (n - 2 + NBT - 1) / NBT;
-  return 2 * (size_t)n * n + 8 * (size_t)n + (size_t)npanel * 2 * NBT * NBT + 2 * (size_t)n;  // last: ints
+  const size_t ldp = (size_t)(n + 31) / 32 * 32;
+  return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + (size_t)npanel * 2 * NBT * NBT + 2 * (size_t)n + 64 * 12;
 }
 
 }  // namespace
@@ -922,7 +1039,8 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       L.H = H[b];
       L.evals = evals[b];
       L.evecs = evecs[b];
-      L.W1 = take((size_t)nb_ * nb_);
+      L.ldp = (nb_ + 31) / 32 * 32;
+      L.W1 = take((size_t)nb_ * L.ldp);
       L.W2 = take((size_t)nb_ * nb_);
       L.d = take(nb_);
       L.e = take(nb_);
@@ -976,10 +1094,10 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         const int N = nd.b - nd.a, nn = L.n;
         nd.gout = (int)gp.outs.size();
         // child-1 columns: C = Zt[a:a+K, a:m] = U[:, 0:k1+k2] * G[a:a+k1+k2, a:m]
-        gp.add_out(L.W1 + (size_t)nd.a * nn + nd.a, nn, N, nd.m - nd.a, 0.0);
+        gp.add_out(L.H + (size_t)nd.a * nn + nd.a, nn, N, nd.m - nd.a, 0.0);
         gp.add_seg(L.evecs + (size_t)nd.a * nn + nd.a, nn, 0, L.W2 + (size_t)nd.a * nn + nd.a, nn, 0, N, 1.0);
         // child-2 columns: C = Zt[a:a+K, m:b] = U[:, k1:K] * G[a+k1:a+K, m:b] (pointers set on device)
-        gp.add_out(L.W1 + (size_t)nd.a * nn + nd.m, nn, N, nd.b - nd.m, 0.0);
+        gp.add_out(L.H + (size_t)nd.a * nn + nd.m, nn, N, nd.b - nd.m, 0.0);
         gp.add_seg(L.evecs + (size_t)nd.a * nn + nd.a, nn, 0, L.W2 + (size_t)nd.a * nn + nd.m, nn, 0, N, 1.0);
       }
       node_off[h] = push(img, levels[h]);
@@ -998,21 +1116,21 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         const int k0 = p * NBT, pnb = std::min(NBT, (nn - 2) - k0), K = nn - k0 - 1;
         panels.push_back(PanelRef{bi, k0, pnb, 0});
         double* Gp = L.GT + (size_t)p * 2 * NBT * NBT;
-        const double* Vrows = L.H + (size_t)k0 * nn + k0 + 1;  // pnb x K, row q = v_{k0+q}
+        const double* Vrows = L.W1 + (size_t)k0 * L.ldp + k0 + 1;  // pnb x K, row q = v_{k0+q}
         gram.add_out(Gp, NBT, pnb, pnb, 0.0);
-        gram.add_seg(Vrows, nn, 0, Vrows, nn, 1, K, 1.0);
-        double* VTp = L.W1 + vt_off;  // K x pnb
+        gram.add_seg(Vrows, L.ldp, 0, Vrows, L.ldp, 1, K, 1.0);
+        double* VTp = L.H + vt_off;  // K x pnb (H is free after the final row permutation)
         vt_off += (size_t)K * NBT;
-        if (vt_off > (size_t)nn * nn) return fail(NRG_ERR_ARG, "internal: VT factors exceed W1 for n=%d", nn);
+        if (vt_off > (size_t)nn * nn) return fail(NRG_ERR_ARG, "internal: VT factors exceed H for n=%d", nn);
         vt.add_out(VTp, NBT, K, pnb, 0.0);
-        vt.add_seg(Vrows, nn, 1, Gp + NBT * NBT, NBT, 0, pnb, 1.0);
+        vt.add_seg(Vrows, L.ldp, 1, Gp + NBT * NBT, NBT, 0, pnb, 1.0);
         // step index counts from the last panel of each block
         const int stp = L.npanel - 1 - p;
         GemmPlan& g1 = bsteps[2 * stp];
         GemmPlan& g2 = bsteps[2 * stp + 1];
         double* Wb = L.W2;  // n x NBT
         g1.add_out(Wb, NBT, nn, pnb, 0.0);
-        g1.add_seg(L.evecs + k0 + 1, nn, 0, Vrows, nn, 1, K, 1.0);
+        g1.add_seg(L.evecs + k0 + 1, nn, 0, Vrows, L.ldp, 1, K, 1.0);
         g2.add_out(L.evecs + k0 + 1, nn, nn, K, 1.0);
         g2.add_seg(Wb, NBT, 0, VTp, NBT, 1, pnb, -1.0);
       }
@@ -1028,9 +1146,12 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
 
     // ---- 1. tridiagonalisation
     {
-      const size_t smem = sizeof(double) * (2 * (size_t)maxn + (kTriThreads / 32) * 2 * NB + 2 * NB + 64);
+      const size_t smem = sizeof(double) * ((size_t)kTriWarps * kStages * 256 + 2 * (size_t)maxn +
+                                            (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
       NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      PhaseScope ps(c, kPhTridiag, s);
+      PhaseScope ps(c, kPhTridiag, s, 2);
+      pack_lower_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
+      NRG_CK(cudaGetLastError());
       tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
       NRG_CK(cudaGetLastError());
     }
