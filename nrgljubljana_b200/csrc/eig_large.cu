@@ -17,6 +17,9 @@
 //   3. sort of the eigenvalues and row permutation of the eigenvectors.
 //   4. back-transform with the compact-WY form of Q, panels of NBT reflectors, as GEMMs.
 // Eigenvectors are kept as ROWS throughout (Zt = Z^T), the layout of the output.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <functional>
@@ -29,7 +32,7 @@
 namespace nrg {
 namespace {
 
-constexpr int kTriThreads = 256;
+constexpr int kTriThreads = 128;
 constexpr int NB = 16;     // tridiagonalisation panel width
 constexpr int NBT = 64;    // back-transform panel width
 constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
@@ -117,13 +120,6 @@ NRG_DEV void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-NRG_DEV void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
 // Orders this thread's earlier generic-proxy global writes before later bulk (async-proxy)
 // reads of the same memory.
 NRG_DEV void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
@@ -145,46 +141,53 @@ NRG_DEV bool mbar_wait(uint64_t* bar, unsigned parity, int bound = (1 << 26)) {
   return false;
 }
 
-constexpr int kStages = 4;                      // slabs in flight per warp
-constexpr int kSlabBytes = 8 * 32 * 8;          // 8 columns x 32 rows of FP64
+// 2-D bulk tensor copy (TMA, non-multicast) of one box at coordinates (x, y) into this
+// CTA's shared memory, completing on an mbarrier.
+NRG_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+constexpr int kStages = 4;                 // slabs in flight per warp
+constexpr int kSlabRows = 64;              // rows of a slab (two per lane)
+constexpr int kSlabD = kSlabRows * 8;      // doubles per slab: 64 rows x 8 columns
 constexpr int kTriWarps = kTriThreads / 32;
 
-// y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n. A is the packed lower triangle:
-// A(i, j) = P[j*ld + i] for i >= j, zero above the diagonal and in the row padding (ld is a
-// multiple of 32). The triangle is cut into 32-row x 8-column slabs; the slabs, in tile-row
-// order, are split evenly between the warps. Each warp streams its slabs through a ring of
-// kStages shared-memory buffers filled by bulk copies (one 256-byte copy per column,
-// completion on an mbarrier per buffer). Row sums stay in registers until the tile row
-// changes; column sums are transposed across the warp; both are added to y (shared memory).
-// `ring` holds kTriWarps * kStages slabs, `bars` kTriWarps * kStages mbarriers, and
-// `parity` the per-warp phase bits of those mbarriers (kept across calls).
-NRG_DEV void symv_lower(const double* __restrict__ P, int n, int ld, int s0, const double* v, double* y, double* ring,
+// y[i] += sum_{j >= s0} A(i, j) v[j] for s0 <= i < n. A is the packed lower triangle
+// (A(i, j) = P[j*ld + i] for i >= j, zero above the diagonal and in the padding) behind the
+// 2-D tensor map `tmap` (inner extent ld rows, outer extent n columns, box 64 x 8). The
+// triangle is cut into 64-row x 8-column slabs; the slabs, in tile-row order, are split
+// evenly between the warps, and each warp streams its slabs through a ring of kStages
+// shared-memory buffers, one TMA box copy per slab completing on the buffer's mbarrier.
+// A lane owns rows l and l+32 of the slab: row sums stay in registers until the tile row
+// changes, column sums are transposed across the warp; both are added to y (shared memory).
+// `parity` holds the warp's mbarrier phase bits across calls.
+NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v, double* y, double* ring,
                         uint64_t* bars, unsigned& parity, int* err) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int T0 = s0 >> 5, Tn = (n - 1) >> 5, sl0 = s0 >> 3, slmax = (n - 1) >> 3;
-  auto rowlen = [&](int I) { return min(4 * I + 3, slmax) - sl0 + 1; };
+  const int T0 = s0 >> 6, Tn = (n - 1) >> 6, sl0 = s0 >> 3, slmax = (n - 1) >> 3;
+  auto rowlen = [&](int I) { return min(8 * I + 7, slmax) - sl0 + 1; };
   long long S = 0;
   for (int I = T0; I <= Tn; I++) S += rowlen(I);
   const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
   if (f0 >= f1) return;
-  double* myring = ring + (size_t)warp * kStages * 256;
+  double* myring = ring + (size_t)warp * kStages * kSlabD;
   uint64_t* mybar = bars + warp * kStages;
   auto advance = [&](int& I_, int& sl_) {
-    if (sl_ < min(4 * I_ + 3, slmax)) {
+    if (sl_ < min(8 * I_ + 7, slmax)) {
       sl_++;
     } else {
       I_++;
       sl_ = sl0;
     }
   };
-  // issue slab (I_, sl_) into stage st (lane 0 only)
   auto issue = [&](int I_, int sl_, int st) {
     if (lane == 0) {
-      const int j0 = sl_ << 3, i0 = I_ << 5;
-      const int ncol = min(8, n - j0);
-      mbar_expect_tx(mybar + st, (unsigned)(ncol * 256));
-      for (int c = 0; c < ncol; c++)
-        bulk_g2s(myring + st * 256 + c * 32, P + (size_t)(j0 + c) * ld + i0, 256u, mybar + st);
+      mbar_expect_tx(mybar + st, (unsigned)(kSlabD * sizeof(double)));
+      tma_load_2d(myring + st * kSlabD, tmap, I_ * kSlabRows, sl_ * 8, mybar + st);
     }
   };
   int I = T0;
@@ -194,14 +197,13 @@ NRG_DEV void symv_lower(const double* __restrict__ P, int n, int ld, int s0, con
     I++;
   }
   int sl = sl0 + (int)(f0 - acc);
-  // prologue: fill the ring
   int pI = I, psl = sl;
   const int npre = (int)((f1 - f0) < (long long)kStages ? (f1 - f0) : (long long)kStages);
   for (int t = 0; t < npre; t++) {
     issue(pI, psl, t);
     advance(pI, psl);
   }
-  double racc = 0.0;
+  double r0 = 0.0, r1 = 0.0;
   int cI = I, csl = sl;
   for (long long f = f0; f < f1; f++) {
     const int st = (int)((f - f0) % kStages);
@@ -219,28 +221,32 @@ NRG_DEV void symv_lower(const double* __restrict__ P, int n, int ld, int s0, con
       return;
     }
     parity ^= 1u << st;
-    const double* buf = myring + st * 256;
-    const int i = (cI << 5) + lane, j0 = csl << 3;
-    const bool iv = (i >= s0) && (i < n);
-    const double vi = iv ? v[i] : 0.0;
+    const double* buf = myring + st * kSlabD;
+    const int ia = cI * kSlabRows + lane, ib = ia + 32, j0 = csl << 3;
+    const double va = (ia >= s0 && ia < n) ? v[ia] : 0.0;
+    const double vb = (ib >= s0 && ib < n) ? v[ib] : 0.0;
     double cp[8];
-    const bool interior = j0 >= s0 && j0 + 8 <= (cI << 5) && j0 + 8 <= n;
-    if (interior) {  // strictly below the diagonal tile, fully inside the trailing block
+    if (j0 >= s0 && j0 + 8 <= cI * kSlabRows && j0 + 8 <= n) {
+      // strictly left of the tile row's diagonal and inside the trailing block: no masks
 #pragma unroll
       for (int c = 0; c < 8; c++) {
-        const double a = buf[c * 32 + lane];
-        racc = fma(a, v[j0 + c], racc);
-        cp[c] = a * vi;
+        const double a0 = buf[c * kSlabRows + lane], a1 = buf[c * kSlabRows + 32 + lane];
+        const double vj = v[j0 + c];
+        r0 = fma(a0, vj, r0);
+        r1 = fma(a1, vj, r1);
+        cp[c] = fma(a0, va, a1 * vb);
       }
     } else {
 #pragma unroll
       for (int c = 0; c < 8; c++) {
         const int jj = j0 + c;
-        const bool ok = iv && jj >= s0 && jj < n && jj <= i;
-        const double a = ok ? buf[c * 32 + lane] : 0.0;
-        const double vj = (jj < n) ? v[jj] : 0.0;
-        racc = fma(a, vj, racc);
-        cp[c] = (jj < i) ? a * vi : 0.0;  // the diagonal enters the row sum only
+        const bool cok = jj >= s0 && jj < n;  // reduced columns hold Householder vectors
+        const double a0 = cok ? buf[c * kSlabRows + lane] : 0.0;
+        const double a1 = cok ? buf[c * kSlabRows + 32 + lane] : 0.0;
+        const double vj = cok ? v[jj] : 0.0;
+        r0 = fma(a0, vj, r0);
+        r1 = fma(a1, vj, r1);
+        cp[c] = (jj < ia ? a0 * va : 0.0) + (jj < ib ? a1 * vb : 0.0);  // diagonal: row sum only
       }
     }
     __syncwarp();
@@ -254,8 +260,9 @@ NRG_DEV void symv_lower(const double* __restrict__ P, int n, int ld, int s0, con
     int nI = cI, nsl = csl;
     advance(nI, nsl);
     if (f + 1 == f1 || nI != cI) {
-      if (iv && racc != 0.0) atomicAdd(&y[i], racc);
-      racc = 0.0;
+      if (ia >= s0 && ia < n && r0 != 0.0) atomicAdd(&y[ia], r0);
+      if (ib >= s0 && ib < n && r1 != 0.0) atomicAdd(&y[ib], r1);
+      r0 = r1 = 0.0;
     }
     cI = nI;
     csl = nsl;
@@ -361,16 +368,18 @@ __global__ void __launch_bounds__(256) pack_lower_kernel(const LargeBlock* __res
 // One CTA per block: blocked (NB) Householder reduction of the packed lower triangle in W1
 // (leading dimension ldp) to tridiagonal form; d, e, tau out; Householder vector k is left
 // in column k (W1[k*ldp + k+1 ..], with a unit at k+1).
-__global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBlock* __restrict__ blocks) {
-  extern __shared__ __align__(128) double sm[];
+__global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBlock* __restrict__ blocks,
+                                                                  const CUtensorMap* __restrict__ tmaps) {
+  extern __shared__ __align__(16) double sm[];
   __shared__ __align__(8) uint64_t bars[kTriWarps * kStages];
   const LargeBlock B = blocks[blockIdx.x];
   const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
   double* A = B.W1;
   double* W = B.W2;
-  double* ring = sm;                                   // kTriWarps * kStages * 256
-  double* v = ring + kTriWarps * kStages * 256;        // n
+  // TMA destinations: 1024-byte aligned ring of kStages slabs per warp
+  double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sm) + 1023) & ~(uintptr_t)1023);
+  double* v = ring + kTriWarps * kStages * kSlabD;     // n
   double* y = v + n;                                   // n
   double* part = y + n;                                // nwarps * 2NB
   double* cwv = part + nwarps * 2 * NB;                // 2NB
@@ -437,7 +446,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        symv_lower(A, n, ld, k + 1, v, y, ring, bars, parity, B.info);
+        symv_lower(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info);
         if (j > 0) {
           double pw[NB], pv[NB];
 #pragma unroll
@@ -995,6 +1004,20 @@ __global__ void __launch_bounds__(NBT) tfactor_kernel(const LargeBlock* __restri
   for (int r = 0; r < NBT; r++) T[r * NBT + t] = Ts[r][t];
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
 size_t large_block_doubles(int n) {
   const int npanel = (n - 2 + NBT - 1) / NBT;
   const size_t ldp = (size_t)(n + 31) / 32 * 32;
@@ -1061,6 +1084,23 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       maxpanel = std::max(maxpanel, L.npanel);
     }
     const int nb = (int)blk.size();
+    // ---- 2-D tensor maps over each block's packed lower triangle (box 64 rows x 8 columns)
+    std::vector<CUtensorMap> tmaps(nb);
+    {
+      auto encode = tensor_map_encoder();
+      if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+      for (int bi = 0; bi < nb; bi++) {
+        const LargeBlock& L = blk[bi];
+        const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
+        const cuuint64_t strides[1] = {(cuuint64_t)L.ldp * sizeof(double)};
+        const cuuint32_t box[2] = {(cuuint32_t)kSlabRows, 8u};
+        const cuuint32_t estr[2] = {1u, 1u};
+        const CUresult r = encode(&tmaps[bi], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, L.W1, dims, strides, box, estr,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for n=%d", (int)r, L.n);
+      }
+    }
     // ---- divide-and-conquer tree (leaves and merge levels by height)
     std::vector<DcLeaf> leaves;
     std::vector<std::vector<DcNode>> levels;
@@ -1084,6 +1124,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     // ---- one staging image for the whole chunk
     std::vector<char> img;
     const size_t blk_off = push(img, blk);
+    const size_t tmap_off = push(img, tmaps);
     const size_t leaf_off = push(img, leaves);
     std::vector<size_t> node_off(levels.size()), st_off(levels.size());
     std::vector<StagedGemm> lvl_gemm(levels.size());
@@ -1146,13 +1187,13 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
 
     // ---- 1. tridiagonalisation
     {
-      const size_t smem = sizeof(double) * ((size_t)kTriWarps * kStages * 256 + 2 * (size_t)maxn +
-                                            (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
+      const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
+                                                   (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
       NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       PhaseScope ps(c, kPhTridiag, s, 2);
       pack_lower_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
       NRG_CK(cudaGetLastError());
-      tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk);
+      tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
       NRG_CK(cudaGetLastError());
     }
     // ---- 2. divide and conquer
