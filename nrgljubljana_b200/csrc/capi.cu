@@ -9,7 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/nrg_b200.h"
+#include "nrg_b200.h"
 #include "ctx.h"
 #include "eig_large.h"
 #include "kernels.h"

@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/nrg_b200.h"
+#include "nrg_b200.h"
 #include "kernels.h"
 
 namespace nrg {

@@ -270,12 +270,13 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
 }
 
 // A(i, j) -= sum_{q < nbp} V(i,q) W(j,q) + W(i,q) V(j,q) for s0 <= j <= i < n, with
-// V(i, q) = P[(p0+q)*ld + i] and W(i, q) = W[q*n + i], on the FP64 tensor cores. In the
-// stored orientation C'(j, i) = P[j*ld + i] = A(i, j) the update is C' -= X Y^T with
-// X = [W_J | V_J] and Y = [V_I | W_I] (32 x 2NB each): per 32 x 32 tile a warp runs DMMA
-// 8x8x4 tiles over K = 2NB in two 16-column halves, operands read straight from the panel
-// rows (L1/L2). The tiles of the trailing lower triangle, in tile-row order, are split
-// evenly between the warps.
+// V(i, q) = P[(p0+q)*ld + i] and W(i, q) = W[q*n + i], on the FP64 tensor cores:
+// A -= Y X^T with Y = [V | W] (rows i) and X = [W | V] (rows j), K = 2NB. A warp owns a
+// 32 x 32 tile (rows i, columns j) as 4 x 4 DMMA 8x8x4 accumulators whose rows run along
+// the contiguous direction of P, so every load and store of the tile and of the operands
+// is 8 consecutive doubles per quarter-warp. The row operands Y of a tile row stay in
+// registers while the warp walks the columns. The tiles of the trailing lower triangle,
+// in tile-row order, are split evenly between the warps.
 NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, int n, int ld, int p0, int nbp,
                           int s0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -292,56 +293,62 @@ NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, 
     I++;
   }
   int J = T0 + (int)(f0 - acc0);
+  double ya[4][2 * NB / 4];  // A fragments of Y for the current tile row
+  int rowI = -1;
   for (long long f = f0; f < f1; f++) {
-    const int j0 = J << 5;
-#pragma unroll 1
-    for (int half = 0; half < 2; half++) {
-      const int i0 = (I << 5) + 16 * half;
-      double acc[4][2][2];
+    const int i0 = I << 5, j0 = J << 5;
+    if (rowI != I) {
+      rowI = I;
 #pragma unroll
-      for (int mi = 0; mi < 4; mi++)
-#pragma unroll
-        for (int ni = 0; ni < 2; ni++)
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
-            const bool ok = jj >= s0 && ii < n && ii >= jj;
-            acc[mi][ni][h] = ok ? P[(size_t)jj * ld + ii] : 0.0;
-          }
-#pragma unroll 2
-      for (int kk = 0; kk < 2 * NB; kk += 4) {
-        const int q = kk + c4;      // column of X and Y
-        const bool first = q < NB;  // X: W part / Y: V part
+      for (int ks = 0; ks < 2 * NB / 4; ks++) {
+        const int q = 4 * ks + c4;
+        const bool first = q < NB;
         const int qq = first ? q : q - NB;
-        const bool qok = qq < nbp;
-        const double* xrow = first ? W + (size_t)qq * n : P + (size_t)(p0 + qq) * ld;
-        const double* yrow = first ? P + (size_t)(p0 + qq) * ld : W + (size_t)qq * n;
-        double a[4], b[2];
+        const double* row = first ? P + (size_t)(p0 + qq) * ld : W + (size_t)qq * n;
 #pragma unroll
         for (int mi = 0; mi < 4; mi++) {
-          const int jj = j0 + 8 * mi + r;
-          a[mi] = (qok && jj < n) ? -xrow[jj] : 0.0;
+          const int ii = i0 + 8 * mi + r;
+          ya[mi][ks] = (qq < nbp && ii < n) ? -row[ii] : 0.0;
+        }
+      }
+    }
+    double acc[4][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+      for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int ii = i0 + 8 * mi + r, jj = j0 + 8 * ni + 2 * c4 + h;
+          const bool ok = jj >= s0 && ii < n && ii >= jj;
+          acc[mi][ni][h] = ok ? P[(size_t)jj * ld + ii] : 0.0;
         }
 #pragma unroll
-        for (int ni = 0; ni < 2; ni++) {
-          const int ii = i0 + 8 * ni + r;
-          b[ni] = (qok && ii < n) ? yrow[ii] : 0.0;
-        }
+    for (int ks = 0; ks < 2 * NB / 4; ks++) {
+      const int q = 4 * ks + c4;
+      const bool first = q < NB;
+      const int qq = first ? q : q - NB;
+      const double* row = first ? W + (size_t)qq * n : P + (size_t)(p0 + qq) * ld;
+      double b[4];
 #pragma unroll
-        for (int mi = 0; mi < 4; mi++)
-#pragma unroll
-          for (int ni = 0; ni < 2; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+      for (int ni = 0; ni < 4; ni++) {
+        const int jj = j0 + 8 * ni + r;
+        b[ni] = (qq < nbp && jj < n) ? row[jj] : 0.0;
       }
 #pragma unroll
       for (int mi = 0; mi < 4; mi++)
 #pragma unroll
-        for (int ni = 0; ni < 2; ni++)
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            const int jj = j0 + 8 * mi + r, ii = i0 + 8 * ni + 2 * c4 + h;
-            if (jj >= s0 && ii < n && ii >= jj) P[(size_t)jj * ld + ii] = acc[mi][ni][h];
-          }
+        for (int ni = 0; ni < 4; ni++) dmma884(acc[mi][ni][0], acc[mi][ni][1], ya[mi][ks], b[ni]);
     }
+#pragma unroll
+    for (int mi = 0; mi < 4; mi++)
+#pragma unroll
+      for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int ii = i0 + 8 * mi + r, jj = j0 + 8 * ni + 2 * c4 + h;
+          if (jj >= s0 && ii < n && ii >= jj) P[(size_t)jj * ld + ii] = acc[mi][ni][h];
+        }
     if (J < I) {
       J++;
     } else {
