@@ -34,7 +34,7 @@ namespace {
 
 constexpr int kTriThreads = 128;
 constexpr int NB = 16;     // tridiagonalisation panel width
-constexpr int NBT = 64;    // back-transform panel width
+constexpr int NBT = 128;   // back-transform panel width
 constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
 constexpr int kMaxLargeN = 4096;
 
@@ -52,7 +52,7 @@ struct LargeBlock {
   double* dsort;  // per node: non-deflated poles, ascending
   double* dgrp;   // per node: non-deflated poles, grouped order
   double* zgrp;   // per node: z in grouped order
-  double* GT;     // per back-transform panel: Gram matrix V^T V (NBT^2) then T (NBT^2)
+  double* GT;     // per back-transform panel of nb reflectors: Gram matrix V^T V then T (nb x nb each)
   int* rank;      // per node: sorted position of grouped entry
   int* perm;      // final eigenvalue order
   int* info;
@@ -979,36 +979,39 @@ __global__ void __launch_bounds__(256) permute_rows_kernel(const LargeBlock* __r
 
 // ---------------------------------------------------------------- back-transform factors
 // T of the compact-WY form H_k0 ... H_k0+nb-1 = I - V T V^T (forward, columnwise), from
-// the Gram matrix G = V^T V already in GT[p] (first NBT^2), written to GT[p] + NBT^2.
+// the Gram matrix G = V^T V (nb x nb) at GT + gt_off, written to GT + gt_off + nb^2.
 struct PanelRef {
   int blk, k0, nb, pad;
+  long long gt_off;
 };
 
 __global__ void __launch_bounds__(NBT) tfactor_kernel(const LargeBlock* __restrict__ blocks,
                                                       const PanelRef* __restrict__ panels) {
-  __shared__ double Ts[NBT][NBT + 1];
-  __shared__ double w[NBT];
+  extern __shared__ __align__(16) double tsm[];
   const PanelRef P = panels[blockIdx.x];
   const LargeBlock B = blocks[P.blk];
-  const int p = P.k0 / NBT, nb = P.nb, t = threadIdx.x;
-  const double* G = B.GT + (size_t)p * 2 * NBT * NBT;
-  double* T = B.GT + (size_t)p * 2 * NBT * NBT + NBT * NBT;
-  for (int r = 0; r < NBT; r++) Ts[r][t] = 0.0;
+  const int nb = P.nb, t = threadIdx.x, lt = NBT + 1;
+  double* Ts = tsm;           // NBT x (NBT+1)
+  double* w = tsm + NBT * lt;  // NBT
+  const double* G = B.GT + P.gt_off;
+  double* T = B.GT + P.gt_off + (size_t)nb * nb;
+  for (int r = 0; r < nb; r++) Ts[r * lt + t] = 0.0;
   __syncthreads();
   for (int q = 0; q < nb; q++) {
     const double tq = B.tau[P.k0 + q];
     // w = -tau_q G[0:q, q]; T[0:q, q] = T[0:q, 0:q] w
-    if (t < q) w[t] = -tq * G[t * NBT + q];
+    if (t < q) w[t] = -tq * G[t * nb + q];
     __syncthreads();
     if (t < q) {
       double s = 0.0;
-      for (int r = t; r < q; r++) s += Ts[t][r] * w[r];
-      Ts[t][q] = s;
+      for (int r = t; r < q; r++) s += Ts[t * lt + r] * w[r];
+      Ts[t * lt + q] = s;
     }
-    if (t == q) Ts[q][q] = tq;
+    if (t == q) Ts[q * lt + q] = tq;
     __syncthreads();
   }
-  for (int r = 0; r < NBT; r++) T[r * NBT + t] = Ts[r][t];
+  if (t < nb)
+    for (int r = 0; r < nb; r++) T[r * nb + t] = Ts[r * lt + t];
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1026,9 +1029,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 size_t large_block_doubles(int n) {
-  const int npanel = (n - 2 + NBT - 1) / NBT;
   const size_t ldp = (size_t)(n + 31) / 32 * 32;
-  return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + (size_t)npanel * 2 * NBT * NBT + 2 * (size_t)n + 64 * 12;
+  return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + 2 * (size_t)NBT * n + 2 * (size_t)n + 64 * 12;
 }
 
 }  // namespace
@@ -1080,7 +1082,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       L.dgrp = take(nb_);
       L.zgrp = take(nb_);
       L.npanel = (nb_ - 2 + NBT - 1) / NBT;
-      L.GT = take((size_t)L.npanel * 2 * NBT * NBT);
+      L.GT = take(2 * (size_t)NBT * nb_);  // >= sum over panels of 2 nb^2
       int* ip = reinterpret_cast<int*>(take(nb_));
       L.rank = ip;
       L.perm = ip + nb_;
@@ -1159,28 +1161,30 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     for (int bi = 0; bi < nb; bi++) {
       const LargeBlock& L = blk[bi];
       const int nn = L.n;
-      size_t vt_off = 0;
+      size_t vt_off = 0, gt_off = 0;
       for (int p = 0; p < L.npanel; p++) {
         const int k0 = p * NBT, pnb = std::min(NBT, (nn - 2) - k0), K = nn - k0 - 1;
-        panels.push_back(PanelRef{bi, k0, pnb, 0});
-        double* Gp = L.GT + (size_t)p * 2 * NBT * NBT;
+        panels.push_back(PanelRef{bi, k0, pnb, 0, (long long)gt_off});
+        double* Gp = L.GT + gt_off;                 // pnb x pnb
+        double* Tp = Gp + (size_t)pnb * pnb;        // pnb x pnb
+        gt_off += 2 * (size_t)pnb * pnb;
         const double* Vrows = L.W1 + (size_t)k0 * L.ldp + k0 + 1;  // pnb x K, row q = v_{k0+q}
-        gram.add_out(Gp, NBT, pnb, pnb, 0.0);
+        gram.add_out(Gp, pnb, pnb, pnb, 0.0);
         gram.add_seg(Vrows, L.ldp, 0, Vrows, L.ldp, 1, K, 1.0);
         double* VTp = L.H + vt_off;  // K x pnb (H is free after the final row permutation)
-        vt_off += (size_t)K * NBT;
+        vt_off += (size_t)K * pnb;
         if (vt_off > (size_t)nn * nn) return fail(NRG_ERR_ARG, "internal: VT factors exceed H for n=%d", nn);
-        vt.add_out(VTp, NBT, K, pnb, 0.0);
-        vt.add_seg(Vrows, L.ldp, 1, Gp + NBT * NBT, NBT, 0, pnb, 1.0);
+        vt.add_out(VTp, pnb, K, pnb, 0.0);
+        vt.add_seg(Vrows, L.ldp, 1, Tp, pnb, 0, pnb, 1.0);
         // step index counts from the last panel of each block
         const int stp = L.npanel - 1 - p;
         GemmPlan& g1 = bsteps[2 * stp];
         GemmPlan& g2 = bsteps[2 * stp + 1];
-        double* Wb = L.W2;  // n x NBT
-        g1.add_out(Wb, NBT, nn, pnb, 0.0);
+        double* Wb = L.W2;  // n x pnb
+        g1.add_out(Wb, pnb, nn, pnb, 0.0);
         g1.add_seg(L.evecs + k0 + 1, nn, 0, Vrows, L.ldp, 1, K, 1.0);
         g2.add_out(L.evecs + k0 + 1, nn, nn, K, 1.0);
-        g2.add_seg(Wb, NBT, 0, VTp, NBT, 1, pnb, -1.0);
+        g2.add_seg(Wb, pnb, 0, VTp, pnb, 1, pnb, -1.0);
       }
     }
     const size_t pan_off = push(img, panels);
@@ -1257,7 +1261,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     if (rc) return rc;
     if (!panels.empty()) {
       PhaseScope sc(c, kPhBtTfactor, s);
-      tfactor_kernel<<<(int)panels.size(), NBT, 0, s>>>(dblk, reinterpret_cast<const PanelRef*>(dbase + pan_off));
+      const size_t ts = sizeof(double) * ((size_t)NBT * (NBT + 1) + NBT);
+      NRG_CK(cudaFuncSetAttribute(tfactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts));
+      tfactor_kernel<<<(int)panels.size(), NBT, ts, s>>>(dblk, reinterpret_cast<const PanelRef*>(dbase + pan_off));
       NRG_CK(cudaGetLastError());
     }
     rc = launch_staged_gemm(c, vt_g, s, kPhBtGemm);
