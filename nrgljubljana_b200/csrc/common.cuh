@@ -71,4 +71,16 @@ NRG_DEV void dmma884(double& d0, double& d1, double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// FP64 tensor-core MMA: D(16x8) += A(16x16) * B(16x8). Fragment layout (per lane l,
+// g = l/4, t = l%4): a[i] = A[g + 8*(i%2)][t + 4*(i/2)] (i < 8), b[i] = B[t + 4*i][g]
+// (i < 4), d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
+NRG_DEV void dmma16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
+}
+
 }  // namespace nrg
