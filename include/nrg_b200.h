@@ -75,6 +75,38 @@ NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* 
 NRG_API int nrg_diag_batch_host(nrg_ctx* ctx, int nblk, const int* n, const double* const* H, double* const* evals,
                         double* const* evecs, int* info, void* stream);
 
+/* ------------------------------------------------------------------ Hamiltonian assembly
+ * Replaces hamiltonian() (c++/core.hpp:72-88) for all blocks of one step: the per-block
+ * matrix initialisation of make_matrix() (c++/symmetry/sym-QS-impl.hpp:111-155) is given
+ * as a list of pieces instead of being run per block on the host. Each H[b] (n[b] x n[b],
+ * row-major, device) is cleared and the pieces with blk == b are added in the order given:
+ *   NRG_HP_DIAG   H[r0+k][c0+k] += factor * src[k] + shift  for k < rows (src NULL: 0)
+ *                 -- the ancestor energies scaled by sqrt(Lambda) (c++/core.hpp:79-82),
+ *                 diag_function_impl (c++/matrix.hpp:67-78) and diag_offdiag_function
+ *                 (c++/matrix.hpp:97-111)
+ *   NRG_HP_BLOCK  H[r0+i][c0+j] += factor * src[i*ld + j]   (trans = 0)
+ *                 H[r0+i][c0+j] += factor * src[j*ld + i]   (trans = 1, the conjugate
+ *                 transpose of c++/matrix.hpp:48-52 for real matrices), i < rows, j < cols
+ *                 -- offdiag_function_impl (c++/matrix.hpp:32-58)
+ * Products and sums are rounded one by one (no fused multiply-add), so the result is
+ * bit-identical to the reference's. The caller keeps every piece inside the upper
+ * triangle, as the reference does; the strictly lower triangle is then zero, as
+ * diagonalise() asserts (c++/diag.hpp:265). A non-finite factor is rejected as
+ * offdiag_function() rejects it (c++/matrix.hpp:40-41). src pointers are device pointers;
+ * n, H and pieces are host arrays. */
+#define NRG_HP_DIAG 0
+#define NRG_HP_BLOCK 1
+typedef struct nrg_hpiece {
+  int blk, kind;
+  int r0, c0, rows, cols;
+  int trans, pad_;
+  int64_t ld;
+  const double* src;
+  double factor, shift;
+} nrg_hpiece;
+NRG_API int nrg_hamiltonian_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* H, int npiece,
+                                  const nrg_hpiece* pieces, void* stream);
+
 /* ------------------------------------------------------------------ GEMM leaves
  * One term M += factor * op(A) * O * op(B), grouped by M. Expresses
  *   product   (c++/numerics_ublas.hpp:108-116): M += f A B^T         O = NULL, transB = 1

@@ -24,7 +24,7 @@ NRG_SPEC_FDMLS = 2
 # Every symbol include/nrg_b200.h declares.
 EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_diag_batch", "nrg_diag_batch_host",
            "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate", "nrg_profile",
-           "nrg_profile_read", "nrg_bins_grid")
+           "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch")
 NRG_NOALLOC_SCRATCH_DOUBLES = 1 << 20
 
 
@@ -33,6 +33,16 @@ class Gemm3(C.Structure):
                 ("O", C.c_void_p), ("ldo", C.c_int64), ("B", C.c_void_p), ("ldb", C.c_int64),
                 ("rows", C.c_int), ("cols", C.c_int), ("ka", C.c_int), ("kb", C.c_int),
                 ("transA", C.c_int), ("transB", C.c_int), ("factor", C.c_double)]
+
+
+NRG_HP_DIAG = 0
+NRG_HP_BLOCK = 1
+
+
+class HPiece(C.Structure):
+    _fields_ = [("blk", C.c_int), ("kind", C.c_int), ("r0", C.c_int), ("c0", C.c_int), ("rows", C.c_int),
+                ("cols", C.c_int), ("trans", C.c_int), ("pad_", C.c_int), ("ld", C.c_int64), ("src", C.c_void_p),
+                ("factor", C.c_double), ("shift", C.c_double)]
 
 
 class SpecPair(C.Structure):
@@ -82,6 +92,7 @@ def load() -> C.CDLL:
     L.nrg_bins_grid.argtypes = [C.POINTER(Bins), C.POINTER(C.c_double)]
     L.nrg_transform_noalloc.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int64, P, C.c_int64, C.c_int, C.c_int,
                                         C.c_int, C.c_int, C.c_double, P]
+    L.nrg_hamiltonian_batch.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(P), C.c_int, C.POINTER(HPiece), P]
     L.nrg_profile.argtypes = [P, C.c_int]
     L.nrg_profile_read.argtypes = [P, C.POINTER(PhaseStat), C.c_int]
     _lib = L

@@ -116,7 +116,7 @@ StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p) {
 const char* phase_name(int p) {
   static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
                                         "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
-                                        "gemm3", "spec_gemm", "spec_bin"};
+                                        "gemm3", "spec_gemm", "spec_bin", "assemble"};
   return (p >= 0 && p < kPhCount) ? names[p] : "?";
 }
 
@@ -359,6 +359,67 @@ int nrg_diag_batch_host(nrg_ctx* c, int nblk, const int* n, const double* const*
 }
 
 // ---------------------------------------------------------------- GEMM leaves
+int nrg_hamiltonian_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, int npiece,
+                          const nrg_hpiece* pieces, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nblk < 0 || npiece < 0 || (nblk > 0 && (!n || !H)) || (npiece > 0 && !pieces))
+    return fail(NRG_ERR_ARG, "bad arguments");
+  auto s = static_cast<cudaStream_t>(stream);
+  for (int b = 0; b < nblk; b++) {
+    if (n[b] < 0 || n[b] > (1 << 20)) return fail(NRG_ERR_ARG, "block %d: bad order %d", b, n[b]);
+    if (n[b] > 0 && !H[b]) return fail(NRG_ERR_ARG, "block %d: null matrix", b);
+  }
+  for (int p = 0; p < npiece; p++) {
+    const nrg_hpiece& q = pieces[p];
+    if (q.blk < 0 || q.blk >= nblk) return fail(NRG_ERR_ARG, "piece %d: block %d out of range", p, q.blk);
+    const int nb = n[q.blk];
+    if (q.kind != NRG_HP_DIAG && q.kind != NRG_HP_BLOCK) return fail(NRG_ERR_ARG, "piece %d: bad kind", p);
+    const int cols = q.kind == NRG_HP_DIAG ? q.rows : q.cols;
+    if (q.rows < 0 || cols < 0 || q.r0 < 0 || q.c0 < 0 || q.r0 + q.rows > nb || q.c0 + cols > nb)
+      return fail(NRG_ERR_ARG, "piece %d: region outside the %d x %d block", p, nb, nb);
+    if (!(q.factor - q.factor == 0.0) || !(q.shift - q.shift == 0.0))
+      return fail(NRG_ERR_ARG, "piece %d: factor not finite", p);  // c++/matrix.hpp:40-41
+    if (q.kind == NRG_HP_BLOCK && q.rows > 0 && q.cols > 0) {
+      if (!q.src) return fail(NRG_ERR_ARG, "piece %d: null source matrix", p);
+      if (q.ld < (q.trans ? q.rows : q.cols)) return fail(NRG_ERR_ARG, "piece %d: leading dimension too small", p);
+    }
+  }
+  // Pieces grouped by block, order inside a block kept.
+  std::vector<int> count(nblk + 1, 0);
+  for (int p = 0; p < npiece; p++) count[pieces[p].blk + 1]++;
+  for (int b = 0; b < nblk; b++) count[b + 1] += count[b];
+  std::vector<nrg_hpiece> sorted(npiece);
+  {
+    std::vector<int> fill(count.begin(), count.end() - 1);
+    for (int p = 0; p < npiece; p++) sorted[fill[pieces[p].blk]++] = pieces[p];
+  }
+  std::vector<nrg::HBlock> blocks;
+  int tiles = 0;
+  for (int b = 0; b < nblk; b++) {
+    if (n[b] == 0) continue;
+    nrg::HBlock hb;
+    hb.H = H[b];
+    hb.n = n[b];
+    hb.tile0 = tiles;
+    hb.p0 = count[b];
+    hb.p1 = count[b + 1];
+    blocks.push_back(hb);
+    tiles += nrg::hamiltonian_tiles(n[b]);
+  }
+  if (blocks.empty()) return NRG_OK;
+  std::vector<char> img;
+  const size_t ob = push(img, blocks);
+  const size_t op = push(img, sorted);
+  rc = stage_desc(c, img, s);
+  if (rc) return rc;
+  auto* base = static_cast<char*>(c->desc);
+  nrg::PhaseScope ps(c, nrg::kPhAssemble, s);
+  CK(nrg::hamiltonian_launch(reinterpret_cast<const nrg::HBlock*>(base + ob), (int)blocks.size(), tiles,
+                             reinterpret_cast<const nrg_hpiece*>(base + op), s));
+  return NRG_OK;
+}
+
 int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "nrg_b200.h"
+
 namespace nrg {
 
 // ---------------------------------------------------------------- batched FP64 GEMM
@@ -56,5 +58,16 @@ struct EigBlock {
 constexpr int kSmallMaxN = 64;   // blocks up to this size are solved entirely in shared memory
 
 cudaError_t eig_small_launch(const EigBlock* d_blocks, int nblk, int maxn, cudaStream_t stream);
+
+// ---------------------------------------------------------------- Hamiltonian assembly
+// One block of nrg_hamiltonian_batch: its matrix, order, first tile and its pieces
+// [p0, p1) in the sorted piece array.
+struct HBlock {
+  double* H;
+  int n, tile0, p0, p1;
+};
+int hamiltonian_tiles(int n);
+cudaError_t hamiltonian_launch(const HBlock* d_blocks, int nblk, int ntiles, const nrg_hpiece* d_pieces,
+                               cudaStream_t stream);
 
 }  // namespace nrg

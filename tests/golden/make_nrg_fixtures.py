@@ -1,0 +1,36 @@
+"""Regenerate the NRG-run fixtures under tests/golden/nrg/ from the reference's regression tests.
+
+Each case directory of the reference's ``test/c++/<case>/`` holds the run's input (``param``,
+``data``) and the outputs the reference produced with a real LAPACK (``ref/td``,
+``ref/custom``, printed to 10 significant digits). They are copied here unchanged so that
+the tests can run where the reference tree is absent. Usage:
+
+    python tests/golden/make_nrg_fixtures.py /path/to/nrgljubljana
+"""
+import os
+import shutil
+import sys
+
+CASES = [
+    "test0_minimal", "test0_minimal_Nmax1", "test0_minimal_Nmax2", "test0_minimal_Nmax3",
+    "test3_disc_z", "test4_disc_c", "test10_keepmin", "test12_Nmax", "test13_strategy_all",
+    "test14_strategy_kept", "test15_safeguard", "test16_safeguardmax", "test35_betabar",
+    "test56_dsyevd", "test56_dsyevr", "test200_data_has", "legacy_simple", "legacy_Himp",
+]
+
+
+def main(ref_root: str) -> None:
+    out_root = os.path.join(os.path.dirname(os.path.abspath(__file__)), "nrg")
+    for case in CASES:
+        src = os.path.join(ref_root, "test", "c++", case)
+        dst = os.path.join(out_root, case)
+        os.makedirs(dst, exist_ok=True)
+        for name, rel in (("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")):
+            p = os.path.join(src, rel)
+            if os.path.exists(p):
+                shutil.copyfile(p, os.path.join(dst, name))
+    print(f"wrote {len(CASES)} cases to {out_root}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
