@@ -214,6 +214,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
+    ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -335,11 +337,114 @@ def main():
         cpu_v = f_eig(sizes[idx]) / t / 1e9
         line["cpu_baseline"] = {"value": cpu_v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{len(idx)} of {nbk} blocks (every {stride}th in size order), {t:.1f} s"}
+    if not args.no_per_block and rank == 0 and world == 1:
+        line["per_block_gpu"] = per_block_arm(torch, pristine, sizes, offs, dev)
+    del pristine
+    torch.cuda.empty_cache()
+    if not args.no_nrg and rank == 0:
+        line["nrg_run"] = nrg_run_arm(torch, local, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def per_block_arm(torch, pristine, sizes, offs, dev, target_flop: float = 1.5e12) -> dict:
+    """The plain GPU path: one cuSOLVER eigensolve (torch.linalg.eigh) per block and launch,
+    on a size-stratified sample of the same blocks; GFLOP/s on the same F_eig count."""
+    order = np.argsort(sizes, kind="stable")
+    f = np.array([f_eig(int(n)) for n in sizes[order]])
+    stride = max(1, int(math.ceil(f.sum() / target_flop)))
+    idx = order[::stride]
+    mats = [pristine[offs[b]:offs[b + 1]].view(int(sizes[b]), int(sizes[b])) for b in idx]
+    for h in mats[:8]:
+        torch.linalg.eigh(h, UPLO="U")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for h in mats:
+        w, q = torch.linalg.eigh(h, UPLO="U")
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    return {"value": f_eig(sizes[idx]) / t / 1e9, "unit": UNIT, "impl": "torch.linalg.eigh (cuSOLVER) per block",
+            "sample": f"{len(idx)} of {len(sizes)} blocks (every {stride}th in size order)", "seconds": t}
+
+
+NRG_CASE = "legacy_Himp"
+NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model (U=2, Gamma=0.1, delta=0), Lambda=2 (Yoshida), "
+                "Nmax=40, keep=1000, keepenergy=8, 6 singlet operators: the reference's regression input "
+                "test/c++/legacy_Himp")
+
+
+def nrg_run_arm(torch, device: int, args) -> dict:
+    """Whole NRG runs (host driver + device step core) in NRG steps/s, beside the same run
+    with one cuSOLVER call per block and the CPU restatement on all host cores."""
+    from nrgljubljana_b200 import context
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import QSRun, RunParams
+    base = os.path.join(ROOT, "tests", "golden", "nrg", NRG_CASE)
+    param = open(os.path.join(base, "param")).read()
+    data = open(os.path.join(base, "data")).read()
+    p, d = RunParams.from_param(parse_param(param)), read_data(data)
+    ctx = context(device)
+
+    class PerBlock(QSRun):
+        def _diagonalise(self, ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff):
+            for b, n in enumerate(ns):
+                h = Hbuf[moff[b]:moff[b + 1]].view(n, n)
+                w, q = torch.linalg.eigh(h, UPLO="U")
+                Ebuf[voff[b]:voff[b + 1]].copy_(w)
+                Vbuf[moff[b]:moff[b + 1]].view(n, n).copy_(q.T)
+            return np.zeros(len(ns), dtype=np.int32)
+
+    def timed(cls, reps):
+        cls(p, d, device).run()  # warm-up
+        torch.cuda.synchronize()
+        best, res = None, None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            res = cls(p, d, device).run()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        return best, res
+
+    ctx.profile(True)
+    ctx.profile_read()
+    t_b200, res = timed(QSRun, 3)
+    phases = ctx.profile_read()
+    ctx.profile(False)
+    t_pb, res_pb = timed(PerBlock, 1)
+    out = {"workload": NRG_WORKLOAD, "steps_per_run": d.nmax, "steps_per_s": d.nmax / t_b200,
+           "ms_per_run": t_b200 * 1e3, "timing": "wall clock of whole runs (host driver included), best of 3",
+           "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
+           "device_phases_ms_per_run": {k: v[0] / 4 for k, v in phases.items() if v[1]},
+           "per_block_gpu": {"steps_per_s": d.nmax / t_pb, "ms_per_run": t_pb * 1e3,
+                             "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch"}}
+    td = np.array(res.td)
+
+    def tddiff(other):
+        """Largest relative difference over the values of size 1e-6 or more (values that
+        vanish by particle-hole symmetry are round-off noise of order 1e-13 in every run)."""
+        o = np.array(other)
+        big = np.abs(td) >= 1e-6
+        return float(np.max(np.abs(o[big] - td[big]) / np.abs(td[big])))
+    out["per_block_gpu"]["td_max_rel_diff"] = tddiff(res_pb.td)
+    if not args.no_cpu:
+        from oracle import oracle as O
+        from oracle import nrg_run_cpu
+        O.build()
+        threads = os.cpu_count() or 1
+        nrg_run_cpu.run(param, data, threads=threads)
+        t0 = time.perf_counter()
+        _, td_cpu, _, _ = nrg_run_cpu.run(param, data, threads=threads)
+        t_cpu = time.perf_counter() - t0
+        out["cpu_baseline"] = {"steps_per_s": d.nmax / t_cpu, "ms_per_run": t_cpu * 1e3, "cores": threads,
+                               "kind": "port", "sample": "one whole run",
+                               "td_max_rel_diff": tddiff(td_cpu)}
+    return out
 
 
 def e2e_arm(torch, ctx, nb, pristine, sizes, offs, voffs, args) -> dict:

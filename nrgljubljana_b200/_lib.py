@@ -45,6 +45,20 @@ class HPiece(C.Structure):
                 ("factor", C.c_double), ("shift", C.c_double)]
 
 
+def _np_layout(struct) -> "np.dtype":
+    """numpy record type with the byte layout of a ctypes Structure, for descriptor arrays
+    built vectorised on the host and handed to the library as one pointer."""
+    import numpy as np
+    kinds = {C.c_void_p: "u8", C.c_int64: "i8", C.c_int: "i4", C.c_double: "f8"}
+    names = [f[0] for f in struct._fields_]
+    return np.dtype({"names": names, "formats": [kinds[f[1]] for f in struct._fields_],
+                     "offsets": [getattr(struct, n).offset for n in names], "itemsize": C.sizeof(struct)})
+
+
+GEMM3_DTYPE = _np_layout(Gemm3)
+HPIECE_DTYPE = _np_layout(HPiece)
+
+
 class SpecPair(C.Structure):
     _fields_ = [("Ei", C.c_void_p), ("Ej", C.c_void_p), ("op1", C.c_void_p), ("ld1", C.c_int64),
                 ("op2", C.c_void_p), ("ld2", C.c_int64), ("rho_i", C.c_void_p), ("ldri", C.c_int64),

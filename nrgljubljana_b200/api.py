@@ -195,6 +195,47 @@ def gemm3_batch(terms: Sequence[Gemm3], host: bool, ctx: Optional[Context] = Non
     check(f(ctx.ptr, len(terms), arr, _stream_ptr(stream)), "nrg_gemm3_batch")
 
 
+def gemm3_batch_array(terms: np.ndarray, ctx: Optional[Context] = None, stream=None) -> None:
+    """nrg_gemm3_batch on a numpy record array of GEMM3_DTYPE (device pointers)."""
+    ctx = ctx or context()
+    if terms.dtype != _lib.GEMM3_DTYPE or not terms.flags.c_contiguous:
+        raise ValueError("terms must be a contiguous GEMM3_DTYPE array")
+    if len(terms) == 0:
+        return
+    check(ctx.lib.nrg_gemm3_batch(ctx.ptr, len(terms), terms.ctypes.data_as(C.POINTER(Gemm3)), _stream_ptr(stream)),
+          "nrg_gemm3_batch")
+
+
+def hamiltonian_batch(n: Sequence[int], H: Sequence[int], pieces: np.ndarray, ctx: Optional[Context] = None,
+                      stream=None) -> None:
+    """nrg_hamiltonian_batch: blocks n[b] at device addresses H[b], pieces a HPIECE_DTYPE array."""
+    ctx = ctx or context()
+    if pieces.dtype != _lib.HPIECE_DTYPE or not pieces.flags.c_contiguous:
+        raise ValueError("pieces must be a contiguous HPIECE_DTYPE array")
+    nb = len(n)
+    n_c = (C.c_int * nb)(*[int(x) for x in n])
+    H_c = (C.c_void_p * nb)(*[int(x) for x in H])
+    check(ctx.lib.nrg_hamiltonian_batch(ctx.ptr, nb, n_c, H_c, len(pieces),
+                                        pieces.ctypes.data_as(C.POINTER(_lib.HPiece)), _stream_ptr(stream)),
+          "nrg_hamiltonian_batch")
+
+
+def diag_batch_ptrs(n: Sequence[int], H: Sequence[int], evals: Sequence[int], evecs: Sequence[int],
+                    ctx: Optional[Context] = None, stream=None) -> np.ndarray:
+    """nrg_diag_batch on raw device addresses; returns the per-block status words."""
+    ctx = ctx or context()
+    nb = len(n)
+    n_c = (C.c_int * nb)(*[int(x) for x in n])
+    Hp = (C.c_void_p * nb)(*[int(x) for x in H])
+    Ep = (C.c_void_p * nb)(*[int(x) for x in evals])
+    Vp = (C.c_void_p * nb)(*[int(x) for x in evecs])
+    info = (C.c_int * nb)()
+    rc = ctx.lib.nrg_diag_batch(ctx.ptr, nb, n_c, Hp, Ep, Vp, info, _stream_ptr(stream))
+    if rc < 0:
+        raise NRGError(rc, "nrg_diag_batch")
+    return np.array(info[:], dtype=np.int32)
+
+
 def _is_host(x) -> bool:
     return not hasattr(x, "data_ptr")
 

@@ -113,6 +113,22 @@ StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p) {
   return g;
 }
 
+int stage_desc_side(nrg_ctx* c, const std::vector<char>& img) {
+  if (img.empty()) return NRG_OK;
+  if (img.size() > c->desc_side_size) {
+    if (c->desc_side) {
+      NRG_CK(cudaStreamSynchronize(c->side));
+      NRG_CK(cudaFree(c->desc_side));
+      c->desc_side = nullptr;
+    }
+    const size_t sz = align_up(img.size() * 2, 1 << 16);
+    NRG_CK(cudaMalloc(&c->desc_side, sz));
+    c->desc_side_size = sz;
+  }
+  NRG_CK(cudaMemcpyAsync(c->desc_side, img.data(), img.size(), cudaMemcpyHostToDevice, c->side));
+  return NRG_OK;
+}
+
 const char* phase_name(int p) {
   static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
                                         "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
@@ -250,6 +266,10 @@ int nrg_destroy(nrg_ctx* c) {
   if (c->ws) cudaFree(c->ws);
   if (c->desc) cudaFree(c->desc);
   if (c->info_dev) cudaFree(c->info_dev);
+  if (c->desc_side) cudaFree(c->desc_side);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->join_ev) cudaEventDestroy(c->join_ev);
+  if (c->side) cudaStreamDestroy(c->side);
   delete c;
   return NRG_OK;
 }
@@ -277,6 +297,14 @@ int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double*
   std::vector<int> small, large;
   for (int b = 0; b < nblk; b++) (n[b] <= nrg::kSmallMaxN ? small : large).push_back(b);
 
+  // With blocks of both kinds the small-block solver runs on the context's side stream,
+  // forked from and joined back into s, so that it overlaps the large-block pipeline.
+  const bool fork = !small.empty() && !large.empty();
+  if (fork && !c->side) {
+    CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming));
+  }
   if (!small.empty()) {
     // Largest first, so that the long CTAs start early.
     std::stable_sort(small.begin(), small.end(), [n](int a, int b) { return n[a] > n[b]; });
@@ -293,14 +321,32 @@ int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double*
     }
     std::vector<char> img;
     const size_t off = push(img, blk);
-    rc = stage_desc(c, img, s);
+    cudaStream_t ss = s;
+    char* base;
+    if (fork) {
+      CK(cudaEventRecord(c->fork_ev, s));
+      CK(cudaStreamWaitEvent(c->side, c->fork_ev, 0));
+      ss = c->side;
+      rc = nrg::stage_desc_side(c, img);
+      base = static_cast<char*>(c->desc_side);
+    } else {
+      rc = stage_desc(c, img, s);
+      base = static_cast<char*>(c->desc);
+    }
     if (rc) return rc;
-    nrg::PhaseScope ps(c, nrg::kPhEigSmall, s);
-    CK(nrg::eig_small_launch(reinterpret_cast<const nrg::EigBlock*>(static_cast<char*>(c->desc) + off),
-                             (int)small.size(), n[small[0]], s));
+    {
+      nrg::PhaseScope ps(c, nrg::kPhEigSmall, ss);
+      CK(nrg::eig_small_launch(reinterpret_cast<const nrg::EigBlock*>(base + off), (int)small.size(),
+                               n[small[0]], ss));
+    }
+    if (fork) CK(cudaEventRecord(c->join_ev, ss));
   }
   if (!large.empty()) {
     rc = nrg::eig_large_run(c, large, n, H, evals, evecs, c->info_dev, s);
+    if (fork) {
+      const cudaError_t e = cudaStreamWaitEvent(s, c->join_ev, 0);  // join even on failure
+      if (!rc && e != cudaSuccess) rc = fail(NRG_ERR_CUDA, "join of the side stream: %s", cudaGetErrorString(e));
+    }
     if (rc) return rc;
   }
   CK(cudaMemcpyAsync(info, c->info_dev, sizeof(int) * (size_t)nblk, cudaMemcpyDeviceToHost, s));

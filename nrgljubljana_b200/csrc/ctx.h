@@ -35,6 +35,11 @@ struct nrg_ctx {
   size_t desc_size = 0;
   int* info_dev = nullptr;
   size_t info_cap = 0;
+  // second stream: the one-CTA small-block solver runs beside the large-block pipeline
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  void* desc_side = nullptr;  // descriptor staging of the side stream
+  size_t desc_side_size = 0;
 };
 
 namespace nrg {
@@ -44,6 +49,8 @@ const char* last_error_text();
 int ensure_ws(nrg_ctx* c, size_t bytes);
 // Copies a host byte image to c->desc (stream-ordered); returns the device base pointer.
 int stage_desc(nrg_ctx* c, const std::vector<char>& img, cudaStream_t s);
+// Same into the side stream's own staging buffer.
+int stage_desc_side(nrg_ctx* c, const std::vector<char>& img);
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

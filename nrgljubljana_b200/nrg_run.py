@@ -30,8 +30,8 @@ import numpy as np
 import torch
 
 from . import qs
-from ._lib import HPiece, NRG_HP_BLOCK, NRG_HP_DIAG, NRGError
-from .api import Context, context, diag_batch_device, gemm3, gemm3_batch, _stream_ptr
+from ._lib import GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG
+from .api import Context, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch
 from .inputs import DataFile, SCALE, parse_param, read_data
 
 Invar = Tuple[int, int]
@@ -102,18 +102,20 @@ def cluster_mapping(energies: np.ndarray, eps: float) -> Dict[float, float]:
     members of a split cluster to its lowest value. The loop, as in the reference, counts
     the first element twice and never closes the last cluster."""
     mapping: Dict[float, float] = {}
-    e = energies
+    if len(energies) < 2 or not np.any(np.diff(energies) < eps):
+        return mapping  # every cluster is a single value: nothing to map
+    e = energies.tolist()
     e0, i0, size = e[0], 0, 1
     for i in range(len(e)):
         if e[i] - e0 < eps:
             size += 1
         else:
-            if size > 1:
-                seg = e[i0:i]
-                if np.any(seg != seg[0]):
+            if size > 1 and i - i0 > 1:
+                first = e[i0]
+                if any(x != first for x in e[i0 + 1:i]):
                     for j in range(i0 + 1, i):
-                        if e[j] != e[i0]:
-                            mapping.setdefault(float(e[j]), float(e[i0]))
+                        if e[j] != first:
+                            mapping.setdefault(e[j], first)
             e0, i0, size = e[i], i, 1
     return mapping
 
@@ -139,7 +141,7 @@ def highest_retained_energy(energies: np.ndarray, p: RunParams) -> float:
 
 @dataclass
 class Sub:
-    """One subspace of a step: host eigenvalues and the device eigenvector rows."""
+    """One subspace of a step: host eigenvalues and the address of its device eigenvectors."""
     I: Invar
     values: np.ndarray                 # computed eigenvalues (relative), ascending
     shift: float = 0.0
@@ -147,12 +149,55 @@ class Sub:
     nstored: int = 0                   # states kept after truncate_perform (all before)
     nkept: int = 0
     dims: List[int] = field(default_factory=list)  # ancestor block widths
-    offs: List[int] = field(default_factory=list)
-    vec: Optional[torch.Tensor] = None  # n x n (device), row r = eigenvector r
+    offs: List[int] = field(default_factory=list)  # their column offsets
+    vptr: int = 0                      # device address of the n x n eigenvector rows
+    n: int = 0
 
-    def block(self, i: int, rows: int) -> torch.Tensor:
-        """U(i) restricted to the first `rows` states (split_in_blocks, c++/recalc.hpp:18-30)."""
-        return self.vec[:rows, self.offs[i]:self.offs[i] + self.dims[i]]
+
+class MatSet:
+    """Matrices of one kind in one flat device buffer, `nops` copies of the same layout
+    (operator-major): the <||f||> of a step (nops = 1) or all singlet operators of a step.
+    Keys map to (offset, rows, cols); every matrix is contiguous (ld = cols)."""
+
+    def __init__(self, dev, shapes: Dict, nops: int = 1, host: Optional[np.ndarray] = None):
+        self.loc: Dict = {}
+        off = 0
+        for k, (r, c) in shapes.items():
+            self.loc[k] = (off, r, c)
+            off += r * c
+        self.total = off
+        self.nops = nops
+        if host is not None:
+            self.buf = torch.from_numpy(host).to(dev)
+        else:
+            self.buf = torch.zeros(max(1, nops * off), dtype=torch.float64, device=dev)
+        self.base = self.buf.data_ptr()
+
+    def ptr(self, key, op: int = 0) -> int:
+        return self.base + 8 * (op * self.total + self.loc[key][0])
+
+
+def _pack(mats: List[Dict], shapes: Dict) -> np.ndarray:
+    """Host image of a MatSet: for each dict in `mats` (one per operator) the matrices in
+    the order of `shapes`; missing entries are zero."""
+    total = sum(r * c for r, c in shapes.values())
+    out = np.zeros(max(1, len(mats) * total))
+    for o, m in enumerate(mats):
+        off = o * total
+        for k, (r, c) in shapes.items():
+            if k in m:
+                out[off:off + r * c] = np.ascontiguousarray(m[k], dtype=np.float64).ravel()
+            off += r * c
+    return out
+
+
+@dataclass
+class _Measure:
+    """What one custom row needs, kept until the end of the run: the device diagonals of
+    every singlet operator over the stored states, and the host Boltzmann weights."""
+    T: float
+    weights: np.ndarray        # mult(I) * exp(-f * corr) per stored state, subspace order
+    diag: torch.Tensor         # nops x states (device)
 
 
 class QSRun:
@@ -170,53 +215,50 @@ class QSRun:
         self.stream = torch.cuda.current_stream(self.dev)
         self.nmax = data.nmax
         self.sqrt_lambda = math.sqrt(params.Lambda)  # nrg_step_scale_factor (c++/params.hpp:639-641)
+        self.op_names = sorted(n for n, (k, _) in data.ops.items() if k in "sg")
 
     # ---- scales (c++/step.hpp:30-39)
     def scale(self, trueN: int) -> float:
         return SCALE(trueN + 1, self.p.Lambda, self.p.discretization, self.p.z, self.p.bandrescale)
 
-    def _to_dev(self, a: np.ndarray) -> torch.Tensor:
-        return torch.from_numpy(np.ascontiguousarray(a)).to(self.dev, non_blocking=False)
+    def _h2d(self, a: np.ndarray) -> torch.Tensor:
+        """Host array to the device without stalling the host: staged through pinned memory
+        that the caching host allocator keeps until the copy on the stream has run."""
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(self.dev, non_blocking=True)
 
     # ---- measurements
     def _td(self, trueN: int, diag: Dict[Invar, Sub]) -> List[float]:
+        """calculate_TD (c++/measurements.hpp:169-186) with SymmetryQS::calculate_TD."""
         f = self.p.betabar  # TD_factor (unscale = 1)
-        Z = E = E2 = 0.0
-        Zs = []
-        for I, s in diag.items():
-            x = s.values - s.shift
-            ex = np.exp(-f * x)
-            m = qs.mult(I)
-            Z += m * float(np.sum(ex))
-            E += m * float(np.sum((f * x) * ex))
-            E2 += m * float(np.sum((f * x) ** 2 * ex))
-            Zs.append(m * float(np.sum(np.exp(-f * s.corr[:s.nstored]))))
+        subs = list(diag.values())
+        counts = np.array([len(s.values) for s in subs])
+        x = np.concatenate([s.values - s.shift for s in subs])
+        m = np.repeat(np.array([qs.mult(s.I) for s in subs], dtype=np.float64), counts)
+        ex = np.exp(-f * x)
+        fx = f * x
+        Z = float(np.sum(m * ex))
+        E = float(np.sum(m * fx * ex))
+        E2 = float(np.sum(m * fx * fx * ex))
+        Zs = [qs.mult(s.I) * float(np.sum(np.exp(-f * s.corr[:s.nstored]))) for s in subs]
         T = self.scale(trueN) / self.p.betabar
-        extra = qs.td_extra(Zs, list(diag.keys()), Z)
+        extra = qs.td_extra(Zs, [s.I for s in subs], Z)
         return [T] + extra + [E / Z, E2 / Z, E2 / Z - (E / Z) ** 2, -math.log(Z), E / Z + math.log(Z)]
 
-    def _custom(self, trueN: int, diag: Dict[Invar, Sub], ops: Dict[str, Dict[Invar, torch.Tensor]]) -> List[float]:
+    def _measure(self, trueN: int, diag: Dict[Invar, Sub], ops: MatSet) -> _Measure:
+        """measure_singlet (c++/measurements.hpp:18-30): the diagonals are gathered on the
+        device now and read back once at the end of the run."""
         f = self.p.betabar
-        Z = 0.0
-        for I, s in diag.items():
-            Z += qs.mult(I) * float(np.sum(np.exp(-f * s.corr[:s.nstored])))
-        row = [self.scale(trueN) / self.p.betabar]
-        names = sorted(ops)
-        # one device->host copy of every needed diagonal
-        diags = []
-        for name in names:
-            for I, s in diag.items():
-                diags.append(torch.diagonal(ops[name][I])[:s.nstored])
-        host = torch.cat(diags).cpu().numpy() if diags else np.zeros(0)
-        k = 0
-        for name in names:
-            tr = 0.0
-            for I, s in diag.items():
-                d = host[k:k + s.nstored]
-                k += s.nstored
-                tr += qs.mult(I) * float(np.sum(np.exp(-f * s.corr[:s.nstored]) * d))
-            row.append(tr / Z)
-        return row
+        w, idx = [], []
+        for s in diag.values():
+            k = s.nstored
+            w.append(qs.mult(s.I) * np.exp(-f * s.corr[:k]))
+            off, r, c = ops.loc[s.I]
+            idx.append(off + np.arange(k) * (c + 1))
+        idx = np.concatenate(idx) if idx else np.zeros(0, dtype=np.int64)
+        full = (np.arange(ops.nops)[:, None] * ops.total + idx[None, :]).ravel()
+        g = self._h2d(full.astype(np.int64))
+        dg = torch.index_select(ops.buf, 0, g).view(ops.nops, len(idx))
+        return _Measure(self.scale(trueN) / self.p.betabar, np.concatenate(w) if w else np.zeros(0), dg)
 
     # ---- the run
     def run(self) -> Result:
@@ -225,23 +267,34 @@ class QSRun:
         diag: Dict[Invar, Sub] = {}
         for I, e in sorted(d.subspaces):
             v = e.copy() if p.data_has_rescaled_energies else e / scale0
-            s = Sub(I, v, 0.0, v.copy(), len(v), len(v))
-            diag[I] = s
-        opch = {k: self._to_dev(m) for k, m in d.opch[0][0].items()}
-        ops: Dict[str, Dict[Invar, torch.Tensor]] = {}
-        for name, (kind, mats) in d.ops.items():
-            if kind in "sg":
-                ops[name] = {I1: self._to_dev(m) for (I1, I2), m in mats.items() if I1 == I2}
-        res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + sorted(ops), [])
+            diag[I] = Sub(I, v, 0.0, v.copy(), len(v), len(v), n=len(v))
+        oc = d.opch[0][0]
+        shapes = {k: m.shape for k, m in oc.items()}
+        opch = MatSet(self.dev, shapes, 1, _pack([oc], shapes))
+        mats = [{I1: m for (I1, I2), m in d.ops[name][1].items() if I1 == I2} for name in self.op_names]
+        oshapes = {I: (s.nstored, s.nstored) for I, s in diag.items()}
+        ops = MatSet(self.dev, oshapes, len(self.op_names), _pack(mats, oshapes))
+        res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + self.op_names, [])
+        meas: List[_Measure] = []
         if p.calc0:
             res.td.append(self._td(-1, diag))
-            res.custom.append(self._custom(-1, diag, ops))
+            meas.append(self._measure(-1, diag, ops))
         # diag0 has identity eigenvectors: its <||f||> and operators are used as read.
         for N in range(0, self.nmax):
-            diag, opch, ops = self._step(N, diag, opch, ops, res)
+            diag, opch, ops = self._step(N, diag, opch, ops, res, meas)
+        # one device->host copy of all measured diagonals
+        if meas:
+            host = torch.cat([m.diag.reshape(-1) for m in meas]).cpu().numpy()
+            k = 0
+            for m in meas:
+                nst = len(m.weights)
+                dg = host[k:k + m.diag.numel()].reshape(len(self.op_names), nst)
+                k += m.diag.numel()
+                Z = float(np.sum(m.weights))
+                res.custom.append([m.T] + [float(np.sum(m.weights * dg[o])) / Z for o in range(len(self.op_names))])
         return res
 
-    def _step(self, N: int, prev: Dict[Invar, Sub], opch, ops, res: Result):
+    def _step(self, N: int, prev: Dict[Invar, Sub], opch: MatSet, ops: MatSet, res: Result, meas: List[_Measure]):
         p, d = self.p, self.d
         last = N == self.nmax - 1
         scale = self.scale(N)
@@ -269,57 +322,55 @@ class QSRun:
         Hbuf = torch.empty(int(moff[-1]), dtype=torch.float64, device=self.dev)
         Vbuf = torch.empty(int(moff[-1]), dtype=torch.float64, device=self.dev)
         Ebuf = torch.empty(int(voff[-1]), dtype=torch.float64, device=self.dev)
-        H = [Hbuf[moff[b]:moff[b + 1]].view(ns[b], ns[b]) for b in range(nb)]
-        V = [Vbuf[moff[b]:moff[b + 1]].view(ns[b], ns[b]) for b in range(nb)]
-        E = [Ebuf[voff[b]:voff[b + 1]] for b in range(nb)]
+        Hp = [Hbuf.data_ptr() + 8 * int(x) for x in moff[:-1]]
+        Vp = [Vbuf.data_ptr() + 8 * int(x) for x in moff[:-1]]
+        Ep = [Ebuf.data_ptr() + 8 * int(x) for x in voff[:-1]]
 
         # corrected ancestor energies on the device (one copy)
-        pkeys = [I for I in prev if prev[I].nstored > 0]
-        poff = {}
-        flat = []
-        o = 0
-        for I in pkeys:
-            poff[I] = o
-            flat.append(prev[I].corr[:prev[I].nstored])
-            o += prev[I].nstored
-        pcorr = self._to_dev(np.concatenate(flat)) if flat else None
+        poff, flat, o = {}, [], 0
+        for I, s in prev.items():
+            if s.nstored:
+                poff[I] = o
+                flat.append(s.corr[:s.nstored])
+                o += s.nstored
+        pcorr = self._h2d(np.concatenate(flat))
+        pbase = pcorr.data_ptr()
 
         # Hamiltonian pieces: hamiltonian() + SymmetryQS::make_matrix
-        pieces: List[HPiece] = []
+        rows = []
         xi, zeta = d.xi[0], d.zeta[0]
         for b, (I, dims, anc) in enumerate(tasks):
-            offs = np.concatenate([[0], np.cumsum(dims)]).astype(int)
+            offs = [0, dims[0], dims[0] + dims[1], dims[0] + dims[1] + dims[2]]
             for i in range(qs.COMBS):
                 if dims[i]:
-                    src = pcorr.data_ptr() + 8 * poff[anc[i]]
-                    pieces.append(HPiece(b, NRG_HP_DIAG, int(offs[i]), int(offs[i]), dims[i], dims[i], 0, 0, 0,
-                                         src, self.sqrt_lambda, 0.0))
+                    rows.append((b, NRG_HP_DIAG, offs[i], offs[i], dims[i], dims[i], 0, 0, 0,
+                                 pbase + 8 * poff[anc[i]], self.sqrt_lambda, 0.0))
             ss = I[1]
             for (i, j, ch, fn) in qs.OFFDIAG:
                 if not (dims[i - 1] and dims[j - 1]):
                     continue
                 factor = fn(ss) * xi[N]
                 key = (anc[i - 1], anc[j - 1])
-                if key not in opch:
+                if key not in opch.loc:
                     raise RuntimeError(f"offdiag_function(): matrix not found {i} {j} {ch} 0")
-                mat = opch[key]
-                if tuple(mat.shape) != (dims[i - 1], dims[j - 1]):
+                _, r, c = opch.loc[key]
+                if (r, c) != (dims[i - 1], dims[j - 1]):
                     raise AssertionError("qq.rmax(i-1) == size1(mat) && qq.rmax(j-1) == size2(mat)")
                 fs = factor / scale
                 if i > j:
-                    pieces.append(HPiece(b, NRG_HP_BLOCK, int(offs[j - 1]), int(offs[i - 1]), dims[j - 1],
-                                         dims[i - 1], 1, 0, mat.stride(0), mat.data_ptr(), fs, 0.0))
+                    rows.append((b, NRG_HP_BLOCK, offs[j - 1], offs[i - 1], dims[j - 1], dims[i - 1], 1, 0, c,
+                                 opch.ptr(key), fs, 0.0))
                 else:
-                    pieces.append(HPiece(b, NRG_HP_BLOCK, int(offs[i - 1]), int(offs[j - 1]), dims[i - 1],
-                                         dims[j - 1], 0, 0, mat.stride(0), mat.data_ptr(), fs, 0.0))
+                    rows.append((b, NRG_HP_BLOCK, offs[i - 1], offs[j - 1], dims[i - 1], dims[j - 1], 0, 0, c,
+                                 opch.ptr(key), fs, 0.0))
             for (i, ch, number) in qs.DIAG:
                 if dims[i - 1]:
                     shift = zeta[N + 1] * (number - 1.0 * qs.AVGOCCUP) / scale
-                    pieces.append(HPiece(b, NRG_HP_DIAG, int(offs[i - 1]), int(offs[i - 1]), dims[i - 1],
-                                         dims[i - 1], 0, 0, 0, None, 0.0, shift))
-        self._assemble(ns, H, pieces)
+                    rows.append((b, NRG_HP_DIAG, offs[i - 1], offs[i - 1], dims[i - 1], dims[i - 1], 0, 0, 0, 0,
+                                 0.0, shift))
+        hamiltonian_batch(ns, Hp, np.array(rows, dtype=HPIECE_DTYPE), self.ctx, self.stream)
 
-        info = diag_batch_device(H, E, V, self.ctx, self.stream)
+        info = self._diagonalise(ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff)
         if np.any(info != 0):
             b = int(np.nonzero(info)[0][0])
             raise RuntimeError(f"dsyev failed. INFO={int(info[b])} (subspace {tasks[b][0]})")
@@ -327,19 +378,28 @@ class QSRun:
 
         diag: Dict[Invar, Sub] = {}
         for b, (I, dims, anc) in enumerate(tasks):
-            offs = [int(x) for x in np.concatenate([[0], np.cumsum(dims)])[:-1]]
-            diag[I] = Sub(I, evals[voff[b]:voff[b + 1]].copy(), dims=list(dims), offs=offs, vec=V[b],
+            offs = [0, dims[0], dims[0] + dims[1], dims[0] + dims[1] + dims[2]]
+            diag[I] = Sub(I, evals[voff[b]:voff[b + 1]], dims=list(dims), offs=offs, vptr=Vp[b], n=ns[b],
                           nstored=ns[b])
         # do_diag: Egs subtraction, splitting correction, truncation (c++/core.hpp:141-143)
-        Egs = min(s.values[0] for s in diag.values())
+        Egs = min(float(s.values[0]) for s in diag.values())  # Egs_subtraction (c++/eigen.hpp:321-333)
         for s in diag.values():
             s.shift = Egs
-        allrel = np.sort(np.concatenate([s.values - s.shift for s in diag.values()]))
+            s.corr = s.values - Egs
+        allrel = np.sort(np.concatenate([s.corr for s in diag.values()]))
         cmap = cluster_mapping(allrel, p.fixeps)
-        for s in diag.values():
-            r = s.values - s.shift
-            s.corr = np.array([cmap.get(float(x), float(x)) for x in r]) if cmap else r
-        allcorr = np.sort(np.concatenate([s.corr for s in diag.values()]))
+        if cmap:
+            keys = np.array(list(cmap.keys()))
+            for s in diag.values():
+                hit = np.isin(s.corr, keys)
+                if np.any(hit):
+                    c = s.corr.copy()
+                    for k in np.nonzero(hit)[0]:
+                        c[k] = cmap[float(c[k])]
+                    s.corr = c
+            allcorr = np.sort(np.concatenate([s.corr for s in diag.values()]))
+        else:
+            allcorr = allrel
         Emax = highest_retained_energy(allcorr, p)
         keep_all = last and p.lastall
         for s in diag.values():
@@ -347,85 +407,76 @@ class QSRun:
 
         # after_diag (c++/core.hpp:193-230)
         res.td.append(self._td(N, diag))
-        new_ops = None
+        new_ops = ops
         if p.strategy == "all":
             new_ops = self._recalc_singlets(diag, ops)
-            res.custom.append(self._custom(N, diag, new_ops))
+            meas.append(self._measure(N, diag, new_ops))
         for s in diag.values():
             s.nstored = s.nkept  # truncate_perform
         new_opch = opch if last else self._recalc_irreducible(diag)
         if p.strategy == "kept":
             new_ops = self._recalc_singlets(diag, ops)
-            res.custom.append(self._custom(N, diag, new_ops))
+            meas.append(self._measure(N, diag, new_ops))
+        self._keep = (Vbuf,)  # eigenvectors stay valid while the step's matrices are in use
         return diag, new_opch, new_ops
 
-    def _assemble(self, ns: List[int], H: List[torch.Tensor], pieces: List[HPiece]) -> None:
-        nb = len(ns)
-        n = (C.c_int * nb)(*ns)
-        Hp = (C.c_void_p * nb)(*[h.data_ptr() for h in H])
-        arr = (HPiece * len(pieces))(*pieces)
-        rc = self.ctx.lib.nrg_hamiltonian_batch(self.ctx.ptr, nb, n, Hp, len(pieces), arr, _stream_ptr(self.stream))
-        if rc < 0:
-            raise NRGError(rc, "nrg_hamiltonian_batch")
+    def _diagonalise(self, ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff) -> np.ndarray:
+        """All blocks of the step in one batched call (diagonalisations, c++/core.hpp:113-120)."""
+        return diag_batch_ptrs(ns, Hp, Ep, Vp, self.ctx, self.stream)
 
-    def _recalc_irreducible(self, diag: Dict[Invar, Sub]) -> Dict[Tuple[Invar, Invar], torch.Tensor]:
+    def _recalc_irreducible(self, diag: Dict[Invar, Sub]) -> MatSet:
         """SymmetryQS::recalc_irreduc with recalc_f (c++/recalc.hpp:52-76): <I1||f||Ip> over the
         kept states, one batched GEMM call for the whole step."""
         plan = []
-        total = 0
         for Ip, sp in diag.items():
             for dq, table in qs.RECALC_F:
                 I1 = (Ip[0] + dq[0], Ip[1] + dq[1])
-                if I1 not in diag:
+                s1 = diag.get(I1)
+                if s1 is None or not (s1.nstored and sp.nstored):
                     continue
-                s1 = diag[I1]
-                if not (s1.nstored and sp.nstored):
-                    continue
-                plan.append((I1, Ip, table, total))
-                total += s1.nstored * sp.nstored
-        buf = torch.zeros(max(total, 1), dtype=torch.float64, device=self.dev)
-        out: Dict[Tuple[Invar, Invar], torch.Tensor] = {}
-        terms = []
-        for I1, Ip, table, off in plan:
+                plan.append((I1, Ip, table))
+        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan})
+        rows = []
+        for I1, Ip, table in plan:
             s1, sp = diag[I1], diag[Ip]
-            f = buf[off:off + s1.nstored * sp.nstored].view(s1.nstored, sp.nstored)
-            out[(I1, Ip)] = f
+            M = out.ptr((I1, Ip))
             for i1, ip, fn in table:
-                A = s1.block(i1 - 1, s1.nstored)
-                B = sp.block(ip - 1, sp.nstored)
-                if A.shape[1] == 0 or B.shape[1] == 0:
+                k = s1.dims[i1 - 1]
+                if k == 0 or sp.dims[ip - 1] == 0:
                     continue
-                terms.append(gemm3(f, fn(Ip[1]), A, None, B))
-        if terms:
-            gemm3_batch(terms, False, self.ctx, self.stream)
+                if k != sp.dims[ip - 1]:
+                    raise AssertionError("size2(A) == size2(B)")  # product, c++/numerics_ublas.hpp:112
+                rows.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, 0, 0,
+                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, fn(Ip[1])))
+        if rows:
+            gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
         return out
 
-    def _recalc_singlets(self, diag: Dict[Invar, Sub], ops) -> Dict[str, Dict[Invar, torch.Tensor]]:
+    def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet) -> MatSet:
         """recalc_singlet (c++/symmetry.hpp:185-200) through recalc_general
-        (c++/recalc.hpp:82-108) for every singlet operator over the stored states."""
-        out: Dict[str, Dict[Invar, torch.Tensor]] = {}
-        total = sum(len(ops) * s.nstored * s.nstored for s in diag.values())
-        buf = torch.zeros(max(total, 1), dtype=torch.float64, device=self.dev)
-        terms = []
-        off = 0
-        for name in sorted(ops):
-            cold = ops[name]
-            cnew = {}
-            for I, s in diag.items():
-                m = buf[off:off + s.nstored * s.nstored].view(s.nstored, s.nstored)
-                off += s.nstored * s.nstored
-                cnew[I] = m
-                if s.nstored == 0:
+        (c++/recalc.hpp:82-108) for every singlet operator over the stored states: the terms of
+        one operator are built once and replicated over the operators (operator-major)."""
+        out = MatSet(self.dev, {I: (s.nstored, s.nstored) for I, s in diag.items()}, len(self.op_names))
+        base = []
+        for I, s in diag.items():
+            k = s.nstored
+            if k == 0:
+                continue
+            M = out.ptr(I)
+            for i, a in enumerate(qs.ancestors(I)):
+                w = s.dims[i]
+                if w == 0 or not qs.allowed(a) or a not in cold.loc:
                     continue
-                for i, a in enumerate(qs.ancestors(I)):
-                    if not qs.allowed(a) or a not in cold or s.dims[i] == 0:
-                        continue
-                    A = s.block(i, s.nstored)
-                    O = cold[a][:s.dims[i], :s.dims[i]]  # trimmed to the kept ancestor states
-                    terms.append(gemm3(m, 1.0, A, O, A))
-            out[name] = cnew
-        if terms:
-            gemm3_batch(terms, False, self.ctx, self.stream)
+                A = s.vptr + 8 * s.offs[i]
+                _, r, c = cold.loc[a]
+                base.append((M, k, A, s.n, cold.ptr(a), c, A, s.n, k, k, w, w, 0, 1, 1.0))
+        if base and self.op_names:
+            b = np.array(base, dtype=GEMM3_DTYPE)
+            t = np.tile(b, len(self.op_names))
+            op = np.repeat(np.arange(len(self.op_names), dtype=np.uint64), len(b))
+            t["M"] += op * np.uint64(8 * out.total)
+            t["O"] += op * np.uint64(8 * cold.total)
+            gemm3_batch_array(t, self.ctx, self.stream)
         return out
 
 
@@ -435,3 +486,44 @@ def run_files(param_text: str, data_text: str, device: int = 0) -> Result:
     if kv.get("symtype", "QS") != "QS":
         raise ValueError("symtype must be QS")
     return QSRun(RunParams.from_param(kv), read_data(data_text), device).run()
+
+
+def _write_table(path: str, fields: List[str], rows: List[List[float]], prec: int = 10, width: int = 16) -> None:
+    """Columns as the reference's td/custom files print them (c++/outfield.hpp)."""
+    with open(path, "w") as f:
+        f.write("#" + "".join(f"{k:>{width}} " for k in fields).rstrip(" ") + " \n")
+        for r in rows:
+            f.write(" " + "".join(f"{v:>{width}.{prec}g} " for v in r) + "\n")
+
+
+def main(argv=None) -> int:
+    """python -m nrgljubljana_b200.nrg_run DIR [--out OUT] [--repeat K]: run DIR/param with
+    DIR/data on the GPU and write OUT/td and OUT/custom (default OUT = DIR)."""
+    import argparse
+    import os
+    import time
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("dir")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--repeat", type=int, default=1, help="run K times (timing); the last run is written")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    param = open(os.path.join(a.dir, "param")).read()
+    data = open(os.path.join(a.dir, "data")).read()
+    kv = parse_param(param)
+    p, d = RunParams.from_param(kv), read_data(data)
+    res = None
+    for k in range(max(1, a.repeat)):
+        t0 = time.perf_counter()
+        res = QSRun(p, d, a.device).run()
+        torch.cuda.synchronize()
+        print(f"run {k}: {d.nmax} steps in {time.perf_counter() - t0:.3f} s", flush=True)
+    out = a.out or a.dir
+    os.makedirs(out, exist_ok=True)
+    _write_table(os.path.join(out, "td"), res.td_fields, res.td)
+    _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

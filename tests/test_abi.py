@@ -66,3 +66,30 @@ def test_diag_argument_errors(lib):
     ptrs = (C.c_void_p * 1)()
     info = (C.c_int * 1)()
     assert lib.nrg_diag_batch(None, 1, n, ptrs, ptrs, ptrs, info, None) == -1
+
+
+def test_descriptor_layouts_match_the_header(tmp_path):
+    """The ctypes structures and numpy record types the host side builds descriptors with
+    have the byte layout the C compiler gives the header's structs."""
+    import ctypes as C
+    import subprocess
+    from nrgljubljana_b200._lib import GEMM3_DTYPE, HPIECE_DTYPE, Gemm3, HPiece
+    src = tmp_path / "layout.c"
+    fields = {"nrg_gemm3": [f[0] for f in Gemm3._fields_], "nrg_hpiece": [f[0] for f in HPiece._fields_]}
+    body = ['#include <stdio.h>', '#include <stddef.h>', '#include "nrg_b200.h"', 'int main(void) {']
+    for st, names in fields.items():
+        body.append(f'printf("%zu\\n", sizeof({st}));')
+        body += [f'printf("%zu\\n", offsetof({st}, {n}));' for n in names]
+    body.append("return 0; }")
+    src.write_text("\n".join(body))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = []
+    for S, dt in ((Gemm3, GEMM3_DTYPE), (HPiece, HPIECE_DTYPE)):
+        assert dt.itemsize == C.sizeof(S)
+        want.append(C.sizeof(S))
+        for name, _ in S._fields_:
+            assert dt.fields[name][1] == getattr(S, name).offset
+            want.append(getattr(S, name).offset)
+    assert got == want
