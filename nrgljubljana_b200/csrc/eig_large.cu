@@ -527,6 +527,120 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
   if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
 }
 
+// ---------------------------------------------------------------- mid-size tridiagonalisation
+// Blocks with kSmallMaxN < n <= kMidMaxN: the whole lower triangle fits in shared memory,
+// packed by columns (column j holds rows j..n-1 at pcol(j)), so the unblocked Householder
+// reduction runs without touching HBM or L2 after the first read of H. Output as
+// tridiag_kernel: d, e, tau, and v_k in row k of W1 (unit at k+1, zeros from the start of
+// its back-transform panel up to k).
+constexpr int kMidMaxN = 224;
+constexpr int kMidThreads = 512;
+
+NRG_DEV int pcol(int j, int n) { return j * n - (j * (j - 1)) / 2; }
+
+__global__ void __launch_bounds__(kMidThreads) tridiag_smem_kernel(const LargeBlock* __restrict__ blocks) {
+  extern __shared__ __align__(16) double sm[];
+  const LargeBlock B = blocks[blockIdx.x];
+  const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  const int tot = n * (n + 1) / 2;
+  double* P = sm;
+  double* v = P + tot;
+  double* w = v + n;
+  double* red = w + n;  // 64 (two halves for block_sum_1b)
+  int phase = 0;
+  // column j of the lower triangle is row j of H from the diagonal on (row-major upper)
+  for (int j = warp; j < n; j += nwarps) {
+    const double* src = B.H + (size_t)j * n;
+    double* dst = P + pcol(j, n) - j;
+    for (int i = j + lane; i < n; i += 32) dst[i] = src[i];
+  }
+  __syncthreads();
+  double* A = B.W1;
+  for (int k = 0; k < n - 2; k++) {
+    const int ck = pcol(k, n) - k;  // P[ck + i] = A(i, k), i >= k
+    double ps = 0.0;
+    for (int i = k + 2 + tid; i < n; i += nt) {
+      const double x = P[ck + i];
+      ps = fma(x, x, ps);
+    }
+    const double sigma = block_sum_1b(ps, red, phase);
+    const double alpha = P[ck + k + 1];
+    double tau = 0.0, beta = alpha, scale = 1.0;
+    if (sigma > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+      tau = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      const double vi = (i == k + 1) ? 1.0 : P[ck + i] * scale;
+      v[i] = vi;
+      A[(size_t)k * ld + i] = vi;
+    }
+    const int kb0 = (k / NBT) * NBT;
+    for (int i = kb0 + 1 + tid; i <= k; i += nt) A[(size_t)k * ld + i] = 0.0;
+    if (tid == 0) {
+      B.d[k] = P[ck + k];
+      B.e[k] = beta;
+      B.tau[k] = tau;
+    }
+    __syncthreads();
+    if (tau == 0.0) continue;  // uniform: every thread computed the same sigma
+    // w = tau * A22 v over rows/columns k+1..n-1; thread i reads row i left of the
+    // diagonal and column i from the diagonal down: n-k-1 entries for every i
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      double s0 = 0.0, s1 = 0.0;
+      int addr = pcol(k + 1, n) + (i - (k + 1));  // A(i, k+1)
+      for (int c = k + 1; c < i; c++) {
+        s0 = fma(P[addr], v[c], s0);
+        addr += n - c - 1;
+      }
+      const int ci = pcol(i, n) - i;
+      for (int r = i; r < n; r++) s1 = fma(P[ci + r], v[r], s1);
+      w[i] = tau * (s0 + s1);
+    }
+    __syncthreads();
+    double pp = 0.0;
+    for (int i = k + 1 + tid; i < n; i += nt) pp = fma(w[i], v[i], pp);
+    const double Kc = 0.5 * tau * block_sum_1b(pp, red, phase);
+    for (int i = k + 1 + tid; i < n; i += nt) w[i] -= Kc * v[i];
+    __syncthreads();
+    // rank-2 update of the trailing triangle, contiguous from pcol(k+1) to the end
+    {
+      int j = k + 1, off = tid;
+      while (j < n && off >= n - j) {
+        off -= n - j;
+        j++;
+      }
+      int p = pcol(k + 1, n) + tid;
+      while (j < n) {
+        const int i = j + off;
+        P[p] -= v[i] * w[j] + w[i] * v[j];
+        p += nt;
+        off += nt;
+        while (j < n && off >= n - j) {
+          off -= n - j;
+          j++;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const int c2 = pcol(n - 2, n);
+    B.d[n - 2] = P[c2];
+    B.e[n - 2] = P[c2 + 1];
+    B.d[n - 1] = P[pcol(n - 1, n)];
+    B.e[n - 1] = 0.0;
+    B.tau[n - 2] = 0.0;
+    B.tau[n - 1] = 0.0;
+  }
+  __syncthreads();
+  int bad = 0;
+  for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
+  if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
+}
+
 // ---------------------------------------------------------------- divide and conquer: leaves
 __global__ void __launch_bounds__(128) dc_leaf_kernel(const LargeBlock* __restrict__ blocks,
                                                       const DcLeaf* __restrict__ leaves) {
@@ -880,39 +994,57 @@ __global__ void __launch_bounds__(256) dc_secular_kernel(const LargeBlock* __res
 }
 
 // ---------------------------------------------------------------- divide and conquer: vectors
-// z-hat by the Gu-Eisenstat product formula, then u_j(g) = zhat_g / (d_g - lambda_j),
-// normalised, written over Dt in place (same grouped column order).
-__global__ void __launch_bounds__(512) dc_vectors_kernel(const LargeBlock* __restrict__ blocks,
-                                                         const DcNode* __restrict__ nodes,
-                                                         const DcState* __restrict__ states) {
-  extern __shared__ __align__(16) double zh[];
+// z-hat by the Gu-Eisenstat product formula (into dgrp, free after the secular solve), then
+// u_j(g) = zhat_g / (d_g - lambda_j), normalised, written over Dt in place (same grouped
+// column order). Both kernels spread a node over gridDim.y CTAs.
+__global__ void __launch_bounds__(256) dc_zhat_kernel(const LargeBlock* __restrict__ blocks,
+                                                      const DcNode* __restrict__ nodes,
+                                                      const DcState* __restrict__ states) {
   const DcNode nd = nodes[blockIdx.x];
   const DcState st = states[blockIdx.x];
   const LargeBlock B = blocks[nd.blk];
   const int K = st.K;
-  const int n = B.n, a = nd.a, tid = threadIdx.x, nt = blockDim.x;
-  {  // deflated rows are final: grouped copy (W2) back to the node's rows a+K.. (W1)
-    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-    for (int r = a + K + warp; r < nd.b; r += nwarps)
-      for (int col = a + lane; col < nd.b; col += 32) B.H[(size_t)r * n + col] = B.W2[(size_t)r * n + col];
-  }
-  if (K == 0) return;
+  const int n = B.n, a = nd.a;
   const double* ds = B.dsort + a;
   const double* zg = B.zgrp + a;
   const int* rk = B.rank + a;
-  double* Dt = B.evecs + (size_t)a * n + a;
+  const double* Dt = B.evecs + (size_t)a * n + a;
   const double rho = st.rho;
-  for (int g = tid; g < K; g += nt) {
+  for (int g = blockIdx.y * blockDim.x + threadIdx.x; g < K; g += gridDim.y * blockDim.x) {
     const int i = rk[g];
     const double di = ds[i];
-    double prod = -Dt[(size_t)(K - 1) * n + g] / rho;
-    for (int j = 0; j < i; j++) prod *= -Dt[(size_t)j * n + g] / (ds[j] - di);
-    for (int j = i; j < K - 1; j++) prod *= -Dt[(size_t)j * n + g] / (ds[j + 1] - di);
-    zh[g] = copysign(sqrt(fabs(prod)), zg[g]);
+    double p0 = -Dt[(size_t)(K - 1) * n + g] / rho, p1 = 1.0;
+    int j = 0;
+    for (; j + 1 < i; j += 2) {  // two independent product chains
+      p0 *= -Dt[(size_t)j * n + g] / (ds[j] - di);
+      p1 *= -Dt[(size_t)(j + 1) * n + g] / (ds[j + 1] - di);
+    }
+    for (; j < i; j++) p0 *= -Dt[(size_t)j * n + g] / (ds[j] - di);
+    for (; j + 1 < K - 1; j += 2) {
+      p0 *= -Dt[(size_t)j * n + g] / (ds[j + 1] - di);
+      p1 *= -Dt[(size_t)(j + 1) * n + g] / (ds[j + 2] - di);
+    }
+    for (; j < K - 1; j++) p0 *= -Dt[(size_t)j * n + g] / (ds[j + 1] - di);
+    B.dgrp[a + g] = copysign(sqrt(fabs(p0 * p1)), zg[g]);
   }
-  __syncthreads();
-  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-  for (int j = warp; j < K; j += nwarps) {
+}
+
+__global__ void __launch_bounds__(256) dc_vectors_kernel(const LargeBlock* __restrict__ blocks,
+                                                         const DcNode* __restrict__ nodes,
+                                                         const DcState* __restrict__ states) {
+  const DcNode nd = nodes[blockIdx.x];
+  const DcState st = states[blockIdx.x];
+  const LargeBlock B = blocks[nd.blk];
+  const int K = st.K;
+  const int n = B.n, a = nd.a, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wg = blockIdx.y * (blockDim.x >> 5) + warp, wstride = gridDim.y * (blockDim.x >> 5);
+  // deflated rows are final: grouped copy (W2) back to the node's rows a+K.. (H)
+  for (int r = a + K + wg; r < nd.b; r += wstride)
+    for (int col = a + lane; col < nd.b; col += 32) B.H[(size_t)r * n + col] = B.W2[(size_t)r * n + col];
+  const double* zh = B.dgrp + a;
+  double* Dt = B.evecs + (size_t)a * n + a;
+  for (int j = wg; j < K; j += wstride) {
     double* row = Dt + (size_t)j * n;
     double ss = 0.0;
     for (int g = lane; g < K; g += 32) {
@@ -1100,6 +1232,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
       for (int bi = 0; bi < nb; bi++) {
         const LargeBlock& L = blk[bi];
+        if (L.n <= kMidMaxN) continue;  // reduced in shared memory, no bulk copies
         const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
         const cuuint64_t strides[1] = {(cuuint64_t)L.ldp * sizeof(double)};
         const cuuint32_t box[2] = {(cuuint32_t)kSlabRows, 8u};
@@ -1196,16 +1329,28 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     char* dbase = static_cast<char*>(c->desc);
     const LargeBlock* dblk = reinterpret_cast<const LargeBlock*>(dbase + blk_off);
 
-    // ---- 1. tridiagonalisation
+    // ---- 1. tridiagonalisation: blocks beyond kMidMaxN (sorted first) stream through TMA,
+    //         the rest are reduced in shared memory
     {
-      const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
-                                                   (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
-      NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      PhaseScope ps(c, kPhTridiag, s, 2);
-      pack_lower_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
-      NRG_CK(cudaGetLastError());
-      tridiag_kernel<<<nb, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
-      NRG_CK(cudaGetLastError());
+      int nbig = 0;
+      while (nbig < nb && blk[nbig].n > kMidMaxN) nbig++;
+      PhaseScope ps(c, kPhTridiag, s, (nbig ? 2 : 0) + (nb > nbig ? 1 : 0));
+      if (nbig) {
+        const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
+                                                     (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
+        NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        pack_lower_kernel<<<dim3((maxn + 7) / 8, nbig), 256, 0, s>>>(dblk);
+        NRG_CK(cudaGetLastError());
+        tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
+        NRG_CK(cudaGetLastError());
+      }
+      if (nb > nbig) {
+        const int mn = blk[nbig].n;
+        const size_t smem = sizeof(double) * ((size_t)mn * (mn + 1) / 2 + 2 * (size_t)mn + 64);
+        NRG_CK(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        tridiag_smem_kernel<<<nb - nbig, kMidThreads, smem, s>>>(dblk + nbig);
+        NRG_CK(cudaGetLastError());
+      }
     }
     // ---- 2. divide and conquer
     {
@@ -1228,17 +1373,18 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs);
         NRG_CK(cudaGetLastError());
       }
-      const int ysplit = std::max(1, std::min(16, maxN / 256));
+      // one warp per root (8 per CTA), at most 64 CTAs per node
+      const int ysplit = std::max(1, std::min(64, (maxN + 7) / 8));
       {
         PhaseScope sc(c, kPhDcSecular, s);
         dc_secular_kernel<<<dim3(nn, ysplit), 256, 0, s>>>(dblk, dn, dst);
         NRG_CK(cudaGetLastError());
       }
-      const size_t vs = sizeof(double) * (size_t)maxN;
-      NRG_CK(cudaFuncSetAttribute(dc_vectors_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vs));
       {
-        PhaseScope sc(c, kPhDcVectors, s);
-        dc_vectors_kernel<<<nn, 512, vs, s>>>(dblk, dn, dst);
+        PhaseScope sc(c, kPhDcVectors, s, 2);
+        dc_zhat_kernel<<<dim3(nn, std::max(1, (maxN + 255) / 256)), 256, 0, s>>>(dblk, dn, dst);
+        NRG_CK(cudaGetLastError());
+        dc_vectors_kernel<<<dim3(nn, ysplit), 256, 0, s>>>(dblk, dn, dst);
         NRG_CK(cudaGetLastError());
       }
       rc = launch_staged_gemm(c, lvl_gemm[h], s, kPhDcGemm);

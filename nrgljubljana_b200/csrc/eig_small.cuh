@@ -108,6 +108,14 @@ NRG_DEV void smem_form_q(const double* A, int ld, int n, const double* taus, dou
   }
 }
 
+// sqrt(f^2 + g^2) with one square root while the squares can neither overflow nor lose
+// their low bits to underflow; the scaled library hypot otherwise.
+NRG_DEV double chain_hypot(double f, double g) {
+  const double mx = fmax(fabs(f), fabs(g));
+  if (mx > 1e-140 && mx < 1e140) return sqrt(fma(f, f, g * g));
+  return hypot(f, g);
+}
+
 // Implicit-shift QL iteration (Wilkinson-type shift) on the symmetric tridiagonal matrix
 // (d, e), e[i] coupling i and i+1, e[n-1] unused. Rotations are accumulated into the
 // columns of Z (nz rows, row stride ld): on exit column r of Z is the eigenvector of d[r].
@@ -139,7 +147,7 @@ NRG_DEV int smem_ql(double* d, double* e, int n, double* Z, int ld, int nz, doub
         bool under = false;
         for (int i = m - 1; i >= l; i--) {
           const double f = s * e[i], b = c * e[i];
-          r = hypot(f, g);
+          r = chain_hypot(f, g);
           e[i + 1] = r;
           if (r == 0.0) {
             d[i + 1] -= p;
@@ -148,8 +156,9 @@ NRG_DEV int smem_ql(double* d, double* e, int n, double* Z, int ld, int nz, doub
             under = true;
             break;
           }
-          s = f / r;
-          c = g / r;
+          const double ir = 1.0 / r;
+          s = f * ir;
+          c = g * ir;
           g = d[i + 1] - p;
           r = (d[i] - g) * s + 2.0 * c * b;
           p = s * r;

@@ -99,24 +99,50 @@ class Result:
 # ------------------------------------------------------------------ host bookkeeping
 def cluster_mapping(energies: np.ndarray, eps: float) -> Dict[float, float]:
     """Clusters(diag, epsilon) of c++/splitting.hpp:48-72 over the sorted energies: maps the
-    members of a split cluster to its lowest value. The loop, as in the reference, counts
-    the first element twice and never closes the last cluster."""
+    members of a split cluster to its lowest value.
+
+    The reference walks every value; a value whose gap to its predecessor is at least eps
+    always starts a new cluster, so only the runs of smaller gaps need the walk, done here
+    exactly as the reference does it. The reference's first cluster counts its first
+    element twice (which changes nothing, a one-value cluster is never split) and the last
+    cluster is never closed: a run that reaches the end of the list maps nothing for its
+    last cluster."""
     mapping: Dict[float, float] = {}
-    if len(energies) < 2 or not np.any(np.diff(energies) < eps):
-        return mapping  # every cluster is a single value: nothing to map
-    e = energies.tolist()
-    e0, i0, size = e[0], 0, 1
-    for i in range(len(e)):
-        if e[i] - e0 < eps:
-            size += 1
-        else:
-            if size > 1 and i - i0 > 1:
-                first = e[i0]
-                if any(x != first for x in e[i0 + 1:i]):
-                    for j in range(i0 + 1, i):
-                        if e[j] != first:
-                            mapping.setdefault(e[j], first)
-            e0, i0, size = e[i], i, 1
+    L = len(energies)
+    if L < 2:
+        return mapping
+    small = np.diff(energies) < eps
+    if not small.any():
+        return mapping
+    e = energies
+    idx = np.flatnonzero(small)
+    # runs of consecutive small gaps: elements a..b with gaps a..b-1 small
+    brk = np.flatnonzero(np.diff(idx) > 1)
+    starts = np.concatenate([[idx[0]], idx[brk + 1]])
+    ends = np.concatenate([idx[brk], [idx[-1]]]) + 1
+    # two-value runs (the common case: pairs split by round-off) in one pass; a pair is one
+    # cluster, closed unless it ends the list
+    pair = ends - starts == 1
+    pa, pb = starts[pair], ends[pair]
+    sel = (pb + 1 < L) & (e[pb] != e[pa])
+    for x, y in zip(e[pb[sel]].tolist(), e[pa[sel]].tolist()):
+        mapping.setdefault(x, y)
+    for a, b in zip(starts[~pair].tolist(), ends[~pair].tolist()):
+        run = e[a:b + 1].tolist()
+        e0, i0 = run[0], 0
+        for i in range(1, len(run) + 1):
+            if i < len(run) and run[i] - e0 < eps:
+                continue
+            if i == len(run) and b + 1 >= L:
+                break  # the last cluster of the list is never closed
+            if i - i0 > 1:
+                first = run[i0]
+                if any(x != first for x in run[i0 + 1:i]):
+                    for x in run[i0 + 1:i]:
+                        if x != first:
+                            mapping.setdefault(x, first)
+            if i < len(run):
+                e0, i0 = run[i], i
     return mapping
 
 
@@ -388,16 +414,18 @@ class QSRun:
             s.corr = s.values - Egs
         allrel = np.sort(np.concatenate([s.corr for s in diag.values()]))
         cmap = cluster_mapping(allrel, p.fixeps)
-        if cmap:
-            keys = np.array(list(cmap.keys()))
+        if cmap:  # Clusters::fix_it: every value found in the mapping is replaced
+            keys = np.array(sorted(cmap))
+            vals = np.array([cmap[k] for k in keys.tolist()])
+            flat = np.concatenate([s.corr for s in diag.values()])
+            pos = np.minimum(np.searchsorted(keys, flat), len(keys) - 1)
+            hit = keys[pos] == flat
+            flat = np.where(hit, vals[pos], flat)
+            o = 0
             for s in diag.values():
-                hit = np.isin(s.corr, keys)
-                if np.any(hit):
-                    c = s.corr.copy()
-                    for k in np.nonzero(hit)[0]:
-                        c[k] = cmap[float(c[k])]
-                    s.corr = c
-            allcorr = np.sort(np.concatenate([s.corr for s in diag.values()]))
+                s.corr = flat[o:o + len(s.corr)]
+                o += len(s.corr)
+            allcorr = np.sort(flat)
         else:
             allcorr = allrel
         Emax = highest_retained_energy(allcorr, p)
