@@ -343,6 +343,8 @@ def main():
     torch.cuda.empty_cache()
     if not args.no_nrg and rank == 0:
         line["nrg_run"] = nrg_run_arm(torch, local, args)
+    if not args.no_nrg and rank == 0:
+        line["serving"] = serving_arm(torch, local, line["nrg_run"])
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -378,6 +380,41 @@ NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model (U=2, Gamma=0.1, del
                 "test/c++/legacy_Himp")
 
 
+SERVE_MIX = ["legacy_Himp", "legacy_simple", "test12_Nmax", "test35_betabar", "test15_safeguard",
+             "test13_strategy_all", "test0_minimal", "test200_data_has"]
+
+
+def serving_arm(torch, device: int, single: dict) -> dict:
+    """The serving loop: (1) saturation -- 16 runs of the reference's regression inputs
+    submitted at once, one batched eigensolve per tick; (2) a Poisson stream of 32 requests
+    at a mean 4 runs/s drawn from the same inputs (seed 20261203); steps/s and p50/p99
+    latency from arrival to result."""
+    from nrgljubljana_b200.serve import Request, Server, poisson_arrivals, summary
+    base = os.path.join(ROOT, "tests", "golden", "nrg")
+    texts = {c: (open(os.path.join(base, c, "param")).read(), open(os.path.join(base, c, "data")).read())
+             for c in SERVE_MIX}
+    mix = SERVE_MIX + SERVE_MIX
+    reqs = [Request(i, *texts[c], 0.0, c) for i, c in enumerate(mix)]
+    Server(device).serve(reqs[:4], realtime=False)  # warm-up
+    torch.cuda.synchronize()
+    srv = Server(device, max_active=16)
+    t0 = time.perf_counter()
+    done = srv.serve(reqs, realtime=False)
+    sat = summary(done, time.perf_counter() - t0)
+    sat["max_blocks_per_tick"] = max(srv.blocks_per_tick)
+    rng = np.random.default_rng(SEED)
+    arr = poisson_arrivals(32, 4.0, SEED)
+    picks = [SERVE_MIX[k] for k in rng.integers(0, len(SERVE_MIX), size=32)]
+    stream = [Request(i, *texts[c], float(arr[i]), c) for i, c in enumerate(picks)]
+    srv = Server(device, max_active=16)
+    t0 = time.perf_counter()
+    done = srv.serve(stream, realtime=True)
+    poi = summary(done, time.perf_counter() - t0)
+    return {"workload": "runs of the reference's regression inputs " + ", ".join(SERVE_MIX),
+            "saturation_16_runs": sat, "poisson_4_per_s_32_requests": poi,
+            "single_run_steps_per_s": single["steps_per_s"]}
+
+
 def nrg_run_arm(torch, device: int, args) -> dict:
     """Whole NRG runs (host driver + device step core) in NRG steps/s, beside the same run
     with one cuSOLVER call per block and the CPU restatement on all host cores."""
@@ -391,13 +428,13 @@ def nrg_run_arm(torch, device: int, args) -> dict:
     ctx = context(device)
 
     class PerBlock(QSRun):
-        def _diagonalise(self, ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff):
-            for b, n in enumerate(ns):
-                h = Hbuf[moff[b]:moff[b + 1]].view(n, n)
+        def _diagonalise(self, job):
+            for b, n in enumerate(job.ns):
+                h = job.Hbuf[job.moff[b]:job.moff[b + 1]].view(n, n)
                 w, q = torch.linalg.eigh(h, UPLO="U")
-                Ebuf[voff[b]:voff[b + 1]].copy_(w)
-                Vbuf[moff[b]:moff[b + 1]].view(n, n).copy_(q.T)
-            return np.zeros(len(ns), dtype=np.int32)
+                job.Ebuf[job.voff[b]:job.voff[b + 1]].copy_(w)
+                job.Vbuf[job.moff[b]:job.moff[b + 1]].view(n, n).copy_(q.T)
+            return np.zeros(len(job.ns), dtype=np.int32)
 
     def timed(cls, reps):
         cls(p, d, device).run()  # warm-up

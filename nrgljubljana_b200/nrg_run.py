@@ -226,8 +226,29 @@ class _Measure:
     diag: torch.Tensor         # nops x states (device)
 
 
+@dataclass
+class StepJob:
+    """The blocks of one step of one run, assembled on the device and waiting for their
+    eigensolve: orders, device addresses of H / eigenvalues / eigenvectors, the buffers
+    that own them, and the subspace tasks in block order."""
+    N: int
+    tasks: list
+    ns: List[int]
+    Hp: List[int]
+    Ep: List[int]
+    Vp: List[int]
+    Hbuf: torch.Tensor
+    Ebuf: torch.Tensor
+    Vbuf: torch.Tensor
+    moff: np.ndarray
+    voff: np.ndarray
+    pcorr: torch.Tensor
+
+
 class QSRun:
-    """One NRG run (QS, one channel) on one device."""
+    """One NRG run (QS, one channel) on one device. ``run()`` does the whole run; a server
+    drives ``start``, ``begin_step``, ``end_step`` and ``finish`` itself to solve the blocks
+    of many runs in one batched call."""
 
     def __init__(self, params: RunParams, data: DataFile, device: int = 0, ctx: Optional[Context] = None):
         if data.symtype != "QS" or data.channels != 1:
@@ -287,7 +308,9 @@ class QSRun:
         return _Measure(self.scale(trueN) / self.p.betabar, np.concatenate(w) if w else np.zeros(0), dg)
 
     # ---- the run
-    def run(self) -> Result:
+    def start(self) -> None:
+        """Initial subspaces, <||f||> and operators from the data file; docalc0
+        (c++/core.hpp:251-260) measures them before the first step."""
         p, d = self.p, self.d
         scale0 = SCALE(0, p.Lambda, p.discretization, p.z, p.bandrescale)  # SCALE(Ninit)
         diag: Dict[Invar, Sub] = {}
@@ -296,33 +319,52 @@ class QSRun:
             diag[I] = Sub(I, v, 0.0, v.copy(), len(v), len(v), n=len(v))
         oc = d.opch[0][0]
         shapes = {k: m.shape for k, m in oc.items()}
-        opch = MatSet(self.dev, shapes, 1, _pack([oc], shapes))
+        self.opch = MatSet(self.dev, shapes, 1, _pack([oc], shapes))
         mats = [{I1: m for (I1, I2), m in d.ops[name][1].items() if I1 == I2} for name in self.op_names]
         oshapes = {I: (s.nstored, s.nstored) for I, s in diag.items()}
-        ops = MatSet(self.dev, oshapes, len(self.op_names), _pack(mats, oshapes))
-        res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + self.op_names, [])
-        meas: List[_Measure] = []
+        self.ops = MatSet(self.dev, oshapes, len(self.op_names), _pack(mats, oshapes))
+        self.res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + self.op_names,
+                          [])
+        self.meas: List[_Measure] = []
         if p.calc0:
-            res.td.append(self._td(-1, diag))
-            meas.append(self._measure(-1, diag, ops))
+            self.res.td.append(self._td(-1, diag))
+            self.meas.append(self._measure(-1, diag, self.ops))
         # diag0 has identity eigenvectors: its <||f||> and operators are used as read.
-        for N in range(0, self.nmax):
-            diag, opch, ops = self._step(N, diag, opch, ops, res, meas)
-        # one device->host copy of all measured diagonals
-        if meas:
-            host = torch.cat([m.diag.reshape(-1) for m in meas]).cpu().numpy()
+        self.diag = diag
+        self.N = 0
+
+    @property
+    def done(self) -> bool:
+        return self.N >= self.nmax
+
+    def run(self) -> Result:
+        """The whole run on this device (nrg_loop, c++/core.hpp:286-293)."""
+        self.start()
+        while not self.done:
+            job = self.begin_step()
+            self.end_step(job, self._diagonalise(job))
+        return self.finish()
+
+    def finish(self) -> Result:
+        """One device->host copy of all measured diagonals, then the custom rows."""
+        res = self.res
+        if self.meas:
+            host = torch.cat([m.diag.reshape(-1) for m in self.meas]).cpu().numpy()
             k = 0
-            for m in meas:
+            for m in self.meas:
                 nst = len(m.weights)
                 dg = host[k:k + m.diag.numel()].reshape(len(self.op_names), nst)
                 k += m.diag.numel()
                 Z = float(np.sum(m.weights))
                 res.custom.append([m.T] + [float(np.sum(m.weights * dg[o])) / Z for o in range(len(self.op_names))])
+        self.meas = []
         return res
 
-    def _step(self, N: int, prev: Dict[Invar, Sub], opch: MatSet, ops: MatSet, res: Result, meas: List[_Measure]):
+    def begin_step(self) -> "StepJob":
+        """Subspace structure of step N and the assembly of its block Hamiltonians on the
+        device; returns the blocks to diagonalise."""
         p, d = self.p, self.d
-        last = N == self.nmax - 1
+        N, prev, opch, res = self.N, self.diag, self.opch, self.res
         scale = self.scale(N)
         # subspace structure (c++/core.hpp:42-58, 62-70; c++/subspaces.hpp:114-121)
         new = set()
@@ -395,8 +437,14 @@ class QSRun:
                     rows.append((b, NRG_HP_DIAG, offs[i - 1], offs[i - 1], dims[i - 1], dims[i - 1], 0, 0, 0, 0,
                                  0.0, shift))
         hamiltonian_batch(ns, Hp, np.array(rows, dtype=HPIECE_DTYPE), self.ctx, self.stream)
+        return StepJob(N, tasks, ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff, pcorr)
 
-        info = self._diagonalise(ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff)
+    def end_step(self, job: "StepJob", info: np.ndarray) -> None:
+        """do_diag and after_diag (c++/core.hpp:122-230) once the step's blocks are solved."""
+        p = self.p
+        N, tasks, ns, Vp, Ebuf, voff = job.N, job.tasks, job.ns, job.Vp, job.Ebuf, job.voff
+        res, meas, opch, ops = self.res, self.meas, self.opch, self.ops
+        last = N == self.nmax - 1
         if np.any(info != 0):
             b = int(np.nonzero(info)[0][0])
             raise RuntimeError(f"dsyev failed. INFO={int(info[b])} (subspace {tasks[b][0]})")
@@ -445,12 +493,13 @@ class QSRun:
         if p.strategy == "kept":
             new_ops = self._recalc_singlets(diag, ops)
             meas.append(self._measure(N, diag, new_ops))
-        self._keep = (Vbuf,)  # eigenvectors stay valid while the step's matrices are in use
-        return diag, new_opch, new_ops
+        self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
+        self.diag, self.opch, self.ops = diag, new_opch, new_ops
+        self.N = N + 1
 
-    def _diagonalise(self, ns, Hp, Ep, Vp, Hbuf, Ebuf, Vbuf, moff, voff) -> np.ndarray:
+    def _diagonalise(self, job: "StepJob") -> np.ndarray:
         """All blocks of the step in one batched call (diagonalisations, c++/core.hpp:113-120)."""
-        return diag_batch_ptrs(ns, Hp, Ep, Vp, self.ctx, self.stream)
+        return diag_batch_ptrs(job.ns, job.Hp, job.Ep, job.Vp, self.ctx, self.stream)
 
     def _recalc_irreducible(self, diag: Dict[Invar, Sub]) -> MatSet:
         """SymmetryQS::recalc_irreduc with recalc_f (c++/recalc.hpp:52-76): <I1||f||Ip> over the

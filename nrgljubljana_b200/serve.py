@@ -1,0 +1,145 @@
+"""Serving loop: many independent NRG runs on one device, continuously batched.
+
+Requests (a ``param`` + ``data`` pair each, with an arrival time) are admitted while the
+device-memory budget and the slot limit allow; every tick, each active run builds and
+assembles its next step (``QSRun.begin_step``), the blocks of all active runs are solved in
+ONE ``nrg_diag_batch`` call, and each run finishes its step (truncation, thermodynamics,
+recalculation; ``QSRun.end_step``). Runs join and leave the batch between ticks, so a
+request that arrives while others are on the GPU starts at the next tick and overlaps
+their work. Every run's matrices stay resident in device memory for its whole life.
+
+Each block is solved by the same kernels whatever else is in the batch, so a run's result
+does not depend on the mix it was served in.
+
+There is no counterpart in the reference (one ``nrg`` process per run); this is the
+serving pattern for z-averaging, parameter sweeps and request streams.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .api import context, diag_batch_ptrs
+from .inputs import parse_param, read_data
+from .nrg_run import QSRun, Result, RunParams
+
+
+@dataclass
+class Request:
+    rid: int
+    param: str
+    data: str
+    arrival: float = 0.0  # seconds after the start of the stream
+    tag: str = ""
+
+
+@dataclass
+class Completed:
+    rid: int
+    tag: str
+    result: Result
+    arrival: float
+    admitted: float
+    done: float
+    steps: int
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def run_bytes(p: RunParams, combs: int = 4) -> int:
+    """Device bytes a run is charged at admission: the step's Hamiltonians, eigenvectors and
+    the previous step's eigenvectors, 3 x 8 B x sum of n^2, bounded by the kept states
+    spread over at least four (Q, S) sectors of combs x keep states each."""
+    states = combs * p.keep
+    return 3 * 8 * states * states // 4
+
+
+class Server:
+    def __init__(self, device: int = 0, hbm_budget: Optional[int] = None, max_active: int = 32):
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device: the server has no CPU fallback")
+        self.device = device
+        self.ctx = context(device)
+        self.stream = torch.cuda.current_stream(torch.device("cuda", device))
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(device)
+            hbm_budget = int(0.5 * free)
+        self.budget = hbm_budget
+        self.max_active = max_active
+        self.ticks = 0
+        self.blocks_per_tick: List[int] = []
+
+    def serve(self, requests: List[Request], realtime: bool = True) -> List[Completed]:
+        """Serve the stream; with realtime=False every request is taken as arrived at once."""
+        pending = sorted(requests, key=lambda r: (r.arrival if realtime else 0.0, r.rid))
+        active: List[tuple] = []  # (request, run, charged bytes, admitted time)
+        out: List[Completed] = []
+        used = 0
+        t0 = time.perf_counter()
+        while pending or active:
+            now = time.perf_counter() - t0
+            # admission: arrived, a free slot, and room in the budget (a run larger than the
+            # whole budget is admitted alone)
+            while pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active:
+                req = pending[0]
+                params = RunParams.from_param(parse_param(req.param))
+                need = run_bytes(params)
+                if active and used + need > self.budget:
+                    break
+                pending.pop(0)
+                run = QSRun(params, read_data(req.data), self.device, self.ctx)
+                run.start()
+                used += need
+                active.append((req, run, need, now))
+            if not active:
+                wait = pending[0].arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.05))
+                continue
+            # one tick: every active run advances one NRG step
+            jobs = [run.begin_step() for _, run, _, _ in active]
+            ns, Hp, Ep, Vp = [], [], [], []
+            for j in jobs:
+                ns += j.ns
+                Hp += j.Hp
+                Ep += j.Ep
+                Vp += j.Vp
+            info = diag_batch_ptrs(ns, Hp, Ep, Vp, self.ctx, self.stream)
+            self.ticks += 1
+            self.blocks_per_tick.append(len(ns))
+            o = 0
+            for (_, run, _, _), j in zip(active, jobs):
+                run.end_step(j, info[o:o + len(j.ns)])
+                o += len(j.ns)
+            still = []
+            for req, run, need, adm in active:
+                if run.done:
+                    res = run.finish()
+                    torch.cuda.synchronize(self.device)
+                    out.append(Completed(req.rid, req.tag, res, req.arrival if realtime else 0.0, adm,
+                                         time.perf_counter() - t0, run.nmax))
+                    used -= need
+                else:
+                    still.append((req, run, need, adm))
+            active = still
+        return out
+
+
+def poisson_arrivals(n: int, rate: float, seed: int) -> np.ndarray:
+    """Arrival times of a Poisson stream of n requests with the given mean rate (1/s)."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def summary(done: List[Completed], wall: float) -> dict:
+    lat = np.array([c.latency for c in done])
+    steps = sum(c.steps for c in done)
+    return {"requests": len(done), "steps": steps, "wall_s": wall, "steps_per_s": steps / wall,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean())}

@@ -1,0 +1,63 @@
+"""Serving loop (nrgljubljana_b200.serve): many runs continuously batched into one
+eigensolve per tick. Each run's result must be the same alone and in the mix."""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden", "nrg")
+MIX = ["test0_minimal", "legacy_simple", "test13_strategy_all", "test15_safeguard", "test35_betabar",
+       "legacy_Himp", "test12_Nmax", "test200_data_has"]
+
+
+def read(case, name):
+    with open(os.path.join(GOLD, case, name)) as f:
+        return f.read()
+
+
+def test_poisson_arrivals_and_budget_rule():
+    from nrgljubljana_b200.nrg_run import RunParams
+    from nrgljubljana_b200.serve import poisson_arrivals, run_bytes
+    a = poisson_arrivals(200, 4.0, 7)
+    assert np.all(np.diff(a) > 0) and np.array_equal(a, poisson_arrivals(200, 4.0, 7))
+    assert abs(200 / a[-1] - 4.0) < 1.0
+    assert run_bytes(RunParams(keep=2000)) == 4 * run_bytes(RunParams(keep=1000))
+
+
+@pytest.fixture(scope="module")
+def alone():
+    from nrgljubljana_b200.nrg_run import run_files
+    return {c: run_files(read(c, "param"), read(c, "data")) for c in MIX}
+
+
+def same(a, b):
+    return (a.td_fields == b.td_fields and a.custom_fields == b.custom_fields
+            and np.array_equal(np.array(a.td), np.array(b.td)) and np.array_equal(np.array(a.custom), np.array(b.custom)))
+
+
+@pytest.mark.gpu
+def test_mix_equals_alone(alone):
+    from nrgljubljana_b200.serve import Request, Server
+    reqs = [Request(i, read(c, "param"), read(c, "data"), 0.0, c) for i, c in enumerate(MIX + MIX[::-1])]
+    srv = Server(max_active=16)
+    done = srv.serve(reqs, realtime=False)
+    assert sorted(d.rid for d in done) == list(range(len(reqs)))
+    for d in done:
+        assert same(d.result, alone[d.tag]), d.tag
+    single = max(max(r.blocks_per_step) for r in alone.values())
+    assert max(srv.blocks_per_tick) > single  # the runs shared batched eigensolves
+
+
+@pytest.mark.gpu
+def test_staggered_arrivals_and_tight_budget(alone):
+    """Requests arriving while others run join the batch at the next tick; a budget that
+    fits one run at a time serialises them; results are unchanged either way."""
+    from nrgljubljana_b200.serve import Request, Server
+    reqs = [Request(i, read(c, "param"), read(c, "data"), 0.02 * i, c) for i, c in enumerate(MIX)]
+    for srv in (Server(max_active=8), Server(hbm_budget=1, max_active=8)):
+        done = srv.serve(reqs, realtime=True)
+        assert len(done) == len(reqs)
+        for d in done:
+            assert same(d.result, alone[d.tag]), d.tag
+            assert d.done >= d.admitted >= d.arrival - 1e-9
