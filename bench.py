@@ -374,10 +374,29 @@ def per_block_arm(torch, pristine, sizes, offs, dev, target_flop: float = 1.5e12
             "sample": f"{len(idx)} of {len(sizes)} blocks (every {stride}th in size order)", "seconds": t}
 
 
-NRG_CASE = "legacy_Himp"
-NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model (U=2, Gamma=0.1, delta=0), Lambda=2 (Yoshida), "
-                "Nmax=40, keep=1000, keepenergy=8, 6 singlet operators: the reference's regression input "
-                "test/c++/legacy_Himp")
+C0_PARAM = """[param]
+symtype=QS
+model=SIAM
+U=1.0
+Gamma=0.04
+delta=0
+band=flat
+discretization=Z
+Lambda=2
+z=1
+keep=1000
+keepenergy=10
+T=1e-8
+ops=n_d
+"""
+NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delta=0), Gamma=0.04, flat band, "
+                "Lambda=2 (Z), z=1, Nmax=40, keep=1000, keepenergy=10, T=1e-8, operator n_d; input generated "
+                "by nrgljubljana_b200.datagen")
+
+
+def c0_inputs():
+    from nrgljubljana_b200.datagen import siam_qs
+    return C0_PARAM, siam_qs(1.0, 0.0, 0.04, 2.0, 40, 1.0, "Z", ops=["n_d"])
 
 
 SERVE_MIX = ["legacy_Himp", "legacy_simple", "test12_Nmax", "test35_betabar", "test15_safeguard",
@@ -421,9 +440,7 @@ def nrg_run_arm(torch, device: int, args) -> dict:
     from nrgljubljana_b200 import context
     from nrgljubljana_b200.inputs import parse_param, read_data
     from nrgljubljana_b200.nrg_run import QSRun, RunParams
-    base = os.path.join(ROOT, "tests", "golden", "nrg", NRG_CASE)
-    param = open(os.path.join(base, "param")).read()
-    data = open(os.path.join(base, "data")).read()
+    param, data = c0_inputs()
     p, d = RunParams.from_param(parse_param(param)), read_data(data)
     ctx = context(device)
 

@@ -17,6 +17,7 @@
 //   3. sort of the eigenvalues and row permutation of the eigenvectors.
 //   4. back-transform with the compact-WY form of Q, panels of NBT reflectors, as GEMMs.
 // Eigenvectors are kept as ROWS throughout (Zt = Z^T), the layout of the output.
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -641,6 +642,180 @@ __global__ void __launch_bounds__(kMidThreads) tridiag_smem_kernel(const LargeBl
   if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
 }
 
+// ---------------------------------------------------------------- cluster tridiagonalisation
+// Blocks with kMidMaxN < n <= kClusterMaxN: the packed lower triangle is spread over the
+// shared memory of a thread-block cluster of C CTAs (column j lives in CTA j mod C) and the
+// unblocked Householder reduction runs there; the CTAs combine their partial mat-vec
+// products through distributed shared memory (plain loads and stores to the other CTAs'
+// shared memory, no bulk copies). Per column: the owner of column k builds v and sends it
+// to every CTA; each CTA forms its part of A v (rows: its columns left of the diagonal;
+// columns: from the diagonal down, one warp each, so the sums are in a fixed order); each
+// CTA reduces one slice of rows over the cluster into w and sends it out; each CTA updates
+// its own columns. Three cluster barriers per column; v and w alternate between two
+// buffers by column parity so that the next column can start without a fourth. Output as
+// tridiag_kernel.
+constexpr int kClusterMaxN = 600;
+constexpr int kClThreads = 512;
+
+// Offset of owned column t (global column j = r + t*C) in the local storage of CTA r.
+__host__ __device__ inline long long cl_loff(int t, int r, int C, int n) {
+  return (long long)t * (n - r) - (long long)C * t * (t - 1) / 2;
+}
+
+// Doubles of shared memory a CTA of a C-cluster needs for a block of order n.
+__host__ __device__ inline long long cl_smem_doubles(int n, int C) {
+  const int T0 = (n + C - 1) / C;  // columns of CTA 0, the largest share
+  return ((cl_loff(T0, 0, C, n) + 1) & ~1LL) + 6LL * n + 16 + 2 + 64;
+}
+
+__global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const LargeBlock* __restrict__ blocks,
+                                                                     int lmax) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks(), r = (int)cl.block_rank();
+  const LargeBlock B = blocks[blockIdx.x / C];
+  extern __shared__ __align__(16) double sm[];
+  const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  double* Pl = sm;            // owned columns, packed
+  double* vb = Pl + lmax;     // 2 x n (parity buffers)
+  double* wb = vb + 2 * n;    // 2 x n
+  double* yp = wb + 2 * n;    // n: row part of this CTA's share of A v
+  double* yc = yp + n;        // n: column part (entries of owned columns)
+  double* dots = yc + n;      // 2 x 8: per-CTA partial w.v
+  double* taus = dots + 16;   // 2
+  double* red = taus + 2;     // 64
+  int phase = 0;
+  const int T = (n - r + C - 1) / C;
+  for (int t = warp; t < T; t += nwarps) {
+    const int j = r + t * C;
+    const double* src = B.H + (size_t)j * n;
+    double* dst = Pl + cl_loff(t, r, C, n) - j;
+    for (int i = j + lane; i < n; i += 32) dst[i] = src[i];
+  }
+  cl.sync();  // every CTA of the cluster runs and holds its columns
+  double* A = B.W1;
+  for (int k = 0; k < n - 2; k++) {
+    const int par = k & 1;
+    double* v = vb + par * n;
+    double* w = wb + par * n;
+    // (a) the owner of column k builds the reflector and sends v and tau to every CTA
+    if (r == k % C) {
+      const double* col = Pl + cl_loff(k / C, r, C, n) - k;  // col[i] = A(i, k)
+      double ps = 0.0;
+      for (int i = k + 2 + tid; i < n; i += nt) {
+        const double x = col[i];
+        ps = fma(x, x, ps);
+      }
+      const double sigma = block_sum_1b(ps, red, phase);
+      const double alpha = col[k + 1];
+      double tau = 0.0, beta = alpha, scale = 1.0;
+      if (sigma > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+        tau = (beta - alpha) / beta;
+        scale = 1.0 / (alpha - beta);
+      }
+      for (int i = k + 1 + tid; i < n; i += nt) {
+        const double vi = (i == k + 1) ? 1.0 : col[i] * scale;
+        for (int q = 0; q < C; q++) cl.map_shared_rank(v, q)[i] = vi;
+        A[(size_t)k * ld + i] = vi;
+      }
+      const int kb0 = (k / NBT) * NBT;
+      for (int i = kb0 + 1 + tid; i <= k; i += nt) A[(size_t)k * ld + i] = 0.0;
+      if (tid == 0) {
+        B.d[k] = col[k];
+        B.e[k] = beta;
+        B.tau[k] = tau;
+        for (int q = 0; q < C; q++) cl.map_shared_rank(taus, q)[par] = tau;
+      }
+    }
+    cl.sync();  // (b)
+    const double tau = taus[par];
+    if (tau == 0.0) continue;  // uniform over the cluster
+    // (c) this CTA's share of A v over rows/columns k+1..n-1
+    const int t0 = (k + 1 - r > 0) ? (k + 1 - r + C - 1) / C : 0;  // first owned column >= k+1
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      double s = 0.0;
+      long long addr = cl_loff(t0, r, C, n) - (r + t0 * C) + i;  // A(i, c) for c = r + t0*C
+      for (int t = t0, c = r + t0 * C; c < i; t++, c += C) {
+        s = fma(Pl[addr], v[c], s);
+        addr += (n - r - (long long)t * C) - C;
+      }
+      yp[i] = s;
+    }
+    for (int t = t0 + warp; t < T; t += nwarps) {
+      const int j = r + t * C;
+      const double* col = Pl + cl_loff(t, r, C, n) - j;
+      double dot = 0.0;
+      for (int i = j + lane; i < n; i += 32) dot = fma(col[i], v[i], dot);
+      dot = warp_sum(dot);
+      if (lane == 0) yc[j] = dot;
+    }
+    cl.sync();  // (d)
+    // (e) rows of this CTA's slice: y over the cluster in a fixed order, w = tau y
+    {
+      const int m = n - (k + 1), L = (m + C - 1) / C;
+      const int i0 = k + 1 + r * L, i1 = min(n, i0 + L);
+      double pd = 0.0;
+      for (int i = i0 + tid; i < i1; i += nt) {
+        double y = 0.0;
+        for (int q = 0; q < C; q++) y += cl.map_shared_rank(yp, q)[i];
+        y += cl.map_shared_rank(yc, i % C)[i];
+        const double wi = tau * y;
+        for (int q = 0; q < C; q++) cl.map_shared_rank(w, q)[i] = wi;
+        pd = fma(wi, v[i], pd);
+      }
+      pd = block_sum_1b(pd, red, phase);
+      if (tid == 0)
+        for (int q = 0; q < C; q++) cl.map_shared_rank(dots, q)[par * 8 + r] = pd;
+    }
+    cl.sync();  // (f)
+    // (g, h) w' = w - K v with K = tau (w.v) / 2; rank-2 update of the owned trailing columns
+    double pw = 0.0;
+    for (int q = 0; q < C; q++) pw += dots[par * 8 + q];
+    const double Kc = 0.5 * tau * pw;
+    {
+      int t = t0, off = tid;
+      while (t < T && off >= n - (r + t * C)) {
+        off -= n - (r + t * C);
+        t++;
+      }
+      long long p = cl_loff(t0, r, C, n) + tid;
+      while (t < T) {
+        const int j = r + t * C, i = j + off;
+        const double wj = w[j] - Kc * v[j], wi = w[i] - Kc * v[i];
+        Pl[p] -= v[i] * wj + wi * v[j];
+        p += nt;
+        off += nt;
+        while (t < T && off >= n - (r + t * C)) {
+          off -= n - (r + t * C);
+          t++;
+        }
+      }
+    }
+  }
+  if (tid == 0) {
+    if (r == (n - 2) % C) {
+      const double* col = Pl + cl_loff((n - 2) / C, r, C, n) - (n - 2);
+      B.d[n - 2] = col[n - 2];
+      B.e[n - 2] = col[n - 1];
+      B.tau[n - 2] = 0.0;
+    }
+    if (r == (n - 1) % C) {
+      const double* col = Pl + cl_loff((n - 1) / C, r, C, n) - (n - 1);
+      B.d[n - 1] = col[n - 1];
+      B.e[n - 1] = 0.0;
+      B.tau[n - 1] = 0.0;
+    }
+  }
+  cl.sync();  // the last remote accesses are done; d and e are complete
+  if (r == 0) {
+    int bad = 0;
+    for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
+    if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
+  }
+}
+
 // ---------------------------------------------------------------- divide and conquer: leaves
 __global__ void __launch_bounds__(128) dc_leaf_kernel(const LargeBlock* __restrict__ blocks,
                                                       const DcLeaf* __restrict__ leaves) {
@@ -1232,7 +1407,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
       for (int bi = 0; bi < nb; bi++) {
         const LargeBlock& L = blk[bi];
-        if (L.n <= kMidMaxN) continue;  // reduced in shared memory, no bulk copies
+        if (L.n <= kClusterMaxN) continue;  // reduced in shared memory, no bulk copies
         const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
         const cuuint64_t strides[1] = {(cuuint64_t)L.ldp * sizeof(double)};
         const cuuint32_t box[2] = {(cuuint32_t)kSlabRows, 8u};
@@ -1329,12 +1504,52 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     char* dbase = static_cast<char*>(c->desc);
     const LargeBlock* dblk = reinterpret_cast<const LargeBlock*>(dbase + blk_off);
 
-    // ---- 1. tridiagonalisation: blocks beyond kMidMaxN (sorted first) stream through TMA,
-    //         the rest are reduced in shared memory
+    // ---- 1. tridiagonalisation: blocks beyond kClusterMaxN (sorted first) stream through
+    //         TMA, blocks beyond kMidMaxN are spread over the shared memory of a cluster,
+    //         the rest are reduced in the shared memory of one CTA
     {
       int nbig = 0;
-      while (nbig < nb && blk[nbig].n > kMidMaxN) nbig++;
-      PhaseScope ps(c, kPhTridiag, s, (nbig ? 2 : 0) + (nb > nbig ? 1 : 0));
+      while (nbig < nb && blk[nbig].n > kClusterMaxN) nbig++;
+      int nclu = nbig;
+      while (nclu < nb && blk[nclu].n > kMidMaxN) nclu++;
+      // cluster size per block: the smallest of 2, 4, 8 whose share fits one CTA
+      auto csize = [](int nn) {
+        for (int C = 2; C <= 8; C *= 2)
+          if (sizeof(double) * cl_smem_doubles(nn, C) <= 232448) return C;
+        return 0;
+      };
+      int nlaunch = (nbig ? 2 : 0) + (nb > nclu ? 1 : 0);
+      for (int a = nbig; a < nclu;) {
+        int e = a;
+        while (e < nclu && csize(blk[e].n) == csize(blk[a].n)) e++;
+        nlaunch++;
+        a = e;
+      }
+      PhaseScope ps(c, kPhTridiag, s, nlaunch);
+      for (int a = nbig; a < nclu;) {
+        const int C = csize(blk[a].n);
+        if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", blk[a].n);
+        int e = a;
+        while (e < nclu && csize(blk[e].n) == C) e++;
+        const long long ld0 = cl_smem_doubles(blk[a].n, C);  // the largest block of the group
+        const int lmax = (int)(ld0 - (6LL * blk[a].n + 16 + 2 + 64));
+        const size_t smem = sizeof(double) * (size_t)ld0;
+        NRG_CK(cudaFuncSetAttribute(tridiag_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)((e - a) * C));
+        cfg.blockDim = dim3(kClThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, dblk + a, lmax));
+        a = e;
+      }
       if (nbig) {
         const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
                                                      (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
@@ -1344,11 +1559,11 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
         NRG_CK(cudaGetLastError());
       }
-      if (nb > nbig) {
-        const int mn = blk[nbig].n;
+      if (nb > nclu) {
+        const int mn = blk[nclu].n;
         const size_t smem = sizeof(double) * ((size_t)mn * (mn + 1) / 2 + 2 * (size_t)mn + 64);
         NRG_CK(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        tridiag_smem_kernel<<<nb - nbig, kMidThreads, smem, s>>>(dblk + nbig);
+        tridiag_smem_kernel<<<nb - nclu, kMidThreads, smem, s>>>(dblk + nclu);
         NRG_CK(cudaGetLastError());
       }
     }

@@ -54,7 +54,8 @@ def test_small_path_random(nb, oracle, n):
         check_eig(h, g.val, g.vec, w, v, oracle)
 
 
-@pytest.mark.parametrize("n", [65, 66, 96, 100, 127, 128, 129, 200, 256, 300, 511, 512, 777])
+@pytest.mark.parametrize("n", [65, 66, 96, 100, 127, 128, 129, 200, 224, 225, 256, 300, 320, 321, 452, 453,
+                               511, 512, 600, 601, 777])
 def test_large_path_random(nb, oracle, n):
     rng = np.random.default_rng(200 + n)
     h = rand_upper(rng, n)
@@ -72,7 +73,7 @@ def test_graded_blocks(nb, oracle, n):
     check_eig(h, g.val, g.vec, w, v, oracle)
 
 
-@pytest.mark.parametrize("n", [10, 80, 200])
+@pytest.mark.parametrize("n", [10, 80, 200, 300, 400, 550])
 def test_degenerate_spectrum(nb, oracle, n):
     # Exactly repeated eigenvalues (a rotated matrix with a 3-fold and a 5-fold level) and
     # a diagonal matrix: exercises deflation by small z and by close poles.
@@ -92,12 +93,12 @@ def test_degenerate_spectrum(nb, oracle, n):
     check_eig(d, g.val, g.vec, w, v, oracle)
 
 
-def test_block_diagonal_and_tridiagonal(nb, oracle):
-    rng = np.random.default_rng(5)
-    n = 160
+@pytest.mark.parametrize("n", [160, 350, 520])
+def test_block_diagonal_and_tridiagonal(nb, oracle, n):
+    rng = np.random.default_rng(5 + n)
     h = np.zeros((n, n))
-    h[:80, :80] = rand_upper(rng, 80)
-    h[80:, 80:] = rand_upper(rng, 80)  # decoupled halves: beta = 0 at the top split
+    h[:n // 2, :n // 2] = rand_upper(rng, n // 2)
+    h[n // 2:, n // 2:] = rand_upper(rng, n - n // 2)  # decoupled halves: beta = 0 at the top split
     h = np.triu(h)
     g = nb.diagonalisations([h])[0]
     w, v = oracle.diagonalise(h)
@@ -110,7 +111,7 @@ def test_block_diagonal_and_tridiagonal(nb, oracle):
 
 def test_mixed_batch(nb, oracle):
     rng = np.random.default_rng(11)
-    sizes = [3, 150, 64, 65, 17, 400, 1, 90]
+    sizes = [3, 150, 64, 65, 17, 400, 1, 90, 230, 590, 330]
     blocks = [rand_upper(rng, n) if i % 2 else graded_block(rng, n) for i, n in enumerate(sizes)]
     got = nb.diagonalisations(blocks)
     for h, g in zip(blocks, got):
