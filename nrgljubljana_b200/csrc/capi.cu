@@ -270,6 +270,9 @@ int nrg_destroy(nrg_ctx* c) {
   if (c->fork_ev) cudaEventDestroy(c->fork_ev);
   if (c->join_ev) cudaEventDestroy(c->join_ev);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->fork2_ev) cudaEventDestroy(c->fork2_ev);
+  if (c->join2_ev) cudaEventDestroy(c->join2_ev);
+  if (c->side2) cudaStreamDestroy(c->side2);
   delete c;
   return NRG_OK;
 }

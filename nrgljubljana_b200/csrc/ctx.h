@@ -40,6 +40,10 @@ struct nrg_ctx {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   void* desc_side = nullptr;  // descriptor staging of the side stream
   size_t desc_side_size = 0;
+  // third stream: the one-CTA tridiagonalisation of mid-size blocks beside the cluster and
+  // bulk-copy reductions of larger blocks
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
 };
 
 namespace nrg {

@@ -1512,31 +1512,45 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       while (nbig < nb && blk[nbig].n > kClusterMaxN) nbig++;
       int nclu = nbig;
       while (nclu < nb && blk[nclu].n > kMidMaxN) nclu++;
-      // cluster size per block: the smallest of 2, 4, 8 whose share fits one CTA
-      auto csize = [](int nn) {
-        for (int C = 2; C <= 8; C *= 2)
-          if (sizeof(double) * cl_smem_doubles(nn, C) <= 232448) return C;
-        return 0;
-      };
-      int nlaunch = (nbig ? 2 : 0) + (nb > nclu ? 1 : 0);
-      for (int a = nbig; a < nclu;) {
-        int e = a;
-        while (e < nclu && csize(blk[e].n) == csize(blk[a].n)) e++;
-        nlaunch++;
-        a = e;
+      // One cluster size for all cluster blocks (one launch): the smallest of 2, 4, 8 that
+      // fits the largest of them, raised while the cluster CTAs still fit the SMs once.
+      int C = 0;
+      if (nclu > nbig) {
+        for (int q = 2; q <= 8 && !C; q *= 2)
+          if (sizeof(double) * cl_smem_doubles(blk[nbig].n, q) <= 232448) C = q;
+        if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", blk[nbig].n);
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+        while (C < 8 && 2 * C * (nclu - nbig) <= nsm) C *= 2;
       }
-      PhaseScope ps(c, kPhTridiag, s, nlaunch);
-      for (int a = nbig; a < nclu;) {
-        const int C = csize(blk[a].n);
-        if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", blk[a].n);
-        int e = a;
-        while (e < nclu && csize(blk[e].n) == C) e++;
-        const long long ld0 = cl_smem_doubles(blk[a].n, C);  // the largest block of the group
-        const int lmax = (int)(ld0 - (6LL * blk[a].n + 16 + 2 + 64));
+      const bool fork = nb > nclu && (nbig > 0 || nclu > nbig);
+      if (fork && !c->side2) {
+        NRG_CK(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking));
+        NRG_CK(cudaEventCreateWithFlags(&c->fork2_ev, cudaEventDisableTiming));
+        NRG_CK(cudaEventCreateWithFlags(&c->join2_ev, cudaEventDisableTiming));
+      }
+      PhaseScope ps(c, kPhTridiag, s, (nbig ? 2 : 0) + (nclu > nbig ? 1 : 0) + (nb > nclu ? 1 : 0));
+      if (nb > nclu) {  // one CTA per block, on the third stream when other launches run beside it
+        cudaStream_t ss = s;
+        if (fork) {
+          NRG_CK(cudaEventRecord(c->fork2_ev, s));
+          NRG_CK(cudaStreamWaitEvent(c->side2, c->fork2_ev, 0));
+          ss = c->side2;
+        }
+        const int mn = blk[nclu].n;
+        const size_t smem = sizeof(double) * ((size_t)mn * (mn + 1) / 2 + 2 * (size_t)mn + 64);
+        NRG_CK(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        tridiag_smem_kernel<<<nb - nclu, kMidThreads, smem, ss>>>(dblk + nclu);
+        NRG_CK(cudaGetLastError());
+        if (fork) NRG_CK(cudaEventRecord(c->join2_ev, ss));
+      }
+      if (nclu > nbig) {
+        const long long ld0 = cl_smem_doubles(blk[nbig].n, C);  // the largest block sets the layout
+        const int lmax = (int)(ld0 - (6LL * blk[nbig].n + 16 + 2 + 64));
         const size_t smem = sizeof(double) * (size_t)ld0;
         NRG_CK(cudaFuncSetAttribute(tridiag_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)((e - a) * C));
+        cfg.gridDim = dim3((unsigned)((nclu - nbig) * C));
         cfg.blockDim = dim3(kClThreads);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = s;
@@ -1547,8 +1561,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         at[0].val.clusterDim.z = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, dblk + a, lmax));
-        a = e;
+        NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, dblk + nbig, lmax));
       }
       if (nbig) {
         const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
@@ -1559,13 +1572,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
         NRG_CK(cudaGetLastError());
       }
-      if (nb > nclu) {
-        const int mn = blk[nclu].n;
-        const size_t smem = sizeof(double) * ((size_t)mn * (mn + 1) / 2 + 2 * (size_t)mn + 64);
-        NRG_CK(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        tridiag_smem_kernel<<<nb - nclu, kMidThreads, smem, s>>>(dblk + nclu);
-        NRG_CK(cudaGetLastError());
-      }
+      if (fork) NRG_CK(cudaStreamWaitEvent(s, c->join2_ev, 0));
     }
     // ---- 2. divide and conquer
     {
