@@ -1407,7 +1407,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
       for (int bi = 0; bi < nb; bi++) {
         const LargeBlock& L = blk[bi];
-        if (L.n <= kClusterMaxN) continue;  // reduced in shared memory, no bulk copies
+        if (L.n <= kMidMaxN) continue;  // reduced in the shared memory of one CTA, no bulk copies
         const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
         const cuuint64_t strides[1] = {(cuuint64_t)L.ldp * sizeof(double)};
         const cuuint32_t box[2] = {(cuuint32_t)kSlabRows, 8u};
@@ -1508,20 +1508,28 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     //         TMA, blocks beyond kMidMaxN are spread over the shared memory of a cluster,
     //         the rest are reduced in the shared memory of one CTA
     {
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
       int nbig = 0;
       while (nbig < nb && blk[nbig].n > kClusterMaxN) nbig++;
       int nclu = nbig;
       while (nclu < nb && blk[nclu].n > kMidMaxN) nclu++;
       // One cluster size for all cluster blocks (one launch): the smallest of 2, 4, 8 that
-      // fits the largest of them, raised while the cluster CTAs still fit the SMs once.
+      // fits the largest of them, raised while the cluster CTAs still fit the SMs once. The
+      // clusters serve latency: when they would not all fit the SMs at once (a batch of many
+      // blocks), the blocks go to the bulk-copy kernel, whose two CTAs per SM give more
+      // throughput.
       int C = 0;
       if (nclu > nbig) {
         for (int q = 2; q <= 8 && !C; q *= 2)
           if (sizeof(double) * cl_smem_doubles(blk[nbig].n, q) <= 232448) C = q;
         if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", blk[nbig].n);
-        int nsm = 148;
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-        while (C < 8 && 2 * C * (nclu - nbig) <= nsm) C *= 2;
+        if (C * (nclu - nbig) > nsm) {
+          nbig = nclu;  // throughput regime
+          C = 0;
+        } else {
+          while (C < 8 && 2 * C * (nclu - nbig) <= nsm) C *= 2;
+        }
       }
       const bool fork = nb > nclu && (nbig > 0 || nclu > nbig);
       if (fork && !c->side2) {
