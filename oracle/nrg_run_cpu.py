@@ -17,6 +17,11 @@ host with LAPACK dsyev and BLAS dgemm through ``oracle.py``. It follows
   measure_singlet             c++/measurements.hpp:18-30
   recalc_irreduc / recalc_f   c++/symmetry/nrg-recalc-QS.hpp:192-330, c++/recalc.hpp:52-76
   recalc_singlet              c++/symmetry.hpp:185-200, c++/recalc.hpp:82-108
+  recalc_doublet (QS)         c++/symmetry/nrg-recalc-QS.hpp:32-117, qs-1ch-doublet{p,m}.dat
+  DM-NRG                      init_rho, cdmI, calc_densitymatrix(_iterN) c++/dmnrg.hpp:43-112;
+                              Algo_DMNRG c++/algo_DMNRG.hpp:29-52; BaseSpectrum::calc c++/algo.hpp:55-67;
+                              mergeNN2half, windowfunction, continuous c++/spectrum.hpp:81-196;
+                              Bins c++/bins.hpp:61-185; BR_NEW c++/spectral.hpp:42-70
 
 Only ``tests/`` and the CPU-baseline leg of ``bench.py`` may import this module.
 """
@@ -48,6 +53,30 @@ _OFFDIAG = [
 _DIAG = [(1, 0), (2, 1), (3, 1), (4, 2)]
 _SPINUP = [(2, 1, lambda s: 1), (4, 3, lambda s: -math.sqrt(1 - 1 / (2. * (1 + _S(s)))))]
 _SPINDOWN = [(3, 1, lambda s: 1), (4, 2, lambda s: math.sqrt(1 + 1 / (2. * _S(s))))]
+# doublet recalculation, Ip = (q1 - 1, ss1 + 1) and (q1 - 1, ss1 - 1): rows (i1, ip, factor(ss1))
+_DOUBLETP = [(1, 1, lambda s: 1), (2, 2, lambda s: (-2 * math.sqrt(_S(s) * (1 + _S(s)))) / (1 + 2 * _S(s))),
+             (3, 2, lambda s: 1 / (1 + 2 * _S(s))), (3, 3, lambda s: -1), (4, 4, lambda s: 1)]
+_DOUBLETM = [(1, 1, lambda s: 1), (2, 2, lambda s: -1), (2, 3, lambda s: 1 / (-1 - 2 * _S(s))),
+             (3, 3, lambda s: (-2 * (1 + _S(s))) / math.sqrt(5 + 1 / _S(s) + 8 * _S(s) + 4 * math.pow(_S(s), 2))),
+             (4, 4, lambda s: 1)]
+
+
+def _specdens_factor(Ip, I1):
+    """SymmetryQS::specdens_factor (c++/symmetry/sym-QS-impl.hpp:64-70)."""
+    return _S(Ip[1]) + 1.0 if I1[1] == Ip[1] + 1 else _S(Ip[1])
+
+
+def _BR_NEW(e, ept, alpha, omega0):
+    """c++/spectral.hpp:42-70."""
+    part_l = 0.0
+    if not ((e < 0.0 and ept > 0.0) or (e > 0.0 and ept < 0.0) or ept == 0.0):
+        gamma = alpha / 4.0
+        part_l = math.exp(-math.pow(math.log(e / ept) / alpha - gamma, 2)) / (alpha * abs(e) * math.sqrt(math.pi))
+    if abs(e) > omega0:
+        return part_l
+    BR_h = math.exp(-math.pow(math.log(abs(e) / omega0) / alpha, 2))
+    BR_G = math.exp(-math.pow((e - ept) / omega0, 2)) / (omega0 * math.sqrt(math.pi))
+    return part_l * BR_h + BR_G * (1.0 - BR_h)
 
 
 def _triangle(I, A, Q):
@@ -67,7 +96,11 @@ class _Eig:
         self.U: List[np.ndarray] = []
 
 
-def run(param_text: str, data_text: str, threads: int = 1) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
+        ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+    """td and custom rows of the run; with dmnrg=true and a `spectra` dict, also the DM-NRG
+    spectral functions of the specd pairs (name -> array of (E, A(E)) rows, as written to
+    spec_DMNRG_dens_<name>.dat)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -96,6 +129,10 @@ def run(param_text: str, data_text: str, threads: int = 1) -> Tuple[List[str], L
     opch = dict(d.opch[0][0])
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
+    dm = kv.get("dmnrg", "false").lower() == "true" and spectra is not None
+    specd = [tuple(t.split("-", 1)) for t in kv.get("specd", "").split()] if dm else []
+    dops = {name: dict(d.ops[name][1]) for name in sorted({x for pr in specd for x in pr})}
+    steps = []  # per step: subspaces, structure, doublet operators (DM-NRG)
 
     td_rows, custom_rows = [], []
 
@@ -244,6 +281,140 @@ def run(param_text: str, data_text: str, threads: int = 1) -> Tuple[List[str], L
         if strategy == "kept":
             ops = recalc_ops(lambda e: e.nrstored)
             custom(N, new, ops)
+        if dm:
+            nd_ = {}
+            for name, cold in dops.items():
+                cn = {}
+                for I1, e1 in new.items():
+                    for dss, table in ((1, _DOUBLETP), (-1, _DOUBLETM)):
+                        Ip = (I1[0] - 1, I1[1] + dss)
+                        if Ip not in new or not (e1.nrstored and new[Ip].nrstored):
+                            continue
+                        ep = new[Ip]
+                        m = np.zeros((e1.nrstored, ep.nrstored))
+                        anc1, dims1 = structure[I1]
+                        ancp, dimsp = structure[Ip]
+                        for i1, ip, fn in table:
+                            IN1, INp = anc1[i1 - 1], ancp[ip - 1]
+                            if IN1[1] <= 0 or INp[1] <= 0 or (IN1, INp) not in cold:
+                                continue
+                            if dims1[i1 - 1] == 0 or dimsp[ip - 1] == 0:
+                                continue
+                            A = np.ascontiguousarray(e1.U[i1 - 1][:e1.nrstored])
+                            B = np.ascontiguousarray(ep.U[ip - 1][:ep.nrstored])
+                            Oa = np.ascontiguousarray(cold[(IN1, INp)][:dims1[i1 - 1], :dimsp[ip - 1]])
+                            O.transform(m, fn(I1[1]), A, Oa, B)
+                        cn[(I1, Ip)] = m
+                nd_[name] = cn
+            dops = nd_
+            steps.append((N, scale, new, structure, dops))
         diag = new
+    if dm and steps:
+        _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, spectra)
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
     return td_fields, td_rows, ["T"] + sorted(ops), custom_rows
+
+
+def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
+    """calc_rho + calc_densitymatrix, then the DMNRG run's spectral part: per step
+    Algo_DMNRG::calc over all subspace pairs, mergeNN2 into the full spectrum, and at the end
+    trim + continuous (log-Gaussian broadening)."""
+    T = float(kv.get("T", 0.001))
+    goodE = float(kv.get("goodE", 2.0))
+    bins = int(kv.get("bins", 1000))
+    NN1 = kv.get("NN1", "false").lower() == "true"
+    NN2avg = kv.get("NN2avg", "false").lower() == "true"
+    NN2even = kv.get("NN2even", "true").lower() == "true"
+    NNtanh = float(kv.get("NNtanh", 0.0))
+    discard_trim = float(kv.get("discard_trim", 1e-16))
+    discard_imm = float(kv.get("discard_immediately", 1e-16))
+    emin_p, emax_p = float(kv.get("emin", -1.0)), float(kv.get("emax", -1.0))
+    alpha = float(kv.get("alpha", 0.3))
+    omega0 = float(kv.get("omega0", -1.0))
+    if omega0 < 0.0:
+        omega0 = float(kv.get("omega0_ratio", 1.0)) * T
+    bmax = float(kv.get("broaden_max", 10.0))
+    bmin = float(kv.get("broaden_min", -99.0))
+    bratio = float(kv.get("broaden_ratio", 1.05))
+    last_scale = SCALE(Nmax, Lam, disc, z)
+    if bmin <= 0.0:
+        bmin = float(kv.get("broaden_min_ratio", 3.0)) * last_scale
+    Efac = Lam  # one channel, no N/N+1 patching
+    if NN1:
+        Efac = math.sqrt(Lam)
+    # density matrix at the last step over the kept states (init_rho)
+    N_last, scale_last, diag_last, _, _ = steps[-1]
+    scT = scale_last / T
+    Z = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrstored]) for I, e in diag_last.items())
+    rho = {I: np.diag([math.exp(-c * scT) for c in e.corr[:e.nrstored]]) / Z for I, e in diag_last.items()}
+    rhos = {N_last: rho}
+    for k in range(len(steps) - 1, 0, -1):
+        N, _, diagN, structN, _ = steps[k]
+        _, _, diagP, _, _ = steps[k - 1]
+        rhoN = rhos[N]
+        prev = {}
+        for I, eP in diagP.items():
+            dim = eP.nrstored
+            M = np.zeros((dim, dim))
+            if dim:
+                for i, dl in enumerate(_IN):
+                    sub = (I[0] - dl[0], I[1] - dl[1])
+                    if sub not in rhoN or sub not in diagN:
+                        continue
+                    nw = rhoN[sub].shape[0]
+                    rmax = structN[sub][1][i]
+                    if nw == 0 or rmax == 0:
+                        continue
+                    assert rmax == dim
+                    U = np.ascontiguousarray(diagN[sub].U[i][:nw])
+                    O.rotate(M, float(sub[1]) / float(I[1]), U, np.ascontiguousarray(rhoN[sub]))
+            prev[I] = M
+        tr = sum(I[1] * np.trace(m) for I, m in prev.items())
+        assert abs(tr - 1.0) < 1e-10, tr
+        rhos[N - 1] = prev
+    emax = emax_p if emax_p > 0 else SCALE(0, Lam, disc, z) * 100.0
+    emin = emin_p if emin_p > 0 else last_scale / 100.0
+    lmin, lmax = math.floor(math.log10(emin)), math.ceil(math.log10(emax))
+    for name1, name2 in specd:
+        full = O.ChainBinning(lmin, lmax, bins, discard_imm)
+        for N, scale, diagN, _, dopsN in steps:
+            merge = NN1 or NN2avg or (N % 2 == 0 if NN2even else N % 2 == 1)
+            if not merge:
+                continue
+            cb = O.ChainBinning(lmin, lmax, bins, discard_imm)
+            rhoN = rhos[N]
+            Emin_w, Emax_w = scale * goodE, scale * goodE * Efac * Efac
+            op1, op2 = dopsN[name1], dopsN[name2]
+            for Ii, ei in diagN.items():
+                for Ij, ej in diagN.items():
+                    if (Ij, Ii) not in op1 or (Ij, Ii) not in op2:
+                        continue
+                    Em = (ei.values[:ei.nrstored] - ei.shift) * scale
+                    Ej = (ej.values[:ej.nrstored] - ej.shift) * scale
+                    cb.dmnrg_pair(Em, Ej, op1[(Ij, Ii)], op2[(Ij, Ii)], rhoN[Ii], rhoN[Ij], _specdens_factor(Ii, Ij), -1,
+                                  Emin_w, Emax_w)
+            Ex = scale * goodE * Efac
+            flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
+            for fr, fi, cr, ci in ((full.pos_re, full.pos_im, cb.pos_re, cb.pos_im),
+                                   (full.neg_re, full.neg_im, cb.neg_re, cb.neg_im)):
+                O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(full.energies),
+                                             full.nbins, Emin_w, Ex, Emax_w, flags, NNtanh, 1 if NN2avg else 0)
+
+        def trim(w):
+            e = full.energies
+            keep = [(e[i], w[i]) for i in range(len(e) - 1) if abs(w[i]) >= discard_trim * (e[i + 1] - e[i])]
+            keep.append((e[-1], w[-1]))
+            return keep
+        pos, neg = trim(full.pos_re), trim(full.neg_re)
+        mesh = []
+        E = bmax
+        while E > bmin:
+            mesh.append(E)
+            E /= bratio
+        rows_pos, rows_neg = [], []
+        for E in mesh:
+            vp = sum(w * _BR_NEW(E, e, alpha, omega0) for e, w in pos) + sum(w * _BR_NEW(E, -e, alpha, omega0) for e, w in neg)
+            vn = sum(w * _BR_NEW(-E, e, alpha, omega0) for e, w in pos) + sum(w * _BR_NEW(-E, -e, alpha, omega0) for e, w in neg)
+            rows_pos.append((E, vp))
+            rows_neg.append((-E, vn))
+        out[f"{name1}-{name2}"] = np.array(sorted(rows_neg) + sorted(rows_pos))

@@ -16,6 +16,7 @@ CASES = [
     "test3_disc_z", "test4_disc_c", "test10_keepmin", "test12_Nmax", "test13_strategy_all",
     "test14_strategy_kept", "test15_safeguard", "test16_safeguardmax", "test35_betabar",
     "test56_dsyevd", "test56_dsyevr", "test200_data_has", "legacy_simple", "legacy_Himp",
+    "test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins",
 ]
 
 
@@ -25,7 +26,8 @@ def main(ref_root: str) -> None:
         src = os.path.join(ref_root, "test", "c++", case)
         dst = os.path.join(out_root, case)
         os.makedirs(dst, exist_ok=True)
-        for name, rel in (("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")):
+        for name, rel in (("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom"),
+                          ("spec_DMNRG_dens_A_d-A_d.dat", "ref/spec_DMNRG_dens_A_d-A_d.dat")):
             p = os.path.join(src, rel)
             if os.path.exists(p):
                 shutil.copyfile(p, os.path.join(dst, name))
