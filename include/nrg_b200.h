@@ -212,6 +212,16 @@ NRG_API int nrg_spec_accumulate(nrg_ctx* ctx, int npair, const nrg_spec_pair* pa
  * later launch group with CUDA events on its stream; nrg_profile_read synchronises on
  * those events and returns one entry per phase that launched (name, total ms, number of
  * kernel launches). Launch counts are kept even when timing is off. */
+/* Log-Gaussian broadening of a spectrum of delta peaks onto an energy mesh: replaces
+ * SpectrumRealFreq::continuous() (c++/spectrum.hpp:168-196) with the kernel BR_NEW
+ * (c++/spectral.hpp:42-70),
+ *   out[k] = sum_s w[s] * BR_NEW(E[k], e[s], alpha, omega0),   k < nmesh, s < nspike.
+ * Peaks of both signs and mesh points of both signs are given in one list each (the
+ * reference's positive and negative halves). e, w, E, out are device arrays; out is
+ * overwritten. The sum over peaks is taken in a fixed order. */
+NRG_API int nrg_broaden(nrg_ctx* ctx, int nspike, const double* e, const double* w, int nmesh, const double* E,
+                        double alpha, double omega0, double* out, void* stream);
+
 typedef struct nrg_phase_stat {
   char name[24];
   double ms;

@@ -24,7 +24,8 @@ NRG_SPEC_FDMLS = 2
 # Every symbol include/nrg_b200.h declares.
 EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_diag_batch", "nrg_diag_batch_host",
            "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate", "nrg_profile",
-           "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch")
+           "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch",
+           "nrg_broaden")
 NRG_NOALLOC_SCRATCH_DOUBLES = 1 << 20
 
 
@@ -64,6 +65,9 @@ class SpecPair(C.Structure):
                 ("op2", C.c_void_p), ("ld2", C.c_int64), ("rho_i", C.c_void_p), ("ldri", C.c_int64),
                 ("rho_j", C.c_void_p), ("ldrj", C.c_int64), ("ni", C.c_int), ("ki", C.c_int),
                 ("nj", C.c_int), ("kj", C.c_int), ("rdi", C.c_int), ("rdj", C.c_int), ("factor", C.c_double)]
+
+
+SPECPAIR_DTYPE = _np_layout(SpecPair)
 
 
 class SpecParams(C.Structure):
@@ -107,6 +111,7 @@ def load() -> C.CDLL:
     L.nrg_transform_noalloc.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int64, P, C.c_int64, C.c_int, C.c_int,
                                         C.c_int, C.c_int, C.c_double, P]
     L.nrg_hamiltonian_batch.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(P), C.c_int, C.POINTER(HPiece), P]
+    L.nrg_broaden.argtypes = [P, C.c_int, P, P, C.c_int, P, C.c_double, C.c_double, P, P]
     L.nrg_profile.argtypes = [P, C.c_int]
     L.nrg_profile_read.argtypes = [P, C.POINTER(PhaseStat), C.c_int]
     _lib = L

@@ -314,3 +314,33 @@ def spec_accumulate(algo: int, pairs: Sequence[SpecPair], grid: BinGrid, pos, ne
     b = grid.c()
     check(ctx.lib.nrg_spec_accumulate(ctx.ptr, len(pairs), arr, C.byref(prm), C.byref(b), C.c_void_p(pos.data_ptr()),
                                       C.c_void_p(neg.data_ptr()), _stream_ptr(stream)), "nrg_spec_accumulate")
+
+
+def spec_accumulate_array(algo: int, pairs: np.ndarray, grid: BinGrid, pos, neg, sign: int = -1, T: float = 0.0,
+                          wnf: float = 0.0, Emin: float = 0.0, Emax: float = 0.0, ctx=None, stream=None) -> None:
+    """nrg_spec_accumulate on a numpy record array of SPECPAIR_DTYPE (device pointers)."""
+    ctx = ctx or context()
+    if pairs.dtype != _lib.SPECPAIR_DTYPE or not pairs.flags.c_contiguous:
+        raise ValueError("pairs must be a contiguous SPECPAIR_DTYPE array")
+    prm = SpecParams(algo, sign, T, wnf, Emin, Emax)
+    b = grid.c()
+    check(ctx.lib.nrg_spec_accumulate(ctx.ptr, len(pairs), pairs.ctypes.data_as(C.POINTER(SpecPair)), C.byref(prm),
+                                      C.byref(b), C.c_void_p(pos.data_ptr()), C.c_void_p(neg.data_ptr()),
+                                      _stream_ptr(stream)), "nrg_spec_accumulate")
+
+
+def broaden(e: np.ndarray, w: np.ndarray, mesh: np.ndarray, alpha: float, omega0: float, ctx=None,
+            stream=None) -> np.ndarray:
+    """Log-Gaussian broadening (nrg_broaden) of peaks (e, w) onto the mesh; host arrays in
+    and out, computed on the device."""
+    import torch
+    ctx = ctx or context()
+    dev = torch.device("cuda", ctx.device)
+    te = torch.from_numpy(np.ascontiguousarray(e, dtype=np.float64)).to(dev)
+    tw = torch.from_numpy(np.ascontiguousarray(w, dtype=np.float64)).to(dev)
+    tm = torch.from_numpy(np.ascontiguousarray(mesh, dtype=np.float64)).to(dev)
+    out = torch.empty(len(mesh), dtype=torch.float64, device=dev)
+    check(ctx.lib.nrg_broaden(ctx.ptr, len(e), C.c_void_p(te.data_ptr()), C.c_void_p(tw.data_ptr()), len(mesh),
+                              C.c_void_p(tm.data_ptr()), float(alpha), float(omega0), C.c_void_p(out.data_ptr()),
+                              _stream_ptr(stream)), "nrg_broaden")
+    return out.cpu().numpy()

@@ -132,7 +132,7 @@ int stage_desc_side(nrg_ctx* c, const std::vector<char>& img) {
 const char* phase_name(int p) {
   static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
                                         "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
-                                        "gemm3", "spec_gemm", "spec_bin", "assemble"};
+                                        "gemm3", "spec_gemm", "spec_bin", "assemble", "broaden"};
   return (p >= 0 && p < kPhCount) ? names[p] : "?";
 }
 
@@ -595,6 +595,18 @@ int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* st
 }
 
 // ---------------------------------------------------------------- spectral accumulation
+int nrg_broaden(nrg_ctx* c, int nspike, const double* e, const double* w, int nmesh, const double* E, double alpha,
+                double omega0, double* out, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nspike < 0 || nmesh < 0 || (nspike > 0 && (!e || !w)) || (nmesh > 0 && (!E || !out)))
+    return fail(NRG_ERR_ARG, "bad arguments");
+  if (!(alpha > 0.0) || !(omega0 > 0.0)) return fail(NRG_ERR_ARG, "alpha and omega0 must be positive");
+  nrg::PhaseScope ps(c, nrg::kPhBroaden, static_cast<cudaStream_t>(stream));
+  CK(nrg::broaden_launch(nspike, e, w, nmesh, E, alpha, omega0, out, static_cast<cudaStream_t>(stream)));
+  return NRG_OK;
+}
+
 int nrg_bins_grid(const nrg_bins* b, double* energies) {
   if (!b || b->bins <= 0) return fail(NRG_ERR_ARG, "bad bins");
   const int nr = (int)((b->log10emax - b->log10emin) * b->bins + 1.0);

@@ -14,7 +14,7 @@ namespace nrg {
 // Launch groups timed by nrg_profile (names in phase_name()).
 enum Phase : int {
   kPhEigSmall, kPhTridiag, kPhDcLeaf, kPhDcPrep, kPhDcSecular, kPhDcVectors, kPhDcGemm, kPhSort, kPhBtGemm,
-  kPhBtTfactor, kPhGemm3, kPhSpecGemm, kPhSpecBin, kPhAssemble, kPhCount
+  kPhBtTfactor, kPhGemm3, kPhSpecGemm, kPhSpecBin, kPhAssemble, kPhBroaden, kPhCount
 };
 const char* phase_name(int p);
 }  // namespace nrg

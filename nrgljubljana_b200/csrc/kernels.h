@@ -70,4 +70,8 @@ int hamiltonian_tiles(int n);
 cudaError_t hamiltonian_launch(const HBlock* d_blocks, int nblk, int ntiles, const nrg_hpiece* d_pieces,
                                cudaStream_t stream);
 
+// ---------------------------------------------------------------- spectrum broadening
+cudaError_t broaden_launch(int nspike, const double* e, const double* w, int nmesh, const double* E, double alpha,
+                           double omega0, double* out, cudaStream_t stream);
+
 }  // namespace nrg

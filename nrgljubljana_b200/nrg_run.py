@@ -30,17 +30,18 @@ import numpy as np
 import torch
 
 from . import qs
-from ._lib import GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG
-from .api import Context, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch
+from ._lib import GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG, SPECPAIR_DTYPE
+from .api import (BinGrid, Context, broaden, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch,
+                  spec_accumulate_array)
 from .inputs import DataFile, SCALE, parse_param, read_data
 
 Invar = Tuple[int, int]
 
 # Parameters that do not change td/custom of a run without spectral functions.
 _IGNORED = {
-    "symtype", "model", "U", "Gamma", "delta", "band", "T", "Tmin", "checksumrules", "logall", "log",
+    "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
     "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
-    "Nmax", "prec_td", "prec_custom", "width_td", "width_custom", "specs", "specd", "spect",
+    "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom", "specs", "spect",
 }
 
 
@@ -62,6 +63,28 @@ class RunParams:
     calc0: bool = True
     lastall: bool = False
     data_has_rescaled_energies: bool = True
+    # DM-NRG spectral functions of the specd pairs (c++/params.hpp:181-396)
+    T: float = 0.001
+    dmnrg: bool = False
+    specd: str = ""
+    bins: int = 1000
+    emin: float = -1.0
+    emax: float = -1.0
+    discard_immediately: float = 1e-16
+    discard_trim: float = 1e-16
+    goodE: float = 2.0
+    NN1: bool = False
+    NN2even: bool = True
+    NN2avg: bool = False
+    NNtanh: float = 0.0
+    broaden: bool = True
+    broaden_max: float = 10.0
+    broaden_min: float = -99.0
+    broaden_min_ratio: float = 3.0
+    broaden_ratio: float = 1.05
+    alpha: float = 0.3
+    omega0: float = -1.0
+    omega0_ratio: float = 1.0
 
     @classmethod
     def from_param(cls, kv: Dict[str, str]) -> "RunParams":
@@ -83,6 +106,10 @@ class RunParams:
                 raise ValueError(f"parameter {k} is not supported by the QS run driver")
         if p.strategy not in ("kept", "all"):
             raise ValueError(f"strategy={p.strategy}")
+        if p.dmnrg and p.strategy != "kept":
+            raise ValueError("DM-NRG spectra are supported with strategy=kept")
+        if p.dmnrg and not p.broaden:
+            raise ValueError("broaden=false is not supported")
         return p
 
 
@@ -94,6 +121,7 @@ class Result:
     custom: List[List[float]]
     blocks_per_step: List[int] = field(default_factory=list)
     max_dim_per_step: List[int] = field(default_factory=list)
+    spectra: Dict[str, np.ndarray] = field(default_factory=dict)  # "op1-op2" -> rows (E, A(E))
 
 
 # ------------------------------------------------------------------ host bookkeeping
@@ -263,6 +291,11 @@ class QSRun:
         self.nmax = data.nmax
         self.sqrt_lambda = math.sqrt(params.Lambda)  # nrg_step_scale_factor (c++/params.hpp:639-641)
         self.op_names = sorted(n for n, (k, _) in data.ops.items() if k in "sg")
+        self.specd = [tuple(t.split("-", 1)) for t in params.specd.split()] if params.dmnrg else []
+        self.dop_names = sorted({x for pr in self.specd for x in pr})
+        for name in self.dop_names:
+            if name not in data.ops or data.ops[name][0] != "d":
+                raise ValueError(f"specd names {name}, which is not a doublet operator of the data file")
 
     # ---- scales (c++/step.hpp:30-39)
     def scale(self, trueN: int) -> float:
@@ -326,6 +359,14 @@ class QSRun:
         self.res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + self.op_names,
                           [])
         self.meas: List[_Measure] = []
+        self.dm_steps: List[tuple] = []
+        if self.dop_names:
+            dmats = [dict(d.ops[name][1]) for name in self.dop_names]
+            dshapes = {}
+            for m in dmats:
+                for k, mat in m.items():
+                    dshapes[k] = mat.shape
+            self.dops = MatSet(self.dev, dshapes, len(self.dop_names), _pack(dmats, dshapes))
         if p.calc0:
             self.res.td.append(self._td(-1, diag))
             self.meas.append(self._measure(-1, diag, self.ops))
@@ -358,6 +399,9 @@ class QSRun:
                 Z = float(np.sum(m.weights))
                 res.custom.append([m.T] + [float(np.sum(m.weights * dg[o])) / Z for o in range(len(self.op_names))])
         self.meas = []
+        if self.dm_steps:
+            res.spectra = self._dmnrg()
+            self.dm_steps = []
         return res
 
     def begin_step(self) -> "StepJob":
@@ -494,6 +538,9 @@ class QSRun:
             new_ops = self._recalc_singlets(diag, ops)
             meas.append(self._measure(N, diag, new_ops))
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
+        if self.dop_names:  # DM-NRG keeps every step's eigenvectors and doublet operators
+            self.dops = self._recalc_doublets(diag, self.dops)
+            self.dm_steps.append((N, self.scale(N), diag, self.dops, job.Vbuf))
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
@@ -557,6 +604,210 @@ class QSRun:
         return out
 
 
+    def _recalc_doublets(self, diag: Dict[Invar, Sub], cold: MatSet) -> MatSet:
+        """SymmetryQS::recalc_doublet (c++/symmetry/nrg-recalc-QS.hpp:32-117) through
+        recalc_general (c++/recalc.hpp:82-108) over the kept states, every doublet operator
+        of the spectra in one batched call (operator-major)."""
+        plan = []
+        for I1, s1 in diag.items():
+            if not s1.nstored:
+                continue
+            for dq, table in qs.DOUBLET:
+                Ip = (I1[0] + dq[0], I1[1] + dq[1])
+                sp = diag.get(Ip)
+                if sp is not None and sp.nstored:
+                    plan.append((I1, Ip, table))
+        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan},
+                     len(self.dop_names))
+        base = []
+        for I1, Ip, table in plan:
+            s1, sp = diag[I1], diag[Ip]
+            anc1, ancp = qs.ancestors(I1), qs.ancestors(Ip)
+            M = out.ptr((I1, Ip))
+            for i1, ip, fn in table:
+                IN1, INp = anc1[i1 - 1], ancp[ip - 1]
+                if not (qs.allowed(IN1) and qs.allowed(INp)) or (IN1, INp) not in cold.loc:
+                    continue
+                w1, wp = s1.dims[i1 - 1], sp.dims[ip - 1]
+                if w1 == 0 or wp == 0:
+                    continue
+                _, r, c = cold.loc[(IN1, INp)]
+                base.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, cold.ptr((IN1, INp)), c,
+                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, w1, wp, 0, 1, fn(I1[1])))
+        if base:
+            b = np.array(base, dtype=GEMM3_DTYPE)
+            t = np.tile(b, len(self.dop_names))
+            op = np.repeat(np.arange(len(self.dop_names), dtype=np.uint64), len(b))
+            t["M"] += op * np.uint64(8 * out.total)
+            t["O"] += op * np.uint64(8 * cold.total)
+            gemm3_batch_array(t, self.ctx, self.stream)
+        return out
+
+    def _dmnrg(self) -> Dict[str, np.ndarray]:
+        """DM-NRG spectral functions of the specd pairs: the density matrix of the last step
+        (init_rho, c++/dmnrg.hpp:43-50), the backward sweep (calc_densitymatrix_iterN / cdmI,
+        c++/dmnrg.hpp:55-102) as batched rotate terms, per step the Algo_DMNRG pair sums binned
+        on the device (c++/algo_DMNRG.hpp:29-52, c++/algo.hpp:55-67), N/N+2 (or N/N+1)
+        patching with the window function (c++/spectrum.hpp:81-124), trimming
+        (c++/bins.hpp:165-185) and log-Gaussian broadening on the device
+        (c++/spectrum.hpp:168-196)."""
+        p, d = self.p, self.d
+        steps = self.dm_steps
+        Lam = p.Lambda
+        # init_rho over the kept states of the last step, scT = scale / T
+        N_last, scale_last, diag_last, _, _ = steps[-1]
+        scT = scale_last / p.T
+        Z = 0.0
+        diagvals = {}
+        for I, s in diag_last.items():
+            ex = np.exp(-s.corr[:s.nstored] * scT)
+            diagvals[I] = ex
+            Z += qs.mult(I) * float(np.sum(ex))
+        shapes = {I: (s.nstored, s.nstored) for I, s in diag_last.items()}
+        host = np.zeros(max(1, sum(r * c for r, c in shapes.values())))
+        o = 0
+        for I, (r, c) in shapes.items():
+            host[o + np.arange(r) * (c + 1)] = diagvals[I] / Z
+            o += r * c
+        rhos = {len(steps) - 1: MatSet(self.dev, shapes, 1, host)}
+        for k in range(len(steps) - 1, 0, -1):
+            _, _, diagN, _, _ = steps[k]
+            _, _, diagP, _, _ = steps[k - 1]
+            rhoN = rhos[k]
+            prev = MatSet(self.dev, {I: (s.nstored, s.nstored) for I, s in diagP.items()})
+            rows = []
+            for I, sP in diagP.items():
+                dim = sP.nstored
+                if dim == 0:
+                    continue
+                for i, dl in enumerate(qs.IN):
+                    sub = (I[0] - dl[0], I[1] - dl[1])
+                    sN = diagN.get(sub)
+                    if sN is None:
+                        continue
+                    nw, rmax = sN.nstored, sN.dims[i]
+                    if nw == 0 or rmax == 0:
+                        continue
+                    if rmax != dim:
+                        raise AssertionError("rmax == dim")  # cdmI, c++/dmnrg.hpp:73
+                    A = sN.vptr + 8 * sN.offs[i]
+                    rows.append((prev.ptr(I), dim, A, sN.n, rhoN.ptr(sub), nw, A, sN.n, dim, dim, nw, nw, 1, 0,
+                                 float(qs.mult(sub)) / float(qs.mult(I))))
+            if rows:
+                gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
+            rhos[k - 1] = prev
+        # Tr rho = 1 at every step (check_trace_rho, c++/dmnrg.hpp:29-33): one gather per step,
+        # one copy to the host
+        diags, mults = [], []
+        for k, (_, _, dg, _, _) in enumerate(steps):
+            idx = []
+            for I, s in dg.items():
+                off, r, c = rhos[k].loc[I]
+                idx.append(off + np.arange(r) * (c + 1))
+                mults.append(np.full(r, float(qs.mult(I))))
+            if idx:
+                diags.append(torch.index_select(rhos[k].buf, 0, self._h2d(np.concatenate(idx).astype(np.int64))))
+        if diags:
+            dvals = torch.cat(diags).cpu().numpy()
+            bounds = np.cumsum([0] + [len(x) for x in diags])
+            mv = np.concatenate(mults)
+            for a, b in zip(bounds[:-1], bounds[1:]):
+                tr = float(np.sum(mv[a:b] * dvals[a:b]))
+                if abs(tr - 1.0) > 1e-9:
+                    raise RuntimeError(f"check_trace_rho() failed: {tr!r}")
+        # spectra
+        last_scale = SCALE(self.nmax, Lam, p.discretization, p.z, p.bandrescale)
+        emax = p.emax if p.emax > 0 else SCALE(0, Lam, p.discretization, p.z, p.bandrescale) * 100.0
+        emin = p.emin if p.emin > 0 else last_scale / 100.0
+        grid = BinGrid.from_limits(emin, emax, p.bins, p.discard_immediately)
+        ebins = grid.energies()
+        nb = grid.nbins
+        Efac = math.sqrt(Lam) if p.NN1 else Lam
+        omega0 = p.omega0 if p.omega0 >= 0.0 else p.omega0_ratio * p.T
+        bmin = p.broaden_min if p.broaden_min > 0.0 else p.broaden_min_ratio * last_scale
+        mesh = []
+        E = p.broaden_max
+        while E > bmin:
+            mesh.append(E)
+            E /= p.broaden_ratio
+        mesh = np.array(mesh)
+        out: Dict[str, np.ndarray] = {}
+        for n1, n2 in self.specd:
+            o1, o2 = self.dop_names.index(n1), self.dop_names.index(n2)
+            full_pos, full_neg = np.zeros(nb), np.zeros(nb)
+            for k, (N, scale, dg, dops, _) in enumerate(steps):
+                merge = p.NN1 or p.NN2avg or ((N % 2 == 0) if p.NN2even else (N % 2 == 1))
+                if not merge:
+                    continue
+                rhoN = rhos[k]
+                # abs_zero energies of the kept states (c++/eigen.hpp:45)
+                eoff, flat, o = {}, [], 0
+                for I, s in dg.items():
+                    eoff[I] = o
+                    flat.append((s.values[:s.nstored] - s.shift) * scale)
+                    o += s.nstored
+                Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+                eb = Edev.data_ptr()
+                pairs = []
+                for Ii, si in dg.items():
+                    for Ij, sj in dg.items():
+                        key = (Ij, Ii)
+                        if key not in dops.loc or si.nstored == 0 or sj.nstored == 0:
+                            continue
+                        ki, kj = si.nstored, sj.nstored
+                        pairs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], dops.ptr(key, o1), ki, dops.ptr(key, o2), ki,
+                                      rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj,
+                                      qs.specdens_factor(Ii, Ij)))
+                pos = torch.zeros(nb, dtype=torch.float64, device=self.dev)
+                neg = torch.zeros(nb, dtype=torch.float64, device=self.dev)
+                Emin_w = scale * p.goodE
+                if pairs:
+                    spec_accumulate_array(0, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg, sign=-1,
+                                          Emin=Emin_w, Emax=Emin_w * Efac * Efac, ctx=self.ctx, stream=self.stream)
+                cp, cn = pos.cpu().numpy(), neg.cpu().numpy()
+                Ex, Emax_w = Emin_w * Efac, Emin_w * Efac * Efac
+                f = (0.5 if p.NN2avg else 1.0)
+                win = window(ebins, Emin_w, Ex, Emax_w, N == self.nmax - 1, N == 0, p.NNtanh)
+                inside = (Emin_w < ebins) & (ebins < Emax_w)
+                for full, cs in ((full_pos, cp), (full_neg, cn)):
+                    sel = inside & (cs != 0.0)
+                    full[sel] += f * cs[sel] * win[sel]
+
+            def trim(w):
+                width = np.diff(ebins)
+                keep = np.concatenate([np.abs(w[:-1]) >= p.discard_trim * width, [True]])
+                return ebins[keep], w[keep]
+            ep, wp = trim(full_pos)
+            en, wn = trim(full_neg)
+            spikes_e = np.concatenate([ep, -en])
+            spikes_w = np.concatenate([wp, wn])
+            mesh_all = np.concatenate([mesh, -mesh])
+            vals = broaden(spikes_e, spikes_w, mesh_all, p.alpha, omega0, self.ctx, self.stream)
+            npos = len(mesh)
+            rows_pos = sorted(zip(mesh_all[:npos].tolist(), vals[:npos].tolist()))
+            rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
+            out[f"{n1}-{n2}"] = np.array(rows_neg + rows_pos)
+        return out
+
+def window(e: np.ndarray, Emin: float, Ex: float, Emax: float, last: bool, first: bool, NNtanh: float) -> np.ndarray:
+    """windowfunction (c++/spectrum.hpp:91-109) for the bin energies inside (Emin, Emax)."""
+    def fnc(x):
+        if NNtanh > 0:
+            t0 = lambda y: np.tanh(NNtanh * (y - 0.5))  # noqa: E731
+            return (t0(x) - t0(0.0)) / (t0(1.0) - t0(0.0))
+        return x
+    f = np.zeros_like(e)
+    lo = (Emin < e) & (e <= Ex)
+    hi = (Ex < e) & (e < Emax)
+    f[lo] = fnc((e[lo] - Emin) / (Ex - Emin))
+    f[hi] = 1.0 - fnc((e[hi] - Ex) / (Emax - Ex))
+    if first:
+        f[e >= Ex] = 1.0
+    if last:
+        f[e <= Ex] = 1.0
+    return f
+
+
 def run_files(param_text: str, data_text: str, device: int = 0) -> Result:
     """Run the reference's ``param`` + ``data`` inputs; returns the td and custom rows."""
     kv = parse_param(param_text)
@@ -599,6 +850,10 @@ def main(argv=None) -> int:
     os.makedirs(out, exist_ok=True)
     _write_table(os.path.join(out, "td"), res.td_fields, res.td)
     _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom)
+    for name, rows in res.spectra.items():  # spec_DMNRG_dens_<name>.dat, as Spikes::save writes it
+        with open(os.path.join(out, f"spec_DMNRG_dens_{name}.dat"), "w") as f:
+            for e, v in rows:
+                f.write(f"{e:.10g} {v:.10g}\n")
     return 0
 
 

@@ -87,3 +87,25 @@ def td_extra(Zs, subspaces, Z: float) -> List[float]:
         trQ2 += sumZ * q * q
         trSZ += sumZ * (ss * ss - 1) / 12.
     return [trSZ / Z, trQ / Z, trQ2 / Z]
+
+# Doublet operators <I1||O||Ip> with Ip = I1 + (-1, +1) (qs-1ch-doubletp.dat) and
+# Ip = I1 + (-1, -1) (qs-1ch-doubletm.dat), driven by SymmetryQS::recalc_doublet
+# (c++/symmetry/nrg-recalc-QS.hpp:32-117): rows (i1, ip, factor(ss1)); the old matrix is the
+# one between the ancestors of I1 through i1 and of Ip through ip.
+DOUBLET: List[Tuple[Invar, List[Tuple[int, int, Callable[[int], float]]]]] = [
+    ((-1, 1), [(1, 1, lambda ss: 1.0),
+               (2, 2, lambda ss: (-2 * math.sqrt(S(ss) * (1 + S(ss)))) / (1 + 2 * S(ss))),
+               (3, 2, lambda ss: 1 / (1 + 2 * S(ss))),
+               (3, 3, lambda ss: -1.0),
+               (4, 4, lambda ss: 1.0)]),
+    ((-1, -1), [(1, 1, lambda ss: 1.0),
+                (2, 2, lambda ss: -1.0),
+                (2, 3, lambda ss: 1 / (-1 - 2 * S(ss))),
+                (3, 3, lambda ss: (-2 * (1 + S(ss))) / math.sqrt(5 + 1 / S(ss) + 8 * S(ss) + 4 * S(ss) ** 2)),
+                (4, 4, lambda ss: 1.0)]),
+]
+
+
+def specdens_factor(Ip: Invar, I1: Invar) -> float:
+    """SymmetryQS::specdens_factor (c++/symmetry/sym-QS-impl.hpp:64-70)."""
+    return S(Ip[1]) + 1.0 if I1[1] == Ip[1] + 1 else S(Ip[1])

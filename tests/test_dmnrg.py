@@ -54,3 +54,16 @@ def oracle_spectra(oracle):
 @pytest.mark.parametrize("case", DM_CASES)
 def test_oracle_dmnrg_spectrum_matches_reference(oracle_spectra, case):
     assert_spectrum(oracle_spectra(case)["A_d-A_d"], ref_spectrum(case), RTOL, ATOL_REL_TO_MAX, case)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", DM_CASES)
+def test_gpu_dmnrg_spectrum(oracle_spectra, case):
+    """The device run (doublet recalculation, density-matrix sweep as batched rotate
+    terms, pair sums binned by nrg_spec_accumulate, broadening by nrg_broaden) against the
+    reference's spectrum and the oracle's."""
+    from nrgljubljana_b200.nrg_run import run_files
+    res = run_files(read(case, "param"), read(case, "data"))
+    got = res.spectra["A_d-A_d"]
+    assert_spectrum(got, ref_spectrum(case), RTOL, ATOL_REL_TO_MAX, f"{case} vs reference")
+    assert_spectrum(got, oracle_spectra(case)["A_d-A_d"], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} vs oracle")
