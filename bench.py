@@ -387,16 +387,18 @@ z=1
 keep=1000
 keepenergy=10
 T=1e-8
-ops=n_d
+ops=n_d A_d
+dmnrg=true
+specd=A_d-A_d
 """
 NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delta=0), Gamma=0.04, flat band, "
-                "Lambda=2 (Z), z=1, Nmax=40, keep=1000, keepenergy=10, T=1e-8, operator n_d; input generated "
-                "by nrgljubljana_b200.datagen")
+                "Lambda=2 (Z), z=1, Nmax=40, keep=1000, keepenergy=10, T=1e-8, operator n_d, DM-NRG spectral "
+                "function A_d-A_d (1000 bins/decade, broadened); input generated by nrgljubljana_b200.datagen")
 
 
 def c0_inputs():
     from nrgljubljana_b200.datagen import siam_qs
-    return C0_PARAM, siam_qs(1.0, 0.0, 0.04, 2.0, 40, 1.0, "Z", ops=["n_d"])
+    return C0_PARAM, siam_qs(1.0, 0.0, 0.04, 2.0, 40, 1.0, "Z", ops=["n_d", "A_d"])
 
 
 SERVE_MIX = ["legacy_Himp", "legacy_simple", "test12_Nmax", "test35_betabar", "test15_safeguard",
@@ -486,18 +488,27 @@ def nrg_run_arm(torch, device: int, args) -> dict:
         big = np.abs(td) >= 1e-6
         return float(np.max(np.abs(o[big] - td[big]) / np.abs(td[big])))
     out["per_block_gpu"]["td_max_rel_diff"] = tddiff(res_pb.td)
+
+    def specdiff(other):
+        """Largest difference of the A_d-A_d spectrum relative to its peak."""
+        a, b = res.spectra["A_d-A_d"][:, 1], np.asarray(other["A_d-A_d"])[:, 1]
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(a)))
+    out["per_block_gpu"]["spectrum_max_diff_rel_to_peak"] = specdiff(res_pb.spectra)
+    out["spectrum_points"] = int(len(res.spectra["A_d-A_d"]))
     if not args.no_cpu:
         from oracle import oracle as O
         from oracle import nrg_run_cpu
         O.build()
         threads = os.cpu_count() or 1
-        nrg_run_cpu.run(param, data, threads=threads)
+        nrg_run_cpu.run(param, data, threads=threads, spectra={})
+        spec_cpu = {}
         t0 = time.perf_counter()
-        _, td_cpu, _, _ = nrg_run_cpu.run(param, data, threads=threads)
+        _, td_cpu, _, _ = nrg_run_cpu.run(param, data, threads=threads, spectra=spec_cpu)
         t_cpu = time.perf_counter() - t0
         out["cpu_baseline"] = {"steps_per_s": d.nmax / t_cpu, "ms_per_run": t_cpu * 1e3, "cores": threads,
-                               "kind": "port", "sample": "one whole run",
-                               "td_max_rel_diff": tddiff(td_cpu)}
+                               "kind": "port", "sample": "one whole run (thermodynamics and DM-NRG spectrum)",
+                               "td_max_rel_diff": tddiff(td_cpu),
+                               "spectrum_max_diff_rel_to_peak": specdiff(spec_cpu)}
     return out
 
 

@@ -74,3 +74,20 @@ def test_gpu_run_on_regenerated_input(case):
     res = run_files(read(case, "param"), txt)
     assert_close(res.td, ref_rows(case, "td")[1], REF_RTOL, REF_ATOL, f"{case} td")
     assert_close(res.custom, ref_rows(case, "custom")[1], REF_RTOL, REF_ATOL, f"{case} custom")
+
+
+@pytest.mark.parametrize("case", ["test2_algorithms_dmnrg", "test23_DMNRG"])
+def test_regenerated_doublet_reproduces_reference_spectrum(oracle, case):
+    """The generator's A_d (d^dag) block: a DM-NRG run on the regenerated input gives the
+    reference's spectral function."""
+    from oracle import nrg_run_cpu
+    from nrgljubljana_b200.datagen import siam_qs
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from test_dmnrg import ATOL_REL_TO_MAX, RTOL, assert_spectrum, ref_spectrum
+    kv = parse_param(read(case, "param"))
+    ref = read_data(read(case, "data"))
+    txt = siam_qs(float(kv["U"]), float(kv["delta"]), float(kv["Gamma"]), float(kv.get("Lambda", 2)), ref.nmax,
+                  float(kv.get("z", 1)), kv.get("discretization", "Z"), ops=["n_d", "A_d"])
+    spec = {}
+    nrg_run_cpu.run(read(case, "param"), txt, threads=os.cpu_count() or 1, spectra=spec)
+    assert_spectrum(spec["A_d-A_d"], ref_spectrum(case), RTOL, ATOL_REL_TO_MAX, case)
