@@ -216,7 +216,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
     ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
+    ap.add_argument("--write-c0", default=None, metavar="DIR",
+                    help="write the param and data files of the NRG-run workload to DIR and exit")
     args = ap.parse_args()
+    if args.write_c0:
+        os.makedirs(args.write_c0, exist_ok=True)
+        param, data = c0_inputs()
+        for name, text in (("param", param), ("data", data)):
+            with open(os.path.join(args.write_c0, name), "w") as f:
+                f.write(text)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

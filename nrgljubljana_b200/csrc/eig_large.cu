@@ -645,15 +645,16 @@ __global__ void __launch_bounds__(kMidThreads) tridiag_smem_kernel(const LargeBl
 // ---------------------------------------------------------------- cluster tridiagonalisation
 // Blocks with kMidMaxN < n <= kClusterMaxN: the packed lower triangle is spread over the
 // shared memory of a thread-block cluster of C CTAs (column j lives in CTA j mod C) and the
-// unblocked Householder reduction runs there; the CTAs combine their partial mat-vec
-// products through distributed shared memory (plain loads and stores to the other CTAs'
-// shared memory, no bulk copies). Per column: the owner of column k builds v and sends it
-// to every CTA; each CTA forms its part of A v (rows: its columns left of the diagonal;
-// columns: from the diagonal down, one warp each, so the sums are in a fixed order); each
-// CTA reduces one slice of rows over the cluster into w and sends it out; each CTA updates
-// its own columns. Three cluster barriers per column; v and w alternate between two
-// buffers by column parity so that the next column can start without a fourth. Output as
-// tridiag_kernel.
+// unblocked Householder reduction runs there; the CTAs read each other's shared memory
+// (distributed shared memory, plain loads, no bulk copies). Two cluster barriers per column:
+//   A  column k is final in its owner, and every CTA has finished reading the partial
+//      products of the previous column;
+//      every CTA reads column k from its owner and builds the same reflector v itself; each
+//      CTA forms its share of A v: per row, the part left of the diagonal from its own
+//      columns; per owned column (one warp), the part from the diagonal down;
+//   B  every CTA sums the shares of all CTAs for every row in a fixed order (so all CTAs
+//      hold the same w) and updates its own columns.
+// Output as tridiag_kernel.
 constexpr int kClusterMaxN = 600;
 constexpr int kClThreads = 512;
 
@@ -665,7 +666,7 @@ __host__ __device__ inline long long cl_loff(int t, int r, int C, int n) {
 // Doubles of shared memory a CTA of a C-cluster needs for a block of order n.
 __host__ __device__ inline long long cl_smem_doubles(int n, int C) {
   const int T0 = (n + C - 1) / C;  // columns of CTA 0, the largest share
-  return ((cl_loff(T0, 0, C, n) + 1) & ~1LL) + 6LL * n + 16 + 2 + 64;
+  return ((cl_loff(T0, 0, C, n) + 1) & ~1LL) + 4LL * n + 64;
 }
 
 __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const LargeBlock* __restrict__ blocks,
@@ -677,14 +678,12 @@ __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const Large
   extern __shared__ __align__(16) double sm[];
   const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
-  double* Pl = sm;            // owned columns, packed
-  double* vb = Pl + lmax;     // 2 x n (parity buffers)
-  double* wb = vb + 2 * n;    // 2 x n
-  double* yp = wb + 2 * n;    // n: row part of this CTA's share of A v
-  double* yc = yp + n;        // n: column part (entries of owned columns)
-  double* dots = yc + n;      // 2 x 8: per-CTA partial w.v
-  double* taus = dots + 16;   // 2
-  double* red = taus + 2;     // 64
+  double* Pl = sm;          // owned columns, packed
+  double* v = Pl + lmax;    // n
+  double* w = v + n;        // n
+  double* yp = w + n;       // n: row part of this CTA's share of A v
+  double* yc = yp + n;      // n: column part (entries of owned columns)
+  double* red = yc + n;     // 64 (two halves for block_sum_1b)
   int phase = 0;
   const int T = (n - r + C - 1) / C;
   for (int t = warp; t < T; t += nwarps) {
@@ -693,46 +692,42 @@ __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const Large
     double* dst = Pl + cl_loff(t, r, C, n) - j;
     for (int i = j + lane; i < n; i += 32) dst[i] = src[i];
   }
-  cl.sync();  // every CTA of the cluster runs and holds its columns
   double* A = B.W1;
   for (int k = 0; k < n - 2; k++) {
-    const int par = k & 1;
-    double* v = vb + par * n;
-    double* w = wb + par * n;
-    // (a) the owner of column k builds the reflector and sends v and tau to every CTA
-    if (r == k % C) {
-      const double* col = Pl + cl_loff(k / C, r, C, n) - k;  // col[i] = A(i, k)
-      double ps = 0.0;
-      for (int i = k + 2 + tid; i < n; i += nt) {
-        const double x = col[i];
-        ps = fma(x, x, ps);
-      }
-      const double sigma = block_sum_1b(ps, red, phase);
-      const double alpha = col[k + 1];
-      double tau = 0.0, beta = alpha, scale = 1.0;
-      if (sigma > 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
-        tau = (beta - alpha) / beta;
-        scale = 1.0 / (alpha - beta);
-      }
-      for (int i = k + 1 + tid; i < n; i += nt) {
-        const double vi = (i == k + 1) ? 1.0 : col[i] * scale;
-        for (int q = 0; q < C; q++) cl.map_shared_rank(v, q)[i] = vi;
-        A[(size_t)k * ld + i] = vi;
-      }
+    cl.sync();  // A
+    const int o = k % C;
+    // column k from its owner: colr[i] = A(i, k)
+    const double* colr = cl.map_shared_rank(Pl + cl_loff(k / C, o, C, n) - k, o);
+    double ps = 0.0;
+    for (int i = k + 2 + tid; i < n; i += nt) {
+      const double x = colr[i];
+      ps = fma(x, x, ps);
+    }
+    const double sigma = block_sum_1b(ps, red, phase);
+    const double alpha = colr[k + 1];
+    double tau = 0.0, beta = alpha, scale = 1.0;
+    if (sigma > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+      tau = (beta - alpha) / beta;
+      scale = 1.0 / (alpha - beta);
+    }
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      const double vi = (i == k + 1) ? 1.0 : colr[i] * scale;
+      v[i] = vi;
+      if (r == o) A[(size_t)k * ld + i] = vi;
+    }
+    if (r == o) {
       const int kb0 = (k / NBT) * NBT;
       for (int i = kb0 + 1 + tid; i <= k; i += nt) A[(size_t)k * ld + i] = 0.0;
       if (tid == 0) {
-        B.d[k] = col[k];
+        B.d[k] = colr[k];
         B.e[k] = beta;
         B.tau[k] = tau;
-        for (int q = 0; q < C; q++) cl.map_shared_rank(taus, q)[par] = tau;
       }
     }
-    cl.sync();  // (b)
-    const double tau = taus[par];
-    if (tau == 0.0) continue;  // uniform over the cluster
-    // (c) this CTA's share of A v over rows/columns k+1..n-1
+    __syncthreads();
+    if (tau == 0.0) continue;  // the same in every CTA
+    // this CTA's share of A v over rows/columns k+1..n-1
     const int t0 = (k + 1 - r > 0) ? (k + 1 - r + C - 1) / C : 0;  // first owned column >= k+1
     for (int i = k + 1 + tid; i < n; i += nt) {
       double s = 0.0;
@@ -751,29 +746,18 @@ __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const Large
       dot = warp_sum(dot);
       if (lane == 0) yc[j] = dot;
     }
-    cl.sync();  // (d)
-    // (e) rows of this CTA's slice: y over the cluster in a fixed order, w = tau y
-    {
-      const int m = n - (k + 1), L = (m + C - 1) / C;
-      const int i0 = k + 1 + r * L, i1 = min(n, i0 + L);
-      double pd = 0.0;
-      for (int i = i0 + tid; i < i1; i += nt) {
-        double y = 0.0;
-        for (int q = 0; q < C; q++) y += cl.map_shared_rank(yp, q)[i];
-        y += cl.map_shared_rank(yc, i % C)[i];
-        const double wi = tau * y;
-        for (int q = 0; q < C; q++) cl.map_shared_rank(w, q)[i] = wi;
-        pd = fma(wi, v[i], pd);
-      }
-      pd = block_sum_1b(pd, red, phase);
-      if (tid == 0)
-        for (int q = 0; q < C; q++) cl.map_shared_rank(dots, q)[par * 8 + r] = pd;
+    cl.sync();  // B
+    double pd = 0.0;
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      double y = 0.0;
+      for (int q = 0; q < C; q++) y += cl.map_shared_rank(yp, q)[i];
+      y += cl.map_shared_rank(yc, i % C)[i];
+      const double wi = tau * y;
+      w[i] = wi;
+      pd = fma(wi, v[i], pd);
     }
-    cl.sync();  // (f)
-    // (g, h) w' = w - K v with K = tau (w.v) / 2; rank-2 update of the owned trailing columns
-    double pw = 0.0;
-    for (int q = 0; q < C; q++) pw += dots[par * 8 + q];
-    const double Kc = 0.5 * tau * pw;
+    const double Kc = 0.5 * tau * block_sum_1b(pd, red, phase);  // its barrier also publishes w
+    // rank-2 update of the owned trailing columns with w' = w - Kc v
     {
       int t = t0, off = tid;
       while (t < T && off >= n - (r + t * C)) {
@@ -808,7 +792,7 @@ __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const Large
       B.tau[n - 1] = 0.0;
     }
   }
-  cl.sync();  // the last remote accesses are done; d and e are complete
+  cl.sync();  // the last remote reads are done; d and e are complete
   if (r == 0) {
     int bad = 0;
     for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
@@ -1554,7 +1538,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       }
       if (nclu > nbig) {
         const long long ld0 = cl_smem_doubles(blk[nbig].n, C);  // the largest block sets the layout
-        const int lmax = (int)(ld0 - (6LL * blk[nbig].n + 16 + 2 + 64));
+        const int lmax = (int)(ld0 - (4LL * blk[nbig].n + 64));
         const size_t smem = sizeof(double) * (size_t)ld0;
         NRG_CK(cudaFuncSetAttribute(tridiag_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaLaunchConfig_t cfg = {};
