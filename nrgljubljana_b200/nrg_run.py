@@ -42,6 +42,7 @@ _IGNORED = {
     "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
     "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
     "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom", "specs", "spect",
+    "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
 }
 
 
@@ -62,6 +63,11 @@ class RunParams:
     strategy: str = "kept"
     calc0: bool = True
     lastall: bool = False
+    # full-density-matrix flags: they keep every state of the last step (params.hpp:535-539);
+    # the FDM outputs themselves (tdfdm, customfdm, FDM spectra) are not produced
+    fdm: bool = False
+    fdmexpv: bool = False
+    lastalloverride: bool = False
     data_has_rescaled_energies: bool = True
     # DM-NRG spectral functions of the specd pairs (c++/params.hpp:181-396)
     T: float = 0.001
@@ -111,6 +117,11 @@ class RunParams:
         if p.dmnrg and not p.broaden:
             raise ValueError("broaden=false is not supported")
         return p
+
+    @property
+    def keep_all_states_in_last_step(self) -> bool:
+        """Params::keep_all_states_in_last_step (c++/params.hpp:539)."""
+        return self.lastall or ((self.fdm or self.fdmexpv) and not self.lastalloverride)
 
 
 @dataclass
@@ -279,8 +290,11 @@ class QSRun:
     of many runs in one batched call."""
 
     def __init__(self, params: RunParams, data: DataFile, device: int = 0, ctx: Optional[Context] = None):
-        if data.symtype != "QS" or data.channels != 1:
-            raise ValueError("the driver covers symtype QS with one channel")
+        if data.symtype != "QS" or data.channels not in (1, 2):
+            raise ValueError("the driver covers symtype QS with one or two channels")
+        self.T = qs.tables(data.channels)
+        if params.dmnrg and data.channels != 1:
+            raise ValueError("DM-NRG spectra are supported for one channel")
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device: the QS run driver has no CPU fallback")
         self.p = params
@@ -350,9 +364,15 @@ class QSRun:
         for I, e in sorted(d.subspaces):
             v = e.copy() if p.data_has_rescaled_energies else e / scale0
             diag[I] = Sub(I, v, 0.0, v.copy(), len(v), len(v), n=len(v))
-        oc = d.opch[0][0]
-        shapes = {k: m.shape for k, m in oc.items()}
-        self.opch = MatSet(self.dev, shapes, 1, _pack([oc], shapes))
+        # <||f||> of every channel in one channel-major set; the keys each channel holds are
+        # kept, as offdiag_function() needs its channel's matrix to exist
+        ocs = [d.opch[ch][0] for ch in range(d.channels)]
+        shapes = {}
+        for oc in ocs:
+            for k, m in oc.items():
+                shapes[k] = m.shape
+        self.opch = MatSet(self.dev, shapes, d.channels, _pack(ocs, shapes))
+        self.opch_keys = [set(oc) for oc in ocs]
         mats = [{I1: m for (I1, I2), m in d.ops[name][1].items() if I1 == I2} for name in self.op_names]
         oshapes = {I: (s.nstored, s.nstored) for I, s in diag.items()}
         self.ops = MatSet(self.dev, oshapes, len(self.op_names), _pack(mats, oshapes))
@@ -413,13 +433,13 @@ class QSRun:
         # subspace structure (c++/core.hpp:42-58, 62-70; c++/subspaces.hpp:114-121)
         new = set()
         for I in prev:
-            for J in qs.new_subspaces(I):
+            for J in self.T.new_subspaces(I):
                 if qs.allowed(J):
                     new.add(J)
         tasks: List[Tuple[Invar, List[int], List[Invar]]] = []
         for I in sorted(new):
-            anc = qs.ancestors(I)
-            dims = [(prev[a].nstored if a in prev else 0) if qs.triangle(I, a, qs.QN[i]) else 0
+            anc = self.T.ancestors(I)
+            dims = [(prev[a].nstored if a in prev else 0) if qs.triangle(I, a, self.T.QN[i]) else 0
                     for i, a in enumerate(anc)]
             if sum(dims):
                 tasks.append((I, dims, anc))
@@ -450,20 +470,20 @@ class QSRun:
 
         # Hamiltonian pieces: hamiltonian() + SymmetryQS::make_matrix
         rows = []
-        xi, zeta = d.xi[0], d.zeta[0]
+        xi, zeta = d.xi, d.zeta
         for b, (I, dims, anc) in enumerate(tasks):
-            offs = [0, dims[0], dims[0] + dims[1], dims[0] + dims[1] + dims[2]]
-            for i in range(qs.COMBS):
+            offs = [0] + np.cumsum(dims).tolist()[:-1]
+            for i in range(self.T.COMBS):
                 if dims[i]:
                     rows.append((b, NRG_HP_DIAG, offs[i], offs[i], dims[i], dims[i], 0, 0, 0,
                                  pbase + 8 * poff[anc[i]], self.sqrt_lambda, 0.0))
             ss = I[1]
-            for (i, j, ch, fn) in qs.OFFDIAG:
+            for (i, j, ch, fn) in self.T.OFFDIAG:
                 if not (dims[i - 1] and dims[j - 1]):
                     continue
-                factor = fn(ss) * xi[N]
+                factor = fn(ss) * xi[ch][N]
                 key = (anc[i - 1], anc[j - 1])
-                if key not in opch.loc:
+                if key not in self.opch_keys[ch]:
                     raise RuntimeError(f"offdiag_function(): matrix not found {i} {j} {ch} 0")
                 _, r, c = opch.loc[key]
                 if (r, c) != (dims[i - 1], dims[j - 1]):
@@ -471,13 +491,13 @@ class QSRun:
                 fs = factor / scale
                 if i > j:
                     rows.append((b, NRG_HP_BLOCK, offs[j - 1], offs[i - 1], dims[j - 1], dims[i - 1], 1, 0, c,
-                                 opch.ptr(key), fs, 0.0))
+                                 opch.ptr(key, ch), fs, 0.0))
                 else:
                     rows.append((b, NRG_HP_BLOCK, offs[i - 1], offs[j - 1], dims[i - 1], dims[j - 1], 0, 0, c,
-                                 opch.ptr(key), fs, 0.0))
-            for (i, ch, number) in qs.DIAG:
+                                 opch.ptr(key, ch), fs, 0.0))
+            for (i, ch, number) in self.T.DIAG:
                 if dims[i - 1]:
-                    shift = zeta[N + 1] * (number - 1.0 * qs.AVGOCCUP) / scale
+                    shift = zeta[ch][N + 1] * (number - 1.0 * qs.AVGOCCUP) / scale
                     rows.append((b, NRG_HP_DIAG, offs[i - 1], offs[i - 1], dims[i - 1], dims[i - 1], 0, 0, 0, 0,
                                  0.0, shift))
         hamiltonian_batch(ns, Hp, np.array(rows, dtype=HPIECE_DTYPE), self.ctx, self.stream)
@@ -496,7 +516,7 @@ class QSRun:
 
         diag: Dict[Invar, Sub] = {}
         for b, (I, dims, anc) in enumerate(tasks):
-            offs = [0, dims[0], dims[0] + dims[1], dims[0] + dims[1] + dims[2]]
+            offs = [0] + np.cumsum(dims).tolist()[:-1]
             diag[I] = Sub(I, evals[voff[b]:voff[b + 1]], dims=list(dims), offs=offs, vptr=Vp[b], n=ns[b],
                           nstored=ns[b])
         # do_diag: Egs subtraction, splitting correction, truncation (c++/core.hpp:141-143)
@@ -521,7 +541,7 @@ class QSRun:
         else:
             allcorr = allrel
         Emax = highest_retained_energy(allcorr, p)
-        keep_all = last and p.lastall
+        keep_all = last and p.keep_all_states_in_last_step
         for s in diag.values():
             s.nkept = len(s.values) if keep_all else int(np.count_nonzero(s.corr <= Emax))
 
@@ -549,31 +569,42 @@ class QSRun:
         return diag_batch_ptrs(job.ns, job.Hp, job.Ep, job.Vp, self.ctx, self.stream)
 
     def _recalc_irreducible(self, diag: Dict[Invar, Sub]) -> MatSet:
-        """SymmetryQS::recalc_irreduc with recalc_f (c++/recalc.hpp:52-76): <I1||f||Ip> over the
-        kept states, one batched GEMM call for the whole step."""
+        """SymmetryQS::recalc_irreduc with recalc_f (c++/recalc.hpp:52-76): <I1||f_ch||Ip> of
+        every channel over the kept states (channel-major), one batched GEMM call for the
+        whole step. Every channel holds every pair of the plan."""
         plan = []
+        dqs = []
+        for dq, _, _ in self.T.RECALC_F:
+            if dq not in dqs:
+                dqs.append(dq)
         for Ip, sp in diag.items():
-            for dq, table in qs.RECALC_F:
+            for dq in dqs:
                 I1 = (Ip[0] + dq[0], Ip[1] + dq[1])
                 s1 = diag.get(I1)
                 if s1 is None or not (s1.nstored and sp.nstored):
                     continue
-                plan.append((I1, Ip, table))
-        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan})
+                plan.append((I1, Ip))
+        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip in plan},
+                     self.T.channels)
         rows = []
-        for I1, Ip, table in plan:
+        for I1, Ip in plan:
             s1, sp = diag[I1], diag[Ip]
-            M = out.ptr((I1, Ip))
-            for i1, ip, fn in table:
-                k = s1.dims[i1 - 1]
-                if k == 0 or sp.dims[ip - 1] == 0:
+            dq = (I1[0] - Ip[0], I1[1] - Ip[1])
+            for tdq, ch, table in self.T.RECALC_F:
+                if tdq != dq:
                     continue
-                if k != sp.dims[ip - 1]:
-                    raise AssertionError("size2(A) == size2(B)")  # product, c++/numerics_ublas.hpp:112
-                rows.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, 0, 0,
-                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, fn(Ip[1])))
+                M = out.ptr((I1, Ip), ch)
+                for i1, ip, fn in table:
+                    k = s1.dims[i1 - 1]
+                    if k == 0 or sp.dims[ip - 1] == 0:
+                        continue
+                    if k != sp.dims[ip - 1]:
+                        raise AssertionError("size2(A) == size2(B)")  # product, c++/numerics_ublas.hpp:112
+                    rows.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, 0, 0,
+                                 sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, fn(Ip[1])))
         if rows:
             gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
+        self.opch_keys = [set(out.loc)] * self.T.channels
         return out
 
     def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet) -> MatSet:
@@ -587,7 +618,7 @@ class QSRun:
             if k == 0:
                 continue
             M = out.ptr(I)
-            for i, a in enumerate(qs.ancestors(I)):
+            for i, a in enumerate(self.T.ancestors(I)):
                 w = s.dims[i]
                 if w == 0 or not qs.allowed(a) or a not in cold.loc:
                     continue
@@ -612,7 +643,7 @@ class QSRun:
         for I1, s1 in diag.items():
             if not s1.nstored:
                 continue
-            for dq, table in qs.DOUBLET:
+            for dq, table in self.T.DOUBLET:
                 Ip = (I1[0] + dq[0], I1[1] + dq[1])
                 sp = diag.get(Ip)
                 if sp is not None and sp.nstored:
@@ -622,7 +653,7 @@ class QSRun:
         base = []
         for I1, Ip, table in plan:
             s1, sp = diag[I1], diag[Ip]
-            anc1, ancp = qs.ancestors(I1), qs.ancestors(Ip)
+            anc1, ancp = self.T.ancestors(I1), self.T.ancestors(Ip)
             M = out.ptr((I1, Ip))
             for i1, ip, fn in table:
                 IN1, INp = anc1[i1 - 1], ancp[ip - 1]
@@ -680,7 +711,7 @@ class QSRun:
                 dim = sP.nstored
                 if dim == 0:
                     continue
-                for i, dl in enumerate(qs.IN):
+                for i, dl in enumerate(self.T.IN):
                     sub = (I[0] - dl[0], I[1] - dl[1])
                     sN = diagN.get(sub)
                     if sN is None:

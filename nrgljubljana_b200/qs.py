@@ -1,14 +1,18 @@
-"""Symmetry type QS (charge Q, total spin SS = 2S+1), one channel, without substeps.
+"""Symmetry type QS (charge Q, total spin SS = 2S+1), one or two channels, without substeps.
 
 The tables below are the reference's coefficient tables for this symmetry, restated:
-  In / QN                c++/symmetry/coefnew/qs/qs-1ch-In2.dat, qs-1ch-QN.dat
-  diagonal shifts        c++/symmetry/coefnew/qs/qs-1ch-diag.dat
-  off-diagonal factors   c++/symmetry/coefnew/qs/qs-1ch-offdiag.dat
-  <||f||> recalculation  c++/symmetry/coefnew/qs/qs-1ch-spinupa.dat, qs-1ch-spindowna.dat
-                         (driven by SymmetryQS::recalc_irreduc, c++/symmetry/nrg-recalc-QS.hpp:192-330)
+  In / QN                c++/symmetry/coefnew/qs/qs-{1,2}ch-In2.dat, qs-{1,2}ch-QN.dat
+  diagonal shifts        c++/symmetry/coefnew/qs/qs-{1,2}ch-diag.dat
+  off-diagonal factors   c++/symmetry/coefnew/qs/qs-{1,2}ch-offdiag.dat
+  <||f||> recalculation  c++/symmetry/coefnew/qs/qs-1ch-spin{up,down}a.dat,
+                         qs-2ch-spin{up,down}{a,b}.dat (channel 0: a, channel 1: b)
+                         (driven by SymmetryQS::recalc_irreduc, c++/symmetry/nrg-recalc-QS.hpp:192-460)
+  doublet recalculation  c++/symmetry/coefnew/qs/qs-1ch-doublet{p,m}.dat
+                         (SymmetryQS::recalc_doublet, c++/symmetry/nrg-recalc-QS.hpp:32-117)
 and the rules of c++/symmetry/sym-QS-impl.hpp:13-93 and c++/symmetry.hpp:31-35, 87-113.
-A factor is evaluated only when its block contributes, as the reference's macros do, so
-that no factor with a division by zero is ever formed.
+A factor is evaluated only when its blocks are not empty, as the reference's macros and
+the empty-block checks of product/transform arrange, so that no factor with a division by
+zero (S = 0) is ever used.
 """
 from __future__ import annotations
 
@@ -16,12 +20,7 @@ import math
 from typing import Callable, List, Tuple
 
 Invar = Tuple[int, int]
-
-COMBS = 4
-# In[i]: the ancestor of subspace I through combination i is I + In[i] (c++/symmetry.hpp:100-105).
-IN: List[Invar] = [(1, 0), (0, -1), (0, 1), (-1, 0)]
-# QN[i]: quantum numbers of the added site's states in combination i.
-QN: List[Invar] = [(-1, 1), (0, 2), (0, 2), (1, 1)]
+Fn = Callable[[int], float]
 
 
 def S(ss: int) -> float:
@@ -45,36 +44,7 @@ def triangle(I1: Invar, I2: Invar, I3: Invar) -> bool:
     return I1[0] == I2[0] + I3[0] and su2_triangle(I1[1], I2[1], I3[1])
 
 
-def ancestors(I: Invar) -> List[Invar]:
-    return [(I[0] + d[0], I[1] + d[1]) for d in IN]
-
-
-def new_subspaces(I: Invar) -> List[Invar]:
-    return [(I[0] - d[0], I[1] - d[1]) for d in IN]
-
-
-# (i, j, channel, factor(ss)) with 1-based combination indexes; the block (i, j) gets
-# factor * xi(N, ch) / scale * <In[i]||f||In[j]>.
-OFFDIAG: List[Tuple[int, int, int, Callable[[int], float]]] = [
-    (1, 2, 0, lambda ss: 1.0),
-    (1, 3, 0, lambda ss: 1.0),
-    (2, 4, 0, lambda ss: -(math.sqrt(2) * math.sqrt(S(ss) / (1 + 2 * S(ss))))),
-    (3, 4, 0, lambda ss: (1 + S(ss)) / math.sqrt(0.5 + (3 * S(ss)) / 2. + S(ss) ** 2)),
-]
-
-# (i, channel, number of electrons added): the diagonal of block i gets
-# zeta(N+1, ch) * (number - avgoccup) / scale, avgoccup = 1 for spin-1/2 electrons.
-DIAG: List[Tuple[int, int, float]] = [(1, 0, 0.0), (2, 0, 1.0), (3, 0, 1.0), (4, 0, 2.0)]
-AVGOCCUP = 1.0
-
-# <I1||f||Ip> for I1 = Ip + (1, +1) and I1 = Ip + (1, -1): rows (i1, ip, factor(ssp)).
-RECALC_F: List[Tuple[Invar, List[Tuple[int, int, Callable[[int], float]]]]] = [
-    ((1, 1), [(2, 1, lambda ssp: 1.0),
-              (4, 3, lambda ssp: -math.sqrt(1 - 1 / (2. * (1 + S(ssp)))))]),
-    ((1, -1), [(3, 1, lambda ssp: 1.0),
-               (4, 2, lambda ssp: math.sqrt(1 + 1 / (2. * S(ssp))))]),
-]
-
+AVGOCCUP = 1.0  # per channel: multiplicity 2 of an electron divided by 2
 TD_FIELDS = ("<Sz^2>", "<Q>", "<Q^2>")
 
 
@@ -88,24 +58,195 @@ def td_extra(Zs, subspaces, Z: float) -> List[float]:
         trSZ += sumZ * (ss * ss - 1) / 12.
     return [trSZ / Z, trQ / Z, trQ2 / Z]
 
-# Doublet operators <I1||O||Ip> with Ip = I1 + (-1, +1) (qs-1ch-doubletp.dat) and
-# Ip = I1 + (-1, -1) (qs-1ch-doubletm.dat), driven by SymmetryQS::recalc_doublet
-# (c++/symmetry/nrg-recalc-QS.hpp:32-117): rows (i1, ip, factor(ss1)); the old matrix is the
-# one between the ancestors of I1 through i1 and of Ip through ip.
-DOUBLET: List[Tuple[Invar, List[Tuple[int, int, Callable[[int], float]]]]] = [
-    ((-1, 1), [(1, 1, lambda ss: 1.0),
-               (2, 2, lambda ss: (-2 * math.sqrt(S(ss) * (1 + S(ss)))) / (1 + 2 * S(ss))),
-               (3, 2, lambda ss: 1 / (1 + 2 * S(ss))),
-               (3, 3, lambda ss: -1.0),
-               (4, 4, lambda ss: 1.0)]),
-    ((-1, -1), [(1, 1, lambda ss: 1.0),
-                (2, 2, lambda ss: -1.0),
-                (2, 3, lambda ss: 1 / (-1 - 2 * S(ss))),
-                (3, 3, lambda ss: (-2 * (1 + S(ss))) / math.sqrt(5 + 1 / S(ss) + 8 * S(ss) + 4 * S(ss) ** 2)),
-                (4, 4, lambda ss: 1.0)]),
-]
-
 
 def specdens_factor(Ip: Invar, I1: Invar) -> float:
     """SymmetryQS::specdens_factor (c++/symmetry/sym-QS-impl.hpp:64-70)."""
     return S(Ip[1]) + 1.0 if I1[1] == Ip[1] + 1 else S(Ip[1])
+
+
+class Tables:
+    """The coefficient tables of one channel count.
+
+    IN[i]       the ancestor of subspace I through combination i is I + IN[i]
+    QN[i]       quantum numbers of the added shell's states of combination i
+    OFFDIAG     (i, j, channel, factor(ss)), 1-based combinations: block (i, j) gets
+                factor * xi(N, ch) / scale * <IN[i]||f_ch||IN[j]>
+    DIAG        (i, channel, electrons added in that channel): the diagonal of block i gets
+                zeta(N+1, ch) * (number - AVGOCCUP) / scale
+    DIAG_FIRST  whether make_matrix lists the diagonal table before the off-diagonal one
+    RECALC_F    (dq, channel, rows (i1, ip, factor(ssp))): <I1||f_ch||Ip> for I1 = Ip + dq
+    DOUBLET     (dq, rows (i1, ip, factor(ss1))): a doublet operator for Ip = I1 + dq
+    """
+
+    def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET):
+        self.channels = channels
+        self.COMBS = len(IN)
+        self.IN, self.QN = IN, QN
+        self.OFFDIAG, self.DIAG, self.DIAG_FIRST = OFFDIAG, DIAG, DIAG_FIRST
+        self.RECALC_F, self.DOUBLET = RECALC_F, DOUBLET
+
+    def ancestors(self, I: Invar) -> List[Invar]:
+        return [(I[0] + d[0], I[1] + d[1]) for d in self.IN]
+
+    def new_subspaces(self, I: Invar) -> List[Invar]:
+        return [(I[0] - d[0], I[1] - d[1]) for d in self.IN]
+
+
+def _one(ss):
+    return 1.0
+
+
+QS1 = Tables(
+    1,
+    IN=[(1, 0), (0, -1), (0, 1), (-1, 0)],
+    QN=[(-1, 1), (0, 2), (0, 2), (1, 1)],
+    OFFDIAG=[
+        (1, 2, 0, _one),
+        (1, 3, 0, _one),
+        (2, 4, 0, lambda ss: -(math.sqrt(2) * math.sqrt(S(ss) / (1 + 2 * S(ss))))),
+        (3, 4, 0, lambda ss: (1 + S(ss)) / math.sqrt(0.5 + (3 * S(ss)) / 2. + S(ss) ** 2)),
+    ],
+    DIAG=[(1, 0, 0.0), (2, 0, 1.0), (3, 0, 1.0), (4, 0, 2.0)],
+    DIAG_FIRST=False,
+    RECALC_F=[
+        ((1, 1), 0, [(2, 1, _one), (4, 3, lambda ssp: -math.sqrt(1 - 1 / (2. * (1 + S(ssp)))))]),
+        ((1, -1), 0, [(3, 1, _one), (4, 2, lambda ssp: math.sqrt(1 + 1 / (2. * S(ssp))))]),
+    ],
+    DOUBLET=[
+        ((-1, 1), [(1, 1, _one),
+                   (2, 2, lambda ss: (-2 * math.sqrt(S(ss) * (1 + S(ss)))) / (1 + 2 * S(ss))),
+                   (3, 2, lambda ss: 1 / (1 + 2 * S(ss))),
+                   (3, 3, lambda ss: -1.0),
+                   (4, 4, _one)]),
+        ((-1, -1), [(1, 1, _one),
+                    (2, 2, lambda ss: -1.0),
+                    (2, 3, lambda ss: 1 / (-1 - 2 * S(ss))),
+                    (3, 3, lambda ss: (-2 * (1 + S(ss))) / math.sqrt(5 + 1 / S(ss) + 8 * S(ss) + 4 * S(ss) ** 2)),
+                    (4, 4, _one)]),
+    ],
+)
+
+
+def _a(ss):  # sqrt(S/(1+2S))
+    return math.sqrt(S(ss) / (1 + 2 * S(ss)))
+
+
+def _b(ss):  # (1+S)/sqrt((1+S)(1+2S))
+    return (1 + S(ss)) / math.sqrt((1 + S(ss)) * (1 + 2 * S(ss)))
+
+
+def _b2(ss):  # sqrt(2)(1+S)/sqrt((1+S)(1+2S))
+    return (math.sqrt(2) * (1 + S(ss))) / math.sqrt((1 + S(ss)) * (1 + 2 * S(ss)))
+
+
+def _c(ssp):  # 1/sqrt(1 + 1/(1+2S))
+    return 1 / math.sqrt(1 + 1 / (1 + 2 * S(ssp)))
+
+
+QS2 = Tables(
+    2,
+    IN=[(2, 0), (1, -1), (1, 1), (1, -1), (1, 1), (0, 0), (0, 0), (0, 0), (0, -2), (0, 0), (0, 2),
+        (-1, -1), (-1, 1), (-1, -1), (-1, 1), (-2, 0)],
+    QN=[(-2, 1), (-1, 2), (-1, 2), (-1, 2), (-1, 2), (0, 1), (0, 1), (0, 1), (0, 3), (0, 3), (0, 3),
+        (1, 2), (1, 2), (1, 2), (1, 2), (2, 1)],
+    OFFDIAG=[
+        (1, 4, 0, _one),
+        (1, 5, 0, _one),
+        (2, 7, 0, lambda ss: -_a(ss)),
+        (2, 9, 0, _one),
+        (2, 10, 0, _b),
+        (3, 7, 0, _b),
+        (3, 10, 0, _a),
+        (3, 11, 0, _one),
+        (4, 8, 0, lambda ss: -(math.sqrt(2) * _a(ss))),
+        (5, 8, 0, _b2),
+        (6, 12, 0, _one),
+        (6, 13, 0, _one),
+        (7, 14, 0, lambda ss: -(1 / math.sqrt(2))),
+        (7, 15, 0, lambda ss: -(1 / math.sqrt(2))),
+        (9, 14, 0, lambda ss: -math.sqrt(1 - 1 / (2. * S(ss)))),
+        (10, 14, 0, lambda ss: math.sqrt(1 + 1 / S(ss)) / math.sqrt(2)),
+        (10, 15, 0, lambda ss: -(1 / math.sqrt(2 + 2 / S(ss)))),
+        (11, 15, 0, lambda ss: math.sqrt(1 + 1 / (2 + 2 * S(ss)))),
+        (12, 16, 0, lambda ss: -(math.sqrt(2) * _a(ss))),
+        (13, 16, 0, _b2),
+        (1, 2, 1, _one),
+        (1, 3, 1, _one),
+        (2, 6, 1, lambda ss: -(math.sqrt(2) * _a(ss))),
+        (3, 6, 1, _b2),
+        (4, 7, 1, lambda ss: -_a(ss)),
+        (4, 9, 1, lambda ss: -1.0),
+        (4, 10, 1, lambda ss: -_b(ss)),
+        (5, 7, 1, _b),
+        (5, 10, 1, lambda ss: -_a(ss)),
+        (5, 11, 1, lambda ss: -1.0),
+        (7, 12, 1, lambda ss: -(1 / math.sqrt(2))),
+        (7, 13, 1, lambda ss: -(1 / math.sqrt(2))),
+        (8, 14, 1, _one),
+        (8, 15, 1, _one),
+        (9, 12, 1, lambda ss: math.sqrt(1 - 1 / (2. * S(ss)))),
+        (10, 12, 1, lambda ss: -(math.sqrt(1 + 1 / S(ss)) / math.sqrt(2))),
+        (10, 13, 1, lambda ss: 1 / math.sqrt(2 + 2 / S(ss))),
+        (11, 13, 1, lambda ss: -(math.sqrt(2 + 1 / (1 + S(ss))) / math.sqrt(2))),
+        (14, 16, 1, lambda ss: -(math.sqrt(2) * _a(ss))),
+        (15, 16, 1, _b2),
+    ],
+    DIAG=[(1, 0, 0.0), (2, 0, 0.0), (3, 0, 0.0), (4, 0, 1.0), (5, 0, 1.0), (6, 0, 0.0), (7, 0, 1.0), (8, 0, 2.0),
+          (9, 0, 1.0), (10, 0, 1.0), (11, 0, 1.0), (12, 0, 1.0), (13, 0, 1.0), (14, 0, 2.0), (15, 0, 2.0),
+          (16, 0, 2.0),
+          (1, 1, 0.0), (2, 1, 1.0), (3, 1, 1.0), (4, 1, 0.0), (5, 1, 0.0), (6, 1, 2.0), (7, 1, 1.0), (8, 1, 0.0),
+          (9, 1, 1.0), (10, 1, 1.0), (11, 1, 1.0), (12, 1, 2.0), (13, 1, 2.0), (14, 1, 1.0), (15, 1, 1.0),
+          (16, 1, 2.0)],
+    DIAG_FIRST=True,
+    RECALC_F=[
+        ((1, 1), 0, [(4, 1, _one),
+                     (7, 3, lambda s: -math.sqrt(2 - 1 / (1 + S(s))) / 2.),
+                     (8, 5, lambda s: -_c(s)),
+                     (9, 2, lambda s: -1.0),
+                     (10, 3, lambda s: -math.sqrt(2 + 1 / (1 + S(s))) / 2.),
+                     (12, 6, _one),
+                     (14, 7, lambda s: -(1 / math.sqrt(2))),
+                     (14, 10, lambda s: S(s) / (math.sqrt(2) * math.sqrt(S(s) * (1 + S(s))))),
+                     (15, 11, _c),
+                     (16, 13, lambda s: -_c(s))]),
+        ((1, 1), 1, [(2, 1, _one),
+                     (6, 3, lambda s: -_c(s)),
+                     (7, 5, lambda s: -math.sqrt(2 - 1 / (1 + S(s))) / 2.),
+                     (9, 4, _one),
+                     (10, 5, lambda s: math.sqrt(2 + 1 / (1 + S(s))) / 2.),
+                     (12, 7, lambda s: -(1 / math.sqrt(2))),
+                     (12, 10, lambda s: -(S(s) / (math.sqrt(2) * math.sqrt(S(s) * (1 + S(s)))))),
+                     (13, 11, lambda s: -_c(s)),
+                     (14, 8, _one),
+                     (16, 15, lambda s: -_c(s))]),
+        ((1, -1), 0, [(5, 1, _one),
+                      (7, 2, lambda s: math.sqrt(2 + 1 / S(s)) / 2.),
+                      (8, 4, lambda s: math.sqrt(1 + 1 / (2. * S(s)))),
+                      (10, 2, lambda s: -math.sqrt(2 - 1 / S(s)) / 2.),
+                      (11, 3, lambda s: -1.0),
+                      (13, 6, _one),
+                      (14, 9, lambda s: -(math.sqrt(2 + 1 / S(s)) / math.sqrt(2))),
+                      (15, 7, lambda s: -(1 / math.sqrt(2))),
+                      (15, 10, lambda s: -(math.sqrt(1 + 1 / S(s)) / math.sqrt(2))),
+                      (16, 12, lambda s: math.sqrt(1 + 1 / (2. * S(s))))]),
+        ((1, -1), 1, [(3, 1, _one),
+                      (6, 2, lambda s: math.sqrt(1 + 1 / (2. * S(s)))),
+                      (7, 4, lambda s: math.sqrt(2 + 1 / S(s)) / 2.),
+                      (10, 4, lambda s: math.sqrt(2 - 1 / S(s)) / 2.),
+                      (11, 5, _one),
+                      (12, 9, lambda s: math.sqrt(1 + 1 / (2. * S(s)))),
+                      (13, 7, lambda s: -(1 / math.sqrt(2))),
+                      (13, 10, lambda s: math.sqrt(1 + 1 / S(s)) / math.sqrt(2)),
+                      (15, 8, _one),
+                      (16, 14, lambda s: math.sqrt(1 + 1 / (2. * S(s))))]),
+    ],
+    DOUBLET=[],
+)
+
+
+def tables(channels: int) -> Tables:
+    if channels == 1:
+        return QS1
+    if channels == 2:
+        return QS2
+    raise ValueError(f"QS with {channels} channels is not supported")

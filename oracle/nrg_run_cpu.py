@@ -35,24 +35,17 @@ import numpy as np
 from . import oracle as O
 from nrgljubljana_b200.inputs import SCALE, parse_param, read_data
 
-# QS one-channel tables (c++/symmetry/coefnew/qs/qs-1ch-*.dat)
-_IN = [(1, 0), (0, -1), (0, 1), (-1, 0)]
-_QN = [(-1, 1), (0, 2), (0, 2), (1, 1)]
+# The QS coefficient tables (In, QN, the diagonal / off-diagonal factors and the <||f||>
+# recalculation rows of c++/symmetry/coefnew/qs/qs-{1,2}ch-*.dat) are data of the symmetry,
+# shared with the product (nrgljubljana_b200.qs); they are pinned by the reference's
+# regression outputs through both implementations.
+from nrgljubljana_b200 import qs as _qs
 
 
 def _S(ss):
     return (ss - 1.0) / 2.0
 
 
-_OFFDIAG = [
-    (1, 2, lambda ss: 1),
-    (1, 3, lambda ss: 1),
-    (2, 4, lambda ss: -(math.sqrt(2) * math.sqrt(_S(ss) / (1 + 2 * _S(ss))))),
-    (3, 4, lambda ss: (1 + _S(ss)) / math.sqrt(0.5 + (3 * _S(ss)) / 2. + math.pow(_S(ss), 2))),
-]
-_DIAG = [(1, 0), (2, 1), (3, 1), (4, 2)]
-_SPINUP = [(2, 1, lambda s: 1), (4, 3, lambda s: -math.sqrt(1 - 1 / (2. * (1 + _S(s)))))]
-_SPINDOWN = [(3, 1, lambda s: 1), (4, 2, lambda s: math.sqrt(1 + 1 / (2. * _S(s))))]
 # doublet recalculation, Ip = (q1 - 1, ss1 + 1) and (q1 - 1, ss1 - 1): rows (i1, ip, factor(ss1))
 _DOUBLETP = [(1, 1, lambda s: 1), (2, 2, lambda s: (-2 * math.sqrt(_S(s) * (1 + _S(s)))) / (1 + 2 * _S(s))),
              (3, 2, lambda s: 1 / (1 + 2 * _S(s))), (3, 3, lambda s: -1), (4, 4, lambda s: 1)]
@@ -113,10 +106,14 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
     fixeps = float(kv.get("fixeps", 1e-15))
     betabar = float(kv.get("betabar", 1.0))
     strategy = kv.get("strategy", "kept")
-    lastall = kv.get("lastall", "false").lower() == "true"
+    flag = lambda k: kv.get(k, "false").lower() == "true"  # noqa: E731
+    # Params::keep_all_states_in_last_step (c++/params.hpp:535-539)
+    lastall = flag("lastall") or ((flag("fdm") or flag("fdmexpv")) and not flag("lastalloverride"))
     rescaled = kv.get("data_has_rescaled_energies", "true").lower() == "true"
     d = read_data(data_text)
     Nmax = d.nmax
+    T = _qs.tables(d.channels)
+    _IN, _QN, C = T.IN, T.QN, T.COMBS
     O.blas_threads(1)  # one BLAS thread per block, as diagonalisations_OpenMP runs dsyev
 
     def scale_of(trueN):
@@ -126,7 +123,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
     for I, e in sorted(d.subspaces):
         v = e.copy() if rescaled else e / SCALE(0, Lam, disc, z)
         diag[I] = _Eig(v)
-    opch = dict(d.opch[0][0])
+    opch = [dict(d.opch[ch][0]) for ch in range(d.channels)]
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
     dm = kv.get("dmnrg", "false").lower() == "true" and spectra is not None
@@ -187,17 +184,20 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
             anc, dims = structure[I]
             off = np.concatenate([[0], np.cumsum(dims)]).astype(int)
             h = np.zeros((off[-1], off[-1]))
-            for i in range(4):
+            for i in range(C):
                 for n in range(dims[i]):
                     h[off[i] + n, off[i] + n] = math.sqrt(Lam) * diag[anc[i]].corr[n]
-            for (i, j, fn) in _OFFDIAG:
+            for (i, j, ch, fn) in T.OFFDIAG:
                 if dims[i - 1] and dims[j - 1]:
-                    fs = (fn(I[1]) * d.xi[0][N]) / scale
-                    mat = opch[(anc[i - 1], anc[j - 1])]
-                    h[off[i - 1]:off[i], off[j - 1]:off[j]] += fs * mat
-            for (i, number) in _DIAG:
+                    fs = (fn(I[1]) * d.xi[ch][N]) / scale
+                    mat = opch[ch][(anc[i - 1], anc[j - 1])]
+                    if i > j:
+                        h[off[j - 1]:off[j], off[i - 1]:off[i]] += fs * mat.T
+                    else:
+                        h[off[i - 1]:off[i], off[j - 1]:off[j]] += fs * mat
+            for (i, ch, number) in T.DIAG:
                 for jj in range(off[i - 1], off[i]):
-                    h[jj, jj] += d.zeta[0][N + 1] * (number - 1 * 1.0) / scale
+                    h[jj, jj] += d.zeta[ch][N + 1] * (number - 1 * 1.0) / scale
             blocks.append(h)
         vals, vecs = O.diag_batch(blocks, nthreads=threads)
         new = {I: _Eig(vals[b], vecs[b]) for b, I in enumerate(tasks)}
@@ -235,7 +235,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
         for I, e in new.items():
             anc, dims = structure[I]
             off = np.concatenate([[0], np.cumsum(dims)]).astype(int)
-            e.U = [np.ascontiguousarray(e.vectors[:, off[i]:off[i + 1]]) for i in range(4)]
+            e.U = [np.ascontiguousarray(e.vectors[:, off[i]:off[i + 1]]) for i in range(C)]
 
         def recalc_ops(nrows):
             out = {}
@@ -246,7 +246,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
                     anc, dims = structure[I]
                     k = nrows(e)
                     m = np.zeros((k, k))
-                    for i in range(4):
+                    for i in range(C):
                         a = anc[i]
                         if a[1] <= 0 or a not in cold or k == 0 or dims[i] == 0:
                             continue
@@ -263,9 +263,9 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
         for e in new.values():
             e.nrstored = e.nrpost
         if not last:
-            nf = {}
+            nf = [dict() for _ in range(d.channels)]
             for Ip, ep in new.items():
-                for dq, table in (((1, 1), _SPINUP), ((1, -1), _SPINDOWN)):
+                for dq, ch, table in T.RECALC_F:
                     I1 = (Ip[0] + dq[0], Ip[1] + dq[1])
                     if I1 not in new or not (new[I1].nrstored and ep.nrstored):
                         continue
@@ -276,7 +276,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
                         B = np.ascontiguousarray(ep.U[ip - 1][:ep.nrstored])
                         if A.shape[1] and B.shape[1]:
                             O.product(f, fn(Ip[1]), A, B)
-                    nf[(I1, Ip)] = f
+                    nf[ch][(I1, Ip)] = f
             opch = nf
         if strategy == "kept":
             ops = recalc_ops(lambda e: e.nrstored)
@@ -357,7 +357,7 @@ def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
             dim = eP.nrstored
             M = np.zeros((dim, dim))
             if dim:
-                for i, dl in enumerate(_IN):
+                for i, dl in enumerate(_qs.QS1.IN):
                     sub = (I[0] - dl[0], I[1] - dl[1])
                     if sub not in rhoN or sub not in diagN:
                         continue

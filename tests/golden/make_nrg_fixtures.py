@@ -1,6 +1,6 @@
 """Regenerate the NRG-run fixtures under tests/golden/nrg/ from the reference's regression tests.
 
-Each case directory of the reference's ``test/c++/<case>/`` holds the run's input (``param``,
+Each case directory of the reference's ``test/c++/<case>/`` (or ``test/c++sym_all/<case>/``) holds the run's input (``param``,
 ``data``) and the outputs the reference produced with a real LAPACK (``ref/td``,
 ``ref/custom``, printed to 10 significant digits). They are copied here unchanged so that
 the tests can run where the reference tree is absent. Usage:
@@ -17,14 +17,16 @@ CASES = [
     "test14_strategy_kept", "test15_safeguard", "test16_safeguardmax", "test35_betabar",
     "test56_dsyevd", "test56_dsyevr", "test200_data_has", "legacy_simple", "legacy_Himp",
     "test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins",
+    "c++sym_all/test300_QS_ref", "c++sym_all/test310_QS_ref",
 ]
 
 
 def main(ref_root: str) -> None:
     out_root = os.path.join(os.path.dirname(os.path.abspath(__file__)), "nrg")
     for case in CASES:
-        src = os.path.join(ref_root, "test", "c++", case)
-        dst = os.path.join(out_root, case)
+        sub, name = case.split("/") if "/" in case else ("c++", case)
+        src = os.path.join(ref_root, "test", sub, case.split("/")[-1])
+        dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
         for name, rel in (("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom"),
                           ("spec_DMNRG_dens_A_d-A_d.dat", "ref/spec_DMNRG_dens_A_d-A_d.dat")):
