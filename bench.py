@@ -400,6 +400,8 @@ ops=n_d A_d
 dmnrg=true
 specd=A_d-A_d
 """
+C0_SPEC = "spec_DMNRG_dens_A_d-A_d"  # the DM-NRG spectral function of the C0 run
+
 NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delta=0), Gamma=0.04, flat band, "
                 "Lambda=2 (Z), z=1, Nmax=40, keep=1000, keepenergy=10, T=1e-8, operator n_d, DM-NRG spectral "
                 "function A_d-A_d (1000 bins/decade, broadened); input generated by nrgljubljana_b200.datagen")
@@ -500,10 +502,10 @@ def nrg_run_arm(torch, device: int, args) -> dict:
 
     def specdiff(other):
         """Largest difference of the A_d-A_d spectrum relative to its peak."""
-        a, b = res.spectra["A_d-A_d"][:, 1], np.asarray(other["A_d-A_d"])[:, 1]
+        a, b = res.spectra[C0_SPEC][:, 1], np.asarray(other[C0_SPEC])[:, 1]
         return float(np.max(np.abs(a - b)) / np.max(np.abs(a)))
     out["per_block_gpu"]["spectrum_max_diff_rel_to_peak"] = specdiff(res_pb.spectra)
-    out["spectrum_points"] = int(len(res.spectra["A_d-A_d"]))
+    out["spectrum_points"] = int(len(res.spectra[C0_SPEC]))
     if not args.no_cpu:
         from oracle import oracle as O
         from oracle import nrg_run_cpu

@@ -41,7 +41,7 @@ Invar = Tuple[int, int]
 _IGNORED = {
     "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
     "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
-    "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom", "specs", "spect",
+    "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom",
     "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
 }
 
@@ -69,10 +69,12 @@ class RunParams:
     fdmexpv: bool = False
     lastalloverride: bool = False
     data_has_rescaled_energies: bool = True
-    # DM-NRG spectral functions of the specd pairs (c++/params.hpp:181-396)
+    # DM-NRG spectra of the specs/specd/spect pairs (c++/params.hpp:181-396)
     T: float = 0.001
     dmnrg: bool = False
-    specd: str = ""
+    specs: str = ""   # correlators of singlet operators
+    specd: str = ""   # spectral functions of doublet operators
+    spect: str = ""   # dynamic spin susceptibilities of triplet operators
     bins: int = 1000
     emin: float = -1.0
     emax: float = -1.0
@@ -132,7 +134,8 @@ class Result:
     custom: List[List[float]]
     blocks_per_step: List[int] = field(default_factory=list)
     max_dim_per_step: List[int] = field(default_factory=list)
-    spectra: Dict[str, np.ndarray] = field(default_factory=dict)  # "op1-op2" -> rows (E, A(E))
+    # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_...", "spin_...") -> rows (E, A(E))
+    spectra: Dict[str, np.ndarray] = field(default_factory=dict)
 
 
 # ------------------------------------------------------------------ host bookkeeping
@@ -305,11 +308,21 @@ class QSRun:
         self.nmax = data.nmax
         self.sqrt_lambda = math.sqrt(params.Lambda)  # nrg_step_scale_factor (c++/params.hpp:639-641)
         self.op_names = sorted(n for n, (k, _) in data.ops.items() if k in "sg")
-        self.specd = [tuple(t.split("-", 1)) for t in params.specd.split()] if params.dmnrg else []
-        self.dop_names = sorted({x for pr in self.specd for x in pr})
-        for name in self.dop_names:
-            if name not in data.ops or data.ops[name][0] != "d":
-                raise ValueError(f"specd names {name}, which is not a doublet operator of the data file")
+        # (file prefix, kind, op1, op2) of the DM-NRG spectra (c++/oprecalc.hpp:160-195)
+        self.specs: List[Tuple[str, str, str, str]] = []
+        if params.dmnrg:
+            for prefix, kind, text in (("corr", "s", params.specs), ("spec", "d", params.specd),
+                                       ("spin", "t", params.spect)):
+                for tok in text.split():
+                    n1, n2 = tok.split("-", 1)
+                    for name in (n1, n2):
+                        k = data.ops.get(name, ("?",))[0]
+                        if not (k == kind or (kind == "s" and k == "g")):
+                            raise ValueError(f"{tok}: {name} is not a {dict(s='singlet', d='doublet', t='triplet')[kind]}"
+                                             " operator of the data file")
+                    self.specs.append((prefix, kind, n1, n2))
+        self.dop_names = sorted({x for sp in self.specs if sp[1] == "d" for x in sp[2:]})
+        self.top_names = sorted({x for sp in self.specs if sp[1] == "t" for x in sp[2:]})
 
     # ---- scales (c++/step.hpp:30-39)
     def scale(self, trueN: int) -> float:
@@ -380,13 +393,15 @@ class QSRun:
                           [])
         self.meas: List[_Measure] = []
         self.dm_steps: List[tuple] = []
-        if self.dop_names:
-            dmats = [dict(d.ops[name][1]) for name in self.dop_names]
-            dshapes = {}
-            for m in dmats:
-                for k, mat in m.items():
-                    dshapes[k] = mat.shape
-            self.dops = MatSet(self.dev, dshapes, len(self.dop_names), _pack(dmats, dshapes))
+        self.tensor_ops = {}
+        for kind, names in (("d", self.dop_names), ("t", self.top_names)):
+            if names:
+                tmats = [dict(d.ops[name][1]) for name in names]
+                tshapes = {}
+                for m in tmats:
+                    for k, mat in m.items():
+                        tshapes[k] = mat.shape
+                self.tensor_ops[kind] = MatSet(self.dev, tshapes, len(names), _pack(tmats, tshapes))
         if p.calc0:
             self.res.td.append(self._td(-1, diag))
             self.meas.append(self._measure(-1, diag, self.ops))
@@ -558,9 +573,11 @@ class QSRun:
             new_ops = self._recalc_singlets(diag, ops)
             meas.append(self._measure(N, diag, new_ops))
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
-        if self.dop_names:  # DM-NRG keeps every step's eigenvectors and doublet operators
-            self.dops = self._recalc_doublets(diag, self.dops)
-            self.dm_steps.append((N, self.scale(N), diag, self.dops, job.Vbuf))
+        if self.specs:  # DM-NRG keeps every step's eigenvectors and the operators of its spectra
+            tables = {"d": (self.T.DOUBLET, lambda fn, ss: fn(ss)), "t": (self.T.TRIPLET, qs.triplet_factor)}
+            for kind, cold in self.tensor_ops.items():
+                self.tensor_ops[kind] = self._recalc_tensor(diag, cold, *tables[kind])
+            self.dm_steps.append((N, self.scale(N), diag, dict(self.tensor_ops, s=new_ops), job.Vbuf))
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
@@ -635,21 +652,21 @@ class QSRun:
         return out
 
 
-    def _recalc_doublets(self, diag: Dict[Invar, Sub], cold: MatSet) -> MatSet:
-        """SymmetryQS::recalc_doublet (c++/symmetry/nrg-recalc-QS.hpp:32-117) through
-        recalc_general (c++/recalc.hpp:82-108) over the kept states, every doublet operator
-        of the spectra in one batched call (operator-major)."""
+    def _recalc_tensor(self, diag: Dict[Invar, Sub], cold: MatSet, tables, factor) -> MatSet:
+        """SymmetryQS::recalc_doublet / recalc_triplet (c++/symmetry/nrg-recalc-QS.hpp:32-117,
+        495-640) through recalc_general (c++/recalc.hpp:82-108) over the kept states, every
+        operator of the set in one batched call (operator-major). `tables` lists (dq, rows)
+        for Ip = I1 + dq; factor(fn, ss1) evaluates a row's coefficient."""
         plan = []
         for I1, s1 in diag.items():
             if not s1.nstored:
                 continue
-            for dq, table in self.T.DOUBLET:
+            for dq, table in tables:
                 Ip = (I1[0] + dq[0], I1[1] + dq[1])
                 sp = diag.get(Ip)
                 if sp is not None and sp.nstored:
                     plan.append((I1, Ip, table))
-        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan},
-                     len(self.dop_names))
+        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan}, cold.nops)
         base = []
         for I1, Ip, table in plan:
             s1, sp = diag[I1], diag[Ip]
@@ -664,18 +681,19 @@ class QSRun:
                     continue
                 _, r, c = cold.loc[(IN1, INp)]
                 base.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, cold.ptr((IN1, INp)), c,
-                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, w1, wp, 0, 1, fn(I1[1])))
+                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, w1, wp, 0, 1,
+                             factor(fn, I1[1])))
         if base:
             b = np.array(base, dtype=GEMM3_DTYPE)
-            t = np.tile(b, len(self.dop_names))
-            op = np.repeat(np.arange(len(self.dop_names), dtype=np.uint64), len(b))
+            t = np.tile(b, cold.nops)
+            op = np.repeat(np.arange(cold.nops, dtype=np.uint64), len(b))
             t["M"] += op * np.uint64(8 * out.total)
             t["O"] += op * np.uint64(8 * cold.total)
             gemm3_batch_array(t, self.ctx, self.stream)
         return out
 
     def _dmnrg(self) -> Dict[str, np.ndarray]:
-        """DM-NRG spectral functions of the specd pairs: the density matrix of the last step
+        """DM-NRG spectra of the specs/specd/spect pairs: the density matrix of the last step
         (init_rho, c++/dmnrg.hpp:43-50), the backward sweep (calc_densitymatrix_iterN / cdmI,
         c++/dmnrg.hpp:55-102) as batched rotate terms, per step the Algo_DMNRG pair sums binned
         on the device (c++/algo_DMNRG.hpp:29-52, c++/algo.hpp:55-67), N/N+2 (or N/N+1)
@@ -763,10 +781,15 @@ class QSRun:
             E /= p.broaden_ratio
         mesh = np.array(mesh)
         out: Dict[str, np.ndarray] = {}
-        for n1, n2 in self.specd:
-            o1, o2 = self.dop_names.index(n1), self.dop_names.index(n2)
+        # gf_type sign and factor of each kind (c++/oprecalc.hpp:160-195)
+        kinds = {"s": (1, qs.correlator_factor, self.op_names), "d": (-1, qs.specdens_factor, self.dop_names),
+                 "t": (1, qs.dynamicsusceptibility_factor, self.top_names)}
+        for prefix, kind, n1, n2 in self.specs:
+            sign, ff, names = kinds[kind]
+            o1, o2 = names.index(n1), names.index(n2)
             full_pos, full_neg = np.zeros(nb), np.zeros(nb)
-            for k, (N, scale, dg, dops, _) in enumerate(steps):
+            for k, (N, scale, dg, opsets, _) in enumerate(steps):
+                dops = opsets[kind]
                 merge = p.NN1 or p.NN2avg or ((N % 2 == 0) if p.NN2even else (N % 2 == 1))
                 if not merge:
                     continue
@@ -782,18 +805,18 @@ class QSRun:
                 pairs = []
                 for Ii, si in dg.items():
                     for Ij, sj in dg.items():
-                        key = (Ij, Ii)
-                        if key not in dops.loc or si.nstored == 0 or sj.nstored == 0:
+                        # singlet sets are keyed by the subspace (the block (I, I))
+                        key = Ii if kind == "s" else (Ij, Ii)
+                        if (kind == "s" and Ij != Ii) or key not in dops.loc or si.nstored == 0 or sj.nstored == 0:
                             continue
                         ki, kj = si.nstored, sj.nstored
                         pairs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], dops.ptr(key, o1), ki, dops.ptr(key, o2), ki,
-                                      rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj,
-                                      qs.specdens_factor(Ii, Ij)))
+                                      rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj, ff(Ii, Ij)))
                 pos = torch.zeros(nb, dtype=torch.float64, device=self.dev)
                 neg = torch.zeros(nb, dtype=torch.float64, device=self.dev)
                 Emin_w = scale * p.goodE
                 if pairs:
-                    spec_accumulate_array(0, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg, sign=-1,
+                    spec_accumulate_array(0, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg, sign=sign,
                                           Emin=Emin_w, Emax=Emin_w * Efac * Efac, ctx=self.ctx, stream=self.stream)
                 cp, cn = pos.cpu().numpy(), neg.cpu().numpy()
                 Ex, Emax_w = Emin_w * Efac, Emin_w * Efac * Efac
@@ -817,7 +840,7 @@ class QSRun:
             npos = len(mesh)
             rows_pos = sorted(zip(mesh_all[:npos].tolist(), vals[:npos].tolist()))
             rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
-            out[f"{n1}-{n2}"] = np.array(rows_neg + rows_pos)
+            out[f"{prefix}_DMNRG_dens_{n1}-{n2}"] = np.array(rows_neg + rows_pos)
         return out
 
 def window(e: np.ndarray, Emin: float, Ex: float, Emax: float, last: bool, first: bool, NNtanh: float) -> np.ndarray:
@@ -881,8 +904,8 @@ def main(argv=None) -> int:
     os.makedirs(out, exist_ok=True)
     _write_table(os.path.join(out, "td"), res.td_fields, res.td)
     _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom)
-    for name, rows in res.spectra.items():  # spec_DMNRG_dens_<name>.dat, as Spikes::save writes it
-        with open(os.path.join(out, f"spec_DMNRG_dens_{name}.dat"), "w") as f:
+    for name, rows in res.spectra.items():  # <prefix>_DMNRG_dens_<op1>-<op2>.dat, as Spikes::save writes it
+        with open(os.path.join(out, f"{name}.dat"), "w") as f:
             for e, v in rows:
                 f.write(f"{e:.10g} {v:.10g}\n")
     return 0

@@ -9,15 +9,21 @@ The tables below are the reference's coefficient tables for this symmetry, resta
                          (driven by SymmetryQS::recalc_irreduc, c++/symmetry/nrg-recalc-QS.hpp:192-460)
   doublet recalculation  c++/symmetry/coefnew/qs/qs-1ch-doublet{p,m}.dat
                          (SymmetryQS::recalc_doublet, c++/symmetry/nrg-recalc-QS.hpp:32-117)
+  triplet recalculation  c++/symmetry/coefnew/qs/qs-{1,2}ch-triplet{s,p,m}.dat
+                         (SymmetryQS::recalc_triplet, c++/symmetry/nrg-recalc-QS.hpp:495-640)
 and the rules of c++/symmetry/sym-QS-impl.hpp:13-93 and c++/symmetry.hpp:31-35, 87-113.
 A factor is evaluated only when its blocks are not empty, as the reference's macros and
 the empty-block checks of product/transform arrange, so that no factor with a division by
-zero (S = 0) is ever used.
+zero (S = 0) is ever used. The triplet factors are evaluated in IEEE double arithmetic, as
+the reference's C++ evaluates them: 1/sqrt(x/0) is 0, and a row whose factor is not finite is
+an error when it is used.
 """
 from __future__ import annotations
 
 import math
 from typing import Callable, List, Tuple
+
+import numpy as np
 
 Invar = Tuple[int, int]
 Fn = Callable[[int], float]
@@ -64,6 +70,32 @@ def specdens_factor(Ip: Invar, I1: Invar) -> float:
     return S(Ip[1]) + 1.0 if I1[1] == Ip[1] + 1 else S(Ip[1])
 
 
+def dynamicsusceptibility_factor(Ip: Invar, I1: Invar) -> float:
+    """SymmetryQS::dynamicsusceptibility_factor (c++/symmetry/sym-QS-impl.hpp:56-62)."""
+    ssp, ss1 = Ip[1], I1[1]
+    if ss1 == ssp + 2:
+        return 1.0 + (ssp - 1) / 3.0
+    if ss1 == ssp:
+        return ssp / 3.0
+    if ss1 == ssp - 2:
+        return (ssp - 2) / 3.0
+    raise AssertionError("abs(ss1 - ssp) == 2 || ss1 == ssp")
+
+
+def correlator_factor(Ip: Invar, I1: Invar) -> float:
+    """CorrelatorFactorFnc (c++/symmetry.hpp:235): the multiplicity of I1."""
+    return float(mult(I1))
+
+
+def triplet_factor(fn, ss1: int) -> float:
+    """A triplet-table factor at SS = ss1 in IEEE double arithmetic."""
+    with np.errstate(all="ignore"):
+        v = float(fn(np.float64((ss1 - 1) / 2.0)))
+    if not math.isfinite(v):
+        raise AssertionError(f"triplet recalculation factor is not finite at SS={ss1}")
+    return v
+
+
 class Tables:
     """The coefficient tables of one channel count.
 
@@ -76,14 +108,16 @@ class Tables:
     DIAG_FIRST  whether make_matrix lists the diagonal table before the off-diagonal one
     RECALC_F    (dq, channel, rows (i1, ip, factor(ssp))): <I1||f_ch||Ip> for I1 = Ip + dq
     DOUBLET     (dq, rows (i1, ip, factor(ss1))): a doublet operator for Ip = I1 + dq
+    TRIPLET     (dq, rows (i1, ip, factor(S1))): a triplet operator for Ip = I1 + dq, the factor
+                a function of the spin S1 of I1 (a numpy float64), see triplet_factor
     """
 
-    def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET):
+    def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET, TRIPLET):
         self.channels = channels
         self.COMBS = len(IN)
         self.IN, self.QN = IN, QN
         self.OFFDIAG, self.DIAG, self.DIAG_FIRST = OFFDIAG, DIAG, DIAG_FIRST
-        self.RECALC_F, self.DOUBLET = RECALC_F, DOUBLET
+        self.RECALC_F, self.DOUBLET, self.TRIPLET = RECALC_F, DOUBLET, TRIPLET
 
     def ancestors(self, I: Invar) -> List[Invar]:
         return [(I[0] + d[0], I[1] + d[1]) for d in self.IN]
@@ -124,6 +158,26 @@ QS1 = Tables(
                     (3, 3, lambda ss: (-2 * (1 + S(ss))) / math.sqrt(5 + 1 / S(ss) + 8 * S(ss) + 4 * S(ss) ** 2)),
                     (4, 4, _one)]),
     ],
+    TRIPLET=[
+        ((0, 0), [(1, 1, lambda s: 1.0),
+                  (2, 2, lambda s: np.sqrt(1 - 1 / s + 2 / (1 + 2 * s))),
+                  (2, 3, lambda s: 1 / np.sqrt((1 + s) * (1 + 2 * s))),
+                  (3, 2, lambda s: -(1 / np.sqrt(s * (1 + 2 * s)))),
+                  (3, 3, lambda s: (1 + s) * np.sqrt((s * (1 + 2 * s)) / ((1 + s) ** 3 * (3 + 2 * s)))
+                   + 2 * np.sqrt(s / (3 + 11 * s + 12 * s ** 2 + 4 * s ** 3))),
+                  (4, 4, lambda s: 1.0)]),
+        ((0, 2), [(1, 1, lambda s: 1.0),
+                  (2, 2, lambda s: np.sqrt(1 + 1 / (1 + s) - 2 / (1 + 2 * s))),
+                  (3, 2, lambda s: -(1 / np.sqrt((1 + s) * (1 + 2 * s)))),
+                  (3, 3, lambda s: 1.0),
+                  (4, 4, lambda s: 1.0)]),
+        ((0, -2), [(1, 1, lambda s: 1.0),
+                   (2, 2, lambda s: 1.0),
+                   (2, 3, lambda s: 1 / np.sqrt(s * (1 + 2 * s))),
+                   (3, 3, lambda s: (np.sqrt((-1 + 4 * s ** 2) / (s + s ** 2))
+                                     + np.sqrt((-1 + 2 * s) / (s + 3 * s ** 2 + 2 * s ** 3))) / 2.),
+                   (4, 4, lambda s: 1.0)]),
+    ],
 )
 
 
@@ -141,6 +195,94 @@ def _b2(ss):  # sqrt(2)(1+S)/sqrt((1+S)(1+2S))
 
 def _c(ssp):  # 1/sqrt(1 + 1/(1+2S))
     return 1 / math.sqrt(1 + 1 / (1 + 2 * S(ssp)))
+
+
+# two-channel triplet rows (qs-2ch-triplet{s,p,m}.dat); combinations 2/4, 3/5, 12/14 and
+# 13/15 carry the same factors
+def _t_lo(s):   # (i, i) for the lower-spin ancestor of a doublet shell
+    return 1 / np.sqrt((s * (1 + 2 * s)) / (-1 + s + 2 * s ** 2))
+
+
+def _t_x(s):    # lower -> higher
+    return 1 / np.sqrt((1 + s) * (1 + 2 * s))
+
+
+def _t_y(s):    # higher -> lower
+    return -(1 / np.sqrt(s * (1 + 2 * s)))
+
+
+def _t_hi(s):   # (i, i) for the higher-spin ancestor
+    return (3 + 2 * s) / np.sqrt(((1 + s) * (3 + 4 * s * (2 + s))) / s)
+
+
+def _t_1111(s):
+    r = (s * (2 + s) * (1 + 2 * s) ** 2) / ((1 + s) * (3 + 2 * s) ** 2)
+    a = s * (1 + s) * (2 + s)
+    num = (12 * np.sqrt(a) + 33 * np.sqrt(s ** 4 * a) + 24 * np.sqrt(s ** 6 * a) + 4 * np.sqrt(s ** 8 * a)
+           + 18 * np.sqrt(r) + s * (29 * np.sqrt(a) + 60 * np.sqrt(r) + 2 * s * np.sqrt(r) * (31 + 10 * s)))
+    return num / ((1 + s) ** 2.5 * (2 + s) * (3 + 2 * s) ** 2)
+
+
+def _u(s):      # 1.0 whatever s
+    return 1.0
+
+
+_T2S = ([(1, 1, _u)]
+        + [r for a, b in ((2, 3), (4, 5)) for r in ((a, a, _t_lo), (a, b, _t_x), (b, a, _t_y), (b, b, _t_hi))]
+        + [(6, 6, _u), (7, 7, _u), (8, 8, _u),
+           (9, 9, lambda s: np.sqrt(-1 + s ** 2) / s),
+           (9, 10, lambda s: np.sqrt(1 - 2 / (1 + 2 * s)) / s),
+           (10, 9, lambda s: -(1 / s)),
+           (10, 10, lambda s: 1 - 1 / s + 1 / (1 + s)),
+           (10, 11, lambda s: 1 / (1 + s)),
+           (11, 10, lambda s: -((3 + 2 * s) / ((1 + s) * np.sqrt(3 + 4 * s * (2 + s))))),
+           (11, 11, _t_1111)]
+        + [r for a, b in ((12, 13), (14, 15)) for r in ((a, a, _t_lo), (a, b, _t_x), (b, a, _t_y), (b, b, _t_hi))]
+        + [(16, 16, _u)])
+
+
+def _tp_a(s):
+    return np.sqrt((s * (1 + s) * (3 + 2 * s)) / (1 + 2 * s)) / (1 + s)
+
+
+def _tp_b(s):
+    return ((-np.sqrt((1 + s) * (1 + 2 * s) * (3 + 2 * s)) + 2 * s * np.sqrt(2 + s + 1 / (1 + 2 * s)))
+            / ((1 + s) * np.sqrt(3 + 2 * s)))
+
+
+_T2P = ([(1, 1, _u)]
+        + [r for a, b in ((2, 3), (4, 5)) for r in ((a, a, _tp_a), (b, a, _tp_b), (b, b, _u))]
+        + [(6, 6, _u), (7, 7, _u), (8, 8, _u),
+           (9, 9, lambda s: np.sqrt(-3 + 4 * s * (1 + s)) / (1 + 2 * s)),
+           (10, 9, lambda s: -(np.sqrt(3 + 4 * s * (2 + s)) / ((1 + s) * (1 + 2 * s)))),
+           (10, 10, lambda s: np.sqrt(s * (2 + s)) / (1 + s)),
+           (11, 9, lambda s: 1 / (1 + 3 * s + 2 * s ** 2)),
+           (11, 10, lambda s: -(1 / (1 + s))),
+           (11, 11, _u)]
+        + [r for a, b in ((12, 13), (14, 15)) for r in ((a, a, _tp_a), (b, a, _tp_b), (b, b, _u))]
+        + [(16, 16, _u)])
+
+
+def _tm_x(s):
+    return 1 / np.sqrt(s * (1 + 2 * s))
+
+
+def _tm_hi(s):
+    return (1 / np.sqrt((s * (1 + s) * (1 + 2 * s)) / (-1 + 2 * s))
+            + 1 / np.sqrt((s * (1 + s)) / (-1 + 4 * s ** 2))) / 2.
+
+
+_T2M = ([(1, 1, _u)]
+        + [r for a, b in ((2, 3), (4, 5)) for r in ((a, a, _u), (a, b, _tm_x), (b, b, _tm_hi))]
+        + [(6, 6, _u), (7, 7, _u), (8, 8, _u),
+           (9, 9, _u),
+           (9, 10, lambda s: 1 / s),
+           (9, 11, lambda s: 1 / (s + 2 * s ** 2)),
+           (10, 10, lambda s: np.sqrt(-1 + s ** 2) / s),
+           (10, 11, lambda s: np.sqrt(1 - 2 / (1 + 2 * s)) / s),
+           (11, 11, lambda s: np.sqrt(-3 + 4 * s * (1 + s)) / (1 + 2 * s))]
+        + [r for a, b in ((12, 13), (14, 15)) for r in ((a, a, _u), (a, b, _tm_x), (b, b, _tm_hi))]
+        + [(16, 16, _u)])
 
 
 QS2 = Tables(
@@ -241,6 +383,11 @@ QS2 = Tables(
                       (16, 14, lambda s: math.sqrt(1 + 1 / (2. * S(s))))]),
     ],
     DOUBLET=[],
+    TRIPLET=[
+        ((0, 0), _T2S),
+        ((0, 2), _T2P),
+        ((0, -2), _T2M),
+    ],
 )
 
 

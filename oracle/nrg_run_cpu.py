@@ -92,8 +92,8 @@ class _Eig:
 def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
         ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
     """td and custom rows of the run; with dmnrg=true and a `spectra` dict, also the DM-NRG
-    spectral functions of the specd pairs (name -> array of (E, A(E)) rows, as written to
-    spec_DMNRG_dens_<name>.dat)."""
+    spectra of the specs, specd and spect pairs (file stem, e.g. spec_DMNRG_dens_A_d-A_d ->
+    array of (E, A(E)) rows as written to that .dat file)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -127,9 +127,19 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
     dm = kv.get("dmnrg", "false").lower() == "true" and spectra is not None
-    specd = [tuple(t.split("-", 1)) for t in kv.get("specd", "").split()] if dm else []
-    dops = {name: dict(d.ops[name][1]) for name in sorted({x for pr in specd for x in pr})}
-    steps = []  # per step: subspaces, structure, doublet operators (DM-NRG)
+
+    def pairs(key):
+        return [tuple(t.split("-", 1)) for t in kv.get(key, "").split()] if dm else []
+    # (file prefix, kind, op1, op2): correlators of singlets, spectral functions of doublets,
+    # dynamic spin susceptibilities of triplets (c++/oprecalc.hpp:160-195)
+    specs = [("corr", "s") + pr for pr in pairs("specs")] + [("spec", "d") + pr for pr in pairs("specd")] + \
+        [("spin", "t") + pr for pr in pairs("spect")]
+    dops = {name: dict(d.ops[name][1]) for name in sorted({x for sp in specs if sp[1] == "d" for x in sp[2:]})}
+    tops = {name: dict(d.ops[name][1]) for name in sorted({x for sp in specs if sp[1] == "t" for x in sp[2:]})}
+    for sp in specs:
+        if sp[1] == "s" and not set(sp[2:]) <= set(ops):
+            raise ValueError(f"specs names an operator that is not a singlet of the data file: {sp}")
+    steps = []  # per step: subspaces, structure, operators of the spectra (DM-NRG)
 
     td_rows, custom_rows = [], []
 
@@ -282,12 +292,12 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
             ops = recalc_ops(lambda e: e.nrstored)
             custom(N, new, ops)
         if dm:
-            nd_ = {}
-            for name, cold in dops.items():
+            def recalc_tensor(cold, tables, factor):
+                """recalc_general (c++/recalc.hpp:82-108) over the pairs Ip = I1 + dq."""
                 cn = {}
                 for I1, e1 in new.items():
-                    for dss, table in ((1, _DOUBLETP), (-1, _DOUBLETM)):
-                        Ip = (I1[0] - 1, I1[1] + dss)
+                    for dq, table in tables:
+                        Ip = (I1[0] + dq[0], I1[1] + dq[1])
                         if Ip not in new or not (e1.nrstored and new[Ip].nrstored):
                             continue
                         ep = new[Ip]
@@ -303,19 +313,24 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
                             A = np.ascontiguousarray(e1.U[i1 - 1][:e1.nrstored])
                             B = np.ascontiguousarray(ep.U[ip - 1][:ep.nrstored])
                             Oa = np.ascontiguousarray(cold[(IN1, INp)][:dims1[i1 - 1], :dimsp[ip - 1]])
-                            O.transform(m, fn(I1[1]), A, Oa, B)
+                            O.transform(m, factor(fn, I1[1]), A, Oa, B)
                         cn[(I1, Ip)] = m
-                nd_[name] = cn
-            dops = nd_
-            steps.append((N, scale, new, structure, dops))
+                return cn
+            # recalc_doublet (nrg-recalc-QS.hpp:32-117), recalc_triplet (495-640)
+            dops = {name: recalc_tensor(cold, (((-1, 1), _DOUBLETP), ((-1, -1), _DOUBLETM)), lambda fn, ss: fn(ss))
+                    for name, cold in dops.items()}
+            tops = {name: recalc_tensor(cold, T.TRIPLET, _qs.triplet_factor) for name, cold in tops.items()}
+            sops = {name: {(I, I): m for I, m in ops[name].items()} for name in {x for sp in specs if sp[1] == "s"
+                                                                                 for x in sp[2:]}}
+            steps.append((N, scale, new, structure, {"s": sops, "d": dops, "t": tops}))
         diag = new
     if dm and steps:
-        _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, spectra)
+        _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specs, spectra)
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
     return td_fields, td_rows, ["T"] + sorted(ops), custom_rows
 
 
-def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
+def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specs, out):
     """calc_rho + calc_densitymatrix, then the DMNRG run's spectral part: per step
     Algo_DMNRG::calc over all subspace pairs, mergeNN2 into the full spectrum, and at the end
     trim + continuous (log-Gaussian broadening)."""
@@ -375,7 +390,10 @@ def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
     emax = emax_p if emax_p > 0 else SCALE(0, Lam, disc, z) * 100.0
     emin = emin_p if emin_p > 0 else last_scale / 100.0
     lmin, lmax = math.floor(math.log10(emin)), math.ceil(math.log10(emax))
-    for name1, name2 in specd:
+    # gf_type and factor of each kind (c++/oprecalc.hpp:160-195; gf_sign, c++/traits.hpp)
+    kinds = {"s": (1, _qs.correlator_factor), "d": (-1, _specdens_factor), "t": (1, _qs.dynamicsusceptibility_factor)}
+    for prefix, kind, name1, name2 in specs:
+        sign, ff = kinds[kind]
         full = O.ChainBinning(lmin, lmax, bins, discard_imm)
         for N, scale, diagN, _, dopsN in steps:
             merge = NN1 or NN2avg or (N % 2 == 0 if NN2even else N % 2 == 1)
@@ -384,14 +402,16 @@ def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
             cb = O.ChainBinning(lmin, lmax, bins, discard_imm)
             rhoN = rhos[N]
             Emin_w, Emax_w = scale * goodE, scale * goodE * Efac * Efac
-            op1, op2 = dopsN[name1], dopsN[name2]
+            op1, op2 = dopsN[kind][name1], dopsN[kind][name2]
             for Ii, ei in diagN.items():
                 for Ij, ej in diagN.items():
                     if (Ij, Ii) not in op1 or (Ij, Ii) not in op2:
                         continue
+                    if ei.nrstored == 0 or ej.nrstored == 0:
+                        continue
                     Em = (ei.values[:ei.nrstored] - ei.shift) * scale
                     Ej = (ej.values[:ej.nrstored] - ej.shift) * scale
-                    cb.dmnrg_pair(Em, Ej, op1[(Ij, Ii)], op2[(Ij, Ii)], rhoN[Ii], rhoN[Ij], _specdens_factor(Ii, Ij), -1,
+                    cb.dmnrg_pair(Em, Ej, op1[(Ij, Ii)], op2[(Ij, Ii)], rhoN[Ii], rhoN[Ij], ff(Ii, Ij), sign,
                                   Emin_w, Emax_w)
             Ex = scale * goodE * Efac
             flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
@@ -417,4 +437,4 @@ def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specd, out):
             vn = sum(w * _BR_NEW(-E, e, alpha, omega0) for e, w in pos) + sum(w * _BR_NEW(-E, -e, alpha, omega0) for e, w in neg)
             rows_pos.append((E, vp))
             rows_neg.append((-E, vn))
-        out[f"{name1}-{name2}"] = np.array(sorted(rows_neg) + sorted(rows_pos))
+        out[f"{prefix}_DMNRG_dens_{name1}-{name2}"] = np.array(sorted(rows_neg) + sorted(rows_pos))

@@ -2,7 +2,8 @@
 
 Each case directory of the reference's ``test/c++/<case>/`` (or ``test/c++sym_all/<case>/``) holds the run's input (``param``,
 ``data``) and the outputs the reference produced with a real LAPACK (``ref/td``,
-``ref/custom``, printed to 10 significant digits). They are copied here unchanged so that
+``ref/custom``, printed to 10 significant digits; for DM-NRG cases also the spectral
+functions ``ref/{spec,corr,spin}_DMNRG_dens_*.dat``). They are copied here unchanged so that
 the tests can run where the reference tree is absent. Usage:
 
     python tests/golden/make_nrg_fixtures.py /path/to/nrgljubljana
@@ -16,7 +17,7 @@ CASES = [
     "test3_disc_z", "test4_disc_c", "test10_keepmin", "test12_Nmax", "test13_strategy_all",
     "test14_strategy_kept", "test15_safeguard", "test16_safeguardmax", "test35_betabar",
     "test56_dsyevd", "test56_dsyevr", "test200_data_has", "legacy_simple", "legacy_Himp",
-    "test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins",
+    "test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins", "test24_NN1", "test25_NN2avg", "test26_NN2even",
     "c++sym_all/test300_QS_ref", "c++sym_all/test310_QS_ref",
 ]
 
@@ -28,8 +29,9 @@ def main(ref_root: str) -> None:
         src = os.path.join(ref_root, "test", sub, case.split("/")[-1])
         dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
-        for name, rel in (("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom"),
-                          ("spec_DMNRG_dens_A_d-A_d.dat", "ref/spec_DMNRG_dens_A_d-A_d.dat")):
+        spectra = ("spec_DMNRG_dens_A_d-A_d.dat", "corr_DMNRG_dens_n_d-n_d.dat", "spin_DMNRG_dens_sigma_d-sigma_d.dat")
+        for name, rel in [("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")] + \
+                [(f, "ref/" + f) for f in spectra]:
             p = os.path.join(src, rel)
             if os.path.exists(p):
                 shutil.copyfile(p, os.path.join(dst, name))

@@ -1,7 +1,10 @@
-"""DM-NRG spectral functions of whole runs against the reference's regression outputs
-(spec_DMNRG_dens_A_d-A_d.dat of test/c++/test2_algorithms_dmnrg, test23_DMNRG and
-test27_bins: doublet recalculation, density-matrix sweep, DM-NRG pair sums into log bins,
-N/N+2 or N/N+1 patching, trimming and log-Gaussian broadening)."""
+"""DM-NRG spectra of whole runs against the reference's regression outputs: the spectral
+function of a doublet (spec_DMNRG_dens_A_d-A_d.dat), the correlator of a singlet
+(corr_DMNRG_dens_n_d-n_d.dat) and the dynamic spin susceptibility of a triplet
+(spin_DMNRG_dens_sigma_d-sigma_d.dat) of test/c++/test2_algorithms_dmnrg, test23_DMNRG,
+test24_NN1 (N/N+1 patching), test25_NN2avg, test26_NN2even and test27_bins (5 bins per
+decade): doublet and triplet recalculation, density-matrix sweep, DM-NRG pair sums into log
+bins with the fermionic or bosonic sign, patching, trimming and log-Gaussian broadening."""
 import os
 
 import numpy as np
@@ -9,8 +12,9 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
-DM_CASES = ["test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins"]
-SPEC = "spec_DMNRG_dens_A_d-A_d.dat"
+DM_CASES = ["test2_algorithms_dmnrg", "test23_DMNRG", "test24_NN1", "test25_NN2avg", "test26_NN2even", "test27_bins"]
+SPECTRA = ["spec_DMNRG_dens_A_d-A_d", "corr_DMNRG_dens_n_d-n_d", "spin_DMNRG_dens_sigma_d-sigma_d"]
+SPEC = SPECTRA[0]
 # the refs print 10 significant digits; values far below the peak are compared absolutely
 RTOL, ATOL_REL_TO_MAX = 2e-9, 1e-10
 # device run against the oracle at full precision
@@ -22,8 +26,8 @@ def read(case, name):
         return f.read()
 
 
-def ref_spectrum(case):
-    rows = [[float(x) for x in line.split()] for line in read(case, SPEC).splitlines()
+def ref_spectrum(case, name=SPEC):
+    rows = [[float(x) for x in line.split()] for line in read(case, name + ".dat").splitlines()
             if line.strip() and not line.startswith("#")]
     return np.array(rows)
 
@@ -52,18 +56,23 @@ def oracle_spectra(oracle):
 
 
 @pytest.mark.parametrize("case", DM_CASES)
-def test_oracle_dmnrg_spectrum_matches_reference(oracle_spectra, case):
-    assert_spectrum(oracle_spectra(case)["A_d-A_d"], ref_spectrum(case), RTOL, ATOL_REL_TO_MAX, case)
+def test_oracle_dmnrg_spectra_match_reference(oracle_spectra, case):
+    got = oracle_spectra(case)
+    assert sorted(got) == sorted(SPECTRA)
+    for name in SPECTRA:
+        assert_spectrum(got[name], ref_spectrum(case, name), RTOL, ATOL_REL_TO_MAX, f"{case} {name}")
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", DM_CASES)
-def test_gpu_dmnrg_spectrum(oracle_spectra, case):
-    """The device run (doublet recalculation, density-matrix sweep as batched rotate
-    terms, pair sums binned by nrg_spec_accumulate, broadening by nrg_broaden) against the
-    reference's spectrum and the oracle's."""
+def test_gpu_dmnrg_spectra(oracle_spectra, case):
+    """The device run (doublet and triplet recalculation, density-matrix sweep as batched
+    rotate terms, pair sums binned by nrg_spec_accumulate, broadening by nrg_broaden) against
+    the reference's spectra and the oracle's."""
     from nrgljubljana_b200.nrg_run import run_files
     res = run_files(read(case, "param"), read(case, "data"))
-    got = res.spectra["A_d-A_d"]
-    assert_spectrum(got, ref_spectrum(case), RTOL, ATOL_REL_TO_MAX, f"{case} vs reference")
-    assert_spectrum(got, oracle_spectra(case)["A_d-A_d"], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} vs oracle")
+    assert sorted(res.spectra) == sorted(SPECTRA)
+    for name in SPECTRA:
+        got = res.spectra[name]
+        assert_spectrum(got, ref_spectrum(case, name), RTOL, ATOL_REL_TO_MAX, f"{case} {name} vs reference")
+        assert_spectrum(got, oracle_spectra(case)[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} {name} vs oracle")
