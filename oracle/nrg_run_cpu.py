@@ -28,6 +28,7 @@ Only ``tests/`` and the CPU-baseline leg of ``bench.py`` may import this module.
 from __future__ import annotations
 
 import math
+from fractions import Fraction
 from typing import Dict, List, Tuple
 
 import numpy as np
@@ -89,11 +90,13 @@ class _Eig:
         self.U: List[np.ndarray] = []
 
 
-def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
+def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None
         ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
-    """td and custom rows of the run; with dmnrg=true and a `spectra` dict, also the DM-NRG
-    spectra of the specs, specd and spect pairs (file stem, e.g. spec_DMNRG_dens_A_d-A_d ->
-    array of (E, A(E)) rows as written to that .dat file)."""
+    """td and custom rows of the run; with a `spectra` dict, also the spectra of the specs,
+    specd and spect pairs for the algorithms dmnrg, fdm, fdmgt, fdmls that are switched on
+    (file stem, e.g. spec_DMNRG_dens_A_d-A_d -> array of (E, A(E)) rows as written to that
+    .dat file); with an `fdm_out` dict and an FDM flag, also fdm_out["tdfdm"] (fields, row)
+    and, with fdmexpv, fdm_out["customfdm"] (fields, row)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -126,7 +129,12 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
     opch = [dict(d.opch[ch][0]) for ch in range(d.channels)]
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
-    dm = kv.get("dmnrg", "false").lower() == "true" and spectra is not None
+    # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
+    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls")) if flag(k)]
+    fdm_flags = any(flag(k) for k in ("fdm", "fdmgt", "fdmls", "fdmexpv"))
+    dm = spectra is not None and bool(algos)
+    fdm_needed = fdm_flags and (spectra is not None or fdm_out is not None)
+    total_energy = d.gs_energy  # Stats::total_energy (c++/stats.hpp:60-71)
 
     def pairs(key):
         return [tuple(t.split("-", 1)) for t in kv.get(key, "").split()] if dm else []
@@ -241,16 +249,18 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
         for e in new.values():
             e.nrpost = len(e.values) if (last and lastall) else int(sum(1 for c in e.corr if c <= Emax))
         # after_diag
+        total_energy += Egs * scale  # Stats::update (c++/stats.hpp:65-71)
         td(N, new)
+        ops_prev = ops
         for I, e in new.items():
             anc, dims = structure[I]
             off = np.concatenate([[0], np.cumsum(dims)]).astype(int)
             e.U = [np.ascontiguousarray(e.vectors[:, off[i]:off[i + 1]]) for i in range(C)]
 
-        def recalc_ops(nrows):
+        def recalc_ops(nrows, names=None):
             out = {}
-            for name in sorted(ops):
-                cold = ops[name]
+            for name in sorted(ops_prev if names is None else names):
+                cold = ops_prev[name]
                 cn = {}
                 for I, e in new.items():
                     anc, dims = structure[I]
@@ -291,17 +301,22 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
         if strategy == "kept":
             ops = recalc_ops(lambda e: e.nrstored)
             custom(N, new, ops)
-        if dm:
+        if dm or fdm_needed:
+            # The DMNRG run recalculates the operators of the spectra over all states when an
+            # FDM flag is set (do_recalc_all, c++/params.hpp:542-547), else over the kept ones.
+            nrows = (lambda e: len(e.values)) if fdm_flags else (lambda e: e.nrstored)  # noqa: E731
+
             def recalc_tensor(cold, tables, factor):
                 """recalc_general (c++/recalc.hpp:82-108) over the pairs Ip = I1 + dq."""
                 cn = {}
                 for I1, e1 in new.items():
                     for dq, table in tables:
                         Ip = (I1[0] + dq[0], I1[1] + dq[1])
-                        if Ip not in new or not (e1.nrstored and new[Ip].nrstored):
+                        if Ip not in new or not (nrows(e1) and nrows(new[Ip])):
                             continue
                         ep = new[Ip]
-                        m = np.zeros((e1.nrstored, ep.nrstored))
+                        r1, rp = nrows(e1), nrows(ep)
+                        m = np.zeros((r1, rp))
                         anc1, dims1 = structure[I1]
                         ancp, dimsp = structure[Ip]
                         for i1, ip, fn in table:
@@ -310,8 +325,8 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
                                 continue
                             if dims1[i1 - 1] == 0 or dimsp[ip - 1] == 0:
                                 continue
-                            A = np.ascontiguousarray(e1.U[i1 - 1][:e1.nrstored])
-                            B = np.ascontiguousarray(ep.U[ip - 1][:ep.nrstored])
+                            A = np.ascontiguousarray(e1.U[i1 - 1][:r1])
+                            B = np.ascontiguousarray(ep.U[ip - 1][:rp])
                             Oa = np.ascontiguousarray(cold[(IN1, INp)][:dims1[i1 - 1], :dimsp[ip - 1]])
                             O.transform(m, factor(fn, I1[1]), A, Oa, B)
                         cn[(I1, Ip)] = m
@@ -320,20 +335,98 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None
             dops = {name: recalc_tensor(cold, (((-1, 1), _DOUBLETP), ((-1, -1), _DOUBLETM)), lambda fn, ss: fn(ss))
                     for name, cold in dops.items()}
             tops = {name: recalc_tensor(cold, T.TRIPLET, _qs.triplet_factor) for name, cold in tops.items()}
-            sops = {name: {(I, I): m for I, m in ops[name].items()} for name in {x for sp in specs if sp[1] == "s"
-                                                                                 for x in sp[2:]}}
-            steps.append((N, scale, new, structure, {"s": sops, "d": dops, "t": tops}))
+            snames = {x for sp in specs if sp[1] == "s" for x in sp[2:]}
+            if fdm_flags:
+                snames |= set(ops) if (fdm_out is not None and flag("fdmexpv")) else set()
+                sops = recalc_ops(nrows, snames)
+            else:
+                sops = {name: ops[name] for name in snames}
+            sops = {name: {(I, I): m for I, m in mats.items()} for name, mats in sops.items()}
+            steps.append((N, scale, new, structure, {"s": sops, "d": dops, "t": tops}, total_energy))
         diag = new
-    if dm and steps:
-        _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specs, spectra)
+    if (dm or fdm_needed) and steps:
+        _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos if dm else [], spectra, fdm_out if fdm_flags else None,
+                    total_energy, C, sorted(ops))
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
     return td_fields, td_rows, ["T"] + sorted(ops), custom_rows
 
 
-def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specs, out):
-    """calc_rho + calc_densitymatrix, then the DMNRG run's spectral part: per step
-    Algo_DMNRG::calc over all subspace pairs, mergeNN2 into the full spectrum, and at the end
-    trim + continuous (log-Gaussian broadening)."""
+def _exact_sum(values) -> Fraction:
+    """The exact sum of doubles (dyadic rationals) as a Fraction."""
+    ratios = [float(v).as_integer_ratio() for v in values]
+    if not ratios:
+        return Fraction(0)
+    D = max(d for _, d in ratios)
+    return Fraction(sum(n * (D // d) for n, d in ratios), D)
+
+
+def _exact_dot(a, b) -> Fraction:
+    """The exact sum of the products a[i] * b[i] of doubles."""
+    ra = [float(v).as_integer_ratio() for v in a]
+    rb = [float(v).as_integer_ratio() for v in b]
+    if not ra:
+        return Fraction(0)
+    terms = [(n1 * n2, d1 * d2) for (n1, d1), (n2, d2) in zip(ra, rb)]
+    D = max(d for _, d in terms)
+    return Fraction(sum(n * (D // d) for n, d in terms), D)
+
+
+def _fdm_weights(steps, T, GS, combs):
+    """calc_ZnD and fdm_thermodynamics (c++/measurements.hpp:60-163). The reference sums in
+    400-bit GMP; exact rational sums of the same double terms stand in for it. Returns the
+    per-step wn, wnfactor, ZnDN (double) and the tdfdm row (T, E, C, F, S)."""
+    Nend = len(steps)
+    ZG, ZN = [], []
+    for k, (N, scale, diagN, _, _, Tshift) in enumerate(steps):
+        last = k == Nend - 1
+        g, n = [], []
+        for I, e in diagN.items():
+            lo = 0 if last else e.nrpost      # Sub::all(), c++/store.hpp:26-31: the D states
+            for x in e.values[lo:]:
+                absz = (x - e.shift) * scale  # Values::abs_zero, abs_T, abs_G (c++/eigen.hpp:42-47)
+                absg = (absz + Tshift) - GS
+                g.append(I[1] * math.exp(-absg / T))
+                n.append(I[1] * math.exp(-absz / T))
+        ZG.append(_exact_sum(g))
+        ZN.append(_exact_sum(n))
+    ZZG = sum(ZG[k] * combs ** (Nend - k - 1) for k in range(Nend))
+    ZZGd = float(ZZG)
+    wnfactor = [math.pow(combs, Nend - k - 1) / ZZGd for k in range(Nend)]
+    wn = [wnfactor[k] * float(ZG[k]) for k in range(Nend)]
+    assert abs(sum(wn) - 1.0) < 1e-12, sum(wn)  # the sum rule, num_equal(sumwn, 1.0)
+    E = Fraction(0)
+    E2 = Fraction(0)
+    for k, (N, scale, diagN, _, _, Tshift) in enumerate(steps):
+        if not wn[k] > 1e-16:
+            continue
+        last = k == Nend - 1
+        d, e1, e2 = [], [], []
+        for I, e in diagN.items():
+            lo = 0 if last else e.nrpost
+            for x in e.values[lo:]:
+                absz = (x - e.shift) * scale
+                absT = absz + Tshift
+                d.append(wn[k] * I[1] * math.exp(-absz / T))
+                e1.append(absT)
+        sd = _exact_dot(d, e1)
+        sd2 = sum((Fraction(w) * Fraction(x) * Fraction(x) for w, x in zip(d, e1)), Fraction(0))
+        E += sd / ZN[k]
+        E2 += sd2 / ZN[k]
+    E_fdm = float(E)
+    C_fdm = float(E2 - E * E) / math.pow(T, 2)
+    F_fdm = -math.log(ZZGd) * T + GS
+    S_fdm = (E_fdm - F_fdm) / T
+    return wn, wnfactor, [float(z) for z in ZN], [T, E_fdm, C_fdm, F_fdm, S_fdm]
+
+
+def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names):
+    """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
+    calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
+    c++/dmnrg.hpp:146-217), then per step the spectra of every algorithm
+    (BaseSpectrum::calc, c++/algo.hpp:55-67): Algo_DMNRG merged with the N/N+2 window
+    (mergeNN2), Algo_FDMgt/ls merged whole (mergeCFS); at the end trim + continuous
+    (log-Gaussian broadening). FDM expectation values at step fdmexpvn
+    (measure_singlet_fdm, c++/measurements.hpp:31-44)."""
     T = float(kv.get("T", 0.001))
     goodE = float(kv.get("goodE", 2.0))
     bins = int(kv.get("bins", 1000))
@@ -351,90 +444,168 @@ def _dmnrg_spectra(kv, steps, Lam, disc, z, Nmax, specs, out):
     bmax = float(kv.get("broaden_max", 10.0))
     bmin = float(kv.get("broaden_min", -99.0))
     bratio = float(kv.get("broaden_ratio", 1.05))
+    fdmexpvn = int(kv.get("fdmexpvn", 0))
     last_scale = SCALE(Nmax, Lam, disc, z)
     if bmin <= 0.0:
         bmin = float(kv.get("broaden_min_ratio", 3.0)) * last_scale
     Efac = Lam  # one channel, no N/N+1 patching
     if NN1:
         Efac = math.sqrt(Lam)
-    # density matrix at the last step over the kept states (init_rho)
-    N_last, scale_last, diag_last, _, _ = steps[-1]
-    scT = scale_last / T
-    Z = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrstored]) for I, e in diag_last.items())
-    rho = {I: np.diag([math.exp(-c * scT) for c in e.corr[:e.nrstored]]) / Z for I, e in diag_last.items()}
-    rhos = {N_last: rho}
-    for k in range(len(steps) - 1, 0, -1):
-        N, _, diagN, structN, _ = steps[k]
-        _, _, diagP, _, _ = steps[k - 1]
-        rhoN = rhos[N]
-        prev = {}
-        for I, eP in diagP.items():
-            dim = eP.nrstored
-            M = np.zeros((dim, dim))
-            if dim:
-                for i, dl in enumerate(_qs.QS1.IN):
-                    sub = (I[0] - dl[0], I[1] - dl[1])
-                    if sub not in rhoN or sub not in diagN:
-                        continue
-                    nw = rhoN[sub].shape[0]
-                    rmax = structN[sub][1][i]
-                    if nw == 0 or rmax == 0:
-                        continue
-                    assert rmax == dim
-                    U = np.ascontiguousarray(diagN[sub].U[i][:nw])
-                    O.rotate(M, float(sub[1]) / float(I[1]), U, np.ascontiguousarray(rhoN[sub]))
-            prev[I] = M
-        tr = sum(I[1] * np.trace(m) for I, m in prev.items())
-        assert abs(tr - 1.0) < 1e-10, tr
-        rhos[N - 1] = prev
+    nst = len(steps)
+    IN = _qs.QS1.IN if combs == 4 else _qs.QS2.IN
+
+    def sweep(rho_last, extra):
+        """calc_densitymatrix_iterN / calc_fulldensitymatrix_iterN (c++/dmnrg.hpp:85-102,
+        165-197) with cdmI (55-80): rho at step k-1 from rho and `extra(k)` at step k."""
+        rhos = {nst - 1: rho_last}
+        for k in range(nst - 1, 0, -1):
+            _, _, diagN, structN, _, _ = steps[k]
+            _, _, diagP, _, _, _ = steps[k - 1]
+            terms = [rhos[k]] + ([extra(k)] if extra and k < nst - 1 else [])  # no DD sector at the last step
+            prev = {}
+            for I, eP in diagP.items():
+                dim = eP.nrpost
+                M = np.zeros((dim, dim))
+                if dim:
+                    for i, dl in enumerate(IN):
+                        sub = (I[0] - dl[0], I[1] - dl[1])
+                        if sub not in diagN:
+                            continue
+                        for rhoN in terms:
+                            if sub not in rhoN:
+                                continue
+                            nw = rhoN[sub].shape[0]
+                            rmax = structN[sub][1][i]
+                            if nw == 0 or rmax == 0:
+                                continue
+                            assert rmax == dim
+                            U = np.ascontiguousarray(diagN[sub].U[i][:nw])
+                            O.rotate(M, float(sub[1]) / float(I[1]), U, np.ascontiguousarray(rhoN[sub]))
+                prev[I] = M
+            rhos[k - 1] = prev
+        return rhos
+
+    def trace(rho):
+        return sum(I[1] * np.trace(m) for I, m in rho.items())
+
+    rhos = fdm = None
+    if "DMNRG" in algos:
+        # init_rho over the kept states of the last step (c++/dmnrg.hpp:43-50)
+        _, scale_last, diag_last, _, _, _ = steps[-1]
+        scT = scale_last / T
+        Z = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrpost]) for I, e in diag_last.items())
+        rho = {I: np.diag([math.exp(-c * scT) for c in e.corr[:e.nrpost]]) / Z for I, e in diag_last.items()}
+        rhos = sweep(rho, None)
+        for k in range(nst):
+            assert abs(trace(rhos[k]) - 1.0) < 1e-10
+    if fdm_out is not None or any(a.startswith("FDM") for a in algos):
+        wn, wnfactor, ZnDNd, tdrow = _fdm_weights(steps, T, GS, combs)
+
+        def init_rho_fdm(k):
+            """init_rho_FDM (c++/dmnrg.hpp:146-162): the D states of step k, all states at the
+            last step; the matrix spans all states."""
+            _, scale, diagN, _, _, _ = steps[k]
+            last = k == nst - 1
+            r = {}
+            for I, e in diagN.items():
+                tot = len(e.values)
+                m = np.zeros((tot, tot))
+                if ZnDNd[k] != 0.0:
+                    for i in range(0 if last else e.nrpost, tot):
+                        m[i, i] = math.exp(-((e.values[i] - e.shift) * scale) / T) * wn[k] / ZnDNd[k]
+                r[I] = m
+            if wn[k] != 0.0:
+                tr = trace(r)
+                if abs((tr - wn[k]) / wn[k]) > 1e-8:
+                    assert wn[k] < 1e-12
+            return r
+        fdm = sweep(init_rho_fdm(nst - 1), init_rho_fdm)
+        for k in range(nst - 1):
+            expected = sum(wn[k + 1:])
+            assert abs((trace(fdm[k]) - expected) / expected) < 1e-10, (k, trace(fdm[k]), expected)
+        if fdm_out is not None:
+            fdm_out["tdfdm"] = (["T", "E_fdm", "C_fdm", "F_fdm", "S_fdm"], tdrow)
+            if kv.get("fdmexpv", "false").lower() == "true" and fdmexpvn < nst:
+                _, _, diagN, _, opsN, _ = steps[fdmexpvn]
+                row = [T]
+                for name in singlet_names:
+                    v = 0.0
+                    for I, r in fdm[fdmexpvn].items():  # trace_contract over the kept range
+                        k_ = diagN[I].nrpost
+                        n = opsN["s"][name][(I, I)]
+                        v += I[1] * float(np.sum(r[:k_, :k_] * n[:k_, :k_].T))
+                    row.append(v)
+                fdm_out["customfdm"] = (["T"] + list(singlet_names), row)
+    if out is None or not algos:
+        return
     emax = emax_p if emax_p > 0 else SCALE(0, Lam, disc, z) * 100.0
     emin = emin_p if emin_p > 0 else last_scale / 100.0
     lmin, lmax = math.floor(math.log10(emin)), math.ceil(math.log10(emax))
     # gf_type and factor of each kind (c++/oprecalc.hpp:160-195; gf_sign, c++/traits.hpp)
     kinds = {"s": (1, _qs.correlator_factor), "d": (-1, _specdens_factor), "t": (1, _qs.dynamicsusceptibility_factor)}
+    mesh = []
+    E = bmax
+    while E > bmin:
+        mesh.append(E)
+        E /= bratio
     for prefix, kind, name1, name2 in specs:
         sign, ff = kinds[kind]
-        full = O.ChainBinning(lmin, lmax, bins, discard_imm)
-        for N, scale, diagN, _, dopsN in steps:
-            merge = NN1 or NN2avg or (N % 2 == 0 if NN2even else N % 2 == 1)
-            if not merge:
-                continue
-            cb = O.ChainBinning(lmin, lmax, bins, discard_imm)
-            rhoN = rhos[N]
-            Emin_w, Emax_w = scale * goodE, scale * goodE * Efac * Efac
-            op1, op2 = dopsN[kind][name1], dopsN[kind][name2]
+        full = {a: O.ChainBinning(lmin, lmax, bins, discard_imm) for a in algos}
+        for k, (N, scale, diagN, _, opsets, Tshift) in enumerate(steps):
+            op1, op2 = opsets[kind][name1], opsets[kind][name2]
+            last = k == nst - 1
+            pairs = []
             for Ii, ei in diagN.items():
                 for Ij, ej in diagN.items():
-                    if (Ij, Ii) not in op1 or (Ij, Ii) not in op2:
-                        continue
-                    if ei.nrstored == 0 or ej.nrstored == 0:
-                        continue
-                    Em = (ei.values[:ei.nrstored] - ei.shift) * scale
-                    Ej = (ej.values[:ej.nrstored] - ej.shift) * scale
-                    cb.dmnrg_pair(Em, Ej, op1[(Ij, Ii)], op2[(Ij, Ii)], rhoN[Ii], rhoN[Ij], ff(Ii, Ij), sign,
-                                  Emin_w, Emax_w)
-            Ex = scale * goodE * Efac
-            flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
-            for fr, fi, cr, ci in ((full.pos_re, full.pos_im, cb.pos_re, cb.pos_im),
-                                   (full.neg_re, full.neg_im, cb.neg_re, cb.neg_im)):
-                O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(full.energies),
-                                             full.nbins, Emin_w, Ex, Emax_w, flags, NNtanh, 1 if NN2avg else 0)
+                    if (Ij, Ii) in op1 and (Ij, Ii) in op2 and op1[(Ij, Ii)].size:
+                        pairs.append((Ii, ei, Ij, ej))
+            if "DMNRG" in algos and (NN1 or NN2avg or (N % 2 == 0 if NN2even else N % 2 == 1)):
+                cb = O.ChainBinning(lmin, lmax, bins, discard_imm)
+                Emin_w, Emax_w = scale * goodE, scale * goodE * Efac * Efac
+                for Ii, ei, Ij, ej in pairs:
+                    ki, kj = ei.nrpost, ej.nrpost
+                    Em = (ei.values[:ki] - ei.shift) * scale
+                    Ej = (ej.values[:kj] - ej.shift) * scale
+                    cb.dmnrg_pair(Em, Ej, op1[(Ij, Ii)][:kj, :ki], op2[(Ij, Ii)][:kj, :ki], rhos[k][Ii], rhos[k][Ij],
+                                  ff(Ii, Ij), sign, Emin_w, Emax_w)
+                Ex = scale * goodE * Efac
+                flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
+                fs = full["DMNRG"]
+                for fr, fi, cr, ci in ((fs.pos_re, fs.pos_im, cb.pos_re, cb.pos_im),
+                                       (fs.neg_re, fs.neg_im, cb.neg_re, cb.neg_im)):
+                    O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(fs.energies),
+                                                 fs.nbins, Emin_w, Ex, Emax_w, flags, NNtanh, 1 if NN2avg else 0)
+            fdm_algos = [a for a in algos if a.startswith("FDM")]
+            if fdm_algos:
+                cbs = {w: O.ChainBinning(lmin, lmax, bins, discard_imm) for w in ("gt", "ls")}
+                for Ii, ei, Ij, ej in pairs:
+                    Ki = 0 if last else ei.nrpost   # Eigen::boundary, c++/eigen.hpp:219
+                    Kj = 0 if last else ej.nrpost
+                    EGi = ((ei.values - ei.shift) * scale + Tshift) - GS
+                    EGj = ((ej.values - ej.shift) * scale + Tshift) - GS
+                    for w, rho in (("gt", fdm[k][Ii]), ("ls", fdm[k][Ij])):
+                        cbs[w].fdm_pair(w, EGi, Ki, EGj, Kj, op1[(Ij, Ii)], op2[(Ij, Ii)], rho, ff(Ii, Ij), sign, T,
+                                        wnfactor[k])
+                for a in fdm_algos:  # mergeCFS: Bins::merge (c++/bins.hpp:153-162)
+                    parts = {"FDM": ("gt", "ls"), "FDMgt": ("gt",), "FDMls": ("ls",)}[a]
+                    for w in parts:
+                        for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
+                            getattr(full[a], arr)[:] += getattr(cbs[w], arr)
+        for a in algos:
+            fs = full[a]
 
-        def trim(w):
-            e = full.energies
-            keep = [(e[i], w[i]) for i in range(len(e) - 1) if abs(w[i]) >= discard_trim * (e[i + 1] - e[i])]
-            keep.append((e[-1], w[-1]))
-            return keep
-        pos, neg = trim(full.pos_re), trim(full.neg_re)
-        mesh = []
-        E = bmax
-        while E > bmin:
-            mesh.append(E)
-            E /= bratio
-        rows_pos, rows_neg = [], []
-        for E in mesh:
-            vp = sum(w * _BR_NEW(E, e, alpha, omega0) for e, w in pos) + sum(w * _BR_NEW(E, -e, alpha, omega0) for e, w in neg)
-            vn = sum(w * _BR_NEW(-E, e, alpha, omega0) for e, w in pos) + sum(w * _BR_NEW(-E, -e, alpha, omega0) for e, w in neg)
-            rows_pos.append((E, vp))
-            rows_neg.append((-E, vn))
-        out[f"{prefix}_DMNRG_dens_{name1}-{name2}"] = np.array(sorted(rows_neg) + sorted(rows_pos))
+            def trim(w):
+                e = fs.energies
+                keep = [(e[i], w[i]) for i in range(len(e) - 1) if abs(w[i]) >= discard_trim * (e[i + 1] - e[i])]
+                keep.append((e[-1], w[-1]))
+                return keep
+            pos, neg = trim(fs.pos_re), trim(fs.neg_re)
+            rows_pos, rows_neg = [], []
+            for E in mesh:
+                vp = sum(w * _BR_NEW(E, e, alpha, omega0) for e, w in pos) + \
+                    sum(w * _BR_NEW(E, -e, alpha, omega0) for e, w in neg)
+                vn = sum(w * _BR_NEW(-E, e, alpha, omega0) for e, w in pos) + \
+                    sum(w * _BR_NEW(-E, -e, alpha, omega0) for e, w in neg)
+                rows_pos.append((E, vp))
+                rows_neg.append((-E, vn))
+            out[f"{prefix}_{a}_dens_{name1}-{name2}"] = np.array(sorted(rows_neg) + sorted(rows_pos))

@@ -3,12 +3,14 @@
 Each case directory of the reference's ``test/c++/<case>/`` (or ``test/c++sym_all/<case>/``) holds the run's input (``param``,
 ``data``) and the outputs the reference produced with a real LAPACK (``ref/td``,
 ``ref/custom``, printed to 10 significant digits; for DM-NRG cases also the spectral
-functions ``ref/{spec,corr,spin}_DMNRG_dens_*.dat``). They are copied here unchanged so that
+functions ``ref/{spec,corr,spin}_{DMNRG,FDM,FDMgt,FDMls}_dens_*.dat`` and the FDM outputs
+``ref/tdfdm``, ``ref/customfdm``). They are copied here unchanged so that
 the tests can run where the reference tree is absent. Usage:
 
     python tests/golden/make_nrg_fixtures.py /path/to/nrgljubljana
 """
 import os
+import re
 import shutil
 import sys
 
@@ -19,7 +21,11 @@ CASES = [
     "test56_dsyevd", "test56_dsyevr", "test200_data_has", "legacy_simple", "legacy_Himp",
     "test2_algorithms_dmnrg", "test23_DMNRG", "test27_bins", "test24_NN1", "test25_NN2avg", "test26_NN2even",
     "c++sym_all/test300_QS_ref", "c++sym_all/test310_QS_ref",
+    "test2_algorithms_fdm", "test2_algorithms_fdmexpv", "test2_algorithms_fdmgtls", "test60_discard_immediately",
+    "test61_discard_trim", "test64_emax", "test66_fdmexpvn", "legacy_fdmexpv2", "legacy_fdmexpv3",
 ]
+# spectra of the DM-NRG and FDM algorithms, FDM thermodynamics and expectation values
+SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls)_dens_.*\.dat$")
 
 
 def main(ref_root: str) -> None:
@@ -29,9 +35,10 @@ def main(ref_root: str) -> None:
         src = os.path.join(ref_root, "test", sub, case.split("/")[-1])
         dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
-        spectra = ("spec_DMNRG_dens_A_d-A_d.dat", "corr_DMNRG_dens_n_d-n_d.dat", "spin_DMNRG_dens_sigma_d-sigma_d.dat")
+        extra = [f for f in sorted(os.listdir(os.path.join(src, "ref")))
+                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm")]
         for name, rel in [("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")] + \
-                [(f, "ref/" + f) for f in spectra]:
+                [(f, "ref/" + f) for f in extra]:
             p = os.path.join(src, rel)
             if os.path.exists(p):
                 shutil.copyfile(p, os.path.join(dst, name))

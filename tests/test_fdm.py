@@ -1,0 +1,90 @@
+"""Full-density-matrix (FDM) outputs of whole runs against the reference's regression outputs:
+the spectra {spec,corr,spin}_{FDM,FDMgt,FDMls}_dens_*.dat, the FDM thermodynamics (tdfdm)
+and the FDM expectation values (customfdm) of test/c++/test2_algorithms_fdm,
+test2_algorithms_fdmexpv, test2_algorithms_fdmgtls, test60_discard_immediately,
+test61_discard_trim, test64_emax, test66_fdmexpvn, legacy_fdmexpv2 and legacy_fdmexpv3:
+partial statistical sums Z_n^D and weights w_n, the FDM density-matrix sweep with its
+discarded-state sectors, the spectra operators recalculated over all states, FDM pair sums
+(gt and ls parts) binned per step, trimming and broadening."""
+import os
+
+import numpy as np
+import pytest
+
+from test_dmnrg import ATOL_REL_TO_MAX, ORA_ATOL_REL_TO_MAX, ORA_RTOL, RTOL, assert_spectrum
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden", "nrg")
+FDM_CASES = ["test2_algorithms_fdm", "test2_algorithms_fdmexpv", "test2_algorithms_fdmgtls",
+             "test60_discard_immediately", "test61_discard_trim", "test64_emax", "test66_fdmexpvn",
+             "legacy_fdmexpv2", "legacy_fdmexpv3"]
+# tdfdm/customfdm: printed to 10 significant digits (20 for the legacy customfdm)
+TAB_RTOL = 2e-9
+
+
+def read(case, name):
+    with open(os.path.join(GOLD, case, name)) as f:
+        return f.read()
+
+
+def rows(case, name):
+    return np.array([[float(x) for x in line.split()] for line in read(case, name).splitlines()
+                     if line.strip() and not line.startswith("#")])
+
+
+def spectrum_files(case):
+    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case)) if f.endswith(".dat"))
+
+
+def assert_row(got, want, what):
+    got, want = np.asarray(got, dtype=float), np.asarray(want, dtype=float)
+    assert got.shape == want.shape, f"{what}: {got.shape} != {want.shape}"
+    bad = np.abs(got - want) > TAB_RTOL * np.abs(want) + 1e-300
+    assert not bad.any(), f"{what}: {got} vs {want}"
+
+
+@pytest.fixture(scope="module")
+def oracle_fdm(oracle):
+    from oracle import nrg_run_cpu
+    cache = {}
+
+    def get(case):
+        if case not in cache:
+            spec, fo = {}, {}
+            nrg_run_cpu.run(read(case, "param"), read(case, "data"), threads=os.cpu_count() or 1, spectra=spec,
+                            fdm_out=fo)
+            cache[case] = (spec, fo)
+        return cache[case]
+    return get
+
+
+@pytest.mark.parametrize("case", FDM_CASES)
+def test_oracle_fdm_outputs_match_reference(oracle_fdm, case):
+    spec, fo = oracle_fdm(case)
+    assert sorted(spec) == spectrum_files(case)
+    for name in spectrum_files(case):
+        assert_spectrum(spec[name], rows(case, name + ".dat"), RTOL, ATOL_REL_TO_MAX, f"{case} {name}")
+    for name in ("tdfdm", "customfdm"):
+        if os.path.exists(os.path.join(GOLD, case, name)):
+            assert_row(fo[name][1], rows(case, name)[-1], f"{case} {name}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", FDM_CASES)
+def test_gpu_fdm_outputs(oracle_fdm, case):
+    """The device run (FDM density-matrix sweep as batched rotate terms with diagonal
+    discarded-state sectors, spectra operators over all states, FDM pair sums binned by
+    nrg_spec_accumulate, broadening by nrg_broaden) against the reference and the oracle."""
+    from nrgljubljana_b200.nrg_run import run_files
+    res = run_files(read(case, "param"), read(case, "data"))
+    spec, fo = oracle_fdm(case)
+    assert sorted(res.spectra) == spectrum_files(case)
+    for name in spectrum_files(case):
+        got = res.spectra[name]
+        assert_spectrum(got, rows(case, name + ".dat"), RTOL, ATOL_REL_TO_MAX, f"{case} {name} vs reference")
+        assert_spectrum(got, spec[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} {name} vs oracle")
+    for name in ("tdfdm", "customfdm"):
+        if os.path.exists(os.path.join(GOLD, case, name)):
+            got = getattr(res, name)
+            assert_row(got[1], rows(case, name)[-1], f"{case} {name} vs reference")
+            assert np.allclose(got[1], fo[name][1], rtol=1e-11, atol=0), f"{case} {name} vs oracle"
