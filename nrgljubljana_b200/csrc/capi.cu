@@ -481,7 +481,9 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     if (g.rows < 0 || g.cols < 0 || g.ka < 0 || g.kb < 0) return fail(NRG_ERR_ARG, "term %d: negative size", t);
     if (g.rows == 0 || g.cols == 0 || g.ka == 0 || g.kb == 0) continue;
     if (!g.M || !g.A || !g.B) return fail(NRG_ERR_ARG, "term %d: null pointer", t);
-    if (!g.O && g.ka != g.kb) return fail(NRG_ERR_ARG, "term %d: O = NULL needs ka == kb", t);
+    if ((!g.O || g.ldo == 0) && g.ka != g.kb)
+      return fail(NRG_ERR_ARG, "term %d: an identity or diagonal O needs ka == kb", t);
+    if (g.O && g.ldo != 0 && g.ldo < g.kb) return fail(NRG_ERR_ARG, "term %d: ldo < kb", t);
     if (!(g.factor == g.factor) || g.factor - g.factor != 0.0)
       return fail(NRG_ERR_ARG, "term %d: non-finite factor", t);  // my_assert(my_isfinite(factor))
     live.push_back(t);
@@ -499,11 +501,13 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     }
     v.push_back(t);
   }
-  // Phase 1: T_t = O_t op(B_t) (ka x cols) for terms with an explicit O.
+  // Phase 1: T_t = O_t op(B_t) (ka x cols) for terms with an explicit dense O. A diagonal
+  // O (ldo == 0) scales the rows of op(B) inside the phase-2 GEMM instead.
+  auto dense_O = [&](int t) { return terms[t].O && terms[t].ldo != 0; };
   std::vector<size_t> toff(nterm, 0);
   size_t need = 0;
   for (int t : live)
-    if (terms[t].O) {
+    if (dense_O(t)) {
       toff[t] = need;
       need += (size_t)terms[t].ka * terms[t].cols;
     }
@@ -513,7 +517,7 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
   GemmPlan p1, p2;
   for (int t : live) {
     const nrg_gemm3& g = terms[t];
-    if (!g.O) continue;
+    if (!dense_O(t)) continue;
     p1.add_out(T + toff[t], g.cols, g.ka, g.cols, 0.0);
     p1.add_seg(g.O, g.ldo, 0, g.B, g.ldb, g.transB, g.kb, 1.0);
   }
@@ -524,8 +528,12 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     p2.add_out(M, f.ldm, f.rows, f.cols, 1.0);
     for (int t : v) {
       const nrg_gemm3& g = terms[t];
-      if (g.O) p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
-      else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
+      if (dense_O(t)) {
+        p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
+      } else {
+        p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
+        p2.segs.back().dscale = g.O;  // null: identity; ldo == 0: the diagonal of O
+      }
     }
   }
   rc = run_gemm_plan(c, p1, s, nrg::kPhGemm3);
@@ -555,7 +563,7 @@ int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* st
     if (g.rows <= 0 || g.cols <= 0 || g.ka <= 0 || g.kb <= 0) continue;
     note(g.M, span_of(g.M, g.rows, g.cols, g.ldm));
     note(g.A, g.transA ? span_of(g.A, g.ka, g.rows, g.lda) : span_of(g.A, g.rows, g.ka, g.lda));
-    if (g.O) note(g.O, span_of(g.O, g.ka, g.kb, g.ldo));
+    if (g.O) note(g.O, g.ldo == 0 ? sizeof(double) * g.ka : span_of(g.O, g.ka, g.kb, g.ldo));
     note(g.B, g.transB ? span_of(g.B, g.cols, g.kb, g.ldb) : span_of(g.B, g.kb, g.cols, g.ldb));
   }
   std::vector<double*> allocs;

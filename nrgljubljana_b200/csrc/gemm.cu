@@ -44,7 +44,10 @@ __device__ __forceinline__ void load_stage(Stage& s, const GemmSeg& g, int M, in
     if (!g.transB) { n = e & (BN - 1); k = e >> 6; } else { k = e & (BK - 1); n = e >> 4; }
     const int gn = n0 + n, gk = k0 + k;
     double v = 0.0;
-    if (gn < N && gk < g.K) v = g.transB ? g.B[(int64_t)gn * g.ldb + gk] : g.B[(int64_t)gk * g.ldb + gn];
+    if (gn < N && gk < g.K) {
+      v = g.transB ? g.B[(int64_t)gn * g.ldb + gk] : g.B[(int64_t)gk * g.ldb + gn];
+      if (g.dscale) v *= g.dscale[gk];
+    }
     s.b[i] = v;
   }
 }

@@ -29,8 +29,9 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 import torch
 
-from . import qs
-from ._lib import GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG, SPECPAIR_DTYPE
+from . import ddsum, qs
+from ._lib import (GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG, NRG_SPEC_DMNRG, NRG_SPEC_FDMGT,
+                   NRG_SPEC_FDMLS, SPECPAIR_DTYPE)
 from .api import (BinGrid, Context, broaden, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch,
                   spec_accumulate_array)
 from .inputs import DataFile, SCALE, parse_param, read_data
@@ -63,10 +64,14 @@ class RunParams:
     strategy: str = "kept"
     calc0: bool = True
     lastall: bool = False
-    # full-density-matrix flags: they keep every state of the last step (params.hpp:535-539);
-    # the FDM outputs themselves (tdfdm, customfdm, FDM spectra) are not produced
+    # full-density-matrix algorithm (c++/params.hpp:240-253): FDM spectra (fdm: greater +
+    # lesser parts, fdmgt/fdmls: each part alone), FDM expectation values at step fdmexpvn;
+    # any of them keeps every state of the last step (params.hpp:535-539)
     fdm: bool = False
+    fdmgt: bool = False
+    fdmls: bool = False
     fdmexpv: bool = False
+    fdmexpvn: int = 0
     lastalloverride: bool = False
     data_has_rescaled_energies: bool = True
     # DM-NRG spectra of the specs/specd/spect pairs (c++/params.hpp:181-396)
@@ -114,16 +119,27 @@ class RunParams:
                 raise ValueError(f"parameter {k} is not supported by the QS run driver")
         if p.strategy not in ("kept", "all"):
             raise ValueError(f"strategy={p.strategy}")
-        if p.dmnrg and p.strategy != "kept":
-            raise ValueError("DM-NRG spectra are supported with strategy=kept")
-        if p.dmnrg and not p.broaden:
+        if (p.dmnrg or p.fdm_flags) and p.strategy != "kept":
+            raise ValueError("density-matrix algorithms are supported with strategy=kept")
+        if p.algorithms and not p.broaden:
             raise ValueError("broaden=false is not supported")
         return p
 
     @property
+    def fdm_flags(self) -> bool:
+        """Params::fdm_flags (c++/params.hpp:535) without the Matsubara variant."""
+        return self.fdm or self.fdmgt or self.fdmls or self.fdmexpv
+
+    @property
+    def algorithms(self) -> List[str]:
+        """The real-frequency spectral algorithms switched on (c++/oprecalc.hpp:123-131)."""
+        return [a for a, on in (("DMNRG", self.dmnrg), ("FDM", self.fdm), ("FDMgt", self.fdmgt),
+                                ("FDMls", self.fdmls)) if on]
+
+    @property
     def keep_all_states_in_last_step(self) -> bool:
         """Params::keep_all_states_in_last_step (c++/params.hpp:539)."""
-        return self.lastall or ((self.fdm or self.fdmexpv) and not self.lastalloverride)
+        return self.lastall or (self.fdm_flags and not self.lastalloverride)
 
 
 @dataclass
@@ -134,8 +150,10 @@ class Result:
     custom: List[List[float]]
     blocks_per_step: List[int] = field(default_factory=list)
     max_dim_per_step: List[int] = field(default_factory=list)
-    # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_...", "spin_...") -> rows (E, A(E))
+    # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_FDM_...", "spin_...") -> rows (E, A(E))
     spectra: Dict[str, np.ndarray] = field(default_factory=dict)
+    tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
+    customfdm: Optional[Tuple[List[str], List[float]]] = None   # fields, row (measure_singlet_fdm)
 
 
 # ------------------------------------------------------------------ host bookkeeping
@@ -287,6 +305,18 @@ class StepJob:
     pcorr: torch.Tensor
 
 
+@dataclass
+class _StepRecord:
+    """What the density-matrix sweeps and the spectral pass need of one step: its subspaces
+    (all eigenvalues, kept counts, eigenvector locations), the eigenvectors, and
+    Stats::total_energy after the step (the T_shift of its absolute energies)."""
+    N: int
+    scale: float
+    diag: Dict[Invar, "Sub"]
+    vecs: torch.Tensor
+    total_energy: float
+
+
 class QSRun:
     """One NRG run (QS, one channel) on one device. ``run()`` does the whole run; a server
     drives ``start``, ``begin_step``, ``end_step`` and ``finish`` itself to solve the blocks
@@ -296,8 +326,6 @@ class QSRun:
         if data.symtype != "QS" or data.channels not in (1, 2):
             raise ValueError("the driver covers symtype QS with one or two channels")
         self.T = qs.tables(data.channels)
-        if params.dmnrg and data.channels != 1:
-            raise ValueError("DM-NRG spectra are supported for one channel")
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device: the QS run driver has no CPU fallback")
         self.p = params
@@ -308,9 +336,10 @@ class QSRun:
         self.nmax = data.nmax
         self.sqrt_lambda = math.sqrt(params.Lambda)  # nrg_step_scale_factor (c++/params.hpp:639-641)
         self.op_names = sorted(n for n, (k, _) in data.ops.items() if k in "sg")
-        # (file prefix, kind, op1, op2) of the DM-NRG spectra (c++/oprecalc.hpp:160-195)
+        # (file prefix, kind, op1, op2) of the spectra (c++/oprecalc.hpp:160-195)
+        self.algos = params.algorithms
         self.specs: List[Tuple[str, str, str, str]] = []
-        if params.dmnrg:
+        if self.algos:
             for prefix, kind, text in (("corr", "s", params.specs), ("spec", "d", params.specd),
                                        ("spin", "t", params.spect)):
                 for tok in text.split():
@@ -323,6 +352,13 @@ class QSRun:
                     self.specs.append((prefix, kind, n1, n2))
         self.dop_names = sorted({x for sp in self.specs if sp[1] == "d" for x in sp[2:]})
         self.top_names = sorted({x for sp in self.specs if sp[1] == "t" for x in sp[2:]})
+        # singlets of the spectral pass: those of the correlators, and all of them for the FDM
+        # expectation values
+        self.sop_names = sorted({x for sp in self.specs if sp[1] == "s" for x in sp[2:]}
+                                | (set(self.op_names) if params.fdmexpv else set()))
+        # the steps are kept (eigenvalues, eigenvectors, energy offsets) for the density
+        # matrices and the spectral pass after the run
+        self.keep_steps = bool(self.specs) or params.fdm_flags
 
     # ---- scales (c++/step.hpp:30-39)
     def scale(self, trueN: int) -> float:
@@ -392,8 +428,14 @@ class QSRun:
         self.res = Result(["T"] + list(qs.TD_FIELDS) + ["<E>", "<E^2>", "C", "F", "S"], [], ["T"] + self.op_names,
                           [])
         self.meas: List[_Measure] = []
-        self.dm_steps: List[tuple] = []
-        self.tensor_ops = {}
+        self.dm_steps: List[_StepRecord] = []
+        self.total_energy = float(d.gs_energy)  # Stats::total_energy (c++/stats.hpp:60-71)
+        # operators of the spectral pass as read: singlets by subspace, doublets and triplets
+        # by subspace pair
+        self.spec_init: Dict[str, MatSet] = {}
+        if self.sop_names:
+            smats = [{I1: m for (I1, I2), m in d.ops[name][1].items() if I1 == I2} for name in self.sop_names]
+            self.spec_init["s"] = MatSet(self.dev, oshapes, len(self.sop_names), _pack(smats, oshapes))
         for kind, names in (("d", self.dop_names), ("t", self.top_names)):
             if names:
                 tmats = [dict(d.ops[name][1]) for name in names]
@@ -401,7 +443,7 @@ class QSRun:
                 for m in tmats:
                     for k, mat in m.items():
                         tshapes[k] = mat.shape
-                self.tensor_ops[kind] = MatSet(self.dev, tshapes, len(names), _pack(tmats, tshapes))
+                self.spec_init[kind] = MatSet(self.dev, tshapes, len(names), _pack(tmats, tshapes))
         if p.calc0:
             self.res.td.append(self._td(-1, diag))
             self.meas.append(self._measure(-1, diag, self.ops))
@@ -435,7 +477,7 @@ class QSRun:
                 res.custom.append([m.T] + [float(np.sum(m.weights * dg[o])) / Z for o in range(len(self.op_names))])
         self.meas = []
         if self.dm_steps:
-            res.spectra = self._dmnrg()
+            self._density_matrix_outputs(res)
             self.dm_steps = []
         return res
 
@@ -536,6 +578,7 @@ class QSRun:
                           nstored=ns[b])
         # do_diag: Egs subtraction, splitting correction, truncation (c++/core.hpp:141-143)
         Egs = min(float(s.values[0]) for s in diag.values())  # Egs_subtraction (c++/eigen.hpp:321-333)
+        self.total_energy += Egs * self.scale(N)  # Stats::update (c++/stats.hpp:65-71)
         for s in diag.values():
             s.shift = Egs
             s.corr = s.values - Egs
@@ -573,11 +616,8 @@ class QSRun:
             new_ops = self._recalc_singlets(diag, ops)
             meas.append(self._measure(N, diag, new_ops))
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
-        if self.specs:  # DM-NRG keeps every step's eigenvectors and the operators of its spectra
-            tables = {"d": (self.T.DOUBLET, lambda fn, ss: fn(ss)), "t": (self.T.TRIPLET, qs.triplet_factor)}
-            for kind, cold in self.tensor_ops.items():
-                self.tensor_ops[kind] = self._recalc_tensor(diag, cold, *tables[kind])
-            self.dm_steps.append((N, self.scale(N), diag, dict(self.tensor_ops, s=new_ops), job.Vbuf))
+        if self.keep_steps:  # the density matrices and spectra need every step's eigenvectors
+            self.dm_steps.append(_StepRecord(N, self.scale(N), diag, job.Vbuf, self.total_energy))
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
@@ -624,14 +664,16 @@ class QSRun:
         self.opch_keys = [set(out.loc)] * self.T.channels
         return out
 
-    def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet) -> MatSet:
+    def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet, rows=None) -> MatSet:
         """recalc_singlet (c++/symmetry.hpp:185-200) through recalc_general
-        (c++/recalc.hpp:82-108) for every singlet operator over the stored states: the terms of
-        one operator are built once and replicated over the operators (operator-major)."""
-        out = MatSet(self.dev, {I: (s.nstored, s.nstored) for I, s in diag.items()}, len(self.op_names))
+        (c++/recalc.hpp:82-108) for every singlet operator of `cold` over the stored states
+        (or the first rows(s) states of each subspace): the terms of one operator are built
+        once and replicated over the operators (operator-major)."""
+        rows = rows or (lambda s: s.nstored)
+        out = MatSet(self.dev, {I: (rows(s), rows(s)) for I, s in diag.items()}, cold.nops)
         base = []
         for I, s in diag.items():
-            k = s.nstored
+            k = rows(s)
             if k == 0:
                 continue
             M = out.ptr(I)
@@ -642,31 +684,33 @@ class QSRun:
                 A = s.vptr + 8 * s.offs[i]
                 _, r, c = cold.loc[a]
                 base.append((M, k, A, s.n, cold.ptr(a), c, A, s.n, k, k, w, w, 0, 1, 1.0))
-        if base and self.op_names:
+        if base and cold.nops:
             b = np.array(base, dtype=GEMM3_DTYPE)
-            t = np.tile(b, len(self.op_names))
-            op = np.repeat(np.arange(len(self.op_names), dtype=np.uint64), len(b))
+            t = np.tile(b, cold.nops)
+            op = np.repeat(np.arange(cold.nops, dtype=np.uint64), len(b))
             t["M"] += op * np.uint64(8 * out.total)
             t["O"] += op * np.uint64(8 * cold.total)
             gemm3_batch_array(t, self.ctx, self.stream)
         return out
 
 
-    def _recalc_tensor(self, diag: Dict[Invar, Sub], cold: MatSet, tables, factor) -> MatSet:
+    def _recalc_tensor(self, diag: Dict[Invar, Sub], cold: MatSet, tables, factor, rows=None) -> MatSet:
         """SymmetryQS::recalc_doublet / recalc_triplet (c++/symmetry/nrg-recalc-QS.hpp:32-117,
-        495-640) through recalc_general (c++/recalc.hpp:82-108) over the kept states, every
-        operator of the set in one batched call (operator-major). `tables` lists (dq, rows)
-        for Ip = I1 + dq; factor(fn, ss1) evaluates a row's coefficient."""
+        495-640) through recalc_general (c++/recalc.hpp:82-108) over the kept states (or the
+        first rows(s) states of each subspace), every operator of the set in one batched call
+        (operator-major). `tables` lists (dq, rows) for Ip = I1 + dq; factor(fn, ss1)
+        evaluates a row's coefficient."""
+        rows = rows or (lambda s: s.nstored)
         plan = []
         for I1, s1 in diag.items():
-            if not s1.nstored:
+            if not rows(s1):
                 continue
             for dq, table in tables:
                 Ip = (I1[0] + dq[0], I1[1] + dq[1])
                 sp = diag.get(Ip)
-                if sp is not None and sp.nstored:
+                if sp is not None and rows(sp):
                     plan.append((I1, Ip, table))
-        out = MatSet(self.dev, {(I1, Ip): (diag[I1].nstored, diag[Ip].nstored) for I1, Ip, _ in plan}, cold.nops)
+        out = MatSet(self.dev, {(I1, Ip): (rows(diag[I1]), rows(diag[Ip])) for I1, Ip, _ in plan}, cold.nops)
         base = []
         for I1, Ip, table in plan:
             s1, sp = diag[I1], diag[Ip]
@@ -680,8 +724,8 @@ class QSRun:
                 if w1 == 0 or wp == 0:
                     continue
                 _, r, c = cold.loc[(IN1, INp)]
-                base.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, cold.ptr((IN1, INp)), c,
-                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, w1, wp, 0, 1,
+                base.append((M, rows(sp), s1.vptr + 8 * s1.offs[i1 - 1], s1.n, cold.ptr((IN1, INp)), c,
+                             sp.vptr + 8 * sp.offs[ip - 1], sp.n, rows(s1), rows(sp), w1, wp, 0, 1,
                              factor(fn, I1[1])))
         if base:
             b = np.array(base, dtype=GEMM3_DTYPE)
@@ -692,86 +736,306 @@ class QSRun:
             gemm3_batch_array(t, self.ctx, self.stream)
         return out
 
-    def _dmnrg(self) -> Dict[str, np.ndarray]:
-        """DM-NRG spectra of the specs/specd/spect pairs: the density matrix of the last step
-        (init_rho, c++/dmnrg.hpp:43-50), the backward sweep (calc_densitymatrix_iterN / cdmI,
-        c++/dmnrg.hpp:55-102) as batched rotate terms, per step the Algo_DMNRG pair sums binned
-        on the device (c++/algo_DMNRG.hpp:29-52, c++/algo.hpp:55-67), N/N+2 (or N/N+1)
-        patching with the window function (c++/spectrum.hpp:81-124), trimming
-        (c++/bins.hpp:165-185) and log-Gaussian broadening on the device
-        (c++/spectrum.hpp:168-196)."""
-        p, d = self.p, self.d
+    # ---- density matrices and spectra (the DMNRG run, c++/nrg-general.hpp:139-168)
+    def _density_matrix_outputs(self, res: Result) -> None:
+        """After the run: the DM-NRG density matrices (calc_rho), the FDM weights and density
+        matrices with the FDM thermodynamics (calc_rhoFDM), then the spectral pass over the
+        kept steps (the second run of the reference without its diagonalisations)."""
+        p = self.p
+        rhos = self._rho_dmnrg() if "DMNRG" in self.algos else None
+        fdm = self._rho_fdm() if p.fdm_flags else None
+        if fdm is not None:
+            res.tdfdm = (["T", "E_fdm", "C_fdm", "F_fdm", "S_fdm"], fdm["tdrow"])
+        res.spectra, expv = self._spectral_pass(rhos, fdm)
+        if expv is not None:
+            res.customfdm = (["T"] + self.sop_names, [p.T] + expv)
+
+    def _sweep(self, rho_last: Optional[MatSet], diag_src) -> List[Optional[MatSet]]:
+        """rho of step k-1 from rho of step k for k = last .. 1: the cdmI terms
+        (c++/dmnrg.hpp:55-80) of calc_densitymatrix_iterN / calc_fulldensitymatrix_iterN
+        (85-102, 165-197), all subspaces of a step in one batched call. rho_last: the dense
+        density matrix of the last step (None: none); diag_src(k): None or (weights, loc)
+        with loc[sub] = (offset, first state, count), a diagonal sector of step k's density
+        matrix (the DD sector of FDM, or the whole last step), applied as U^T diag(w) U."""
         steps = self.dm_steps
-        Lam = p.Lambda
-        # init_rho over the kept states of the last step, scT = scale / T
-        N_last, scale_last, diag_last, _, _ = steps[-1]
-        scT = scale_last / p.T
+        nst = len(steps)
+        rhos: List[Optional[MatSet]] = [None] * nst
+        rhos[nst - 1] = rho_last
+        for k in range(nst - 1, 0, -1):
+            cur, prv = steps[k], steps[k - 1]
+            out = MatSet(self.dev, {I: (s.nkept, s.nkept) for I, s in prv.diag.items()})
+            dsrc = diag_src(k) if diag_src else None
+            R = rhos[k]
+            rows = []
+            for I, sP in prv.diag.items():
+                dim = sP.nkept
+                if dim == 0:
+                    continue
+                for i, dl in enumerate(self.T.IN):
+                    sub = (I[0] - dl[0], I[1] - dl[1])
+                    sN = cur.diag.get(sub)
+                    if sN is None or sN.dims[i] == 0:
+                        continue
+                    if sN.dims[i] != dim:
+                        raise AssertionError("rmax == dim")  # cdmI, c++/dmnrg.hpp:73
+                    coef = float(qs.mult(sub)) / float(qs.mult(I))
+                    A = sN.vptr + 8 * sN.offs[i]
+                    if R is not None and sub in R.loc and R.loc[sub][1]:
+                        nw = R.loc[sub][1]
+                        rows.append((out.ptr(I), dim, A, sN.n, R.ptr(sub), nw, A, sN.n, dim, dim, nw, nw, 1, 0, coef))
+                    if dsrc is not None and sub in dsrc[1]:
+                        off, r0, cnt = dsrc[1][sub]
+                        if cnt:
+                            Ad = A + 8 * r0 * sN.n
+                            rows.append((out.ptr(I), dim, Ad, sN.n, dsrc[0].data_ptr() + 8 * off, 0, Ad, sN.n, dim,
+                                         dim, cnt, cnt, 1, 0, coef))
+            if rows:
+                gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
+            rhos[k - 1] = out
+        return rhos
+
+    def _traces(self, rhos: List[Optional[MatSet]]) -> List[float]:
+        """Tr rho = sum_I mult(I) Tr rho_I of every step (one gather per step, one copy)."""
+        diags, mults, counts = [], [], []
+        for k, st in enumerate(self.dm_steps):
+            R = rhos[k]
+            idx, mv = [], []
+            if R is not None:
+                for I, (off, r, c) in R.loc.items():
+                    idx.append(off + np.arange(r) * (c + 1))
+                    mv.append(np.full(r, float(qs.mult(I))))
+            ix = np.concatenate(idx).astype(np.int64) if idx else np.zeros(0, dtype=np.int64)
+            counts.append(len(ix))
+            mults.append(np.concatenate(mv) if mv else np.zeros(0))
+            if len(ix):
+                diags.append(torch.index_select(R.buf, 0, self._h2d(ix)))
+        vals = torch.cat(diags).cpu().numpy() if diags else np.zeros(0)
+        out, o = [], 0
+        for cnt, mv in zip(counts, mults):
+            out.append(float(np.sum(mv * vals[o:o + cnt])))
+            o += cnt
+        return out
+
+    def _rho_dmnrg(self) -> List[Optional[MatSet]]:
+        """init_rho over the kept states of the last step with scT = scale / T
+        (c++/dmnrg.hpp:43-50) and the backward sweep; Tr rho = 1 at every step
+        (check_trace_rho, c++/dmnrg.hpp:29-33)."""
+        p = self.p
+        last = self.dm_steps[-1]
+        scT = last.scale / p.T
         Z = 0.0
         diagvals = {}
-        for I, s in diag_last.items():
-            ex = np.exp(-s.corr[:s.nstored] * scT)
+        for I, s in last.diag.items():
+            ex = np.exp(-s.corr[:s.nkept] * scT)
             diagvals[I] = ex
             Z += qs.mult(I) * float(np.sum(ex))
-        shapes = {I: (s.nstored, s.nstored) for I, s in diag_last.items()}
+        shapes = {I: (s.nkept, s.nkept) for I, s in last.diag.items()}
         host = np.zeros(max(1, sum(r * c for r, c in shapes.values())))
         o = 0
         for I, (r, c) in shapes.items():
             host[o + np.arange(r) * (c + 1)] = diagvals[I] / Z
             o += r * c
-        rhos = {len(steps) - 1: MatSet(self.dev, shapes, 1, host)}
-        for k in range(len(steps) - 1, 0, -1):
-            _, _, diagN, _, _ = steps[k]
-            _, _, diagP, _, _ = steps[k - 1]
-            rhoN = rhos[k]
-            prev = MatSet(self.dev, {I: (s.nstored, s.nstored) for I, s in diagP.items()})
-            rows = []
-            for I, sP in diagP.items():
-                dim = sP.nstored
-                if dim == 0:
-                    continue
-                for i, dl in enumerate(self.T.IN):
-                    sub = (I[0] - dl[0], I[1] - dl[1])
-                    sN = diagN.get(sub)
-                    if sN is None:
-                        continue
-                    nw, rmax = sN.nstored, sN.dims[i]
-                    if nw == 0 or rmax == 0:
-                        continue
-                    if rmax != dim:
-                        raise AssertionError("rmax == dim")  # cdmI, c++/dmnrg.hpp:73
-                    A = sN.vptr + 8 * sN.offs[i]
-                    rows.append((prev.ptr(I), dim, A, sN.n, rhoN.ptr(sub), nw, A, sN.n, dim, dim, nw, nw, 1, 0,
-                                 float(qs.mult(sub)) / float(qs.mult(I))))
-            if rows:
-                gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
-            rhos[k - 1] = prev
-        # Tr rho = 1 at every step (check_trace_rho, c++/dmnrg.hpp:29-33): one gather per step,
-        # one copy to the host
-        diags, mults = [], []
-        for k, (_, _, dg, _, _) in enumerate(steps):
-            idx = []
-            for I, s in dg.items():
-                off, r, c = rhos[k].loc[I]
-                idx.append(off + np.arange(r) * (c + 1))
-                mults.append(np.full(r, float(qs.mult(I))))
-            if idx:
-                diags.append(torch.index_select(rhos[k].buf, 0, self._h2d(np.concatenate(idx).astype(np.int64))))
-        if diags:
-            dvals = torch.cat(diags).cpu().numpy()
-            bounds = np.cumsum([0] + [len(x) for x in diags])
-            mv = np.concatenate(mults)
-            for a, b in zip(bounds[:-1], bounds[1:]):
-                tr = float(np.sum(mv[a:b] * dvals[a:b]))
-                if abs(tr - 1.0) > 1e-9:
-                    raise RuntimeError(f"check_trace_rho() failed: {tr!r}")
-        # spectra
+        rhos = self._sweep(MatSet(self.dev, shapes, 1, host), None)
+        for tr in self._traces(rhos):
+            if abs(tr - 1.0) > 1e-9:
+                raise RuntimeError(f"check_trace_rho() failed: {tr!r}")
+        return rhos
+
+    def _rho_fdm(self) -> Dict:
+        """calc_ZnD and fdm_thermodynamics (c++/measurements.hpp:60-163) on the host in
+        extended precision, init_rho_FDM (c++/dmnrg.hpp:146-162) and the FDM sweep
+        (calc_fulldensitymatrix, 165-217) on the device: the KK sector as dense rotate terms,
+        the DD sector of every step (and the whole last step) as diagonal ones."""
+        p = self.p
+        steps = self.dm_steps
+        nst = len(steps)
+        T = p.T
+        GS = self.total_energy  # GS_energy = total_energy at the end (c++/nrg-general.hpp:133)
+        combs = self.T.COMBS
+        absz, mults, lo = [], [], []
+        for k, st in enumerate(steps):
+            last = k == nst - 1
+            az, mu, l0 = {}, {}, {}
+            for I, s in st.diag.items():
+                az[I] = (s.values - s.shift) * st.scale  # Values::abs_zero (c++/eigen.hpp:45)
+                mu[I] = float(qs.mult(I))
+                l0[I] = 0 if last else s.nkept  # the D states, Sub::all() (c++/store.hpp:26-31)
+            absz.append(az)
+            mults.append(mu)
+            lo.append(l0)
+        ZG_terms, ZN_terms = [], []
+        for k, st in enumerate(steps):
+            g, n = [], []
+            for I in st.diag:
+                z = absz[k][I][lo[k][I]:]
+                g.append(mults[k][I] * np.exp(-((z + st.total_energy) - GS) / T))  # abs_G (eigen.hpp:47)
+                n.append(mults[k][I] * np.exp(-z / T))
+            ZG_terms.append(np.concatenate(g) if g else np.zeros(0))
+            ZN_terms.append(np.concatenate(n) if n else np.zeros(0))
+        # ZZG = sum_N ZnDG[N] combs^(Nend-N-1); the powers are powers of two, so the scaled terms
+        # are exact and one exactly rounded sum gives the 400-bit result rounded to double
+        ZZG = math.fsum(np.concatenate([ZG_terms[k] * float(combs) ** (nst - k - 1) for k in range(nst)]))
+        ZnDG = [math.fsum(ZG_terms[k]) for k in range(nst)]
+        ZnDN = [ddsum.exact_sum([ZN_terms[k]]) for k in range(nst)]
+        ZnDNd = [float(z) for z in ZnDN]
+        wnfactor = [math.pow(combs, nst - k - 1) / ZZG for k in range(nst)]
+        wn = [wnfactor[k] * ZnDG[k] for k in range(nst)]
+        if abs(sum(wn) - 1.0) > 1e-12:
+            raise RuntimeError(f"sum of w_n is {sum(wn)!r}, not 1")  # calc_ZnD sum rule
+        # fdm_thermodynamics: E and E^2 moments over the D states of every shell
+        from fractions import Fraction
+        E = Fraction(0)
+        E2 = Fraction(0)
+        for k, st in enumerate(steps):
+            if not wn[k] > 1e-16:
+                continue
+            dd, ee = [], []
+            for I in st.diag:
+                z = absz[k][I][lo[k][I]:]
+                dd.append((wn[k] * mults[k][I]) * np.exp(-z / T))
+                ee.append(z + st.total_energy)  # abs_T (eigen.hpp:46)
+            d_ = np.concatenate(dd) if dd else np.zeros(0)
+            e_ = np.concatenate(ee) if ee else np.zeros(0)
+            E += ddsum.dot(d_, e_) / ZnDN[k]
+            E2 += ddsum.dot_sq(d_, e_) / ZnDN[k]
+        E_fdm = float(E)
+        C_fdm = float(E2 - E * E) / math.pow(T, 2)
+        F_fdm = -math.log(ZZG) * T + GS
+        S_fdm = (E_fdm - F_fdm) / T
+        # diagonal sectors of init_rho_FDM: exp(-E/T) w_n / Z_n^D over the D states
+        dsrc = {}
+        for k, st in enumerate(steps):
+            loc, parts, o = {}, [], 0
+            if ZnDNd[k] != 0.0 and wn[k] != 0.0:
+                for I in st.diag:
+                    w = (np.exp(-absz[k][I][lo[k][I]:] / T) * wn[k]) / ZnDNd[k]
+                    loc[I] = (o, lo[k][I], len(w))
+                    parts.append(w)
+                    o += len(w)
+            buf = self._h2d(np.concatenate(parts)) if parts else torch.zeros(1, dtype=torch.float64, device=self.dev)
+            dsrc[k] = (buf, loc)
+        rhos = self._sweep(None, lambda k: dsrc[k])
+        traces = self._traces(rhos)
+        for k in range(nst - 1):
+            expected = sum(wn[k + 1:])
+            if expected > 0 and abs((traces[k] - expected) / expected) > 1e-9:
+                raise RuntimeError(f"Tr rhoFDM({k}) = {traces[k]!r}, expected {expected!r}")
+        return {"rhos": rhos, "wn": wn, "wnfactor": wnfactor, "last": dsrc[nst - 1], "GS": GS,
+                "tdrow": [T, E_fdm, C_fdm, F_fdm, S_fdm]}
+
+    def _spectral_pass(self, rhos, fdm) -> Tuple[Dict[str, np.ndarray], Optional[List[float]]]:
+        """The spectra of the DMNRG run: per step the operators of the spectra recalculated
+        (over all states when an FDM flag is set, do_recalc_all, c++/params.hpp:542-547;
+        else over the kept ones), BaseSpectrum::calc over all subspace pairs
+        (c++/algo.hpp:55-67) with Algo_DMNRG (c++/algo_DMNRG.hpp:29-52; merged with the
+        N/N+2 or N/N+1 window, c++/spectrum.hpp:81-128) and Algo_FDMgt/ls
+        (c++/algo_FDM.hpp:30-151; merged whole); the FDM expectation values at step
+        fdmexpvn (c++/measurements.hpp:31-44, 218-221). At the end trim (c++/bins.hpp:165-185)
+        and broaden on the device (c++/spectrum.hpp:168-196)."""
+        p, d = self.p, self.d
+        steps = self.dm_steps
+        nst = len(steps)
+        Lam = p.Lambda
         last_scale = SCALE(self.nmax, Lam, p.discretization, p.z, p.bandrescale)
         emax = p.emax if p.emax > 0 else SCALE(0, Lam, p.discretization, p.z, p.bandrescale) * 100.0
         emin = p.emin if p.emin > 0 else last_scale / 100.0
         grid = BinGrid.from_limits(emin, emax, p.bins, p.discard_immediately)
         ebins = grid.energies()
         nb = grid.nbins
-        Efac = math.sqrt(Lam) if p.NN1 else Lam
+        Efac = Lam if (d.channels == 1 and not p.NN1) else math.sqrt(Lam)  # Params::getEfactor
+        rows = (lambda s: s.n) if p.fdm_flags else (lambda s: s.nkept)  # noqa: E731
+        kinds = {"s": (1, qs.correlator_factor, self.sop_names), "d": (-1, qs.specdens_factor, self.dop_names),
+                 "t": (1, qs.dynamicsusceptibility_factor, self.top_names)}
+        tables = {"d": (self.T.DOUBLET, lambda fn, ss: fn(ss)), "t": (self.T.TRIPLET, qs.triplet_factor)}
+        parts_of = {"FDM": ("gt", "ls"), "FDMgt": ("gt",), "FDMls": ("ls",)}
+        fdm_parts = sorted({w for a in self.algos if a in parts_of for w in parts_of[a]})
+        zeros = lambda: torch.zeros(nb, dtype=torch.float64, device=self.dev)  # noqa: E731
+        dm_acc = {j: (np.zeros(nb), np.zeros(nb)) for j in range(len(self.specs))} if rhos is not None else {}
+        fdm_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in fdm_parts}
+        cur = dict(self.spec_init)
+        expv = None
+        for k, st in enumerate(steps):
+            last = k == nst - 1
+            cur = {kind: (self._recalc_singlets(st.diag, m, rows) if kind == "s"
+                          else self._recalc_tensor(st.diag, m, *tables[kind], rows)) for kind, m in cur.items()}
+            dg = st.diag
+            merge = p.NN1 or p.NN2avg or ((st.N % 2 == 0) if p.NN2even else (st.N % 2 == 1))
+            if rhos is not None and merge and self.specs:
+                rhoN = rhos[k]
+                eoff, flat, o = {}, [], 0
+                for I, s in dg.items():  # abs_zero energies of the kept states (c++/eigen.hpp:45)
+                    eoff[I] = o
+                    flat.append((s.values[:s.nkept] - s.shift) * st.scale)
+                    o += s.nkept
+                Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+                eb = Edev.data_ptr()
+                Emin_w = st.scale * p.goodE
+                Ex, Emax_w = Emin_w * Efac, Emin_w * Efac * Efac
+                win = window(ebins, Emin_w, Ex, Emax_w, st.N == self.nmax - 1, st.N == 0, p.NNtanh)
+                inside = (Emin_w < ebins) & (ebins < Emax_w)
+                f = 0.5 if p.NN2avg else 1.0
+                for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+                    sign, ff, names = kinds[kind]
+                    ops = cur[kind]
+                    o1, o2 = names.index(n1), names.index(n2)
+                    pairs = []
+                    for Ii, si in dg.items():
+                        for Ij, sj in dg.items():
+                            key = Ii if kind == "s" else (Ij, Ii)  # singlet sets are keyed by subspace
+                            if (kind == "s" and Ij != Ii) or key not in ops.loc:
+                                continue
+                            ki, kj = si.nkept, sj.nkept
+                            if ki == 0 or kj == 0:
+                                continue
+                            ld = ops.loc[key][2]
+                            pairs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2),
+                                          ld, rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj, ff(Ii, Ij)))
+                    if not pairs:
+                        continue
+                    pos, neg = zeros(), zeros()
+                    spec_accumulate_array(NRG_SPEC_DMNRG, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
+                                          sign=sign, Emin=Emin_w, Emax=Emax_w, ctx=self.ctx, stream=self.stream)
+                    for full, cs in zip(dm_acc[j], (pos.cpu().numpy(), neg.cpu().numpy())):
+                        sel = inside & (cs != 0.0)  # mergeNN2half (c++/spectrum.hpp:114-128)
+                        full[sel] += f * cs[sel] * win[sel]
+            if fdm_parts and self.specs:
+                GS = fdm["GS"]
+                eoff, flat, o = {}, [], 0
+                for I, s in dg.items():  # abs_G energies of all states (c++/eigen.hpp:47)
+                    eoff[I] = o
+                    flat.append(((s.values - s.shift) * st.scale + st.total_energy) - GS)
+                    o += s.n
+                Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+                eb = Edev.data_ptr()
+                R = fdm["rhos"][k]
+                for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+                    sign, ff, names = kinds[kind]
+                    ops = cur[kind]
+                    o1, o2 = names.index(n1), names.index(n2)
+                    gt, ls = [], []
+                    for Ii, si in dg.items():
+                        for Ij, sj in dg.items():
+                            key = Ii if kind == "s" else (Ij, Ii)
+                            if (kind == "s" and Ij != Ii) or key not in ops.loc:
+                                continue
+                            ni, nj = si.n, sj.n
+                            Ki = 0 if last else si.nkept  # Eigen::boundary (c++/eigen.hpp:219-224)
+                            Kj = 0 if last else sj.nkept
+                            ld = ops.loc[key][2]
+                            ri = R.ptr(Ii) if (R is not None and Ki) else 0
+                            rj = R.ptr(Ij) if (R is not None and Kj) else 0
+                            base = (eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2), ld)
+                            gt.append(base + (ri, max(Ki, 1), 0, 1, ni, Ki, nj, Kj, Ki, 0, ff(Ii, Ij)))
+                            ls.append(base + (0, 1, rj, max(Kj, 1), ni, Ki, nj, Kj, 0, Kj, ff(Ii, Ij)))
+                    for w, prs, algo in (("gt", gt, NRG_SPEC_FDMGT), ("ls", ls, NRG_SPEC_FDMLS)):
+                        if w in fdm_parts and prs:
+                            pos, neg = fdm_acc[(j, w)]
+                            spec_accumulate_array(algo, np.array(prs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
+                                                  sign=sign, T=p.T, wnf=fdm["wnfactor"][k], ctx=self.ctx,
+                                                  stream=self.stream)
+            if fdm is not None and p.fdmexpv and st.N == p.fdmexpvn:
+                expv = self._fdm_expv(k, st, cur["s"], fdm)
+        out: Dict[str, np.ndarray] = {}
         omega0 = p.omega0 if p.omega0 >= 0.0 else p.omega0_ratio * p.T
         bmin = p.broaden_min if p.broaden_min > 0.0 else p.broaden_min_ratio * last_scale
         mesh = []
@@ -780,68 +1044,61 @@ class QSRun:
             mesh.append(E)
             E /= p.broaden_ratio
         mesh = np.array(mesh)
-        out: Dict[str, np.ndarray] = {}
-        # gf_type sign and factor of each kind (c++/oprecalc.hpp:160-195)
-        kinds = {"s": (1, qs.correlator_factor, self.op_names), "d": (-1, qs.specdens_factor, self.dop_names),
-                 "t": (1, qs.dynamicsusceptibility_factor, self.top_names)}
-        for prefix, kind, n1, n2 in self.specs:
-            sign, ff, names = kinds[kind]
-            o1, o2 = names.index(n1), names.index(n2)
-            full_pos, full_neg = np.zeros(nb), np.zeros(nb)
-            for k, (N, scale, dg, opsets, _) in enumerate(steps):
-                dops = opsets[kind]
-                merge = p.NN1 or p.NN2avg or ((N % 2 == 0) if p.NN2even else (N % 2 == 1))
-                if not merge:
-                    continue
-                rhoN = rhos[k]
-                # abs_zero energies of the kept states (c++/eigen.hpp:45)
-                eoff, flat, o = {}, [], 0
-                for I, s in dg.items():
-                    eoff[I] = o
-                    flat.append((s.values[:s.nstored] - s.shift) * scale)
-                    o += s.nstored
-                Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
-                eb = Edev.data_ptr()
-                pairs = []
-                for Ii, si in dg.items():
-                    for Ij, sj in dg.items():
-                        # singlet sets are keyed by the subspace (the block (I, I))
-                        key = Ii if kind == "s" else (Ij, Ii)
-                        if (kind == "s" and Ij != Ii) or key not in dops.loc or si.nstored == 0 or sj.nstored == 0:
-                            continue
-                        ki, kj = si.nstored, sj.nstored
-                        pairs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], dops.ptr(key, o1), ki, dops.ptr(key, o2), ki,
-                                      rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj, ff(Ii, Ij)))
-                pos = torch.zeros(nb, dtype=torch.float64, device=self.dev)
-                neg = torch.zeros(nb, dtype=torch.float64, device=self.dev)
-                Emin_w = scale * p.goodE
-                if pairs:
-                    spec_accumulate_array(0, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg, sign=sign,
-                                          Emin=Emin_w, Emax=Emin_w * Efac * Efac, ctx=self.ctx, stream=self.stream)
-                cp, cn = pos.cpu().numpy(), neg.cpu().numpy()
-                Ex, Emax_w = Emin_w * Efac, Emin_w * Efac * Efac
-                f = (0.5 if p.NN2avg else 1.0)
-                win = window(ebins, Emin_w, Ex, Emax_w, N == self.nmax - 1, N == 0, p.NNtanh)
-                inside = (Emin_w < ebins) & (ebins < Emax_w)
-                for full, cs in ((full_pos, cp), (full_neg, cn)):
-                    sel = inside & (cs != 0.0)
-                    full[sel] += f * cs[sel] * win[sel]
+        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+            for a in self.algos:
+                if a == "DMNRG":
+                    full_pos, full_neg = dm_acc[j]
+                else:
+                    full_pos = sum(fdm_acc[(j, w)][0] for w in parts_of[a]).cpu().numpy()
+                    full_neg = sum(fdm_acc[(j, w)][1] for w in parts_of[a]).cpu().numpy()
+                out[f"{prefix}_{a}_dens_{n1}-{n2}"] = self._broadened(full_pos, full_neg, ebins, mesh, omega0)
+        return out, expv
 
-            def trim(w):
-                width = np.diff(ebins)
-                keep = np.concatenate([np.abs(w[:-1]) >= p.discard_trim * width, [True]])
-                return ebins[keep], w[keep]
-            ep, wp = trim(full_pos)
-            en, wn = trim(full_neg)
-            spikes_e = np.concatenate([ep, -en])
-            spikes_w = np.concatenate([wp, wn])
-            mesh_all = np.concatenate([mesh, -mesh])
-            vals = broaden(spikes_e, spikes_w, mesh_all, p.alpha, omega0, self.ctx, self.stream)
-            npos = len(mesh)
-            rows_pos = sorted(zip(mesh_all[:npos].tolist(), vals[:npos].tolist()))
-            rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
-            out[f"{prefix}_DMNRG_dens_{n1}-{n2}"] = np.array(rows_neg + rows_pos)
-        return out
+    def _fdm_expv(self, k: int, st: "_StepRecord", sops: MatSet, fdm: Dict) -> List[float]:
+        """measure_singlet_fdm (c++/measurements.hpp:31-44): sum_I mult(I) Tr[rhoFDM_I O_I] over
+        the kept states of step k, for every singlet operator."""
+        R = fdm["rhos"][k]
+        vals = []
+        for o, name in enumerate(self.sop_names):
+            acc = torch.zeros((), dtype=torch.float64, device=self.dev)
+            for I, s in st.diag.items():
+                kk = s.nkept
+                if kk == 0 or I not in sops.loc:
+                    continue
+                off, r, c = sops.loc[I]
+                Om = sops.buf[o * sops.total + off: o * sops.total + off + r * c].view(r, c)[:kk, :kk]
+                if R is not None:  # dense KK density matrix
+                    roff, rr, rc = R.loc[I]
+                    Rm = R.buf[roff: roff + rr * rc].view(rr, rc)[:kk, :kk]
+                    acc = acc + qs.mult(I) * torch.sum(Rm * Om.T)
+                else:  # the last step: the diagonal init_rho_FDM
+                    buf, loc = fdm["last"]
+                    if I in loc:
+                        woff, r0, cnt = loc[I]
+                        acc = acc + qs.mult(I) * torch.sum(buf[woff: woff + kk] * torch.diagonal(Om))
+            vals.append(acc)
+        return [float(v) for v in torch.stack(vals).cpu().numpy()] if vals else []
+
+    def _broadened(self, full_pos: np.ndarray, full_neg: np.ndarray, ebins: np.ndarray, mesh: np.ndarray,
+                   omega0: float) -> np.ndarray:
+        """Bins::trim (c++/bins.hpp:165-185) of both halves, then SpectrumRealFreq::continuous
+        (c++/spectrum.hpp:168-196) on the device; rows (E, A(E)) sorted by E."""
+        p = self.p
+
+        def trim(w):
+            width = np.diff(ebins)
+            keep = np.concatenate([np.abs(w[:-1]) >= p.discard_trim * width, [True]])
+            return ebins[keep], w[keep]
+        ep, wp = trim(full_pos)
+        en, wn = trim(full_neg)
+        spikes_e = np.concatenate([ep, -en])
+        spikes_w = np.concatenate([wp, wn])
+        mesh_all = np.concatenate([mesh, -mesh])
+        vals = broaden(spikes_e, spikes_w, mesh_all, p.alpha, omega0, self.ctx, self.stream)
+        npos = len(mesh)
+        rows_pos = sorted(zip(mesh_all[:npos].tolist(), vals[:npos].tolist()))
+        rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
+        return np.array(rows_neg + rows_pos)
 
 def window(e: np.ndarray, Emin: float, Ex: float, Emax: float, last: bool, first: bool, NNtanh: float) -> np.ndarray:
     """windowfunction (c++/spectrum.hpp:91-109) for the bin energies inside (Emin, Emax)."""
@@ -904,7 +1161,10 @@ def main(argv=None) -> int:
     os.makedirs(out, exist_ok=True)
     _write_table(os.path.join(out, "td"), res.td_fields, res.td)
     _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom)
-    for name, rows in res.spectra.items():  # <prefix>_DMNRG_dens_<op1>-<op2>.dat, as Spikes::save writes it
+    for name, tab in (("tdfdm", res.tdfdm), ("customfdm", res.customfdm)):
+        if tab is not None:
+            _write_table(os.path.join(out, name), tab[0], [tab[1]])
+    for name, rows in res.spectra.items():  # <prefix>_<algo>_dens_<op1>-<op2>.dat, as Spikes::save writes it
         with open(os.path.join(out, f"{name}.dat"), "w") as f:
             for e, v in rows:
                 f.write(f"{e:.10g} {v:.10g}\n")

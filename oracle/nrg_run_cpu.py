@@ -448,9 +448,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
     last_scale = SCALE(Nmax, Lam, disc, z)
     if bmin <= 0.0:
         bmin = float(kv.get("broaden_min_ratio", 3.0)) * last_scale
-    Efac = Lam  # one channel, no N/N+1 patching
-    if NN1:
-        Efac = math.sqrt(Lam)
+    Efac = Lam if (combs == 4 and not NN1) else math.sqrt(Lam)  # Params::getEfactor (c++/params.hpp:650-652)
     nst = len(steps)
     IN = _qs.QS1.IN if combs == 4 else _qs.QS2.IN
 
