@@ -66,7 +66,7 @@ NRG_API int nrg_destroy(nrg_ctx* ctx);
  *   info       host array of nblk status words: 0 ok; -2 non-finite input; > 0 the
  *              tridiagonal iteration did not converge (the reference's INFO != 0)
  * H, evals, evecs are host arrays of device pointers; evecs[b] must not alias H[b]. */
-#define NRG_DIAG_MAX_N 4096
+#define NRG_DIAG_MAX_N 10240
 NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* H, double* const* evals,
                    double* const* evecs, int* info, void* stream);
 

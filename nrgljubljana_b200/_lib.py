@@ -15,7 +15,7 @@ NRG_ERR_ARG = -1
 NRG_ERR_CUDA = -2
 NRG_ERR_OOM = -3
 NRG_ERR_NODEV = -4
-NRG_DIAG_MAX_N = 4096
+NRG_DIAG_MAX_N = 10240
 
 NRG_SPEC_DMNRG = 0
 NRG_SPEC_FDMGT = 1

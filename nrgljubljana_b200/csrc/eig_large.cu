@@ -37,7 +37,11 @@ constexpr int kTriThreads = 128;
 constexpr int NB = 16;     // tridiagonalisation panel width
 constexpr int NBT = 128;   // back-transform panel width
 constexpr int kLeaf = 32;  // divide-and-conquer leaves have at most this order
-constexpr int kMaxLargeN = 4096;
+constexpr int kMaxLargeN = 10240;  // the tridiagonalisation's shared memory (68 KB + 16 n bytes) fits to here
+// Merge nodes whose prep arrays exceed this many bytes keep them in global scratch (kPrepGlobalB
+// bytes per row of the block) instead of shared memory.
+constexpr size_t kPrepSmemMax = 200 * 1024;
+constexpr size_t kPrepGlobalB = 80;
 
 struct LargeBlock {
   double* H;      // input (consumed); then the eigenvector rows of T during divide and
@@ -56,6 +60,7 @@ struct LargeBlock {
   double* GT;     // per back-transform panel of nb reflectors: Gram matrix V^T V then T (nb x nb each)
   int* rank;      // per node: sorted position of grouped entry
   int* perm;      // final eigenvalue order
+  char* pscr;     // kPrepGlobalB bytes per row: merge-prep arrays of nodes too large for shared memory
   int* info;
   int n, npanel;
   int ldp, pad_;  // leading dimension of the packed lower triangle in W1 (multiple of 32)
@@ -856,7 +861,8 @@ __host__ __device__ inline PrepLayout prep_layout(int N) {
 
 __global__ void __launch_bounds__(512) dc_prep_kernel(const LargeBlock* __restrict__ blocks,
                                                       const DcNode* __restrict__ nodes, DcState* __restrict__ states,
-                                                      GemmOut* __restrict__ gouts, GemmSeg* __restrict__ gsegs) {
+                                                      GemmOut* __restrict__ gouts, GemmSeg* __restrict__ gsegs,
+                                                      size_t smem_bytes) {
   extern __shared__ __align__(16) double sm[];
   __shared__ double red[32];
   __shared__ int cnt[8];
@@ -867,7 +873,9 @@ __global__ void __launch_bounds__(512) dc_prep_kernel(const LargeBlock* __restri
   int P = 1;
   while (P < N) P <<= 1;
   const PrepLayout PL = prep_layout(N);
-  char* smc = reinterpret_cast<char*>(sm);
+  // a node whose arrays do not fit the shared memory of the launch uses its rows' slice of the
+  // block's global scratch (nodes of one level cover disjoint rows)
+  char* smc = PL.total <= smem_bytes ? reinterpret_cast<char*>(sm) : B.pscr + kPrepGlobalB * (size_t)a;
   double* key = reinterpret_cast<double*>(smc + PL.key);
   int* sidx = reinterpret_cast<int*>(smc + PL.sidx);
   double* zs = reinterpret_cast<double*>(smc + PL.zs);
@@ -1321,7 +1329,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 size_t large_block_doubles(int n) {
   const size_t ldp = (size_t)(n + 31) / 32 * 32;
-  return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + 2 * (size_t)NBT * n + 2 * (size_t)n + 64 * 12;
+  return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + 2 * (size_t)NBT * n + 2 * (size_t)n + 64 * 13 +
+         (prep_layout(n).total > kPrepSmemMax ? (kPrepGlobalB * (size_t)n + 7) / 8 : 0);
 }
 
 }  // namespace
@@ -1377,6 +1386,8 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       int* ip = reinterpret_cast<int*>(take(nb_));
       L.rank = ip;
       L.perm = ip + nb_;
+      L.pscr = prep_layout(nb_).total > kPrepSmemMax
+                   ? reinterpret_cast<char*>(take((kPrepGlobalB * (size_t)nb_ + 7) / 8)) : nullptr;
       L.info = info_dev + b;
       L.n = nb_;
       blk.push_back(L);
@@ -1580,11 +1591,16 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       DcState* dst = reinterpret_cast<DcState*>(dbase + st_off[h]);
       GemmOut* go = reinterpret_cast<GemmOut*>(dbase + lvl_gemm[h].outs_off);
       GemmSeg* gs = reinterpret_cast<GemmSeg*>(dbase + lvl_gemm[h].segs_off);
-      const size_t ps = prep_layout(maxN).total;
+      // shared memory for the largest node that fits it; larger nodes use global scratch
+      size_t ps = 16;
+      for (auto& nd : levels[h]) {
+        const size_t t = prep_layout(nd.b - nd.a).total;
+        if (t <= kPrepSmemMax) ps = std::max(ps, t);
+      }
       NRG_CK(cudaFuncSetAttribute(dc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
       {
         PhaseScope sc(c, kPhDcPrep, s);
-        dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs);
+        dc_prep_kernel<<<nn, 512, ps, s>>>(dblk, dn, dst, go, gs, ps);
         NRG_CK(cudaGetLastError());
       }
       // one warp per root (8 per CTA), at most 64 CTAs per node

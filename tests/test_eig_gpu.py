@@ -162,3 +162,27 @@ def test_dsyevr_ratio(nb, oracle):
     w, v = oracle.diagonalise(h, "dsyevr", 0.5)
     assert len(r.val) == len(w) == 15
     assert np.abs(r.val - w).max() < 1e-12 * np.linalg.norm(full_from_upper(h), 2)
+
+
+@pytest.mark.parametrize("n,kind", [(4097, "random"), (6000, "graded"), (10240, "random")])
+def test_large_orders(nb, n, kind):
+    """Orders above 4096, where the merge prep of the divide and conquer keeps its arrays in
+    global scratch: eigenvalues against host LAPACK (eigvalsh), residuals and orthogonality
+    of the vectors computed on the device."""
+    import torch
+    rng = np.random.default_rng(300 + n)
+    h = rand_upper(rng, n) if kind == "random" else graded_block(rng, n)
+    g = nb.diagonalisations([h])[0]
+    H = full_from_upper(h)
+    w_ref = np.linalg.eigvalsh(H)
+    nrm = max(abs(w_ref[0]), abs(w_ref[-1]))
+    assert np.all(np.diff(g.val) >= 0)
+    assert np.max(np.abs(g.val - w_ref)) <= 1e-12 * nrm * max(1.0, math.sqrt(n / 1000.0))
+    Hd = torch.tensor(H, device="cuda")
+    V = torch.tensor(g.vec, device="cuda")
+    w = torch.tensor(g.val, device="cuda")
+    res = torch.linalg.norm(V @ Hd - w[:, None] * V, dim=1).max().item()
+    assert res <= 1e-12 * nrm * math.sqrt(n)
+    G = V @ V.T
+    assert (torch.diagonal(G) - 1).abs().max().item() < 1e-12
+    assert (G - torch.diag(torch.diagonal(G))).abs().max().item() < 1e-10
