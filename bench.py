@@ -216,6 +216,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
     ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
+    ap.add_argument("--no-c3", action="store_true", help="skip the two-channel Kondo FDM run")
     ap.add_argument("--write-c0", default=None, metavar="DIR",
                     help="write the param and data files of the NRG-run workload to DIR and exit")
     args = ap.parse_args()
@@ -354,6 +355,12 @@ def main():
         line["nrg_run"] = nrg_run_arm(torch, local, args)
     if not args.no_nrg and rank == 0:
         line["serving"] = serving_arm(torch, local, line["nrg_run"])
+    if not args.no_c3 and rank == 0:
+        torch.cuda.empty_cache()
+        try:
+            line["c3_run"] = c3_arm(torch, local, args)
+        except (RuntimeError, MemoryError) as err:
+            line["c3_run"] = {"workload": C3_WORKLOAD, "error": str(err)[:300]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -405,6 +412,120 @@ C0_SPEC = "spec_DMNRG_dens_A_d-A_d"  # the DM-NRG spectral function of the C0 ru
 NRG_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delta=0), Gamma=0.04, flat band, "
                 "Lambda=2 (Z), z=1, Nmax=40, keep=1000, keepenergy=10, T=1e-8, operator n_d, DM-NRG spectral "
                 "function A_d-A_d (1000 bins/decade, broadened); input generated by nrgljubljana_b200.datagen")
+
+
+C3_PARAM = """[param]
+symtype=QS
+Lambda=3
+keep=5000
+T=1e-6
+fdm=true
+spect=S_imp-S_imp
+"""
+C3_WORKLOAD = ("NRG run, QS two-channel Kondo model, impurity spin 1/2, J=0.2 on both flat channels, "
+               "Lambda=3 (Z), z=1, Nmax=50, keep=5000, T=1e-6, FDM dynamic spin susceptibility S_imp-S_imp "
+               "(1000 bins/decade, broadened) and FDM thermodynamics; input generated by nrgljubljana_b200.datagen")
+
+
+def c3_inputs():
+    from nrgljubljana_b200.datagen import kondo_qs
+    return C3_PARAM, kondo_qs([0.2, 0.2], 0.5, 3.0, 50, ops=["S_imp"])
+
+
+def cpu_dsyev_estimate(dims, threads: int) -> dict:
+    """The CPU time of one step's diagonalisations (dsyev, eigenvalues and vectors) on the host
+    cores, estimated from measured sample blocks: t(n) = c n^3 fitted on single-thread dsyev
+    of n = 600 and 1200 (layout i: OpenMP over blocks, one BLAS thread each, as
+    diagonalisations_OpenMP runs; the step takes the longest-processing-time schedule of the
+    blocks on `threads` cores) and on threaded dsyev of n = 2000 (layout ii: blocks one after
+    another, all BLAS threads)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(SEED)
+
+    def block(n):
+        h = np.triu(rng.standard_normal((n, n)) * 0.1, 1)
+        h[np.diag_indices(n)] = 2.0 ** (-np.arange(n) / 2.0)
+        return h
+    O.build()
+    O.blas_threads(1)
+    t1 = {}
+    for n in (600, 1200):
+        h = block(n)
+        t0 = time.perf_counter()
+        O.diagonalise(h)
+        t1[n] = time.perf_counter() - t0
+    c1 = t1[1200] / 1200.0 ** 3
+    O.blas_threads(threads)
+    h = block(2000)
+    t0 = time.perf_counter()
+    O.diagonalise(h)
+    tt = time.perf_counter() - t0
+    O.blas_threads(1)
+    ct = tt / 2000.0 ** 3
+    load = np.zeros(threads)
+    for n in sorted(dims, reverse=True):  # longest processing time first
+        load[np.argmin(load)] += c1 * float(n) ** 3
+    return {"openmp_over_blocks_s": float(load.max()),
+            "threaded_blas_s": float(sum(ct * float(n) ** 3 for n in dims)),
+            "measured": {"dsyev_1_thread_s": {str(k): v for k, v in t1.items()},
+                         f"dsyev_{threads}_threads_n2000_s": tt}}
+
+
+def c3_arm(torch, device: int, args) -> dict:
+    """One whole run of the two-channel Kondo FDM workload: the forward sweep (assembly, batched
+    eigensolve, recalculation) and the FDM density matrices and spectral pass, wall clock on the
+    device; the reference's CPU dsyev path on the host cores estimated for the same steps."""
+    from nrgljubljana_b200 import context
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import QSRun, RunParams
+    param, data = c3_inputs()
+    p, d = RunParams.from_param(parse_param(param)), read_data(data)
+    ctx = context(device)
+    torch.cuda.reset_peak_memory_stats(device)
+    run = QSRun(p, d, device, ctx)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run.start()
+    while not run.done:
+        job = run.begin_step()
+        run.end_step(job, run._diagonalise(job))
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    res = run.finish()
+    torch.cuda.synchronize()
+    t_all = time.perf_counter() - t0
+    flop = sum(f_eig(np.array(ns)) for ns in res.block_dims)
+    out = {"workload": C3_WORKLOAD, "steps_per_run": d.nmax, "steps_per_s": d.nmax / t_all,
+           "s_per_run": t_all, "forward_s": t_fwd, "fdm_and_spectra_s": t_all - t_fwd,
+           "timing": "wall clock of one run (host driver included)",
+           "eig_flop_per_run": flop, "eig_gflops_forward": flop / t_fwd / 1e9,
+           "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
+           "peak_device_gib": torch.cuda.max_memory_allocated(device) / 2 ** 30,
+           "tdfdm": dict(zip(*res.tdfdm)) if res.tdfdm else None,
+           "spectrum": {k: int(len(v)) for k, v in res.spectra.items()}}
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        heavy = max(range(len(res.block_dims)), key=lambda k: sum(float(n) ** 3 for n in res.block_dims[k]))
+        est = cpu_dsyev_estimate(res.block_dims[heavy], threads)
+        scale = sum(sum(float(n) ** 3 for n in ns) for ns in res.block_dims) / \
+            sum(float(n) ** 3 for n in res.block_dims[heavy])
+        # layout i: every step's own schedule of its blocks on the cores
+        tot_i = 0.0
+        c1 = est["measured"]["dsyev_1_thread_s"]["1200"] / 1200.0 ** 3
+        for ns in res.block_dims:
+            load = np.zeros(threads)
+            for n in sorted(ns, reverse=True):
+                load[np.argmin(load)] += c1 * float(n) ** 3
+            tot_i += float(load.max())
+        per_run = {"openmp_over_blocks_s": tot_i, "threaded_blas_s": est["threaded_blas_s"] * scale}
+        best = min(per_run.values())
+        out["cpu_baseline"] = {"steps_per_s_estimated": d.nmax / best, "diag_s_per_run_estimated": per_run,
+                               "cores": threads, "kind": "port",
+                               "sample": "dsyev of n = 600, 1200 (1 thread) and 2000 (all threads), scaled by n^3 "
+                                         "to every block of the run; diagonalisations only (the reference's "
+                                         "recalculation and FDM sums come on top)",
+                               "measured": est["measured"]}
+    return out
 
 
 def c0_inputs():

@@ -171,14 +171,16 @@ constexpr int kTriWarps = kTriThreads / 32;
 // A lane owns rows l and l+32 of the slab: row sums stay in registers until the tile row
 // changes, column sums are transposed across the warp; both are added to y (shared memory).
 // `parity` holds the warp's mbarrier phase bits across calls.
+// gwarp / gnwarps: this warp's index among the warps that share the product (the warps of
+// one CTA, or of every CTA of a cluster), and their number; y receives this warp's part.
 NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v, double* y, double* ring,
-                        uint64_t* bars, unsigned& parity, int* err) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+                        uint64_t* bars, unsigned& parity, int* err, int gwarp, int gnwarps) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int T0 = s0 >> 6, Tn = (n - 1) >> 6, sl0 = s0 >> 3, slmax = (n - 1) >> 3;
   auto rowlen = [&](int I) { return min(8 * I + 7, slmax) - sl0 + 1; };
   long long S = 0;
   for (int I = T0; I <= Tn; I++) S += rowlen(I);
-  const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
+  const long long f0 = S * gwarp / gnwarps, f1 = S * (gwarp + 1) / gnwarps;
   if (f0 >= f1) return;
   double* myring = ring + (size_t)warp * kStages * kSlabD;
   uint64_t* mybar = bars + warp * kStages;
@@ -283,14 +285,23 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
 // is 8 consecutive doubles per quarter-warp. The row operands Y of a tile row stay in
 // registers while the warp walks the columns. The tiles of the trailing lower triangle,
 // in tile-row order, are split evenly between the warps.
+// CG: read P and W past the L1 cache (ld.global.cg); needed when other CTAs wrote them,
+// since an SM's L1 may still hold lines it read before those writes.
+template <bool CG>
+NRG_DEV double ldp(const double* p) {
+  if constexpr (CG) return __ldcg(p);
+  else return *p;
+}
+
+template <bool CG>
 NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, int n, int ld, int p0, int nbp,
-                          int s0) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+                          int s0, int gwarp, int gnwarps) {
+  const int lane = threadIdx.x & 31;
   const int r = lane >> 2, c4 = lane & 3;
   const int T0 = s0 >> 5, Tn = (n - 1) >> 5;
   const int nt = Tn - T0 + 1;
   const long long S = (long long)nt * (nt + 1) / 2;
-  const long long f0 = S * warp / nwarps, f1 = S * (warp + 1) / nwarps;
+  const long long f0 = S * gwarp / gnwarps, f1 = S * (gwarp + 1) / gnwarps;
   if (f0 >= f1) return;
   int I = T0;
   long long acc0 = 0;
@@ -314,7 +325,7 @@ NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, 
 #pragma unroll
         for (int mi = 0; mi < 4; mi++) {
           const int ii = i0 + 8 * mi + r;
-          ya[mi][ks] = (qq < nbp && ii < n) ? -row[ii] : 0.0;
+          ya[mi][ks] = (qq < nbp && ii < n) ? -ldp<CG>(row + ii) : 0.0;
         }
       }
     }
@@ -327,7 +338,7 @@ NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, 
         for (int h = 0; h < 2; h++) {
           const int ii = i0 + 8 * mi + r, jj = j0 + 8 * ni + 2 * c4 + h;
           const bool ok = jj >= s0 && ii < n && ii >= jj;
-          acc[mi][ni][h] = ok ? P[(size_t)jj * ld + ii] : 0.0;
+          acc[mi][ni][h] = ok ? ldp<CG>(P + (size_t)jj * ld + ii) : 0.0;
         }
 #pragma unroll
     for (int ks = 0; ks < 2 * NB / 4; ks++) {
@@ -339,7 +350,7 @@ NRG_DEV void panel_update(double* __restrict__ P, const double* __restrict__ W, 
 #pragma unroll
       for (int ni = 0; ni < 4; ni++) {
         const int jj = j0 + 8 * ni + r;
-        b[ni] = (qq < nbp && jj < n) ? row[jj] : 0.0;
+        b[ni] = (qq < nbp && jj < n) ? ldp<CG>(row + jj) : 0.0;
       }
 #pragma unroll
       for (int mi = 0; mi < 4; mi++)
@@ -459,7 +470,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        symv_lower(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info);
+        symv_lower(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info, warp, nwarps);
         if (j > 0) {
           double pw[NB], pv[NB];
 #pragma unroll
@@ -515,7 +526,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       }
       __syncthreads();
     }
-    panel_update(A, W, n, ld, p0, pe - p0, pe);
+    panel_update<false>(A, W, n, ld, p0, pe - p0, pe, warp, nwarps);
     fence_proxy_async_global();  // the next symv reads the updated trailing block by bulk copies
     __syncthreads();
   }
@@ -531,6 +542,192 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
   int bad = 0;
   for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
   if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
+}
+
+// ---------------------------------------------------------------- large blocks, few of them
+// One thread-block cluster per block: the blocked reduction of tridiag_kernel with the TMA
+// slabs of A v and the tiles of the panel update split over the warps of every CTA of the
+// cluster. The column work (current column, reflector) is repeated by every CTA on its own
+// copy of the vectors; each CTA writes its slice of rows to global memory. The parts of A v
+// and of the dot products are summed through distributed shared memory: after the first
+// barrier each CTA reduces its slice of rows, after the second the scalar y^T v is summed;
+// the third makes the column of W visible to the cluster, a fourth follows each panel update.
+// Every CTA executes the same sequence of barriers whatever the data.
+constexpr int kTclC = 8;  // CTAs per cluster
+
+__global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const LargeBlock* __restrict__ blocks,
+                                                                     const CUtensorMap* __restrict__ tmaps) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) double sm[];
+  __shared__ __align__(8) uint64_t bars[kTriWarps * kStages];
+  const int C = (int)cl.num_blocks(), rk = (int)cl.block_rank();
+  const int bi = blockIdx.x / C;
+  const LargeBlock B = blocks[bi];
+  const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+  const int gw = rk * nwarps + warp, gnw = C * nwarps;
+  double* A = B.W1;
+  double* W = B.W2;
+  // The arrays that other CTAs read (y, dots, pps) sit at fixed offsets from the start of the
+  // dynamic shared memory, so that map_shared_rank finds them at the same offsets in every
+  // CTA; the 1024-byte aligned TMA ring comes last (its padding depends on where the CTA's
+  // shared memory window starts, which differs between CTAs sharing an SM).
+  double* y = sm;                                   // n: this CTA's part of A v; its slice: the reduced y
+  double* dots = y + n;                             // 2NB: this CTA's part of W^T v, V^T v
+  double* pps = dots + 2 * NB;                      // 2: this CTA's part of y^T v
+  double* v = pps + 2;                              // n: current column, then the reflector
+  double* part = v + n;                             // nwarps * 2NB
+  double* cwv = part + nwarps * 2 * NB;             // 2NB: the sums
+  double* red = cwv + 2 * NB;                       // 64 (two halves for block_sum_1b)
+  double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red + 64) + 1023) & ~(uintptr_t)1023);
+  int phase = 0;
+  unsigned parity = 0;
+  if (lane == 0) {
+    for (int st = 0; st < kStages; st++) mbar_init(bars + warp * kStages + st, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  for (int p0 = 0; p0 < n - 2; p0 += NB) {
+    const int pe = min(p0 + NB, n - 2);
+    for (int k = p0; k < pe; k++) {
+      const int j = k - p0;
+      // (1) current column k (rows k..n-1) = stored column minus the pending panel terms
+      {
+        double wk[NB], vk[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          wk[q] = (q < j) ? __ldcg(W + (size_t)q * n + k) : 0.0;
+          vk[q] = (q < j) ? __ldcg(A + (size_t)(p0 + q) * ld + k) : 0.0;
+        }
+        for (int i = k + tid; i < n; i += nt) {
+          double a = __ldcg(A + (size_t)k * ld + i);
+#pragma unroll
+          for (int q = 0; q < NB; q++)
+            if (q < j) a -= __ldcg(A + (size_t)(p0 + q) * ld + i) * wk[q] + __ldcg(W + (size_t)q * n + i) * vk[q];
+          v[i] = a;
+          y[i] = 0.0;
+        }
+      }
+      __syncthreads();
+      // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
+      double ps = 0.0;
+      for (int i = k + 2 + tid; i < n; i += nt) ps += v[i] * v[i];
+      const double sigma = block_sum_1b(ps, red, phase);
+      const double alpha = v[k + 1];
+      double tau = 0.0, beta = alpha, scale = 1.0;
+      if (sigma > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+        tau = (beta - alpha) / beta;
+        scale = 1.0 / (alpha - beta);
+      }
+      if (rk == 0 && tid == 0) {
+        B.d[k] = v[k];
+        B.e[k] = beta;
+        B.tau[k] = tau;
+      }
+      for (int i = k + 2 + tid; i < n; i += nt) v[i] *= scale;
+      if (tid == 0) v[k + 1] = 1.0;
+      __syncthreads();
+      // column k of A is written back only in (5): other CTAs may still be reading it in (1)
+      // (3) this CTA's part of A v and of the dot products W^T v, V^T v over its slice of rows
+      const int ch1 = (n - k - 1 + C - 1) / C, lo1 = k + 1 + rk * ch1, hi1 = min(n, lo1 + ch1);
+      if (tau != 0.0) symv_lower(tmaps + bi, n, k + 1, v, y, ring, bars, parity, B.info, gw, gnw);
+      {
+        double pw[NB], pv[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) pw[q] = pv[q] = 0.0;
+        if (tau != 0.0 && j > 0) {
+          for (int i = lo1 + tid; i < hi1; i += nt) {
+            const double vi = v[i];
+#pragma unroll
+            for (int q = 0; q < NB; q++)
+              if (q < j) {
+                pw[q] = fma(__ldcg(W + (size_t)q * n + i), vi, pw[q]);
+                pv[q] = fma(__ldcg(A + (size_t)(p0 + q) * ld + i), vi, pv[q]);
+              }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          const double a = warp_sum(pw[q]);
+          const double b = warp_sum(pv[q]);
+          if (lane == 0) {
+            part[warp * 2 * NB + q] = a;
+            part[warp * 2 * NB + NB + q] = b;
+          }
+        }
+        __syncthreads();
+        if (tid < 2 * NB) {
+          double t = 0.0;
+          for (int w = 0; w < nwarps; w++) t += part[w * 2 * NB + tid];
+          dots[tid] = t;
+        }
+      }
+      cl.sync();  // (B1) the parts of A v and of the dot products are complete
+      // (4) this CTA's slice: y = (sum of the parts - V (W^T v) - W (V^T v)) tau
+      if (tid < 2 * NB) {
+        double t = 0.0;
+        for (int q = 0; q < C; q++) t += cl.map_shared_rank(dots, q)[tid];
+        cwv[tid] = t;
+      }
+      __syncthreads();
+      double pp = 0.0;
+      if (tau != 0.0) {
+        double cw[NB], cv[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+          cw[q] = (q < j) ? cwv[q] : 0.0;
+          cv[q] = (q < j) ? cwv[NB + q] : 0.0;
+        }
+        for (int i = lo1 + tid; i < hi1; i += nt) {
+          double yi = 0.0;
+          for (int q = 0; q < C; q++) yi += cl.map_shared_rank(y, q)[i];
+#pragma unroll
+          for (int q = 0; q < NB; q++)
+            if (q < j) yi -= __ldcg(A + (size_t)(p0 + q) * ld + i) * cw[q] + __ldcg(W + (size_t)q * n + i) * cv[q];
+          yi *= tau;
+          pp = fma(yi, v[i], pp);
+          y[i] = yi;  // only this CTA's slice is read from here on, and only by this CTA
+        }
+      }
+      const double ppb = block_sum_1b(pp, red, phase);
+      if (tid == 0) pps[0] = ppb;
+      cl.sync();  // (B2) every CTA has its slice of y and its part of y^T v
+      double yv = 0.0;
+      for (int q = 0; q < C; q++) yv += cl.map_shared_rank(pps, q)[0];
+      const double Kc = 0.5 * tau * yv;
+      for (int i = lo1 + tid; i < hi1; i += nt) {
+        W[(size_t)j * n + i] = (tau != 0.0) ? y[i] - Kc * v[i] : 0.0;
+        A[(size_t)k * ld + i] = v[i];  // the reflector, unit at k+1
+      }
+      if (rk == 0) {  // zeros from the start of its back-transform panel down to the diagonal
+        const int kb0 = (k / NBT) * NBT;
+        for (int i = kb0 + 1 + tid; i <= k; i += nt) A[(size_t)k * ld + i] = 0.0;
+      }
+      cl.sync();  // (B3) column j of W and column k of the reflectors are visible to the cluster
+    }
+    panel_update<true>(A, W, n, ld, p0, pe - p0, pe, gw, gnw);
+    fence_proxy_async_global();  // the next products read the updated trailing block by bulk copies
+    cl.sync();                   // (B4)
+    fence_proxy_async_global();
+  }
+  if (rk == 0) {
+    if (tid == 0) {
+      B.d[n - 2] = __ldcg(A + (size_t)(n - 2) * ld + n - 2);
+      B.e[n - 2] = __ldcg(A + (size_t)(n - 2) * ld + n - 1);
+      B.d[n - 1] = __ldcg(A + (size_t)(n - 1) * ld + n - 1);
+      B.e[n - 1] = 0.0;
+      B.tau[n - 2] = 0.0;
+      B.tau[n - 1] = 0.0;
+    }
+    __syncthreads();
+    int bad = 0;
+    for (int i = tid; i < n; i += nt) bad |= !(isfinite(B.d[i]) && isfinite(B.e[i]));
+    if (__syncthreads_or(bad) && tid == 0) atomicMin(B.info, -2);
+  }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
 // ---------------------------------------------------------------- mid-size tridiagonalisation
@@ -1569,11 +1766,49 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       if (nbig) {
         const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
                                                      (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
-        NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(dbase + tmap_off);
         pack_lower_kernel<<<dim3((maxn + 7) / 8, nbig), 256, 0, s>>>(dblk);
         NRG_CK(cudaGetLastError());
-        tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, reinterpret_cast<const CUtensorMap*>(dbase + tmap_off));
-        NRG_CK(cudaGetLastError());
+        // Few large blocks: one cluster of kTclC CTAs per block, when the clusters fill at most
+        // about two waves of the SMs and the device can hold one such cluster at a time.
+        bool tcl = false;
+        // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
+        // CTAs on one SM the reductions came out wrong on B200 (cause not found); with one per
+        // SM every check passes. A cluster holds 8 SMs per block either way.
+        int smsm = 0;
+        cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+        const size_t smem_tcl =
+            std::max(smem + sizeof(double) * (2 * NB + 2), (size_t)smsm / 2 + 1024);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        if ((long long)nbig * kTclC <= 2LL * nsm && smem_tcl + 256 <= (size_t)optin) {
+          NRG_CK(cudaFuncSetAttribute(tridiag_tcl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tcl));
+          cfg.gridDim = dim3((unsigned)(nbig * kTclC));
+          cfg.blockDim = dim3(kTriThreads);
+          cfg.dynamicSmemBytes = smem_tcl;
+          cfg.stream = s;
+          at[0].id = cudaLaunchAttributeClusterDimension;
+          at[0].val.clusterDim.x = (unsigned)kTclC;
+          at[0].val.clusterDim.y = 1;
+          at[0].val.clusterDim.z = 1;
+          cfg.attrs = at;
+          cfg.numAttrs = 1;
+          int ncl = 0;
+          if (cudaOccupancyMaxActiveClusters(&ncl, tridiag_tcl_kernel, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            ncl = 0;
+          }
+          tcl = ncl > 0;
+        }
+        if (tcl) {
+          NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_tcl_kernel, (const LargeBlock*)dblk, tm));
+        } else {
+          NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, tm);
+          NRG_CK(cudaGetLastError());
+        }
       }
       if (fork) NRG_CK(cudaStreamWaitEvent(s, c->join2_ev, 0));
     }

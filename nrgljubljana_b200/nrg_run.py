@@ -150,6 +150,7 @@ class Result:
     custom: List[List[float]]
     blocks_per_step: List[int] = field(default_factory=list)
     max_dim_per_step: List[int] = field(default_factory=list)
+    block_dims: List[List[int]] = field(default_factory=list)  # orders of the blocks of every step
     # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_FDM_...", "spin_...") -> rows (E, A(E))
     spectra: Dict[str, np.ndarray] = field(default_factory=dict)
     tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
@@ -504,6 +505,7 @@ class QSRun:
         ns = [sum(t[1]) for t in tasks]
         res.blocks_per_step.append(nb)
         res.max_dim_per_step.append(max(ns))
+        res.block_dims.append(ns)
         moff = np.zeros(nb + 1, dtype=np.int64)
         moff[1:] = np.cumsum(np.array(ns, dtype=np.int64) ** 2)
         voff = np.zeros(nb + 1, dtype=np.int64)

@@ -186,3 +186,25 @@ def test_large_orders(nb, n, kind):
     G = V @ V.T
     assert (torch.diagonal(G) - 1).abs().max().item() < 1e-12
     assert (G - torch.diag(torch.diagonal(G))).abs().max().item() < 1e-10
+
+
+def test_few_large_blocks_batch(nb):
+    """A batch like a step of the two-channel Kondo runs: a few large blocks, each reduced by
+    its own cluster of CTAs at the same time, beside mid-size and small ones."""
+    import torch
+    rng = np.random.default_rng(77)
+    sizes = [3000, 2500, 1800, 1200, 900, 700, 650, 601, 400, 230, 64, 10]
+    blocks = [graded_block(rng, n) if i % 2 else rand_upper(rng, n) for i, n in enumerate(sizes)]
+    got = nb.diagonalisations(blocks)
+    for h, g in zip(blocks, got):
+        n = h.shape[0]
+        H = full_from_upper(h)
+        w_ref = np.linalg.eigvalsh(H)
+        nrm = max(abs(w_ref[0]), abs(w_ref[-1]))
+        assert np.max(np.abs(g.val - w_ref)) <= 1e-12 * nrm * max(1.0, math.sqrt(n / 1000.0)), n
+        Hd = torch.tensor(H, device="cuda")
+        V = torch.tensor(g.vec, device="cuda")
+        w = torch.tensor(g.val, device="cuda")
+        assert torch.linalg.norm(V @ Hd - w[:, None] * V, dim=1).max().item() <= 1e-12 * nrm * math.sqrt(n), n
+        G = V @ V.T
+        assert (G - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item() < 1e-10, n
