@@ -216,7 +216,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
     ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
-    ap.add_argument("--no-c3", action="store_true", help="skip the two-channel Kondo FDM run")
+    ap.add_argument("--c3", action="store_true",
+                    help="also run the two-channel Kondo FDM workload (keep=5000, Nmax=50; minutes)")
     ap.add_argument("--write-c0", default=None, metavar="DIR",
                     help="write the param and data files of the NRG-run workload to DIR and exit")
     args = ap.parse_args()
@@ -355,7 +356,7 @@ def main():
         line["nrg_run"] = nrg_run_arm(torch, local, args)
     if not args.no_nrg and rank == 0:
         line["serving"] = serving_arm(torch, local, line["nrg_run"])
-    if not args.no_c3 and rank == 0:
+    if args.c3 and rank == 0:
         torch.cuda.empty_cache()
         try:
             line["c3_run"] = c3_arm(torch, local, args)

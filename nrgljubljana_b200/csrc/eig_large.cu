@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
 // barrier each CTA reduces its slice of rows, after the second the scalar y^T v is summed;
 // the third makes the column of W visible to the cluster, a fourth follows each panel update.
 // Every CTA executes the same sequence of barriers whatever the data.
-constexpr int kTclC = 8;  // CTAs per cluster
+constexpr int kTclC = 8;  // CTAs per cluster (16 when the blocks are few)
 
 __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const LargeBlock* __restrict__ blocks,
                                                                      const CUtensorMap* __restrict__ tmaps) {
@@ -1785,22 +1785,31 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
         if ((long long)nbig * kTclC <= 2LL * nsm && smem_tcl + 256 <= (size_t)optin) {
           NRG_CK(cudaFuncSetAttribute(tridiag_tcl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tcl));
-          cfg.gridDim = dim3((unsigned)(nbig * kTclC));
+          NRG_CK(cudaFuncSetAttribute(tridiag_tcl_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
           cfg.blockDim = dim3(kTriThreads);
           cfg.dynamicSmemBytes = smem_tcl;
           cfg.stream = s;
           at[0].id = cudaLaunchAttributeClusterDimension;
-          at[0].val.clusterDim.x = (unsigned)kTclC;
           at[0].val.clusterDim.y = 1;
           at[0].val.clusterDim.z = 1;
           cfg.attrs = at;
           cfg.numAttrs = 1;
-          int ncl = 0;
-          if (cudaOccupancyMaxActiveClusters(&ncl, tridiag_tcl_kernel, &cfg) != cudaSuccess) {
-            cudaGetLastError();
-            ncl = 0;
+          // 16 CTAs per block when the blocks are few enough for all their clusters to be active
+          // at once, else 8
+          for (int C : {2 * kTclC, kTclC}) {
+            if (C > kTclC && (long long)nbig * C > nsm) continue;
+            cfg.gridDim = dim3((unsigned)(nbig * C));
+            at[0].val.clusterDim.x = (unsigned)C;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, tridiag_tcl_kernel, &cfg) != cudaSuccess) {
+              cudaGetLastError();
+              ncl = 0;
+            }
+            if (C > kTclC ? ncl >= nbig : ncl > 0) {
+              tcl = true;
+              break;
+            }
           }
-          tcl = ncl > 0;
         }
         if (tcl) {
           NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_tcl_kernel, (const LargeBlock*)dblk, tm));
