@@ -216,6 +216,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
     ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
+    ap.add_argument("--c2", action="store_true",
+                    help="also run the keep-4000 Anderson DM-NRG workload (Nmax=60)")
+    ap.add_argument("--c4", action="store_true", help="also serve the generated z-averaged request stream")
+    ap.add_argument("--c4-requests", type=int, default=6, help="requests of the --c4 stream")
     ap.add_argument("--c3", action="store_true",
                     help="also run the two-channel Kondo FDM workload (keep=5000, Nmax=50; minutes)")
     ap.add_argument("--write-c0", default=None, metavar="DIR",
@@ -356,6 +360,18 @@ def main():
         line["nrg_run"] = nrg_run_arm(torch, local, args)
     if not args.no_nrg and rank == 0:
         line["serving"] = serving_arm(torch, local, line["nrg_run"])
+    if args.c2 and rank == 0:
+        torch.cuda.empty_cache()
+        try:
+            line["c2_run"] = c2_arm(torch, local, args)
+        except (RuntimeError, MemoryError) as err:
+            line["c2_run"] = {"workload": C2_WORKLOAD, "error": str(err)[:300]}
+    if args.c4 and rank == 0:
+        torch.cuda.empty_cache()
+        try:
+            line["c4_serving"] = c4_arm(torch, local, args)
+        except (RuntimeError, MemoryError) as err:
+            line["c4_serving"] = {"workload": C4_WORKLOAD, "error": str(err)[:300]}
     if args.c3 and rank == 0:
         torch.cuda.empty_cache()
         try:
@@ -426,6 +442,171 @@ spect=S_imp-S_imp
 C3_WORKLOAD = ("NRG run, QS two-channel Kondo model, impurity spin 1/2, J=0.2 on both flat channels, "
                "Lambda=3 (Z), z=1, Nmax=50, keep=5000, T=1e-6, FDM dynamic spin susceptibility S_imp-S_imp "
                "(1000 bins/decade, broadened) and FDM thermodynamics; input generated by nrgljubljana_b200.datagen")
+
+
+C2_PARAM = """[param]
+symtype=QS
+model=SIAM
+U=1.0
+Gamma=0.04
+delta=0
+band=flat
+discretization=Z
+Lambda=2
+z=1
+keep=4000
+T=1e-8
+ops=n_d A_d
+dmnrg=true
+specd=A_d-A_d
+bins=10
+emin=1e-10
+emax=1
+"""
+C2_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delta=0), Gamma=0.04, flat band, "
+               "Lambda=2 (Z), z=1, Nmax=60, keep=4000, T=1e-8, operators n_d and A_d, DM-NRG spectral function "
+               "A_d-A_d in 10 bins per decade over [1e-10, 1] (101 bins per sign), broadened; input generated by "
+               "nrgljubljana_b200.datagen")
+
+
+def c2_inputs():
+    from nrgljubljana_b200.datagen import siam_qs
+    return C2_PARAM, siam_qs(1.0, 0.0, 0.04, 2.0, 60, 1.0, "Z", ops=["n_d", "A_d"])
+
+
+def c2_arm(torch, device: int, args) -> dict:
+    """One whole run of the keep-4000 Anderson DM-NRG workload (wall clock, device synchronised),
+    beside the same driver with one cuSOLVER eigh per block and launch; the CPU dsyev path
+    estimated as for the two-channel run."""
+    from nrgljubljana_b200 import context
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import QSRun, RunParams
+    param, data = c2_inputs()
+    p, d = RunParams.from_param(parse_param(param)), read_data(data)
+    ctx = context(device)
+
+    class PerBlock(QSRun):
+        def _diagonalise(self, job):
+            for b, n in enumerate(job.ns):
+                h = job.Hbuf[job.moff[b]:job.moff[b + 1]].view(n, n)
+                w, q = torch.linalg.eigh(h, UPLO="U")
+                job.Ebuf[job.voff[b]:job.voff[b + 1]].copy_(w)
+                job.Vbuf[job.moff[b]:job.moff[b + 1]].view(n, n).copy_(q.T)
+            return np.zeros(len(job.ns), dtype=np.int32)
+
+    def timed(cls):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = cls(p, d, device, ctx).run()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, res
+    torch.cuda.reset_peak_memory_stats(device)
+    t, res = timed(QSRun)
+    peak = torch.cuda.max_memory_allocated(device) / 2 ** 30
+    t_pb, res_pb = timed(PerBlock)
+    flop = sum(f_eig(np.array(ns)) for ns in res.block_dims)
+    td, tdp = np.array(res.td), np.array(res_pb.td)
+    big = np.abs(td) >= 1e-6
+    a = res.spectra["spec_DMNRG_dens_A_d-A_d"][:, 1]
+    b = res_pb.spectra["spec_DMNRG_dens_A_d-A_d"][:, 1]
+    out = {"workload": C2_WORKLOAD, "steps_per_run": d.nmax, "steps_per_s": d.nmax / t, "s_per_run": t,
+           "timing": "wall clock of one run (host driver included)", "eig_flop_per_run": flop,
+           "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
+           "peak_device_gib": peak,
+           "per_block_gpu": {"steps_per_s": d.nmax / t_pb, "s_per_run": t_pb,
+                             "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch",
+                             "td_max_rel_diff": float(np.max(np.abs(tdp[big] - td[big]) / np.abs(td[big]))),
+                             "spectrum_max_diff_rel_to_peak": float(np.max(np.abs(a - b)) / np.max(np.abs(a)))}}
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        heavy = max(range(len(res.block_dims)), key=lambda k: sum(float(n) ** 3 for n in res.block_dims[k]))
+        est = cpu_dsyev_estimate(res.block_dims[heavy], threads)
+        c1 = est["measured"]["dsyev_1_thread_s"]["1200"] / 1200.0 ** 3
+        tot_i = 0.0
+        for ns in res.block_dims:
+            load = np.zeros(threads)
+            for n in sorted(ns, reverse=True):
+                load[np.argmin(load)] += c1 * float(n) ** 3
+            tot_i += float(load.max())
+        scale = sum(sum(float(n) ** 3 for n in ns) for ns in res.block_dims) / \
+            sum(float(n) ** 3 for n in res.block_dims[heavy])
+        per_run = {"openmp_over_blocks_s": tot_i, "threaded_blas_s": est["threaded_blas_s"] * scale}
+        out["cpu_baseline"] = {"steps_per_s_estimated": d.nmax / min(per_run.values()),
+                               "diag_s_per_run_estimated": per_run, "cores": threads, "kind": "port",
+                               "sample": "dsyev of n = 600, 1200 (1 thread) and 2000 (all threads), scaled by n^3 "
+                                         "to every block of the run; diagonalisations only",
+                               "measured": est["measured"]}
+    return out
+
+
+C4_WORKLOAD = ("serving: a Poisson stream (mean 4 requests/s, seed 20261203) of z-averaged QS Anderson-model "
+               "requests, each eps_d ~ U[-0.7, -0.3] (delta = eps_d + 0.5), U = 1, Gamma ~ U[0.02, 0.08], "
+               "keep ~ U{1000..3000}, Nmax = 50, Lambda = 2, and 8-32 twist values z ~ U(0, 1], one run per z; "
+               "inputs generated by nrgljubljana_b200.datagen; runs admitted by slots (16) and HBM budget")
+
+
+def _c4_data(args):
+    from nrgljubljana_b200.datagen import siam_qs
+    delta, gam, z = args
+    return siam_qs(1.0, delta, gam, 2.0, 50, z, "Z", ops=["n_d"])
+
+
+def c4_requests(nreq: int, seed: int = SEED):
+    """The seeded requests of the serving workload: one Request per (request, z), tag = request.
+    The inputs are generated on all host cores (a spawned process pool: the parent already
+    holds a CUDA context)."""
+    import multiprocessing
+    from concurrent.futures import ProcessPoolExecutor
+    from nrgljubljana_b200.serve import Request, poisson_arrivals
+    rng = np.random.default_rng(seed)
+    arr = poisson_arrivals(nreq, 4.0, seed)
+    specs = []
+    for k in range(nreq):
+        eps = rng.uniform(-0.7, -0.3)
+        gam = rng.uniform(0.02, 0.08)
+        keep = int(rng.integers(1000, 3001))
+        nz = int(rng.integers(8, 33))
+        zs = 1.0 - rng.random(nz)  # (0, 1]
+        for z in zs:
+            specs.append((k, eps + 0.5, gam, keep, float(z)))
+    with ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=multiprocessing.get_context("spawn")) as ex:
+        datas = list(ex.map(_c4_data, [(dl, g, z) for _, dl, g, _, z in specs], chunksize=1))
+    out = []
+    for rid, ((k, delta, gam, keep, z), data) in enumerate(zip(specs, datas)):
+        param = (f"[param]\nsymtype=QS\nmodel=SIAM\nU=1.0\nGamma={gam!r}\ndelta={delta!r}\n"
+                 f"band=flat\ndiscretization=Z\nLambda=2\nz={z!r}\nkeep={keep}\nT=1e-8\nops=n_d\n")
+        out.append(Request(rid, param, data, float(arr[k]), f"request{k}"))
+    return out
+
+
+def c4_arm(torch, device: int, args) -> dict:
+    """The serving workload with generated requests, served in real time; the first run is
+    also run alone and its thermodynamics compared bit for bit with the one from the mix."""
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import QSRun, RunParams
+    from nrgljubljana_b200.serve import Server, group_summary, summary
+    t0 = time.perf_counter()
+    reqs = c4_requests(args.c4_requests)
+    t_gen = time.perf_counter() - t0
+    srv = Server(device, max_active=16)
+    t0 = time.perf_counter()
+    done = srv.serve(reqs, realtime=True)
+    wall = time.perf_counter() - t0
+    out = {"workload": C4_WORKLOAD, "requests": args.c4_requests, "runs": len(reqs),
+           "input_generation_s": t_gen, "runs_summary": summary(done, wall), "requests_summary": group_summary(done),
+           "max_blocks_per_tick": max(srv.blocks_per_tick)}
+    first = min(done, key=lambda c: c.rid)
+    r0 = reqs[first.rid]
+    alone = QSRun(RunParams.from_param(parse_param(r0.param)), read_data(r0.data), device).run()
+    a, m = np.array(alone.td), np.array(first.result.td)
+    big = np.abs(a) >= 1e-6  # values that vanish by symmetry are round-off noise in every run
+    # Alone, a run's large blocks go to the cluster reduction; in a full tick to the one-CTA
+    # reduction (the kernel choice depends on the batch): same arithmetic, another summation
+    # order, so the results agree to round-off rather than bit for bit.
+    out["alone_vs_mix"] = {"bitwise_equal": bool(np.array_equal(a, m)),
+                           "td_max_rel_diff": float(np.max(np.abs(a[big] - m[big]) / np.abs(a[big]))),
+                           "tolerance": 1e-9}
+    return out
 
 
 def c3_inputs():

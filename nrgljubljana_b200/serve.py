@@ -137,6 +137,18 @@ def poisson_arrivals(n: int, rate: float, seed: int) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate, size=n))
 
 
+def group_summary(done: List[Completed]) -> dict:
+    """Latency of request groups -- the runs that share a tag, e.g. the twist values z of one
+    z-averaged request -- from the group's arrival to the end of its last run."""
+    groups: dict = {}
+    for c in done:
+        a, d = groups.get(c.tag, (c.arrival, c.done))
+        groups[c.tag] = (min(a, c.arrival), max(d, c.done))
+    lat = np.array([d - a for a, d in groups.values()])
+    return {"groups": len(groups), "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean())}
+
+
 def summary(done: List[Completed], wall: float) -> dict:
     lat = np.array([c.latency for c in done])
     steps = sum(c.steps for c in done)

@@ -61,3 +61,31 @@ def test_staggered_arrivals_and_tight_budget(alone):
         for d in done:
             assert same(d.result, alone[d.tag]), d.tag
             assert d.done >= d.admitted >= d.arrival - 1e-9
+
+
+@pytest.mark.gpu
+def test_mix_with_large_blocks_within_tolerance():
+    """Runs whose blocks reach order ~900: alone, a run's few large blocks are reduced by
+    clusters of CTAs, in a tick of twelve runs by the one-CTA kernel. The arithmetic is the
+    same with another summation order, so the results agree to round-off (1e-10 relative on
+    the thermodynamics and measured expectation values)."""
+    from nrgljubljana_b200.datagen import siam_qs
+    from nrgljubljana_b200.nrg_run import run_files
+    from nrgljubljana_b200.serve import Request, Server
+    reqs = []
+    for i in range(12):
+        z = 0.1 + 0.075 * i
+        param = (f"[param]\nsymtype=QS\nmodel=SIAM\nU=1.0\nGamma=0.05\ndelta=0.05\nband=flat\ndiscretization=Z\n"
+                 f"Lambda=2\nz={z!r}\nkeep=2000\nT=1e-8\nops=n_d\n")
+        reqs.append(Request(i, param, siam_qs(1.0, 0.05, 0.05, 2.0, 8, z, "Z", ops=["n_d"]), 0.0, str(i)))
+    srv = Server(max_active=16)
+    done = srv.serve(reqs, realtime=False)
+    assert max(srv.blocks_per_tick) > 100
+    for d in done:
+        a = run_files(reqs[d.rid].param, reqs[d.rid].data)
+        assert max(a.max_dim_per_step) > 600
+        for x, y in ((a.td, d.result.td), (a.custom, d.result.custom)):
+            x, y = np.array(x), np.array(y)
+            big = np.abs(x) >= 1e-6
+            assert np.all(np.abs(x[big] - y[big]) <= 1e-10 * np.abs(x[big])), d.rid
+            assert np.all(np.abs(x[~big] - y[~big]) <= 1e-12), d.rid
