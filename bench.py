@@ -224,13 +224,19 @@ def main():
                     help="also run the two-channel Kondo FDM workload (keep=5000, Nmax=50; minutes)")
     ap.add_argument("--write-c0", default=None, metavar="DIR",
                     help="write the param and data files of the NRG-run workload to DIR and exit")
+    ap.add_argument("--write-c3", default=None, metavar="DIR",
+                    help="write the param and data files of the two-channel Kondo FDM workload to DIR and exit")
+    ap.add_argument("--c3-keep", type=int, default=5000, help="keep of --write-c3 (smaller cases for profiling)")
+    ap.add_argument("--c3-nmax", type=int, default=50, help="Nmax of --write-c3")
     args = ap.parse_args()
-    if args.write_c0:
-        os.makedirs(args.write_c0, exist_ok=True)
-        param, data = c0_inputs()
-        for name, text in (("param", param), ("data", data)):
-            with open(os.path.join(args.write_c0, name), "w") as f:
-                f.write(text)
+    for out_dir, make in ((args.write_c0, c0_inputs), (args.write_c3, lambda: c3_inputs(args.c3_keep, args.c3_nmax))):
+        if out_dir:
+            os.makedirs(out_dir, exist_ok=True)
+            param, data = make()
+            for name, text in (("param", param), ("data", data)):
+                with open(os.path.join(out_dir, name), "w") as f:
+                    f.write(text)
+    if args.write_c0 or args.write_c3:
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -609,9 +615,9 @@ def c4_arm(torch, device: int, args) -> dict:
     return out
 
 
-def c3_inputs():
+def c3_inputs(keep: int = 5000, nmax: int = 50):
     from nrgljubljana_b200.datagen import kondo_qs
-    return C3_PARAM, kondo_qs([0.2, 0.2], 0.5, 3.0, 50, ops=["S_imp"])
+    return C3_PARAM.replace("keep=5000", f"keep={keep}"), kondo_qs([0.2, 0.2], 0.5, 3.0, nmax, ops=["S_imp"])
 
 
 def cpu_dsyev_estimate(dims, threads: int) -> dict:
