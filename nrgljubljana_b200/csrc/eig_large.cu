@@ -173,6 +173,7 @@ constexpr int kTriWarps = kTriThreads / 32;
 // `parity` holds the warp's mbarrier phase bits across calls.
 // gwarp / gnwarps: this warp's index among the warps that share the product (the warps of
 // one CTA, or of every CTA of a cluster), and their number; y receives this warp's part.
+template <int STAGES = kStages>
 NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v, double* y, double* ring,
                         uint64_t* bars, unsigned& parity, int* err, int gwarp, int gnwarps) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -182,8 +183,8 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
   for (int I = T0; I <= Tn; I++) S += rowlen(I);
   const long long f0 = S * gwarp / gnwarps, f1 = S * (gwarp + 1) / gnwarps;
   if (f0 >= f1) return;
-  double* myring = ring + (size_t)warp * kStages * kSlabD;
-  uint64_t* mybar = bars + warp * kStages;
+  double* myring = ring + (size_t)warp * STAGES * kSlabD;
+  uint64_t* mybar = bars + warp * STAGES;
   auto advance = [&](int& I_, int& sl_) {
     if (sl_ < min(8 * I_ + 7, slmax)) {
       sl_++;
@@ -206,7 +207,7 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
   }
   int sl = sl0 + (int)(f0 - acc);
   int pI = I, psl = sl;
-  const int npre = (int)((f1 - f0) < (long long)kStages ? (f1 - f0) : (long long)kStages);
+  const int npre = (int)((f1 - f0) < (long long)STAGES ? (f1 - f0) : (long long)STAGES);
   for (int t = 0; t < npre; t++) {
     issue(pI, psl, t);
     advance(pI, psl);
@@ -214,14 +215,14 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
   double r0 = 0.0, r1 = 0.0;
   int cI = I, csl = sl;
   for (long long f = f0; f < f1; f++) {
-    const int st = (int)((f - f0) % kStages);
+    const int st = (int)((f - f0) % STAGES);
     if (!mbar_wait(mybar + st, (parity >> st) & 1u)) {
       // a copy never completed: flag the block, wait (bounded) for the copies still in
       // flight so that none lands after this call, and stop streaming
       if (lane == 0) atomicExch(err, -5);
-      const long long last = (f + kStages < f1) ? f + kStages : f1;
+      const long long last = (f + STAGES < f1) ? f + STAGES : f1;
       for (long long g = f + 1; g < last; g++) {
-        const int sg = (int)((g - f0) % kStages);
+        const int sg = (int)((g - f0) % STAGES);
         mbar_wait(mybar + sg, (parity >> sg) & 1u, 1 << 22);
         parity ^= 1u << sg;
       }
@@ -258,7 +259,7 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
       }
     }
     __syncwarp();
-    if (f + kStages < f1) {  // refill this stage with the slab kStages ahead
+    if (f + STAGES < f1) {  // refill this stage with the slab STAGES ahead
       issue(pI, psl, st);
       advance(pI, psl);
     }
@@ -555,12 +556,13 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
 // Every CTA executes the same sequence of barriers whatever the data.
 constexpr int kTclC = 8;  // CTAs per cluster (16 when the blocks are few)
 
+template <int STAGES>
 __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const LargeBlock* __restrict__ blocks,
                                                                      const CUtensorMap* __restrict__ tmaps) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) double sm[];
-  __shared__ __align__(8) uint64_t bars[kTriWarps * kStages];
+  __shared__ __align__(8) uint64_t bars[kTriWarps * STAGES];
   const int C = (int)cl.num_blocks(), rk = (int)cl.block_rank();
   const int bi = blockIdx.x / C;
   const LargeBlock B = blocks[bi];
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const Large
   int phase = 0;
   unsigned parity = 0;
   if (lane == 0) {
-    for (int st = 0; st < kStages; st++) mbar_init(bars + warp * kStages + st, 1);
+    for (int st = 0; st < STAGES; st++) mbar_init(bars + warp * STAGES + st, 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const Large
       // column k of A is written back only in (5): other CTAs may still be reading it in (1)
       // (3) this CTA's part of A v and of the dot products W^T v, V^T v over its slice of rows
       const int ch1 = (n - k - 1 + C - 1) / C, lo1 = k + 1 + rk * ch1, hi1 = min(n, lo1 + ch1);
-      if (tau != 0.0) symv_lower(tmaps + bi, n, k + 1, v, y, ring, bars, parity, B.info, gw, gnw);
+      if (tau != 0.0) symv_lower<STAGES>(tmaps + bi, n, k + 1, v, y, ring, bars, parity, B.info, gw, gnw);
       {
         double pw[NB], pv[NB];
 #pragma unroll
@@ -1774,18 +1776,26 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         bool tcl = false;
         // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
         // CTAs on one SM the reductions came out wrong on B200 (cause not found); with one per
-        // SM every check passes. A cluster holds 8 SMs per block either way.
-        int smsm = 0;
+        // SM every check passes. A cluster holds 8 SMs per block either way. The ring gets 8,
+        // 6 or 4 slabs per warp, the most that fit: one CTA per SM leaves the room.
+        int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
-        const size_t smem_tcl =
-            std::max(smem + sizeof(double) * (2 * NB + 2), (size_t)smsm / 2 + 1024);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        auto tcl_bytes = [&](int st) {
+          return std::max(1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)maxn +
+                                                   (size_t)kTriWarps * 2 * NB + 4 * NB + 66),
+                          (size_t)smsm / 2 + 1024);
+        };
+        int stages = 8;
+        while (stages > 4 && tcl_bytes(stages) + 256 > (size_t)optin) stages -= 2;
+        const size_t smem_tcl = tcl_bytes(stages);
+        const void* tcl_fn = stages == 8 ? (const void*)tridiag_tcl_kernel<8>
+                             : stages == 6 ? (const void*)tridiag_tcl_kernel<6> : (const void*)tridiag_tcl_kernel<4>;
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
-        int optin = 0;
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
         if ((long long)nbig * kTclC <= 2LL * nsm && smem_tcl + 256 <= (size_t)optin) {
-          NRG_CK(cudaFuncSetAttribute(tridiag_tcl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tcl));
-          NRG_CK(cudaFuncSetAttribute(tridiag_tcl_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+          NRG_CK(cudaFuncSetAttribute(tcl_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tcl));
+          NRG_CK(cudaFuncSetAttribute(tcl_fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
           cfg.blockDim = dim3(kTriThreads);
           cfg.dynamicSmemBytes = smem_tcl;
           cfg.stream = s;
@@ -1801,7 +1811,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
             cfg.gridDim = dim3((unsigned)(nbig * C));
             at[0].val.clusterDim.x = (unsigned)C;
             int ncl = 0;
-            if (cudaOccupancyMaxActiveClusters(&ncl, tridiag_tcl_kernel, &cfg) != cudaSuccess) {
+            if (cudaOccupancyMaxActiveClusters(&ncl, tcl_fn, &cfg) != cudaSuccess) {
               cudaGetLastError();
               ncl = 0;
             }
@@ -1812,7 +1822,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           }
         }
         if (tcl) {
-          NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_tcl_kernel, (const LargeBlock*)dblk, tm));
+          const LargeBlock* db = dblk;
+          void* kargs[] = {(void*)&db, (void*)&tm};
+          NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
           NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
           tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, tm);

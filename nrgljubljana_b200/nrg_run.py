@@ -44,6 +44,8 @@ _IGNORED = {
     "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
     "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom",
     "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
+    # model parameters of the generated data and of its discretisation
+    "U1", "U2", "Gamma1", "Gamma2", "eps1", "eps2", "U12", "J12", "tri", "mMAX",
 }
 
 
@@ -948,7 +950,7 @@ class QSRun:
         rows = (lambda s: s.n) if p.fdm_flags else (lambda s: s.nkept)  # noqa: E731
         kinds = {"s": (1, qs.correlator_factor, self.sop_names), "d": (-1, qs.specdens_factor, self.dop_names),
                  "t": (1, qs.dynamicsusceptibility_factor, self.top_names)}
-        tables = {"d": (self.T.DOUBLET, lambda fn, ss: fn(ss)), "t": (self.T.TRIPLET, qs.triplet_factor)}
+        tables = {"d": (self.T.DOUBLET, self.T.doublet_factor), "t": (self.T.TRIPLET, qs.triplet_factor)}
         parts_of = {"FDM": ("gt", "ls"), "FDMgt": ("gt",), "FDMls": ("ls",)}
         fdm_parts = sorted({w for a in self.algos if a in parts_of for w in parts_of[a]})
         zeros = lambda: torch.zeros(nb, dtype=torch.float64, device=self.dev)  # noqa: E731

@@ -7,7 +7,7 @@ The tables below are the reference's coefficient tables for this symmetry, resta
   <||f||> recalculation  c++/symmetry/coefnew/qs/qs-1ch-spin{up,down}a.dat,
                          qs-2ch-spin{up,down}{a,b}.dat (channel 0: a, channel 1: b)
                          (driven by SymmetryQS::recalc_irreduc, c++/symmetry/nrg-recalc-QS.hpp:192-460)
-  doublet recalculation  c++/symmetry/coefnew/qs/qs-1ch-doublet{p,m}.dat
+  doublet recalculation  c++/symmetry/coefnew/qs/qs-{1,2}ch-doublet{p,m}.dat
                          (SymmetryQS::recalc_doublet, c++/symmetry/nrg-recalc-QS.hpp:32-117)
   triplet recalculation  c++/symmetry/coefnew/qs/qs-{1,2}ch-triplet{s,p,m}.dat
                          (SymmetryQS::recalc_triplet, c++/symmetry/nrg-recalc-QS.hpp:495-640)
@@ -107,17 +107,25 @@ class Tables:
                 zeta(N+1, ch) * (number - AVGOCCUP) / scale
     DIAG_FIRST  whether make_matrix lists the diagonal table before the off-diagonal one
     RECALC_F    (dq, channel, rows (i1, ip, factor(ssp))): <I1||f_ch||Ip> for I1 = Ip + dq
-    DOUBLET     (dq, rows (i1, ip, factor(ss1))): a doublet operator for Ip = I1 + dq
+    DOUBLET     (dq, rows (i1, ip, factor)): a doublet operator for Ip = I1 + dq; the factor is
+                evaluated by doublet_factor(fn, ss1)
     TRIPLET     (dq, rows (i1, ip, factor(S1))): a triplet operator for Ip = I1 + dq, the factor
                 a function of the spin S1 of I1 (a numpy float64), see triplet_factor
     """
 
-    def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET, TRIPLET):
+    def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET, TRIPLET,
+                 doublet_of_spin=False):
         self.channels = channels
         self.COMBS = len(IN)
         self.IN, self.QN = IN, QN
         self.OFFDIAG, self.DIAG, self.DIAG_FIRST = OFFDIAG, DIAG, DIAG_FIRST
         self.RECALC_F, self.DOUBLET, self.TRIPLET = RECALC_F, DOUBLET, TRIPLET
+        self._doublet_of_spin = doublet_of_spin
+
+    def doublet_factor(self, fn, ss1: int) -> float:
+        """A doublet-table factor at SS = ss1 (rows of the two-channel tables are functions of
+        the spin, evaluated as the triplet rows are)."""
+        return triplet_factor(fn, ss1) if self._doublet_of_spin else fn(ss1)
 
     def ancestors(self, I: Invar) -> List[Invar]:
         return [(I[0] + d[0], I[1] + d[1]) for d in self.IN]
@@ -285,6 +293,49 @@ _T2M = ([(1, 1, _u)]
         + [(16, 16, _u)])
 
 
+# two-channel doublet rows (qs-2ch-doublet{p,m}.dat), functions of the spin of I1; combinations
+# 2/4, 3/5, 12/14 and 13/15 carry the same factors
+def _d_a(s):
+    return (-2 * np.sqrt(s * (1 + s))) / (1 + 2 * s)
+
+
+def _d_b(s):
+    return 1 / (1 + 2 * s)
+
+
+def _d_m1(s):
+    return -1.0
+
+
+_D2P = ([(1, 1, _u)]
+        + [r for a, b in ((2, 3), (4, 5)) for r in ((a, a, _d_a), (b, a, _d_b), (b, b, _d_m1))]
+        + [(6, 6, _u), (7, 7, _u), (8, 8, _u),
+           (9, 9, lambda s: 1 / np.sqrt((s * (1 + 2 * s)) / (-1 + s + 2 * s ** 2))),
+           (10, 9, lambda s: -(1 / np.sqrt(s * (1 + 2 * s)))),
+           (10, 10, lambda s: (s * (3 + 2 * s)) / np.sqrt(s * (1 + s) * (3 + 4 * s * (2 + s)))),
+           (11, 10, lambda s: -(1 / np.sqrt((1 + s) * (1 + 2 * s)))),
+           (11, 11, _u)]
+        + [r for a, b in ((12, 13), (14, 15)) for r in ((a, a, _d_a), (b, a, _d_b), (b, b, _d_m1))]
+        + [(16, 16, _u)])
+
+
+def _dm_c(s):
+    return 1 / (-1 - 2 * s)
+
+
+_D2M = ([(1, 1, _u)]
+        + [r for a, b in ((2, 3), (4, 5)) for r in ((a, a, _d_m1), (a, b, _dm_c), (b, b, _d_a))]
+        + [(6, 6, _u), (7, 7, _u), (8, 8, _u),
+           (9, 9, _u),
+           (9, 10, lambda s: 1 / np.sqrt(s * (1 + 2 * s))),
+           (10, 10, lambda s: (-1 + s + 2 * s ** 2) / np.sqrt(s * (1 + s) * (-1 + 4 * s ** 2))),
+           (10, 11, lambda s: 1 / np.sqrt((1 + s) * (1 + 2 * s))),
+           (11, 11, lambda s: np.sqrt((s * (1 + 2 * s)) / ((1 + s) ** 3 * (3 + 2 * s)))
+            + np.sqrt(s / ((1 + s) ** 3 * (3 + 4 * s * (2 + s)))) + np.sqrt(1 + 1 / (1 + s) - 6 / (3 + 2 * s)))]
+        + [r for a, b in ((12, 13), (14, 15)) for r in ((a, a, _d_m1), (a, b, _dm_c), (b, b, _d_a))]
+        + [(16, 16, _u)])
+
+
 QS2 = Tables(
     2,
     IN=[(2, 0), (1, -1), (1, 1), (1, -1), (1, 1), (0, 0), (0, 0), (0, 0), (0, -2), (0, 0), (0, 2),
@@ -382,12 +433,13 @@ QS2 = Tables(
                       (15, 8, _one),
                       (16, 14, lambda s: math.sqrt(1 + 1 / (2. * S(s))))]),
     ],
-    DOUBLET=[],
+    DOUBLET=[((-1, 1), _D2P), ((-1, -1), _D2M)],
     TRIPLET=[
         ((0, 0), _T2S),
         ((0, 2), _T2P),
         ((0, -2), _T2M),
     ],
+    doublet_of_spin=True,
 )
 
 

@@ -332,8 +332,11 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
                         cn[(I1, Ip)] = m
                 return cn
             # recalc_doublet (nrg-recalc-QS.hpp:32-117), recalc_triplet (495-640)
-            dops = {name: recalc_tensor(cold, (((-1, 1), _DOUBLETP), ((-1, -1), _DOUBLETM)), lambda fn, ss: fn(ss))
-                    for name, cold in dops.items()}
+            if d.channels == 1:
+                dtab, dfac = (((-1, 1), _DOUBLETP), ((-1, -1), _DOUBLETM)), (lambda fn, ss: fn(ss))
+            else:
+                dtab, dfac = T.DOUBLET, T.doublet_factor
+            dops = {name: recalc_tensor(cold, dtab, dfac) for name, cold in dops.items()}
             tops = {name: recalc_tensor(cold, T.TRIPLET, _qs.triplet_factor) for name, cold in tops.items()}
             snames = {x for sp in specs if sp[1] == "s" for x in sp[2:]}
             if fdm_flags:

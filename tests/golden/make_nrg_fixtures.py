@@ -23,6 +23,8 @@ CASES = [
     "c++sym_all/test300_QS_ref", "c++sym_all/test310_QS_ref",
     "test2_algorithms_fdm", "test2_algorithms_fdmexpv", "test2_algorithms_fdmgtls", "test60_discard_immediately",
     "test61_discard_trim", "test64_emax", "test66_fdmexpvn", "legacy_fdmexpv2", "legacy_fdmexpv3",
+    "regr2defaults", "regr2lastall_false", "regr2lastall_true", "legacy_one_jkondonew",
+    "c++sym_all/test314_model=ZERO",
 ]
 # spectra of the DM-NRG and FDM algorithms, FDM thermodynamics and expectation values
 SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls)_dens_.*\.dat$")

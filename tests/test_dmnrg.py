@@ -76,3 +76,32 @@ def test_gpu_dmnrg_spectra(oracle_spectra, case):
         got = res.spectra[name]
         assert_spectrum(got, ref_spectrum(case, name), RTOL, ATOL_REL_TO_MAX, f"{case} {name} vs reference")
         assert_spectrum(got, oracle_spectra(case)[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} {name} vs oracle")
+
+
+# two channels (model.m of the reference's regression tests): doublet recalculation with the
+# two-channel tables, N/N+1-type window factor sqrt(Lambda) of two channels
+DM2_CASES = ["regr2defaults", "regr2lastall_false", "regr2lastall_true"]
+
+
+def spectrum_names(case):
+    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case)) if f.endswith(".dat"))
+
+
+@pytest.mark.parametrize("case", DM2_CASES)
+def test_oracle_two_channel_dmnrg_spectra(oracle_spectra, case):
+    got = oracle_spectra(case)
+    assert sorted(got) == spectrum_names(case)
+    for name in spectrum_names(case):
+        assert_spectrum(got[name], ref_spectrum(case, name), RTOL, ATOL_REL_TO_MAX, f"{case} {name}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", DM2_CASES)
+def test_gpu_two_channel_dmnrg_spectra(oracle_spectra, case):
+    from nrgljubljana_b200.nrg_run import run_files
+    res = run_files(read(case, "param"), read(case, "data"))
+    assert sorted(res.spectra) == spectrum_names(case)
+    for name in spectrum_names(case):
+        assert_spectrum(res.spectra[name], ref_spectrum(case, name), RTOL, ATOL_REL_TO_MAX, f"{case} {name} vs reference")
+        assert_spectrum(res.spectra[name], oracle_spectra(case)[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX,
+                        f"{case} {name} vs oracle")

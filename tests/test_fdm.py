@@ -2,7 +2,8 @@
 the spectra {spec,corr,spin}_{FDM,FDMgt,FDMls}_dens_*.dat, the FDM thermodynamics (tdfdm)
 and the FDM expectation values (customfdm) of test/c++/test2_algorithms_fdm,
 test2_algorithms_fdmexpv, test2_algorithms_fdmgtls, test60_discard_immediately,
-test61_discard_trim, test64_emax, test66_fdmexpvn, legacy_fdmexpv2 and legacy_fdmexpv3:
+test61_discard_trim, test64_emax, test66_fdmexpvn, legacy_fdmexpv2, legacy_fdmexpv3 and the
+two-channel c++sym_all/test314_model=ZERO:
 partial statistical sums Z_n^D and weights w_n, the FDM density-matrix sweep with its
 discarded-state sectors, the spectra operators recalculated over all states, FDM pair sums
 (gt and ls parts) binned per step, trimming and broadening."""
@@ -17,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
 FDM_CASES = ["test2_algorithms_fdm", "test2_algorithms_fdmexpv", "test2_algorithms_fdmgtls",
              "test60_discard_immediately", "test61_discard_trim", "test64_emax", "test66_fdmexpvn",
-             "legacy_fdmexpv2", "legacy_fdmexpv3"]
+             "legacy_fdmexpv2", "legacy_fdmexpv3", "test314_model=ZERO"]
 # tdfdm/customfdm: printed to 10 significant digits (20 for the legacy customfdm)
 TAB_RTOL = 2e-9
 
