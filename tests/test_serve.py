@@ -67,8 +67,12 @@ def test_staggered_arrivals_and_tight_budget(alone):
 def test_mix_with_large_blocks_within_tolerance():
     """Runs whose blocks reach order ~900: alone, a run's few large blocks are reduced by
     clusters of CTAs, in a tick of twelve runs by the one-CTA kernel. The arithmetic is the
-    same with another summation order, so the results agree to round-off (1e-10 relative on
-    the thermodynamics and measured expectation values)."""
+    same with another summation order, so the results agree to round-off (1e-10 relative) as
+    long as the truncation keeps the same states. A hard cut at `keep` states can fall inside
+    a near-degeneracy, where round-off decides which of two multiplets is kept (as it does
+    between LAPACK builds for the reference); from the first step whose kept sets differ the
+    runs are different calculations, so the comparison stops there and must cover steps with
+    blocks above order 600."""
     from nrgljubljana_b200.datagen import siam_qs
     from nrgljubljana_b200.nrg_run import run_files
     from nrgljubljana_b200.serve import Request, Server
@@ -82,9 +86,13 @@ def test_mix_with_large_blocks_within_tolerance():
     done = srv.serve(reqs, realtime=False)
     assert max(srv.blocks_per_tick) > 100
     for d in done:
-        a = run_files(reqs[d.rid].param, reqs[d.rid].data)
-        assert max(a.max_dim_per_step) > 600
-        for x, y in ((a.td, d.result.td), (a.custom, d.result.custom)):
+        a, m = run_files(reqs[d.rid].param, reqs[d.rid].data), d.result
+        # first step whose blocks differ: the kept sets of the step before it differ
+        k = next((j for j, (x, y) in enumerate(zip(a.block_dims, m.block_dims)) if x != y), len(a.block_dims))
+        assert k >= 4 and max(max(ns) for ns in a.block_dims[:k]) > 600, (d.rid, k)
+        # td rows 0..k (calc0 and steps 0..k-1, measured before truncation); custom rows
+        # 0..k-1 (measured over the kept states)
+        for x, y in ((a.td[:k + 1], m.td[:k + 1]), (a.custom[:k], m.custom[:k])):
             x, y = np.array(x), np.array(y)
             big = np.abs(x) >= 1e-6
             assert np.all(np.abs(x[big] - y[big]) <= 1e-10 * np.abs(x[big])), d.rid
