@@ -68,11 +68,12 @@ def test_mix_with_large_blocks_within_tolerance():
     """Runs whose blocks reach order ~900: alone, a run's few large blocks are reduced by
     clusters of CTAs, in a tick of twelve runs by the one-CTA kernel. The arithmetic is the
     same with another summation order, so the results agree to round-off (1e-10 relative) as
-    long as the truncation keeps the same states. A hard cut at `keep` states can fall inside
-    a near-degeneracy, where round-off decides which of two multiplets is kept (as it does
-    between LAPACK builds for the reference); from the first step whose kept sets differ the
-    runs are different calculations, so the comparison stops there and must cover steps with
-    blocks above order 600."""
+    long as the truncation keeps the same states. The runs truncate at an energy
+    (keepenergy), not at a number of states: a hard cut at `keep` states can fall inside a
+    near-degeneracy, where round-off decides which multiplet is kept (as it does between
+    LAPACK builds for the reference). Should the kept sets still differ at some step, the
+    runs are different calculations from there on and the comparison stops; it must cover
+    steps with blocks above order 600."""
     from nrgljubljana_b200.datagen import siam_qs
     from nrgljubljana_b200.nrg_run import run_files
     from nrgljubljana_b200.serve import Request, Server
@@ -80,7 +81,7 @@ def test_mix_with_large_blocks_within_tolerance():
     for i in range(12):
         z = 0.1 + 0.075 * i
         param = (f"[param]\nsymtype=QS\nmodel=SIAM\nU=1.0\nGamma=0.05\ndelta=0.05\nband=flat\ndiscretization=Z\n"
-                 f"Lambda=2\nz={z!r}\nkeep=2000\nT=1e-8\nops=n_d\n")
+                 f"Lambda=2\nz={z!r}\nkeep=100000\nkeepenergy=13\nT=1e-8\nops=n_d\n")
         reqs.append(Request(i, param, siam_qs(1.0, 0.05, 0.05, 2.0, 8, z, "Z", ops=["n_d"]), 0.0, str(i)))
     srv = Server(max_active=16)
     done = srv.serve(reqs, realtime=False)
