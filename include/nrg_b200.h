@@ -117,8 +117,8 @@ NRG_API int nrg_hamiltonian_batch(nrg_ctx* ctx, int nblk, const int* n, double* 
  * ka == kb; ldo == 0 means a diagonal O given as its ka diagonal entries, ka == kb, as
  * the discarded-state sector of the FDM density matrix of init_rho_FDM,
  * c++/dmnrg.hpp:146-162, enters calc_fulldensitymatrix_iterN), op(B) is kb x cols. The
- * product O op(B) is formed first, as in the reference (a diagonal O scales the rows of
- * op(B) as they are loaded). Terms with the same M are summed in the order given; distinct M regions must
+ * product O op(B) is formed first, as in the reference (for a diagonal O by scaling the
+ * rows of op(B)). Terms with the same M are summed in the order given; distinct M regions must
  * not overlap. A term with rows, cols, ka or kb zero is skipped (finite_size checks of the
  * reference). Pointers are device pointers. */
 typedef struct nrg_gemm3 {

@@ -501,13 +501,13 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     }
     v.push_back(t);
   }
-  // Phase 1: T_t = O_t op(B_t) (ka x cols) for terms with an explicit dense O. A diagonal
-  // O (ldo == 0) scales the rows of op(B) inside the phase-2 GEMM instead.
+  // Phase 1: T_t = O_t op(B_t) (ka x cols) for every term with an O: a GEMM for a dense O, a
+  // row scaling for a diagonal one (ldo == 0).
   auto dense_O = [&](int t) { return terms[t].O && terms[t].ldo != 0; };
   std::vector<size_t> toff(nterm, 0);
   size_t need = 0;
   for (int t : live)
-    if (dense_O(t)) {
+    if (terms[t].O) {
       toff[t] = need;
       need += (size_t)terms[t].ka * terms[t].cols;
     }
@@ -521,6 +521,23 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     p1.add_out(T + toff[t], g.cols, g.ka, g.cols, 0.0);
     p1.add_seg(g.O, g.ldo, 0, g.B, g.ldb, g.transB, g.kb, 1.0);
   }
+  std::vector<nrg::RowScale> rsc;
+  int64_t rtotal = 0;
+  for (int t : live) {
+    const nrg_gemm3& g = terms[t];
+    if (!g.O || dense_O(t)) continue;
+    nrg::RowScale r{};
+    r.T = T + toff[t];
+    r.d = g.O;
+    r.B = g.B;
+    r.ldb = g.ldb;
+    r.off = rtotal;
+    r.rows = g.ka;
+    r.cols = g.cols;
+    r.transB = g.transB;
+    rsc.push_back(r);
+    rtotal += (int64_t)g.ka * g.cols;
+  }
   // Phase 2: M += sum_t factor_t op(A_t) T_t.
   for (double* M : order) {
     const auto& v = groups[M];
@@ -528,13 +545,18 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     p2.add_out(M, f.ldm, f.rows, f.cols, 1.0);
     for (int t : v) {
       const nrg_gemm3& g = terms[t];
-      if (dense_O(t)) {
-        p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
-      } else {
-        p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
-        p2.segs.back().dscale = g.O;  // null: identity; ldo == 0: the diagonal of O
-      }
+      if (g.O) p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
+      else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
     }
+  }
+  if (!rsc.empty()) {
+    std::vector<char> img;
+    const size_t ro = push(img, rsc);
+    rc = stage_desc(c, img, s);
+    if (rc) return rc;
+    nrg::PhaseScope ps(c, nrg::kPhGemm3, s);
+    CK(nrg::row_scale_launch(reinterpret_cast<const nrg::RowScale*>(static_cast<char*>(c->desc) + ro),
+                             (int)rsc.size(), rtotal, s));
   }
   rc = run_gemm_plan(c, p1, s, nrg::kPhGemm3);
   if (rc) return rc;

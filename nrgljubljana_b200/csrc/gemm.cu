@@ -12,6 +12,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <algorithm>
+
 namespace nrg {
 namespace {
 
@@ -44,10 +46,7 @@ __device__ __forceinline__ void load_stage(Stage& s, const GemmSeg& g, int M, in
     if (!g.transB) { n = e & (BN - 1); k = e >> 6; } else { k = e & (BK - 1); n = e >> 4; }
     const int gn = n0 + n, gk = k0 + k;
     double v = 0.0;
-    if (gn < N && gk < g.K) {
-      v = g.transB ? g.B[(int64_t)gn * g.ldb + gk] : g.B[(int64_t)gk * g.ldb + gn];
-      if (g.dscale) v *= g.dscale[gk];
-    }
+    if (gn < N && gk < g.K) v = g.transB ? g.B[(int64_t)gn * g.ldb + gk] : g.B[(int64_t)gk * g.ldb + gn];
     s.b[i] = v;
   }
 }
@@ -179,7 +178,31 @@ __global__ void __launch_bounds__(NT) gemm_one_kernel(const __grid_constant__ Ge
   gemm_tile(o, &g, blockIdx.x);
 }
 
+// Element e of the batch belongs to the last term whose off <= e; one product per element.
+__global__ void __launch_bounds__(256) row_scale_kernel(const RowScale* __restrict__ terms, int nterm,
+                                                        int64_t total) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nterm - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (terms[mid].off <= e) lo = mid; else hi = mid - 1;
+    }
+    const RowScale& r = terms[lo];
+    const int64_t q = e - r.off;
+    const int k = (int)(q / r.cols), c = (int)(q % r.cols);
+    const double b = r.transB ? r.B[(int64_t)c * r.ldb + k] : r.B[(int64_t)k * r.ldb + c];
+    r.T[q] = r.d[k] * b;
+  }
+}
+
 }  // namespace
+
+cudaError_t row_scale_launch(const RowScale* d_terms, int nterm, int64_t total, cudaStream_t stream) {
+  if (nterm <= 0 || total <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((total + 255) / 256, 148 * 16);
+  row_scale_kernel<<<(unsigned)blocks, 256, 0, stream>>>(d_terms, nterm, total);
+  return cudaGetLastError();
+}
 
 cudaError_t gemm_one_launch(const GemmOut& o, const GemmSeg& g, cudaStream_t stream) {
   const int tiles = ((o.M + BM - 1) / BM) * ((o.N + BN - 1) / BN);

@@ -8,18 +8,26 @@
 namespace nrg {
 
 // ---------------------------------------------------------------- batched FP64 GEMM
-// One K-segment of an output: alpha * op(A) * D * op(B), op(A) is M x K, op(B) is K x N.
+// One K-segment of an output: alpha * op(A) * op(B), op(A) is M x K, op(B) is K x N.
 // transA: A is stored K x M row-major (op(A) = A^T); transB: B is stored N x K (op(B) = B^T).
-// D = diag(dscale) (K entries) when dscale is set, the identity when it is null: row k of
-// op(B) is scaled by dscale[k] as it is loaded.
 struct GemmSeg {
   const double* A;
   const double* B;
   int64_t lda, ldb;
   int K, transA, transB, pad_;
   double alpha;
-  const double* dscale;
 };
+
+// T = diag(d) op(B) for one term (rows x cols, row-major, ld = cols); off is the term's first
+// element in the batch's flattened element range.
+struct RowScale {
+  double* T;
+  const double* d;
+  const double* B;
+  int64_t ldb, off;
+  int rows, cols, transB, pad_;
+};
+cudaError_t row_scale_launch(const RowScale* d_terms, int nterm, int64_t total, cudaStream_t stream);
 
 // One output C (M x N, row-major, ldc): C = beta*C + sum over its segments. Tiles of
 // 64 x 64 are numbered from tile0 in row-major tile order.

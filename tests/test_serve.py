@@ -81,7 +81,7 @@ def test_mix_with_large_blocks_within_tolerance():
     for i in range(12):
         z = 0.1 + 0.075 * i
         param = (f"[param]\nsymtype=QS\nmodel=SIAM\nU=1.0\nGamma=0.05\ndelta=0.05\nband=flat\ndiscretization=Z\n"
-                 f"Lambda=2\nz={z!r}\nkeep=100000\nkeepenergy=13\nT=1e-8\nops=n_d\n")
+                 f"Lambda=2\nz={z!r}\nkeep=10000\nkeepenergy=13\nT=1e-8\nops=n_d\n")
         reqs.append(Request(i, param, siam_qs(1.0, 0.05, 0.05, 2.0, 8, z, "Z", ops=["n_d"]), 0.0, str(i)))
     srv = Server(max_active=16)
     done = srv.serve(reqs, realtime=False)
