@@ -343,6 +343,26 @@ def main():
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "clocks": clk.summary()}
 
+    # validation: residuals and orthogonality of a sample of the last step's blocks (all 20
+    # largest and 150 more, seeded), computed from the pristine inputs on the device
+    try:
+        vrng = np.random.default_rng(SEED)
+        pick = sorted(set(vrng.choice(nbk, min(150, nbk), replace=False).tolist())
+                      | set(np.argsort(sizes)[-20:].tolist()))
+        worst_r = worst_o = 0.0
+        for b in pick:
+            n = int(sizes[b])
+            h = pristine[offs[b]:offs[b + 1]].view(n, n)
+            Hf = torch.triu(h) + torch.triu(h, 1).T
+            v = evecs[offs[b]:offs[b + 1]].view(n, n)
+            w = evals[voffs[b]:voffs[b + 1]]
+            nrm = max(float(w.abs().max()), 1e-300)
+            worst_r = max(worst_r, float(torch.linalg.norm(v @ Hf - w[:, None] * v, dim=1).max()) / nrm)
+            worst_o = max(worst_o, float((v @ v.T - torch.eye(n, dtype=torch.float64, device=dev)).abs().max()))
+        line["validation"] = {"blocks": len(pick), "max_residual_rel": worst_r, "max_orthogonality_err": worst_o,
+                              "ok": worst_r <= 1e-10 and worst_o <= 1e-9}
+    except (RuntimeError, MemoryError) as err:
+        line["validation"] = {"error": str(err)[:200]}
     del work, evecs, evals
     torch.cuda.empty_cache()
     if not args.no_e2e and rank == 0 and world == 1:

@@ -1826,8 +1826,12 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           void* kargs[] = {(void*)&db, (void*)&tm};
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
-          NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          tridiag_kernel<<<nbig, kTriThreads, smem, s>>>(dblk, tm);
+          // One CTA per SM here too: batches with more of these CTAs than SMs, where two of them
+          // shared an SM, gave wrong reductions for some blocks (cause not found, as for the
+          // cluster kernel); with one per SM every check passes.
+          const size_t smem1 = std::max(smem, (size_t)smsm / 2 + 1024);
+          NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+          tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(dblk, tm);
           NRG_CK(cudaGetLastError());
         }
       }

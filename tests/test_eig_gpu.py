@@ -208,3 +208,29 @@ def test_few_large_blocks_batch(nb):
         assert torch.linalg.norm(V @ Hd - w[:, None] * V, dim=1).max().item() <= 1e-12 * nrm * math.sqrt(n), n
         G = V @ V.T
         assert (G - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item() < 1e-10, n
+
+
+def test_more_reduction_ctas_than_sms(nb):
+    """320 blocks of order 250-900 in one call: with this many the large-block reductions all
+    run on the one-CTA bulk-copy kernel, more CTAs than the GPU has SMs (two waves). Every
+    block's residual and orthogonality are checked on the device."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(91)
+    sizes = [250 + (i * 37) % 651 for i in range(320)]
+    H, E, V, H0 = [], [], [], []
+    for n in sizes:
+        a = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+        h = torch.triu(a + a.T)
+        H0.append(h.clone())
+        H.append(h)
+        E.append(torch.empty(n, dtype=torch.float64, device="cuda"))
+        V.append(torch.empty(n, n, dtype=torch.float64, device="cuda"))
+    info = nb.diag_batch_device(H, E, V)
+    torch.cuda.synchronize()
+    assert (info == 0).all()
+    for h, e, v in zip(H0, E, V):
+        n = h.shape[0]
+        Hf = h + torch.triu(h, 1).T
+        nrm = e.abs().max().item()
+        assert torch.linalg.norm(v @ Hf - e[:, None] * v, dim=1).max().item() <= 1e-12 * nrm * math.sqrt(n), n
+        assert (v @ v.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item() < 1e-10, n
