@@ -542,7 +542,7 @@ class QSRun:
             for (i, j, ch, fn) in self.T.OFFDIAG:
                 if not (dims[i - 1] and dims[j - 1]):
                     continue
-                factor = fn(ss) * xi[ch][N]
+                factor = qs.ieee(fn, ss) * xi[ch][N]
                 key = (anc[i - 1], anc[j - 1])
                 if key not in self.opch_keys[ch]:
                     raise RuntimeError(f"offdiag_function(): matrix not found {i} {j} {ch} 0")
@@ -662,7 +662,7 @@ class QSRun:
                     if k != sp.dims[ip - 1]:
                         raise AssertionError("size2(A) == size2(B)")  # product, c++/numerics_ublas.hpp:112
                     rows.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, 0, 0,
-                                 sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, fn(Ip[1])))
+                                 sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, qs.ieee(fn, Ip[1])))
         if rows:
             gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
         self.opch_keys = [set(out.loc)] * self.T.channels

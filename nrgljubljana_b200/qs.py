@@ -29,9 +29,22 @@ Invar = Tuple[int, int]
 Fn = Callable[[int], float]
 
 
-def S(ss: int) -> float:
-    """Spin from multiplicity (c++/invar.hpp:22)."""
-    return (ss - 1.0) / 2.0
+def S(ss: int) -> np.float64:
+    """Spin from multiplicity (c++/invar.hpp:22), as a numpy double so that the table factors
+    divide by zero as the reference's C++ does (see ieee)."""
+    return np.float64((ss - 1.0) / 2.0)
+
+
+def ieee(fn, ss: int) -> float:
+    """A table factor at SS = ss, evaluated as the reference's C++ evaluates it: in IEEE double
+    arithmetic, x/0 is +-inf and the square root of a negative number is nan (the rows where
+    that happens are never used, but a factor at S = 0 may still come out finite, e.g.
+    1/sqrt(2 + 2/S) = 0)."""
+    with np.errstate(all="ignore"):
+        try:
+            return float(fn(ss))
+        except ValueError:  # math.sqrt of a negative number
+            return math.nan
 
 
 def mult(I: Invar) -> int:
@@ -125,7 +138,7 @@ class Tables:
     def doublet_factor(self, fn, ss1: int) -> float:
         """A doublet-table factor at SS = ss1 (rows of the two-channel tables are functions of
         the spin, evaluated as the triplet rows are)."""
-        return triplet_factor(fn, ss1) if self._doublet_of_spin else fn(ss1)
+        return triplet_factor(fn, ss1) if self._doublet_of_spin else ieee(fn, ss1)
 
     def ancestors(self, I: Invar) -> List[Invar]:
         return [(I[0] + d[0], I[1] + d[1]) for d in self.IN]

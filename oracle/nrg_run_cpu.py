@@ -207,7 +207,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
                     h[off[i] + n, off[i] + n] = math.sqrt(Lam) * diag[anc[i]].corr[n]
             for (i, j, ch, fn) in T.OFFDIAG:
                 if dims[i - 1] and dims[j - 1]:
-                    fs = (fn(I[1]) * d.xi[ch][N]) / scale
+                    fs = (_qs.ieee(fn, I[1]) * d.xi[ch][N]) / scale
                     mat = opch[ch][(anc[i - 1], anc[j - 1])]
                     if i > j:
                         h[off[j - 1]:off[j], off[i - 1]:off[i]] += fs * mat.T
@@ -295,7 +295,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
                         A = np.ascontiguousarray(e1.U[i1 - 1][:e1.nrstored])
                         B = np.ascontiguousarray(ep.U[ip - 1][:ep.nrstored])
                         if A.shape[1] and B.shape[1]:
-                            O.product(f, fn(Ip[1]), A, B)
+                            O.product(f, _qs.ieee(fn, Ip[1]), A, B)
                     nf[ch][(I1, Ip)] = f
             opch = nf
         if strategy == "kept":
