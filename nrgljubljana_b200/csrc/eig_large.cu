@@ -132,6 +132,14 @@ NRG_DEV void fence_proxy_async_global() { asm volatile("fence.proxy.async.global
 
 NRG_DEV void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// Acquire a tensor map that lives in global memory and was written by a host copy: orders the
+// copy's generic-proxy writes before this thread's tensormap-proxy reads of the 128-byte map,
+// so that no descriptor cached from an earlier map at the same address is used. The maps are
+// rewritten at the same addresses for every chunk of blocks and every call.
+NRG_DEV void tmap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(map) : "memory");
+}
+
 // Bounded wait for phase `parity` of an mbarrier; false if the bound ran out.
 NRG_DEV bool mbar_wait(uint64_t* bar, unsigned parity, int bound = (1 << 26)) {
   const unsigned a = smem_u32(bar);
@@ -414,6 +422,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
   if (lane == 0) {
     for (int st = 0; st < kStages; st++) mbar_init(bars + warp * kStages + st, 1);
     fence_mbar_init();
+    tmap_acquire(tmaps + blockIdx.x);  // lane 0 issues this warp's bulk copies
   }
   __syncthreads();
 
@@ -588,6 +597,7 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const Large
   if (lane == 0) {
     for (int st = 0; st < STAGES; st++) mbar_init(bars + warp * STAGES + st, 1);
     fence_mbar_init();
+    tmap_acquire(tmaps + bi);  // lane 0 issues this warp's bulk copies
   }
   __syncthreads();
 
@@ -1775,8 +1785,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         // about two waves of the SMs and the device can hold one such cluster at a time.
         bool tcl = false;
         // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
-        // CTAs on one SM the reductions came out wrong on B200 (cause not found); with one per
-        // SM every check passes. A cluster holds 8 SMs per block either way. The ring gets 8,
+        // CTAs on one SM the reductions came out wrong on B200 (cause not established; those
+        // runs had no tensor-map acquire fence, see tmap_acquire); with one per SM every check
+        // passes. A cluster holds 8 SMs per block either way. The ring gets 8,
         // 6 or 4 slabs per warp, the most that fit: one CTA per SM leaves the room.
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
