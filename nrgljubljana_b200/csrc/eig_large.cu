@@ -1785,9 +1785,8 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         // about two waves of the SMs and the device can hold one such cluster at a time.
         bool tcl = false;
         // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
-        // CTAs on one SM the reductions came out wrong on B200 (cause not established; those
-        // runs had no tensor-map acquire fence, see tmap_acquire); with one per SM every check
-        // passes. A cluster holds 8 SMs per block either way. The ring gets 8,
+        // CTAs on one SM the reductions came out wrong on B200, with the tensor-map acquire
+        // fence as without it (cause not established); with one per SM every check passes. A cluster holds 8 SMs per block either way. The ring gets 8,
         // 6 or 4 slabs per warp, the most that fit: one CTA per SM leaves the room.
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
