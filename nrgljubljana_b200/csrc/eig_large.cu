@@ -451,8 +451,11 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
       double ps = 0.0;
       for (int i = k + 2 + tid; i < n; i += nt) ps += v[i] * v[i];
-      const double sigma = block_sum_1b(ps, red, phase);
+      // alpha is read before the barrier inside block_sum_1b: thread 0 overwrites v[k+1] with
+      // the unit below, with no barrier between, and a warp that read it late would scale its
+      // part of the reflector with a wrong beta (and disagree with the others on tau)
       const double alpha = v[k + 1];
+      const double sigma = block_sum_1b(ps, red, phase);
       double tau = 0.0, beta = alpha, scale = 1.0;
       if (sigma > 0.0) {
         beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
@@ -626,8 +629,8 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const Large
       // (2) Householder reflector for rows k+1..n-1 (dlarfg convention, v[k+1] = 1)
       double ps = 0.0;
       for (int i = k + 2 + tid; i < n; i += nt) ps += v[i] * v[i];
+      const double alpha = v[k + 1];  // before the barrier: thread 0 sets v[k+1] = 1 below
       const double sigma = block_sum_1b(ps, red, phase);
-      const double alpha = v[k + 1];
       double tau = 0.0, beta = alpha, scale = 1.0;
       if (sigma > 0.0) {
         beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
@@ -1785,8 +1788,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         // about two waves of the SMs and the device can hold one such cluster at a time.
         bool tcl = false;
         // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
-        // CTAs on one SM the reductions came out wrong on B200, with the tensor-map acquire
-        // fence as without it (cause not established); with one per SM every check passes. A cluster holds 8 SMs per block either way. The ring gets 8,
+        // CTAs on one SM the reductions came out wrong on B200; with one per SM every check
+        // passes. The likely cause, a race on alpha = v[k+1] in the reflector step that grows
+        // with the skew between warps, is fixed; two per SM wait for a run that confirms it. A cluster holds 8 SMs per block either way. The ring gets 8,
         // 6 or 4 slabs per warp, the most that fit: one CTA per SM leaves the room.
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
@@ -1837,8 +1841,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
           // One CTA per SM here too: batches with more of these CTAs than SMs, where two of them
-          // shared an SM, gave wrong reductions for some blocks (cause not found, as for the
-          // cluster kernel); with one per SM every check passes.
+          // shared an SM, gave wrong reductions for some blocks (the same alpha race as the
+          // cluster kernel, now fixed, pending a confirming run); with one per SM every check
+          // passes.
           const size_t smem1 = std::max(smem, (size_t)smsm / 2 + 1024);
           NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
           tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(dblk, tm);
