@@ -176,6 +176,18 @@ def sample_blocks_host(torch, sizes, idx, device):
     return out
 
 
+def max_over_ranks(dist, x: float, device) -> float:
+    """The largest x of all ranks; x itself without a process group. Every rank takes this
+    collective step, also after its own failure (pass math.inf there), so that no rank is left
+    waiting for another."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def reference_arm(args, rank: int) -> None:
     import torch
     if rank != 0:
@@ -301,10 +313,7 @@ def main():
     elapsed = e0.elapsed_time(e1) / 1e3
     phases = ctx.profile_read()
     ctx.profile(False)
-    if dist:
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(dist, elapsed, dev)
     flop_step = f_eig(sizes)
     value = world * args.steps * flop_step / elapsed / 1e9
     launches = int(sum(v[1] for v in phases.values()))
@@ -365,11 +374,10 @@ def main():
         line["validation"] = {"error": str(err)[:200]}
     del work, evecs, evals
     torch.cuda.empty_cache()
-    if not args.no_e2e and rank == 0 and world == 1:
-        try:
-            line["e2e"] = e2e_arm(torch, ctx, nb, pristine, sizes, offs, voffs, args)
-        except (RuntimeError, MemoryError) as err:
-            line["e2e"] = {"value": None, "unit": UNIT, "error": str(err)[:300]}
+    if not args.no_e2e:  # every rank: its own replica through the host API, max over ranks
+        e2e = e2e_arm(torch, ctx, pristine, sizes, offs, voffs, args, dist, dev)
+        if rank == 0:
+            line["e2e"] = e2e
     if not args.no_cpu and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         idx, stride = cpu_sample(sizes, args.cpu_seconds, threads)
@@ -858,31 +866,59 @@ def nrg_run_arm(torch, device: int, args) -> dict:
     return out
 
 
-def e2e_arm(torch, ctx, nb, pristine, sizes, offs, voffs, args) -> dict:
-    """Same metric through the host-pointer entry point, from pinned host memory."""
+def e2e_arm(torch, ctx, pristine, sizes, offs, voffs, args, dist=None, dev=None) -> dict:
+    """Same metric through the host-pointer entry point, from pinned host memory: each step
+    copies the step's blocks in and the eigenpairs out (nrg_diag_batch_host returns when they
+    are in host memory). Timed with CUDA events around the synchronous calls, after a barrier
+    under torchrun; the whole-job value uses the slowest rank's time. Every rank takes the
+    same collective steps whether or not its own calls failed."""
     import ctypes as C
     nbk = len(sizes)
-    hostH = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
-    hostH.copy_(pristine)
-    hostV = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
-    hostE = torch.empty(int(voffs[-1]), dtype=torch.float64, pin_memory=True)
-    n_c = (C.c_int * nbk)(*[int(x) for x in sizes])
-    Hp = (C.c_void_p * nbk)(*[hostH.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
-    Vp = (C.c_void_p * nbk)(*[hostV.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
-    Ep = (C.c_void_p * nbk)(*[hostE.data_ptr() + 8 * int(voffs[b]) for b in range(nbk)])
-    info = (C.c_int * nbk)()
-    rc = ctx.lib.nrg_diag_batch_host(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)  # warm-up
-    if rc != 0:
-        raise RuntimeError(f"nrg_diag_batch_host returned {rc}")
+    world = dist.get_world_size() if dist else 1
     k = max(1, min(args.steps, 3))
-    t0 = time.perf_counter()
-    for _ in range(k):
-        rc = ctx.lib.nrg_diag_batch_host(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)
-        if rc != 0:
-            raise RuntimeError(f"nrg_diag_batch_host returned {rc}")
-    dt = (time.perf_counter() - t0) / k
-    return {"value": f_eig(sizes) / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(8 * offs[-1]),
-            "d2h_bytes_per_step": int(8 * (offs[-1] + voffs[-1])), "steps": k, "ms_per_step": dt * 1e3}
+    err, dt = None, math.inf
+    try:
+        hostH = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+        hostH.copy_(pristine)
+        hostV = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+        hostE = torch.empty(int(voffs[-1]), dtype=torch.float64, pin_memory=True)
+        n_c = (C.c_int * nbk)(*[int(x) for x in sizes])
+        Hp = (C.c_void_p * nbk)(*[hostH.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+        Vp = (C.c_void_p * nbk)(*[hostV.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])
+        Ep = (C.c_void_p * nbk)(*[hostE.data_ptr() + 8 * int(voffs[b]) for b in range(nbk)])
+        info = (C.c_int * nbk)()
+
+        def call():
+            rc = ctx.lib.nrg_diag_batch_host(ctx.ptr, nbk, n_c, Hp, Ep, Vp, info, None)
+            if rc != 0:
+                raise RuntimeError(f"nrg_diag_batch_host returned {rc}")
+        call()  # warm-up
+    except (RuntimeError, MemoryError) as e:
+        err = str(e)[:300]
+    if dist:
+        dist.barrier()
+    if err is None:
+        try:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(k):
+                call()
+            e1.record()
+            torch.cuda.synchronize()
+            dt = e0.elapsed_time(e1) / 1e3 / k
+        except (RuntimeError, MemoryError) as e:
+            err = str(e)[:300]
+    dt = max_over_ranks(dist, dt, dev)
+    out = {"value": world * f_eig(sizes) / dt / 1e9 if math.isfinite(dt) else None, "unit": UNIT,
+           "h2d_bytes_per_step": int(8 * offs[-1]) * world,
+           "d2h_bytes_per_step": int(8 * (offs[-1] + voffs[-1])) * world, "steps": k,
+           "ms_per_step": dt * 1e3 if math.isfinite(dt) else None}
+    if err is not None:
+        out["error"] = err
+    elif not math.isfinite(dt):
+        out["error"] = "another rank's host-API calls failed"
+    return out
 
 
 if __name__ == "__main__":
