@@ -42,7 +42,7 @@ Invar = Tuple[int, int]
 _IGNORED = {
     "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
     "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
-    "Nmax", "prec_td", "prec_custom", "prec_xy", "width_td", "width_custom",
+    "Nmax",
     "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
     # model parameters of the generated data and of its discretisation
     "U1", "U2", "Gamma1", "Gamma2", "eps1", "eps2", "U12", "J12", "tri", "mMAX",
@@ -100,6 +100,15 @@ class RunParams:
     alpha: float = 0.3
     omega0: float = -1.0
     omega0_ratio: float = 1.0
+    # output (c++/params.hpp:310, 332, 394-400): the raw trimmed bins as <name>.bin, a third
+    # (imaginary) column, and the precision and width of the written numbers
+    savebins: bool = False
+    reim: bool = False
+    prec_td: int = 10
+    prec_custom: int = 10
+    prec_xy: int = 10
+    width_td: int = 16
+    width_custom: int = 16
 
     @classmethod
     def from_param(cls, kv: Dict[str, str]) -> "RunParams":
@@ -123,8 +132,6 @@ class RunParams:
             raise ValueError(f"strategy={p.strategy}")
         if (p.dmnrg or p.fdm_flags) and p.strategy != "kept":
             raise ValueError("density-matrix algorithms are supported with strategy=kept")
-        if p.algorithms and not p.broaden:
-            raise ValueError("broaden=false is not supported")
         return p
 
     @property
@@ -153,8 +160,11 @@ class Result:
     blocks_per_step: List[int] = field(default_factory=list)
     max_dim_per_step: List[int] = field(default_factory=list)
     block_dims: List[List[int]] = field(default_factory=list)  # orders of the blocks of every step
-    # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_FDM_...", "spin_...") -> rows (E, A(E))
+    # file stem ("spec_DMNRG_dens_A_d-A_d", "corr_FDM_...", "spin_...") -> rows (E, A(E)),
+    # the broadened spectra (broaden=true)
     spectra: Dict[str, np.ndarray] = field(default_factory=dict)
+    # the same stems -> rows (E, Re w[, Im w]) of the trimmed raw bins (savebins=true)
+    bins: Dict[str, np.ndarray] = field(default_factory=dict)
     tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
     customfdm: Optional[Tuple[List[str], List[float]]] = None   # fields, row (measure_singlet_fdm)
 
@@ -750,7 +760,7 @@ class QSRun:
         fdm = self._rho_fdm() if p.fdm_flags else None
         if fdm is not None:
             res.tdfdm = (["T", "E_fdm", "C_fdm", "F_fdm", "S_fdm"], fdm["tdrow"])
-        res.spectra, expv = self._spectral_pass(rhos, fdm)
+        res.spectra, res.bins, expv = self._spectral_pass(rhos, fdm)
         if expv is not None:
             res.customfdm = (["T"] + self.sop_names, [p.T] + expv)
 
@@ -927,7 +937,7 @@ class QSRun:
         return {"rhos": rhos, "wn": wn, "wnfactor": wnfactor, "last": dsrc[nst - 1], "GS": GS,
                 "tdrow": [T, E_fdm, C_fdm, F_fdm, S_fdm]}
 
-    def _spectral_pass(self, rhos, fdm) -> Tuple[Dict[str, np.ndarray], Optional[List[float]]]:
+    def _spectral_pass(self, rhos, fdm) -> Tuple[Dict[str, np.ndarray], Dict[str, np.ndarray], Optional[List[float]]]:
         """The spectra of the DMNRG run: per step the operators of the spectra recalculated
         (over all states when an FDM flag is set, do_recalc_all, c++/params.hpp:542-547;
         else over the kept ones), BaseSpectrum::calc over all subspace pairs
@@ -1040,6 +1050,7 @@ class QSRun:
             if fdm is not None and p.fdmexpv and st.N == p.fdmexpvn:
                 expv = self._fdm_expv(k, st, cur["s"], fdm)
         out: Dict[str, np.ndarray] = {}
+        raw: Dict[str, np.ndarray] = {}
         omega0 = p.omega0 if p.omega0 >= 0.0 else p.omega0_ratio * p.T
         bmin = p.broaden_min if p.broaden_min > 0.0 else p.broaden_min_ratio * last_scale
         mesh = []
@@ -1055,8 +1066,12 @@ class QSRun:
                 else:
                     full_pos = sum(fdm_acc[(j, w)][0] for w in parts_of[a]).cpu().numpy()
                     full_neg = sum(fdm_acc[(j, w)][1] for w in parts_of[a]).cpu().numpy()
-                out[f"{prefix}_{a}_dens_{n1}-{n2}"] = self._broadened(full_pos, full_neg, ebins, mesh, omega0)
-        return out, expv
+                name = f"{prefix}_{a}_dens_{n1}-{n2}"
+                if p.broaden:
+                    out[name] = self._broadened(full_pos, full_neg, ebins, mesh, omega0)
+                if p.savebins:
+                    raw[name] = raw_bins(full_pos, full_neg, ebins, p.discard_trim, p.reim)
+        return out, raw, expv
 
     def _fdm_expv(self, k: int, st: "_StepRecord", sops: MatSet, fdm: Dict) -> List[float]:
         """measure_singlet_fdm (c++/measurements.hpp:31-44): sum_I mult(I) Tr[rhoFDM_I O_I] over
@@ -1089,12 +1104,8 @@ class QSRun:
         (c++/spectrum.hpp:168-196) on the device; rows (E, A(E)) sorted by E."""
         p = self.p
 
-        def trim(w):
-            width = np.diff(ebins)
-            keep = np.concatenate([np.abs(w[:-1]) >= p.discard_trim * width, [True]])
-            return ebins[keep], w[keep]
-        ep, wp = trim(full_pos)
-        en, wn = trim(full_neg)
+        ep, wp = trim_bins(ebins, full_pos, p.discard_trim)
+        en, wn = trim_bins(ebins, full_neg, p.discard_trim)
         spikes_e = np.concatenate([ep, -en])
         spikes_w = np.concatenate([wp, wn])
         mesh_all = np.concatenate([mesh, -mesh])
@@ -1103,6 +1114,33 @@ class QSRun:
         rows_pos = sorted(zip(mesh_all[:npos].tolist(), vals[:npos].tolist()))
         rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
         return np.array(rows_neg + rows_pos)
+
+def trim_bins(ebins: np.ndarray, w: np.ndarray, discard_trim: float) -> Tuple[np.ndarray, np.ndarray]:
+    """Bins::trim (c++/bins.hpp:165-185) of one half: bin i (energy ebins[i], weight w[i]) is
+    kept if |w[i]| >= discard_trim * (ebins[i+1] - ebins[i]); the last bin is always kept."""
+    width = np.diff(ebins)
+    keep = np.concatenate([np.abs(w[:-1]) >= discard_trim * width, [True]])
+    return ebins[keep], w[keep]
+
+
+def raw_bins(full_pos: np.ndarray, full_neg: np.ndarray, ebins: np.ndarray, discard_trim: float,
+             reim: bool = False) -> np.ndarray:
+    """SpectrumRealFreq::savebins (c++/spectrum.hpp:146-170) after the trim of both halves:
+    rows (E, Re w) -- (E, Re w, Im w) with reim -- of the kept positive-energy bins by ascending
+    E, then of the kept negative-energy bins by ascending |E|, with E = -|E|. The weights of
+    these real runs have no imaginary part, written as 0."""
+    ep, wp = trim_bins(ebins, full_pos, discard_trim)
+    en, wn = trim_bins(ebins, full_neg, discard_trim)
+    cols = [np.concatenate([ep, -en]), np.concatenate([wp, wn])]
+    if reim:
+        cols.append(np.zeros(len(cols[0])))
+    return np.stack(cols, axis=1)
+
+
+def write_bins(path: str, rows: np.ndarray) -> None:
+    """The binary file of savebins: the rows' doubles in order, native byte order, no header."""
+    np.ascontiguousarray(rows, dtype=np.float64).tofile(path)
+
 
 def window(e: np.ndarray, Emin: float, Ex: float, Emax: float, last: bool, first: bool, NNtanh: float) -> np.ndarray:
     """windowfunction (c++/spectrum.hpp:91-109) for the bin energies inside (Emin, Emax)."""
@@ -1162,17 +1200,28 @@ def main(argv=None) -> int:
         torch.cuda.synchronize()
         print(f"run {k}: {d.nmax} steps in {time.perf_counter() - t0:.3f} s", flush=True)
     out = a.out or a.dir
+    write_outputs(out, p, res)
+    return 0
+
+
+def write_outputs(out: str, p: RunParams, res: Result) -> None:
+    """td, custom, tdfdm, customfdm, the broadened spectra <stem>.dat (as Spikes::save and
+    outputxy write them, c++/spectral.hpp:24-30, c++/io.hpp:33-38) and the raw bins <stem>.bin
+    into the folder `out`."""
+    import os
     os.makedirs(out, exist_ok=True)
-    _write_table(os.path.join(out, "td"), res.td_fields, res.td)
-    _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom)
-    for name, tab in (("tdfdm", res.tdfdm), ("customfdm", res.customfdm)):
+    _write_table(os.path.join(out, "td"), res.td_fields, res.td, p.prec_td, p.width_td)
+    _write_table(os.path.join(out, "custom"), res.custom_fields, res.custom, p.prec_custom, p.width_custom)
+    for name, tab, prec, width in (("tdfdm", res.tdfdm, p.prec_td, p.width_td),
+                                   ("customfdm", res.customfdm, p.prec_custom, p.width_custom)):
         if tab is not None:
-            _write_table(os.path.join(out, name), tab[0], [tab[1]])
-    for name, rows in res.spectra.items():  # <prefix>_<algo>_dens_<op1>-<op2>.dat, as Spikes::save writes it
+            _write_table(os.path.join(out, name), tab[0], [tab[1]], prec, width)
+    for name, rows in res.spectra.items():  # <prefix>_<algo>_dens_<op1>-<op2>.dat
         with open(os.path.join(out, f"{name}.dat"), "w") as f:
             for e, v in rows:
-                f.write(f"{e:.10g} {v:.10g}\n")
-    return 0
+                f.write(f"{e:.{p.prec_xy}g} {v:.{p.prec_xy}g}" + (" 0\n" if p.reim else "\n"))
+    for name, rows in res.bins.items():
+        write_bins(os.path.join(out, f"{name}.bin"), rows)
 
 
 if __name__ == "__main__":

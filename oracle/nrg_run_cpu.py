@@ -90,13 +90,16 @@ class _Eig:
         self.U: List[np.ndarray] = []
 
 
-def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None
-        ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None,
+        bins_out: dict = None) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
     """td and custom rows of the run; with a `spectra` dict, also the spectra of the specs,
     specd and spect pairs for the algorithms dmnrg, fdm, fdmgt, fdmls that are switched on
     (file stem, e.g. spec_DMNRG_dens_A_d-A_d -> array of (E, A(E)) rows as written to that
     .dat file); with an `fdm_out` dict and an FDM flag, also fdm_out["tdfdm"] (fields, row)
-    and, with fdmexpv, fdm_out["customfdm"] (fields, row)."""
+    and, with fdmexpv, fdm_out["customfdm"] (fields, row); with a `bins_out` dict and a
+    `spectra` dict, also the trimmed raw bins of every spectrum as savebins writes them
+    (SpectrumRealFreq::savebins, c++/spectrum.hpp:146-170): rows (E, Re w), or (E, Re w, Im w)
+    with reim=true, the positive energies ascending, then -|E| by ascending |E|."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -349,7 +352,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         diag = new
     if (dm or fdm_needed) and steps:
         _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos if dm else [], spectra, fdm_out if fdm_flags else None,
-                    total_energy, C, sorted(ops))
+                    total_energy, C, sorted(ops), bins_out=bins_out)
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
     return td_fields, td_rows, ["T"] + sorted(ops), custom_rows
 
@@ -422,7 +425,7 @@ def _fdm_weights(steps, T, GS, combs):
     return wn, wnfactor, [float(z) for z in ZN], [T, E_fdm, C_fdm, F_fdm, S_fdm]
 
 
-def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names):
+def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None):
     """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
     calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
     c++/dmnrg.hpp:146-217), then per step the spectra of every algorithm
@@ -438,6 +441,8 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
     NN2even = kv.get("NN2even", "true").lower() == "true"
     NNtanh = float(kv.get("NNtanh", 0.0))
     discard_trim = float(kv.get("discard_trim", 1e-16))
+    reim = kv.get("reim", "false").lower() == "true"
+    broaden_on = kv.get("broaden", "true").lower() == "true"
     discard_imm = float(kv.get("discard_immediately", 1e-16))
     emin_p, emax_p = float(kv.get("emin", -1.0)), float(kv.get("emax", -1.0))
     alpha = float(kv.get("alpha", 0.3))
@@ -601,6 +606,16 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                 keep.append((e[-1], w[-1]))
                 return keep
             pos, neg = trim(fs.pos_re), trim(fs.neg_re)
+            if bins_out is not None:  # savebins: Bins::trim keeps |w| (complex modulus) >= discard_trim * width
+                rows = []
+                for sgn, wr, wi in ((1.0, fs.pos_re, fs.pos_im), (-1.0, fs.neg_re, fs.neg_im)):
+                    e = fs.energies
+                    for i in range(len(e)):
+                        if i == len(e) - 1 or abs(complex(wr[i], wi[i])) >= discard_trim * (e[i + 1] - e[i]):
+                            rows.append((sgn * e[i], wr[i], wi[i]) if reim else (sgn * e[i], wr[i]))
+                bins_out[f"{prefix}_{a}_dens_{name1}-{name2}"] = np.array(rows)
+            if not broaden_on:  # SpectrumRealFreq::save: continuous() only with broaden=true
+                continue
             rows_pos, rows_neg = [], []
             for E in mesh:
                 vp = sum(w * _BR_NEW(E, e, alpha, omega0) for e, w in pos) + \
