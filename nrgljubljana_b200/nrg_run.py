@@ -75,6 +75,10 @@ class RunParams:
     fdmexpv: bool = False
     fdmexpvn: int = 0
     lastalloverride: bool = False
+    # complete-Fock-space spectra (c++/params.hpp:233-237): greater + lesser parts, or each alone
+    cfs: bool = False
+    cfsgt: bool = False
+    cfsls: bool = False
     data_has_rescaled_energies: bool = True
     # DM-NRG spectra of the specs/specd/spect pairs (c++/params.hpp:181-396)
     T: float = 0.001
@@ -130,7 +134,7 @@ class RunParams:
                 raise ValueError(f"parameter {k} is not supported by the QS run driver")
         if p.strategy not in ("kept", "all"):
             raise ValueError(f"strategy={p.strategy}")
-        if (p.dmnrg or p.fdm_flags) and p.strategy != "kept":
+        if (p.dmnrg or p.fdm_flags or p.cfs_flags) and p.strategy != "kept":
             raise ValueError("density-matrix algorithms are supported with strategy=kept")
         return p
 
@@ -140,15 +144,21 @@ class RunParams:
         return self.fdm or self.fdmgt or self.fdmls or self.fdmexpv
 
     @property
+    def cfs_flags(self) -> bool:
+        """Params::cfs_flags (c++/params.hpp:534)."""
+        return self.cfs or self.cfsgt or self.cfsls
+
+    @property
     def algorithms(self) -> List[str]:
         """The real-frequency spectral algorithms switched on (c++/oprecalc.hpp:123-131)."""
         return [a for a, on in (("DMNRG", self.dmnrg), ("FDM", self.fdm), ("FDMgt", self.fdmgt),
-                                ("FDMls", self.fdmls)) if on]
+                                ("FDMls", self.fdmls), ("CFS", self.cfs), ("CFSgt", self.cfsgt),
+                                ("CFSls", self.cfsls)) if on]
 
     @property
     def keep_all_states_in_last_step(self) -> bool:
         """Params::keep_all_states_in_last_step (c++/params.hpp:539)."""
-        return self.lastall or (self.fdm_flags and not self.lastalloverride)
+        return self.lastall or ((self.cfs_flags or self.fdm_flags) and not self.lastalloverride)
 
 
 @dataclass
@@ -756,7 +766,7 @@ class QSRun:
         matrices with the FDM thermodynamics (calc_rhoFDM), then the spectral pass over the
         kept steps (the second run of the reference without its diagonalisations)."""
         p = self.p
-        rhos = self._rho_dmnrg() if "DMNRG" in self.algos else None
+        rhos = self._rho_dmnrg() if ("DMNRG" in self.algos or p.cfs_flags) else None  # Params::need_rho
         fdm = self._rho_fdm() if p.fdm_flags else None
         if fdm is not None:
             res.tdfdm = (["T", "E_fdm", "C_fdm", "F_fdm", "S_fdm"], fdm["tdrow"])
@@ -849,6 +859,7 @@ class QSRun:
         for I, (r, c) in shapes.items():
             host[o + np.arange(r) * (c + 1)] = diagvals[I] / Z
             o += r * c
+        self.Zft = Z  # calc_Z at the last step (c++/measurements.hpp:189-191): the same kept-state sum
         rhos = self._sweep(MatSet(self.dev, shapes, 1, host), None)
         for tr in self._traces(rhos):
             if abs(tr - 1.0) > 1e-9:
@@ -957,7 +968,8 @@ class QSRun:
         ebins = grid.energies()
         nb = grid.nbins
         Efac = Lam if (d.channels == 1 and not p.NN1) else math.sqrt(Lam)  # Params::getEfactor
-        rows = (lambda s: s.n) if p.fdm_flags else (lambda s: s.nkept)  # noqa: E731
+        # do_recalc_all (c++/params.hpp:542-547): the operators over all states for CFS and FDM
+        rows = (lambda s: s.n) if (p.fdm_flags or p.cfs_flags) else (lambda s: s.nkept)  # noqa: E731
         kinds = {"s": (1, qs.correlator_factor, self.sop_names), "d": (-1, qs.specdens_factor, self.dop_names),
                  "t": (1, qs.dynamicsusceptibility_factor, self.top_names)}
         tables = {"d": (self.T.DOUBLET, self.T.doublet_factor), "t": (self.T.TRIPLET, qs.triplet_factor)}
@@ -966,6 +978,9 @@ class QSRun:
         zeros = lambda: torch.zeros(nb, dtype=torch.float64, device=self.dev)  # noqa: E731
         dm_acc = {j: (np.zeros(nb), np.zeros(nb)) for j in range(len(self.specs))} if rhos is not None else {}
         fdm_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in fdm_parts}
+        cfs_parts_of = {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}
+        cfs_parts = sorted({w for a in self.algos if a in cfs_parts_of for w in cfs_parts_of[a]})
+        cfs_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in cfs_parts}
         cur = dict(self.spec_init)
         expv = None
         for k, st in enumerate(steps):
@@ -974,7 +989,7 @@ class QSRun:
                           else self._recalc_tensor(st.diag, m, *tables[kind], rows)) for kind, m in cur.items()}
             dg = st.diag
             merge = p.NN1 or p.NN2avg or ((st.N % 2 == 0) if p.NN2even else (st.N % 2 == 1))
-            if rhos is not None and merge and self.specs:
+            if "DMNRG" in self.algos and merge and self.specs:
                 rhoN = rhos[k]
                 eoff, flat, o = {}, [], 0
                 for I, s in dg.items():  # abs_zero energies of the kept states (c++/eigen.hpp:45)
@@ -1047,6 +1062,8 @@ class QSRun:
                             spec_accumulate_array(algo, np.array(prs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
                                                   sign=sign, T=p.T, wnf=fdm["wnfactor"][k], ctx=self.ctx,
                                                   stream=self.stream)
+            if cfs_parts and self.specs:
+                self._cfs_step(st, last, None if last else rhos[k], cur, kinds, grid, cfs_parts, cfs_acc)
             if fdm is not None and p.fdmexpv and st.N == p.fdmexpvn:
                 expv = self._fdm_expv(k, st, cur["s"], fdm)
         out: Dict[str, np.ndarray] = {}
@@ -1063,6 +1080,9 @@ class QSRun:
             for a in self.algos:
                 if a == "DMNRG":
                     full_pos, full_neg = dm_acc[j]
+                elif a in cfs_parts_of:
+                    full_pos = sum(cfs_acc[(j, w)][0] for w in cfs_parts_of[a]).cpu().numpy()
+                    full_neg = sum(cfs_acc[(j, w)][1] for w in cfs_parts_of[a]).cpu().numpy()
                 else:
                     full_pos = sum(fdm_acc[(j, w)][0] for w in parts_of[a]).cpu().numpy()
                     full_neg = sum(fdm_acc[(j, w)][1] for w in parts_of[a]).cpu().numpy()
@@ -1072,6 +1092,64 @@ class QSRun:
                 if p.savebins:
                     raw[name] = raw_bins(full_pos, full_neg, ebins, p.discard_trim, p.reim)
         return out, raw, expv
+
+    def _cfs_step(self, st: "_StepRecord", last: bool, rhoN: Optional[MatSet], cur: Dict, kinds: Dict,
+                  grid: BinGrid, cfs_parts: List[str], cfs_acc: Dict) -> None:
+        """Algo_CFSgt / Algo_CFSls::calc (c++/algo_CFS.hpp:28-53, 80-105) of one step for every
+        spectrum, merged whole (mergeCFS), built from the FDM pair modes of nrg_spec_accumulate
+        with the abs_zero energies of all states (c++/eigen.hpp:45) and the DM-NRG rho:
+          last step: the kept x kept term e^{-E/T}/Z_ft is the FDMgt (greater) and FDMls
+            (lesser) D x D term of the pair cut to its kept states (K = 0) with wnf = 1/Z_ft;
+          other steps: CFSls, sum over discarded(Ij) x kept(Ii) of op1 (op2 rho(Ii)) (-sign), is
+            the FDMgt K(Ii) x D(Ij) term with rho(Ii); CFSgt, over kept(Ij) x discarded(Ii) of
+            (op1^T rho(Ij))^T op2, is the FDMls D(Ii) x K(Ij) term with the operators swapped
+            and rho(Ij) (rho is symmetric); both with wnf = 0, which zeroes the other FDM
+            terms, and the factor times -sign, which cancels or supplies the FDM sign."""
+        p = self.p
+        dg = st.diag
+        eoff, flat, o = {}, [], 0
+        for I, s in dg.items():
+            eoff[I] = o
+            flat.append((s.values - s.shift) * st.scale)
+            o += s.n
+        Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+        eb = Edev.data_ptr()
+        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+            sign, ff, names = kinds[kind]
+            ops = cur[kind]
+            o1, o2 = names.index(n1), names.index(n2)
+            gt, ls = [], []
+            for Ii, si in dg.items():
+                for Ij, sj in dg.items():
+                    key = Ii if kind == "s" else (Ij, Ii)
+                    if (kind == "s" and Ij != Ii) or key not in ops.loc:
+                        continue
+                    ld = ops.loc[key][2]
+                    ki, kj, ni, nj = si.nkept, sj.nkept, si.n, sj.n
+                    Ep_i, Ep_j, p1, p2, f = eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ops.ptr(key, o2), ff(Ii, Ij)
+                    if last:
+                        if ki and kj:
+                            row = (Ep_i, Ep_j, p1, ld, p2, ld, 0, 1, 0, 1, ki, 0, kj, 0, 0, 0, f)
+                            gt.append(row)
+                            ls.append(row)
+                    else:
+                        if ki and nj > kj:
+                            ls.append((Ep_i, Ep_j, p1, ld, p2, ld, rhoN.ptr(Ii), ki, 0, 1, ni, ki, nj, kj, ki, 0,
+                                       -sign * f))
+                        if kj and ni > ki:
+                            gt.append((Ep_i, Ep_j, p2, ld, p1, ld, 0, 1, rhoN.ptr(Ij), kj, ni, ki, nj, kj, 0, kj,
+                                       -sign * f))
+            if last:
+                calls = (("gt", gt, NRG_SPEC_FDMGT), ("ls", ls, NRG_SPEC_FDMLS))
+                wnf = 1.0 / self.Zft
+            else:
+                calls = (("gt", gt, NRG_SPEC_FDMLS), ("ls", ls, NRG_SPEC_FDMGT))
+                wnf = 0.0
+            for w, prs, algo in calls:
+                if w in cfs_parts and prs:
+                    pos, neg = cfs_acc[(j, w)]
+                    spec_accumulate_array(algo, np.array(prs, dtype=SPECPAIR_DTYPE), grid, pos, neg, sign=sign,
+                                          T=p.T, wnf=wnf, ctx=self.ctx, stream=self.stream)
 
     def _fdm_expv(self, k: int, st: "_StepRecord", sops: MatSet, fdm: Dict) -> List[float]:
         """measure_singlet_fdm (c++/measurements.hpp:31-44): sum_I mult(I) Tr[rhoFDM_I O_I] over

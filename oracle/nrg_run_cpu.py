@@ -113,8 +113,10 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     betabar = float(kv.get("betabar", 1.0))
     strategy = kv.get("strategy", "kept")
     flag = lambda k: kv.get(k, "false").lower() == "true"  # noqa: E731
-    # Params::keep_all_states_in_last_step (c++/params.hpp:535-539)
-    lastall = flag("lastall") or ((flag("fdm") or flag("fdmexpv")) and not flag("lastalloverride"))
+    # Params::cfs_flags, fdm_flags, keep_all_states_in_last_step (c++/params.hpp:534-539)
+    cfs_flags = any(flag(k) for k in ("cfs", "cfsgt", "cfsls"))
+    fdm_flags = any(flag(k) for k in ("fdm", "fdmgt", "fdmls", "fdmexpv"))
+    lastall = flag("lastall") or ((cfs_flags or fdm_flags) and not flag("lastalloverride"))
     rescaled = kv.get("data_has_rescaled_energies", "true").lower() == "true"
     d = read_data(data_text)
     Nmax = d.nmax
@@ -133,8 +135,8 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
     # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
-    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls")) if flag(k)]
-    fdm_flags = any(flag(k) for k in ("fdm", "fdmgt", "fdmls", "fdmexpv"))
+    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"),
+                            ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls")) if flag(k)]
     dm = spectra is not None and bool(algos)
     fdm_needed = fdm_flags and (spectra is not None or fdm_out is not None)
     total_energy = d.gs_energy  # Stats::total_energy (c++/stats.hpp:60-71)
@@ -305,9 +307,9 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             ops = recalc_ops(lambda e: e.nrstored)
             custom(N, new, ops)
         if dm or fdm_needed:
-            # The DMNRG run recalculates the operators of the spectra over all states when an
-            # FDM flag is set (do_recalc_all, c++/params.hpp:542-547), else over the kept ones.
-            nrows = (lambda e: len(e.values)) if fdm_flags else (lambda e: e.nrstored)  # noqa: E731
+            # The DMNRG run recalculates the operators of the spectra over all states when a CFS
+            # or FDM flag is set (do_recalc_all, c++/params.hpp:542-547), else over the kept ones.
+            nrows = (lambda e: len(e.values)) if (cfs_flags or fdm_flags) else (lambda e: e.nrstored)  # noqa: E731
 
             def recalc_tensor(cold, tables, factor):
                 """recalc_general (c++/recalc.hpp:82-108) over the pairs Ip = I1 + dq."""
@@ -342,7 +344,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             dops = {name: recalc_tensor(cold, dtab, dfac) for name, cold in dops.items()}
             tops = {name: recalc_tensor(cold, T.TRIPLET, _qs.triplet_factor) for name, cold in tops.items()}
             snames = {x for sp in specs if sp[1] == "s" for x in sp[2:]}
-            if fdm_flags:
+            if cfs_flags or fdm_flags:
                 snames |= set(ops) if (fdm_out is not None and flag("fdmexpv")) else set()
                 sops = recalc_ops(nrows, snames)
             else:
@@ -425,6 +427,31 @@ def _fdm_weights(steps, T, GS, combs):
     return wn, wnfactor, [float(z) for z in ZN], [T, E_fdm, C_fdm, F_fdm, S_fdm]
 
 
+def cfs_terms(last, Ei, ki, Ej, kj, o1, o2, rho_i, rho_j, sign, T, Zft):
+    """The (energy, weight) terms of Algo_CFSgt::calc and Algo_CFSls::calc (c++/algo_CFS.hpp:
+    28-53, 80-105) for one pair, in the reference's loop order, with Ip = Ii and I1 = Ij:
+    o1, o2 = op(Ij, Ii) (r1 in Ij rows, rp in Ii columns) over all states; Ei, Ej the abs_zero
+    energies of all states; ki, kj the kept states; rho_i, rho_j the DM-NRG density matrices
+    (kept x kept) of Ii, Ij; Zft the last step's kept-state partition function. Returns
+    {"gt": (E, w), "ls": (E, w)} before the factor ff(Ii, Ij)."""
+    if last:  # i-term, Eq. (11): r1 in kept(I1), rp in kept(Ip)
+        E = (Ej[:kj, None] - Ei[None, :ki]).ravel()
+        base = o1[:kj, :ki] * o2[:kj, :ki]
+        return {"gt": (E, (base * np.exp(-Ei[None, :ki] / T) / Zft).ravel()),
+                "ls": (E, (base * np.exp(-Ej[:kj, None] / T) * (-sign) / Zft).ravel())}
+    # ii-term, Eq. (15): rk in kept(I1), rl in discarded(Ip);
+    # op1_rho = prod_adj_fit_left(op1, rho(I1)) (c++/numerics.hpp:310-316)
+    o1rho = o1[:kj, :].T @ rho_j
+    E_gt = (Ej[:kj, None] - Ei[None, ki:]).ravel()
+    w_gt = (o1rho[ki:, :].T * o2[:kj, ki:]).ravel()
+    # iii-term, Eq. (16): rl in discarded(I1), rk in kept(Ip);
+    # op2_rho = prod_fit_left(op2, rho(Ip)) (c++/numerics.hpp:285-291)
+    o2rho = o2[:, :ki] @ rho_i
+    E_ls = (Ej[kj:, None] - Ei[None, :ki]).ravel()
+    w_ls = (o1[kj:, :ki] * o2rho[kj:, :] * (-sign)).ravel()
+    return {"gt": (E_gt, w_gt), "ls": (E_ls, w_ls)}
+
+
 def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None):
     """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
     calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
@@ -495,12 +522,14 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
         return sum(I[1] * np.trace(m) for I, m in rho.items())
 
     rhos = fdm = None
-    if "DMNRG" in algos:
+    Zft = None
+    if "DMNRG" in algos or any(a.startswith("CFS") for a in algos):  # Params::need_rho
         # init_rho over the kept states of the last step (c++/dmnrg.hpp:43-50)
         _, scale_last, diag_last, _, _, _ = steps[-1]
         scT = scale_last / T
         Z = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrpost]) for I, e in diag_last.items())
         rho = {I: np.diag([math.exp(-c * scT) for c in e.corr[:e.nrpost]]) / Z for I, e in diag_last.items()}
+        Zft = Z  # calc_Z at the last step (c++/measurements.hpp:189-191): the same kept-state sum
         rhos = sweep(rho, None)
         for k in range(nst):
             assert abs(trace(rhos[k]) - 1.0) < 1e-10
@@ -581,6 +610,24 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                                        (fs.neg_re, fs.neg_im, cb.neg_re, cb.neg_im)):
                     O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(fs.energies),
                                                  fs.nbins, Emin_w, Ex, Emax_w, flags, NNtanh, 1 if NN2avg else 0)
+            cfs_algos = [a for a in algos if a.startswith("CFS")]
+            if cfs_algos:
+                # Algo_CFSgt / Algo_CFSls::calc (c++/algo_CFS.hpp:28-53, 80-105) with Ip = Ii,
+                # I1 = Ij; op(r1, rp) has r1 in Ij, rp in Ii; abs_zero energies of all states
+                cbs = {w: O.ChainBinning(lmin, lmax, bins, discard_imm) for w in ("gt", "ls")}
+                for Ii, ei, Ij, ej in pairs:
+                    ki, kj = ei.nrpost, ej.nrpost
+                    Ei = (ei.values - ei.shift) * scale
+                    Ej = (ej.values - ej.shift) * scale
+                    terms = cfs_terms(last, Ei, ki, Ej, kj, op1[(Ij, Ii)], op2[(Ij, Ii)],
+                                      None if last else rhos[k][Ii], None if last else rhos[k][Ij], sign, T, Zft)
+                    for w, (E, wt) in terms.items():
+                        if E.size:
+                            cbs[w].add(E, wt, ff(Ii, Ij))
+                for a in cfs_algos:  # mergeCFS
+                    for w in {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}[a]:
+                        for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
+                            getattr(full[a], arr)[:] += getattr(cbs[w], arr)
             fdm_algos = [a for a in algos if a.startswith("FDM")]
             if fdm_algos:
                 cbs = {w: O.ChainBinning(lmin, lmax, bins, discard_imm) for w in ("gt", "ls")}
