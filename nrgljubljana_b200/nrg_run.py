@@ -79,6 +79,8 @@ class RunParams:
     cfs: bool = False
     cfsgt: bool = False
     cfsls: bool = False
+    # conventional finite-temperature spectra (c++/params.hpp, "finite"; Algo_FT)
+    finite: bool = False
     data_has_rescaled_energies: bool = True
     # DM-NRG spectra of the specs/specd/spect pairs (c++/params.hpp:181-396)
     T: float = 0.001
@@ -153,7 +155,7 @@ class RunParams:
         """The real-frequency spectral algorithms switched on (c++/oprecalc.hpp:123-131)."""
         return [a for a, on in (("DMNRG", self.dmnrg), ("FDM", self.fdm), ("FDMgt", self.fdmgt),
                                 ("FDMls", self.fdmls), ("CFS", self.cfs), ("CFSgt", self.cfsgt),
-                                ("CFSls", self.cfsls)) if on]
+                                ("CFSls", self.cfsls), ("FT", self.finite)) if on]
 
     @property
     def keep_all_states_in_last_step(self) -> bool:
@@ -981,6 +983,7 @@ class QSRun:
         cfs_parts_of = {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}
         cfs_parts = sorted({w for a in self.algos if a in cfs_parts_of for w in cfs_parts_of[a]})
         cfs_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in cfs_parts}
+        ft_acc = {j: (np.zeros(nb), np.zeros(nb)) for j in range(len(self.specs))} if "FT" in self.algos else {}
         cur = dict(self.spec_init)
         expv = None
         for k, st in enumerate(steps):
@@ -1062,6 +1065,8 @@ class QSRun:
                             spec_accumulate_array(algo, np.array(prs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
                                                   sign=sign, T=p.T, wnf=fdm["wnfactor"][k], ctx=self.ctx,
                                                   stream=self.stream)
+            if "FT" in self.algos and merge and self.specs:
+                self._ft_step(st, cur, kinds, grid, ebins, Efac, ft_acc)
             if cfs_parts and self.specs:
                 self._cfs_step(st, last, None if last else rhos[k], cur, kinds, grid, cfs_parts, cfs_acc)
             if fdm is not None and p.fdmexpv and st.N == p.fdmexpvn:
@@ -1080,6 +1085,8 @@ class QSRun:
             for a in self.algos:
                 if a == "DMNRG":
                     full_pos, full_neg = dm_acc[j]
+                elif a == "FT":
+                    full_pos, full_neg = ft_acc[j]
                 elif a in cfs_parts_of:
                     full_pos = sum(cfs_acc[(j, w)][0] for w in cfs_parts_of[a]).cpu().numpy()
                     full_neg = sum(cfs_acc[(j, w)][1] for w in cfs_parts_of[a]).cpu().numpy()
@@ -1092,6 +1099,58 @@ class QSRun:
                 if p.savebins:
                     raw[name] = raw_bins(full_pos, full_neg, ebins, p.discard_trim, p.reim)
         return out, raw, expv
+
+    def _ft_step(self, st: "_StepRecord", cur: Dict, kinds: Dict, grid: BinGrid, ebins: np.ndarray, Efac: float,
+                 ft_acc: Dict) -> None:
+        """Algo_FT::calc (c++/algo_FT.hpp:28-43) of one step for every spectrum: over kept(Ij) x
+        kept(Ii), op1 op2 ((-sign) e^{-E1/T} + e^{-Ep/T}) / Z_ft at E1 - Ep, with the abs_zero
+        energies and stats.Zft of this step (calc_Z, c++/measurements.hpp:189-191). The two
+        exponentials are the FDMls and the FDMgt D x D terms of the pair cut to its kept states
+        (K = 0) with wnf = 1/Z_ft, accumulated into one bin set; the step's bins are then merged
+        with the N/N+2 window (mergeNN2half, c++/spectrum.hpp:114-128) as for DMNRG."""
+        p = self.p
+        dg = st.diag
+        scT = st.scale / p.T
+        Z = sum(qs.mult(I) * float(np.sum(np.exp(-s.corr[:s.nkept] * scT))) for I, s in dg.items())
+        eoff, flat, o = {}, [], 0
+        for I, s in dg.items():  # abs_zero energies of the kept states (c++/eigen.hpp:45)
+            eoff[I] = o
+            flat.append((s.values[:s.nkept] - s.shift) * st.scale)
+            o += s.nkept
+        Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+        eb = Edev.data_ptr()
+        Emin_w = st.scale * p.goodE
+        Ex, Emax_w = Emin_w * Efac, Emin_w * Efac * Efac
+        win = window(ebins, Emin_w, Ex, Emax_w, st.N == self.nmax - 1, st.N == 0, p.NNtanh)
+        inside = (Emin_w < ebins) & (ebins < Emax_w)
+        f = 0.5 if p.NN2avg else 1.0
+        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+            sign, ff, names = kinds[kind]
+            ops = cur[kind]
+            o1, o2 = names.index(n1), names.index(n2)
+            prs = []
+            for Ii, si in dg.items():
+                for Ij, sj in dg.items():
+                    key = Ii if kind == "s" else (Ij, Ii)
+                    if (kind == "s" and Ij != Ii) or key not in ops.loc:
+                        continue
+                    ki, kj = si.nkept, sj.nkept
+                    if ki == 0 or kj == 0:
+                        continue
+                    ld = ops.loc[key][2]
+                    prs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2), ld,
+                                0, 1, 0, 1, ki, 0, kj, 0, 0, 0, ff(Ii, Ij)))
+            if not prs:
+                continue
+            arr = np.array(prs, dtype=SPECPAIR_DTYPE)
+            pos = torch.zeros(grid.nbins, dtype=torch.float64, device=self.dev)
+            neg = torch.zeros(grid.nbins, dtype=torch.float64, device=self.dev)
+            for algo in (NRG_SPEC_FDMGT, NRG_SPEC_FDMLS):
+                spec_accumulate_array(algo, arr, grid, pos, neg, sign=sign, T=p.T, wnf=1.0 / Z, ctx=self.ctx,
+                                      stream=self.stream)
+            for full, cs in zip(ft_acc[j], (pos.cpu().numpy(), neg.cpu().numpy())):
+                sel = inside & (cs != 0.0)
+                full[sel] += f * cs[sel] * win[sel]
 
     def _cfs_step(self, st: "_StepRecord", last: bool, rhoN: Optional[MatSet], cur: Dict, kinds: Dict,
                   grid: BinGrid, cfs_parts: List[str], cfs_acc: Dict) -> None:

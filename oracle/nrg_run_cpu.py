@@ -136,7 +136,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
     # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
     algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"),
-                            ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls")) if flag(k)]
+                            ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls"), ("FT", "finite")) if flag(k)]
     dm = spectra is not None and bool(algos)
     fdm_needed = fdm_flags and (spectra is not None or fdm_out is not None)
     total_energy = d.gs_energy  # Stats::total_energy (c++/stats.hpp:60-71)
@@ -452,6 +452,16 @@ def cfs_terms(last, Ei, ki, Ej, kj, o1, o2, rho_i, rho_j, sign, T, Zft):
     return {"gt": (E_gt, w_gt), "ls": (E_ls, w_ls)}
 
 
+def ft_terms(Ei, Ej, o1, o2, sign, T, Z):
+    """The (energy, weight) terms of Algo_FT::calc (c++/algo_FT.hpp:28-43) for one pair in the
+    reference's loop order (r1 in kept(I1 = Ij) outer, rp in kept(Ip = Ii) inner): Ei, Ej the
+    abs_zero energies of the kept states, o1, o2 the kept x kept blocks of op(Ij, Ii), Z the
+    step's Z_ft. Weight op1 op2 ((-sign) e^{-E1/T} + e^{-Ep/T}) / Z at energy E1 - Ep."""
+    E = (Ej[:, None] - Ei[None, :]).ravel()
+    stat = ((-sign) * np.exp(-Ej[:, None] / T) + np.exp(-Ei[None, :] / T)) / Z
+    return E, (o1 * o2 * stat).ravel()
+
+
 def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None):
     """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
     calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
@@ -606,6 +616,27 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                 Ex = scale * goodE * Efac
                 flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
                 fs = full["DMNRG"]
+                for fr, fi, cr, ci in ((fs.pos_re, fs.pos_im, cb.pos_re, cb.pos_im),
+                                       (fs.neg_re, fs.neg_im, cb.neg_re, cb.neg_im)):
+                    O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(fs.energies),
+                                                 fs.nbins, Emin_w, Ex, Emax_w, flags, NNtanh, 1 if NN2avg else 0)
+            if "FT" in algos and (NN1 or NN2avg or (N % 2 == 0 if NN2even else N % 2 == 1)):
+                # Algo_FT with stats.Zft of this step (calc_Z, c++/measurements.hpp:189-191), merged
+                # with the N/N+2 window as DMNRG (mergeNN2)
+                scT = scale / T
+                Zk = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrpost]) for I, e in diagN.items())
+                cb = O.ChainBinning(lmin, lmax, bins, discard_imm)
+                for Ii, ei, Ij, ej in pairs:
+                    ki, kj = ei.nrpost, ej.nrpost
+                    if not (ki and kj):
+                        continue
+                    E, wt = ft_terms((ei.values[:ki] - ei.shift) * scale, (ej.values[:kj] - ej.shift) * scale,
+                                     op1[(Ij, Ii)][:kj, :ki], op2[(Ij, Ii)][:kj, :ki], sign, T, Zk)
+                    cb.add(E, wt, ff(Ii, Ij))
+                Emin_w, Emax_w = scale * goodE, scale * goodE * Efac * Efac
+                Ex = scale * goodE * Efac
+                flags = (1 if N == Nmax - 1 else 0) | (2 if N == 0 else 0)
+                fs = full["FT"]
                 for fr, fi, cr, ci in ((fs.pos_re, fs.pos_im, cb.pos_re, cb.pos_im),
                                        (fs.neg_re, fs.neg_im, cb.neg_re, cb.neg_im)):
                     O.lib().oracle_merge_nn2half(O._ptr(fr), O._ptr(fi), O._ptr(cr), O._ptr(ci), O._ptr(fs.energies),

@@ -25,10 +25,10 @@ CASES = [
     "test61_discard_trim", "test64_emax", "test66_fdmexpvn", "legacy_fdmexpv2", "legacy_fdmexpv3",
     "regr2defaults", "regr2lastall_false", "regr2lastall_true", "legacy_one_jkondonew",
     "c++sym_all/test314_model=ZERO",
-    "test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only",
+    "test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only", "test2_algorithms", "test11_T",
 ]
-# spectra of the DM-NRG, FDM and CFS algorithms, FDM thermodynamics and expectation values
-SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls|CFS|CFSgt|CFSls)_dens_.*\.dat$")
+# spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values
+SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls|CFS|CFSgt|CFSls|FT)_dens_.*\.dat$")
 
 
 def main(ref_root: str) -> None:

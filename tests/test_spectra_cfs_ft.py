@@ -1,11 +1,15 @@
-"""Complete-Fock-space (CFS) spectra of whole runs against the reference's regression outputs
-({spec,corr,spin}_{CFS,CFSgt,CFSls}_dens_*.dat of test/c++/test2_algorithms_cfs,
-test2_algorithms_cfsgtls and test_cfs_only): the DM-NRG density matrices, the operators of
-the spectra recalculated over all states, the last step's kept-kept term with Boltzmann
-weights over Z_ft and, at the other steps, the discarded-kept terms with rho (Algo_CFSgt,
-Algo_CFSls, c++/algo_CFS.hpp), merged whole, trimmed and broadened. The device run builds
-these terms from the FDM pair modes of nrg_spec_accumulate; `test_cfs_terms_by_fdm_modes`
-checks that composition term by term with the oracle's own CFS and FDM pair sums."""
+"""Complete-Fock-space (CFS) and conventional finite-temperature (FT) spectra of whole runs
+against the reference's regression outputs: {spec,corr,spin}_{CFS,CFSgt,CFSls}_dens_*.dat of
+test/c++/test2_algorithms_cfs, test2_algorithms_cfsgtls and test_cfs_only, and every
+spectrum (DMNRG, FDM, CFS, FT) and the FDM expectation values of test2_algorithms and
+test11_T, which run the four algorithms together.
+CFS (Algo_CFSgt, Algo_CFSls, c++/algo_CFS.hpp): the DM-NRG density matrices, the operators
+recalculated over all states, the last step's kept-kept term with Boltzmann weights over
+Z_ft and, at the other steps, the discarded-kept terms with rho, merged whole. FT (Algo_FT,
+c++/algo_FT.hpp): kept-kept terms with ((-sign) e^{-E1/T} + e^{-Ep/T}) / Z_ft of the step,
+merged with the N/N+2 window. The device run builds both from the FDM pair modes of
+nrg_spec_accumulate; `test_cfs_terms_by_fdm_modes` and `test_ft_terms_by_fdm_modes` check
+that composition bin by bin with the oracle's direct terms and its FDM pair sums."""
 import os
 
 import numpy as np
@@ -16,6 +20,8 @@ from test_dmnrg import ATOL_REL_TO_MAX, ORA_ATOL_REL_TO_MAX, ORA_RTOL, RTOL, ass
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
 CFS_CASES = ["test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only"]
+ALL_CASES = ["test2_algorithms", "test11_T"]  # DMNRG + FDM + CFS + FT, fdmexpv
+TAB_RTOL = 2e-9  # customfdm printed to 10 significant digits
 
 
 def read(case, name):
@@ -39,33 +45,45 @@ def oracle_cfs(oracle):
 
     def get(case):
         if case not in cache:
-            spec = {}
-            nrg_run_cpu.run(read(case, "param"), read(case, "data"), threads=os.cpu_count() or 1, spectra=spec)
-            cache[case] = spec
+            spec, fo = {}, {}
+            nrg_run_cpu.run(read(case, "param"), read(case, "data"), threads=os.cpu_count() or 1, spectra=spec,
+                            fdm_out=fo)
+            cache[case] = (spec, fo)
         return cache[case]
     return get
 
 
-@pytest.mark.parametrize("case", CFS_CASES)
+def assert_customfdm(got, case, what):
+    if os.path.exists(os.path.join(GOLD, case, "customfdm")):
+        want = rows(case, "customfdm")[-1]
+        got = np.asarray(got, dtype=float)
+        assert got.shape == want.shape and np.all(np.abs(got - want) <= TAB_RTOL * np.abs(want) + 1e-300), what
+
+
+@pytest.mark.parametrize("case", CFS_CASES + ALL_CASES)
 def test_oracle_cfs_spectra_match_reference(oracle_cfs, case):
-    spec = oracle_cfs(case)
+    spec, fo = oracle_cfs(case)
     assert sorted(spec) == spectrum_files(case)
     for name in spectrum_files(case):
         assert_spectrum(spec[name], rows(case, name + ".dat"), RTOL, ATOL_REL_TO_MAX, f"{case} {name}")
+    if "customfdm" in fo:
+        assert_customfdm(fo["customfdm"][1], case, case)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CFS_CASES)
+@pytest.mark.parametrize("case", CFS_CASES + ALL_CASES)
 def test_gpu_cfs_spectra(oracle_cfs, case):
-    """The device run's CFS, CFSgt and CFSls spectra against the reference and the oracle."""
+    """The device run's CFS (and FT, DMNRG, FDM) spectra against the reference and the oracle."""
     from nrgljubljana_b200.nrg_run import run_files
     res = run_files(read(case, "param"), read(case, "data"))
-    spec = oracle_cfs(case)
+    spec, fo = oracle_cfs(case)
     assert sorted(res.spectra) == spectrum_files(case)
     for name in spectrum_files(case):
         got = res.spectra[name]
         assert_spectrum(got, rows(case, name + ".dat"), RTOL, ATOL_REL_TO_MAX, f"{case} {name} vs reference")
         assert_spectrum(got, spec[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{case} {name} vs oracle")
+    if res.customfdm is not None:
+        assert_customfdm(res.customfdm[1], case, f"{case} customfdm")
 
 
 def fdm_mode_composition(cb, last, Ei, ki, Ej, kj, o1, o2, rho_i, rho_j, factor, sign, T, Zft):
@@ -110,3 +128,34 @@ def test_cfs_terms_by_fdm_modes(oracle, sign, last, keep_all):
         y = np.concatenate([comp[w].pos_re, comp[w].neg_re])
         assert np.abs(x).max() > 0.0  # one half may be empty (kept minus discarded energies are < 0)
         assert np.allclose(x, y, rtol=1e-12, atol=1e-13 * np.abs(x).max()), w
+
+
+def ft_fdm_mode_composition(cb, Ei, ki, Ej, kj, o1, o2, factor, sign, T, Z):
+    """FT of one pair as the device run forms it: the FDMgt and the FDMls D x D terms of the
+    pair cut to its kept states (K = 0) with wnf = 1/Z_ft, into one bin set."""
+    empty = np.zeros((0, 0))
+    for mode in ("gt", "ls"):
+        cb.fdm_pair(mode, Ei[:ki], 0, Ej[:kj], 0, o1[:kj, :ki], o2[:kj, :ki], empty, factor, sign, T, 1.0 / Z)
+
+
+@pytest.mark.parametrize("sign", [1, -1])
+def test_ft_terms_by_fdm_modes(oracle, sign):
+    from oracle import nrg_run_cpu
+    from oracle.oracle import ChainBinning
+    rng = np.random.default_rng(23 + sign)
+    ni, nj, ki, kj = 9, 7, 6, 5
+    Ei = np.sort(rng.uniform(0.0, 3.0, ni))
+    Ej = np.sort(rng.uniform(0.0, 3.0, nj))
+    Ei -= Ei[0]
+    Ej -= Ej[0]
+    o1, o2 = rng.standard_normal((nj, ni)), rng.standard_normal((nj, ni))
+    T, Z, f = 0.3, 2.5, 0.7
+    direct = ChainBinning(-4, 2, 50)
+    E, wt = nrg_run_cpu.ft_terms(Ei[:ki], Ej[:kj], o1[:kj, :ki], o2[:kj, :ki], sign, T, Z)
+    direct.add(E, wt, f)
+    comp = ChainBinning(-4, 2, 50)
+    ft_fdm_mode_composition(comp, Ei, ki, Ej, kj, o1, o2, f, sign, T, Z)
+    x = np.concatenate([direct.pos_re, direct.neg_re])
+    y = np.concatenate([comp.pos_re, comp.neg_re])
+    assert np.abs(x).max() > 0.0
+    assert np.allclose(x, y, rtol=1e-12, atol=1e-13 * np.abs(x).max())
