@@ -41,7 +41,7 @@ Invar = Tuple[int, int]
 # Parameters that do not change td/custom of a run without spectral functions.
 _IGNORED = {
     "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
-    "dumpannotated", "dumpscaled", "dumpabs", "dumpgroups", "dumpenergies", "ops", "diag", "diagth",
+    "dumpenergies", "ops", "diag", "diagth",
     "Nmax",
     "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
     # model parameters of the generated data and of its discretisation
@@ -110,6 +110,13 @@ class RunParams:
     # (imaginary) column, and the precision and width of the written numbers
     savebins: bool = False
     reim: bool = False
+    # annotated.dat (c++/params.hpp:312-320): the lowest `dumpannotated` levels of every step
+    dumpannotated: int = 0
+    dumpprecision: int = 8
+    dumpgroups: bool = True
+    grouptol: float = 1e-6
+    dumpscaled: bool = True
+    dumpabs: bool = False
     prec_td: int = 10
     prec_custom: int = 10
     prec_xy: int = 10
@@ -177,6 +184,7 @@ class Result:
     spectra: Dict[str, np.ndarray] = field(default_factory=dict)
     # the same stems -> rows (E, Re w[, Im w]) of the trimmed raw bins (savebins=true)
     bins: Dict[str, np.ndarray] = field(default_factory=dict)
+    annotated: List[str] = field(default_factory=list)  # lines of annotated.dat (dumpannotated > 0)
     tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
     customfdm: Optional[Tuple[List[str], List[float]]] = None   # fields, row (measure_singlet_fdm)
 
@@ -395,6 +403,13 @@ class QSRun:
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(self.dev, non_blocking=True)
 
     # ---- measurements
+    def _annotate(self, trueN: int, diag: Dict[Invar, Sub]) -> None:
+        """perform_basic_measurements' annotated.dump (c++/measurements.hpp:229-233) over all
+        computed states, before the truncation."""
+        if self.p.dumpannotated > 0:
+            entries = [(float(x), s.I) for s in diag.values() for x in (s.values - s.shift)]
+            self.res.annotated += annotated_lines(entries, self.p, self.scale(trueN), self.total_energy)
+
     def _td(self, trueN: int, diag: Dict[Invar, Sub]) -> List[float]:
         """calculate_TD (c++/measurements.hpp:169-186) with SymmetryQS::calculate_TD."""
         f = self.p.betabar  # TD_factor (unscale = 1)
@@ -470,6 +485,7 @@ class QSRun:
                         tshapes[k] = mat.shape
                 self.spec_init[kind] = MatSet(self.dev, tshapes, len(names), _pack(tmats, tshapes))
         if p.calc0:
+            self._annotate(-1, diag)
             self.res.td.append(self._td(-1, diag))
             self.meas.append(self._measure(-1, diag, self.ops))
         # diag0 has identity eigenvectors: its <||f||> and operators are used as read.
@@ -630,6 +646,7 @@ class QSRun:
             s.nkept = len(s.values) if keep_all else int(np.count_nonzero(s.corr <= Emax))
 
         # after_diag (c++/core.hpp:193-230)
+        self._annotate(N, diag)
         res.td.append(self._td(N, diag))
         new_ops = ops
         if p.strategy == "all":
@@ -1252,6 +1269,47 @@ class QSRun:
         rows_neg = sorted(zip(mesh_all[npos:].tolist(), vals[npos:].tolist()))
         return np.array(rows_neg + rows_pos)
 
+def my_fcmp(x: float, y: float, eps: float) -> int:
+    """my_fcmp (c++/numerics.hpp:107-114) with one epsilon: 0 when x and y are both zero, both
+    below eps in magnitude, or closer than eps * (|x| + |y|); else the sign of x - y."""
+    if (x == 0.0 and y == 0.0) or (abs(x) < eps and abs(y) < eps) or abs(x - y) < eps * (abs(x) + abs(y)):
+        return 0
+    return 1 if x > y else -1
+
+
+def annotated_lines(entries: List[Tuple[float, Invar]], p: "RunParams", scale: float, total_energy: float) -> List[str]:
+    """Annotated::dump (c++/output.hpp:77-125) for one step: `entries` are (energy relative to
+    the step's ground state, subspace) of all computed states. The lowest p.dumpannotated of
+    them, extended while the next one is within p.grouptol of the last (a cluster is dumped
+    whole), one line per group of levels within p.grouptol of its first, "E (Q SS) ...
+    [multiplicity]" with the labels sorted as strings (dumpgroups), or one line "E Q SS" per
+    level; E in units of the step (dumpscaled) or times `scale`, plus `total_energy` with
+    dumpabs; a blank line ends the step."""
+    lst = sorted(entries)
+    n = min(len(lst), p.dumpannotated)
+    while n < len(lst) - 1 and my_fcmp(lst[n][0], lst[n - 1][0], p.grouptol) == 0:
+        n += 1
+
+    def num(x: float) -> str:
+        return f"{x * (1.0 if p.dumpscaled else scale) + (total_energy if p.dumpabs else 0.0):.{p.dumpprecision}g}"
+    out = []
+    if p.dumpgroups:
+        i = 0
+        while i < n:
+            e0 = lst[i][0]
+            labels, deg = [], 0
+            while i < n and my_fcmp(lst[i][0], e0, p.grouptol) == 0:
+                I = lst[i][1]
+                labels.append(f"{I[0]} {I[1]}")
+                deg += qs.mult(I)
+                i += 1
+            out.append(num(e0) + "".join(f" ({q})" for q in sorted(labels)) + f" [{deg}]")
+    else:
+        out.extend(f"{num(e)} {I[0]} {I[1]}" for e, I in lst[:n])
+    out.append("")
+    return out
+
+
 def trim_bins(ebins: np.ndarray, w: np.ndarray, discard_trim: float) -> Tuple[np.ndarray, np.ndarray]:
     """Bins::trim (c++/bins.hpp:165-185) of one half: bin i (energy ebins[i], weight w[i]) is
     kept if |w[i]| >= discard_trim * (ebins[i+1] - ebins[i]); the last bin is always kept."""
@@ -1359,6 +1417,9 @@ def write_outputs(out: str, p: RunParams, res: Result) -> None:
                 f.write(f"{e:.{p.prec_xy}g} {v:.{p.prec_xy}g}" + (" 0\n" if p.reim else "\n"))
     for name, rows in res.bins.items():
         write_bins(os.path.join(out, f"{name}.bin"), rows)
+    if p.dumpannotated > 0:
+        with open(os.path.join(out, "annotated.dat"), "w") as f:
+            f.write("\n".join(res.annotated) + ("\n" if res.annotated else ""))
 
 
 if __name__ == "__main__":

@@ -91,7 +91,8 @@ class _Eig:
 
 
 def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None,
-        bins_out: dict = None) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+        bins_out: dict = None, annotated_out: list = None, annotated_entries: list = None
+        ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
     """td and custom rows of the run; with a `spectra` dict, also the spectra of the specs,
     specd and spect pairs for the algorithms dmnrg, fdm, fdmgt, fdmls that are switched on
     (file stem, e.g. spec_DMNRG_dens_A_d-A_d -> array of (E, A(E)) rows as written to that
@@ -99,7 +100,10 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     and, with fdmexpv, fdm_out["customfdm"] (fields, row); with a `bins_out` dict and a
     `spectra` dict, also the trimmed raw bins of every spectrum as savebins writes them
     (SpectrumRealFreq::savebins, c++/spectrum.hpp:146-170): rows (E, Re w), or (E, Re w, Im w)
-    with reim=true, the positive energies ascending, then -|E| by ascending |E|."""
+    with reim=true, the positive energies ascending, then -|E| by ascending |E|; with an
+    `annotated_out` list, the lines of annotated.dat (Annotated::dump, c++/output.hpp:77-125)
+    for dumpannotated > 0 (and, in `annotated_entries`, each step's (energy, subspace) pairs
+    with its scale and total energy, the formatter's input)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -183,7 +187,49 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             row.append(tr / Z)
         custom_rows.append(row)
 
+    dumpannotated = int(kv.get("dumpannotated", 0))
+
+    def annotate(diag, scale):
+        """Annotated::dump (c++/output.hpp:77-125): the lowest dumpannotated energies of all
+        computed states (extended over a cluster at the cut), grouped by degeneracy with
+        my_fcmp (c++/numerics.hpp:107-114) at grouptol."""
+        if annotated_out is None or dumpannotated <= 0:
+            return
+        tol = float(kv.get("grouptol", 1e-6))
+        prec = int(kv.get("dumpprecision", 8))
+        groups = kv.get("dumpgroups", "true").lower() == "true"
+        scaled = kv.get("dumpscaled", "true").lower() == "true"
+        absolute = kv.get("dumpabs", "false").lower() == "true"
+
+        def cmp(x, y):
+            if (x == 0.0 and y == 0.0) or (abs(x) < tol and abs(y) < tol) or abs(x - y) < tol * (abs(x) + abs(y)):
+                return 0
+            return 1 if x > y else -1
+        if annotated_entries is not None:
+            annotated_entries.append(([(x - e.shift, I) for I, e in diag.items() for x in e.values], scale, total_energy))
+        lst = sorted((x - e.shift, I) for I, e in diag.items() for x in e.values)
+        n = min(len(lst), dumpannotated)
+        while n < len(lst) - 1 and cmp(lst[n][0], lst[n - 1][0]) == 0:
+            n += 1
+
+        def num(x):
+            return "%.*g" % (prec, x * (1.0 if scaled else scale) + (total_energy if absolute else 0.0))
+        if groups:
+            i = 0
+            while i < n:
+                e0 = lst[i][0]
+                names, deg = [], 0
+                while i < n and cmp(lst[i][0], e0) == 0:
+                    names.append("%d %d" % lst[i][1])
+                    deg += lst[i][1][1]  # multiplicity of a QS subspace: 2S+1 = SS
+                    i += 1
+                annotated_out.append(num(e0) + "".join(" (%s)" % q for q in sorted(names)) + " [%d]" % deg)
+        else:
+            annotated_out.extend("%s %d %d" % (num(e), I[0], I[1]) for e, I in lst[:n])
+        annotated_out.append("")
+
     if kv.get("calc0", "true").lower() == "true":
+        annotate(diag, SCALE(0, Lam, disc, z))
         td(-1, diag)
         custom(-1, diag, ops)
 
@@ -255,6 +301,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             e.nrpost = len(e.values) if (last and lastall) else int(sum(1 for c in e.corr if c <= Emax))
         # after_diag
         total_energy += Egs * scale  # Stats::update (c++/stats.hpp:65-71)
+        annotate(new, scale)
         td(N, new)
         ops_prev = ops
         for I, e in new.items():

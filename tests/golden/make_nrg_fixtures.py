@@ -27,7 +27,8 @@ CASES = [
     "c++sym_all/test314_model=ZERO",
     "test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only", "test2_algorithms", "test11_T",
 ]
-# spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values
+# spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
+# and the annotated eigenvalue lists (annotated.dat)
 SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls|CFS|CFSgt|CFSls|FT)_dens_.*\.dat$")
 
 
@@ -39,7 +40,7 @@ def main(ref_root: str) -> None:
         dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
         extra = [f for f in sorted(os.listdir(os.path.join(src, "ref")))
-                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm")]
+                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm", "annotated.dat")]
         for name, rel in [("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")] + \
                 [(f, "ref/" + f) for f in extra]:
             p = os.path.join(src, rel)

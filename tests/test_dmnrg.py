@@ -84,7 +84,8 @@ DM2_CASES = ["regr2defaults", "regr2lastall_false", "regr2lastall_true"]
 
 
 def spectrum_names(case):
-    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case)) if f.endswith(".dat"))
+    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case))
+                  if f.endswith(".dat") and f.startswith(("spec_", "corr_", "spin_")))
 
 
 @pytest.mark.parametrize("case", DM2_CASES)

@@ -34,7 +34,8 @@ def rows(case, name):
 
 
 def spectrum_files(case):
-    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case)) if f.endswith(".dat"))
+    return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case))
+                  if f.endswith(".dat") and f.startswith(("spec_", "corr_", "spin_")))
 
 
 def assert_row(got, want, what):

@@ -86,6 +86,14 @@ def test_param_reader_rejects_unsupported():
             RunParams.from_param(parse_param("[param]\n" + bad + "\n"))
 
 
+def test_param_reader_accepts_every_fixture():
+    """Every regression input the GPU tests run is accepted by the driver's parameter reader."""
+    from nrgljubljana_b200.inputs import parse_param
+    from nrgljubljana_b200.nrg_run import RunParams
+    for case in CASES:
+        RunParams.from_param(parse_param(read(case, "param")))
+
+
 def test_cluster_mapping_quirks():
     # c++/splitting.hpp:48-72: split clusters map to their lowest member; the last cluster
     # is never closed, so its members stay as they are.
