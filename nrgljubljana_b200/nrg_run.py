@@ -358,6 +358,10 @@ class QSRun:
     def __init__(self, params: RunParams, data: DataFile, device: int = 0, ctx: Optional[Context] = None):
         if data.symtype != "QS" or data.channels not in (1, 2):
             raise ValueError("the driver covers symtype QS with one or two channels")
+        if data.nmax == 0 and params.algorithms:
+            # Params::ZBW (Nmax = 0): the reference bins the initial cluster's spectra with its own
+            # window rules (c++/spectrum.hpp:91-95); not restated here
+            raise ValueError("zero-bandwidth runs (Nmax = 0) with spectral functions are not supported")
         self.T = qs.tables(data.channels)
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device: the QS run driver has no CPU fallback")

@@ -26,6 +26,11 @@ CASES = [
     "regr2defaults", "regr2lastall_false", "regr2lastall_true", "legacy_one_jkondonew",
     "c++sym_all/test314_model=ZERO",
     "test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only", "test2_algorithms", "test11_T",
+    "test0_minimal_Nmax1_td", "test0_minimal_Nmax2_td", "test0_minimal_Nmax3_td", "test17_dumpannotated",
+    "test18_dumpscaled", "test19_dumpabs", "test20_dumpgroups", "test24_NN1_Nmax=10", "test24_NN1_Nmax=11",
+    "test27_NN2odd", "test2_algorithms_finite", "test30_cosine_band", "test31_flat_band", "test55_gt_ls",
+    "test58_dsyev", "test5_disc_y", "test62_dumpenergies", "test67_fixeps", "test68_grouptol", "test8_keep",
+    "test9_keepenergy",
 ]
 # spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)

@@ -1,7 +1,7 @@
 """annotated.dat (Annotated::dump, c++/output.hpp:77-125): the lowest `dumpannotated` energies
 of every step's computed states (and of the initial subspaces, calc0), extended over a
 degenerate cluster at the cut and grouped by degeneracy, "E (Q SS) ... [multiplicity]".
-The oracle against the reference's files of 18 regression cases; the run driver's formatter
+The oracle against the reference's files of every regression case that has one; the run driver's formatter
 (nrg_run.annotated_lines) against the oracle on the same cases and on hand-made edge cases;
 the device run against the reference."""
 import os
@@ -54,7 +54,7 @@ def oracle_annotated(oracle):
 
 
 def test_cases_present():
-    assert len(CASES) == 18
+    assert len(CASES) >= 18
 
 
 @pytest.mark.parametrize("case", CASES)

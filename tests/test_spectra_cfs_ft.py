@@ -20,7 +20,8 @@ from test_dmnrg import ATOL_REL_TO_MAX, ORA_ATOL_REL_TO_MAX, ORA_RTOL, RTOL, ass
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
 CFS_CASES = ["test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only"]
-ALL_CASES = ["test2_algorithms", "test11_T"]  # DMNRG + FDM + CFS + FT, fdmexpv
+ALL_CASES = ["test2_algorithms", "test11_T", "test55_gt_ls",  # DMNRG + FDM + CFS + FT (and gt/ls parts)
+             "test2_algorithms_finite"]  # FT alone
 TAB_RTOL = 2e-9  # customfdm printed to 10 significant digits
 
 
