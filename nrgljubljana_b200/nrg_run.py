@@ -41,7 +41,7 @@ Invar = Tuple[int, int]
 # Parameters that do not change td/custom of a run without spectral functions.
 _IGNORED = {
     "symtype", "model", "U", "Gamma", "delta", "band", "Tmin", "checksumrules", "logall", "log",
-    "dumpenergies", "ops", "diag", "diagth",
+    "ops", "diag", "diagth",
     "Nmax",
     "variant", "spin", "Jkondo", "Jkondo1", "Jkondo2",
     # model parameters of the generated data and of its discretisation
@@ -117,6 +117,7 @@ class RunParams:
     grouptol: float = 1e-6
     dumpscaled: bool = True
     dumpabs: bool = False
+    dumpenergies: bool = False  # energies.nrg: every computed level of every step
     prec_td: int = 10
     prec_custom: int = 10
     prec_xy: int = 10
@@ -185,6 +186,7 @@ class Result:
     # the same stems -> rows (E, Re w[, Im w]) of the trimmed raw bins (savebins=true)
     bins: Dict[str, np.ndarray] = field(default_factory=dict)
     annotated: List[str] = field(default_factory=list)  # lines of annotated.dat (dumpannotated > 0)
+    energies: List[str] = field(default_factory=list)   # blocks of energies.nrg (dumpenergies)
     tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
     customfdm: Optional[Tuple[List[str], List[float]]] = None   # fields, row (measure_singlet_fdm)
 
@@ -413,6 +415,8 @@ class QSRun:
         if self.p.dumpannotated > 0:
             entries = [(float(x), s.I) for s in diag.values() for x in (s.values - s.shift)]
             self.res.annotated += annotated_lines(entries, self.p, self.scale(trueN), self.total_energy)
+        if self.p.dumpenergies:  # Output::dump_energies with the step index max(N, 0)
+            self.res.energies.append(energies_block(max(trueN, 0), {s.I: s.values for s in diag.values()}))
 
     def _td(self, trueN: int, diag: Dict[Invar, Sub]) -> List[float]:
         """calculate_TD (c++/measurements.hpp:169-186) with SymmetryQS::calculate_TD."""
@@ -1314,6 +1318,18 @@ def annotated_lines(entries: List[Tuple[float, Invar]], p: "RunParams", scale: f
     return out
 
 
+def energies_block(label: int, levels: Dict[Invar, np.ndarray]) -> str:
+    """Output::dump_energies (c++/output.hpp:157-161) with DiagInfo::dump_energies
+    (c++/eigen.hpp:349-352): "===== Iteration number: <label>" after a blank line, then every
+    subspace in order, "Subspace: Q SS" and its raw eigenvalues (Values::all_rel, the
+    ground-state shift not subtracted), each followed by a space, in the default 6-digit form
+    of a C++ stream."""
+    text = f"\n===== Iteration number: {label}\n"
+    for I in sorted(levels):
+        text += f"Subspace: {I[0]} {I[1]}\n" + "".join(f"{x:g} " for x in levels[I]) + "\n"
+    return text
+
+
 def trim_bins(ebins: np.ndarray, w: np.ndarray, discard_trim: float) -> Tuple[np.ndarray, np.ndarray]:
     """Bins::trim (c++/bins.hpp:165-185) of one half: bin i (energy ebins[i], weight w[i]) is
     kept if |w[i]| >= discard_trim * (ebins[i+1] - ebins[i]); the last bin is always kept."""
@@ -1421,6 +1437,9 @@ def write_outputs(out: str, p: RunParams, res: Result) -> None:
                 f.write(f"{e:.{p.prec_xy}g} {v:.{p.prec_xy}g}" + (" 0\n" if p.reim else "\n"))
     for name, rows in res.bins.items():
         write_bins(os.path.join(out, f"{name}.bin"), rows)
+    if p.dumpenergies:
+        with open(os.path.join(out, "energies.nrg"), "w") as f:
+            f.write("".join(res.energies))
     if p.dumpannotated > 0:
         with open(os.path.join(out, "annotated.dat"), "w") as f:
             f.write("\n".join(res.annotated) + ("\n" if res.annotated else ""))

@@ -91,8 +91,8 @@ class _Eig:
 
 
 def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None,
-        bins_out: dict = None, annotated_out: list = None, annotated_entries: list = None
-        ) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+        bins_out: dict = None, annotated_out: list = None, annotated_entries: list = None,
+        energies_out: list = None) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
     """td and custom rows of the run; with a `spectra` dict, also the spectra of the specs,
     specd and spect pairs for the algorithms dmnrg, fdm, fdmgt, fdmls that are switched on
     (file stem, e.g. spec_DMNRG_dens_A_d-A_d -> array of (E, A(E)) rows as written to that
@@ -103,7 +103,8 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     with reim=true, the positive energies ascending, then -|E| by ascending |E|; with an
     `annotated_out` list, the lines of annotated.dat (Annotated::dump, c++/output.hpp:77-125)
     for dumpannotated > 0 (and, in `annotated_entries`, each step's (energy, subspace) pairs
-    with its scale and total energy, the formatter's input)."""
+    with its scale and total energy, the formatter's input); with an `energies_out` list and
+    dumpenergies=true, the text of energies.nrg (Output::dump_energies, c++/output.hpp:157-161)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -189,6 +190,19 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
 
     dumpannotated = int(kv.get("dumpannotated", 0))
 
+    def dump_energies(diag, trueN):
+        """Output::dump_energies with DiagInfo::dump_energies (c++/eigen.hpp:349-352): per call
+        a header with the step index max(N, 0), then every subspace in order with its raw
+        eigenvalues (all_rel: the ground-state shift is not subtracted), printed as a C++
+        stream prints a vector of doubles."""
+        if energies_out is None or not flag("dumpenergies"):
+            return
+        text = "\n===== Iteration number: %d\n" % max(trueN, 0)
+        for I in sorted(diag):
+            e = diag[I]
+            text += "Subspace: %d %d\n" % I + "".join("%g " % x for x in e.values) + "\n"
+        energies_out.append(text)
+
     def annotate(diag, scale):
         """Annotated::dump (c++/output.hpp:77-125): the lowest dumpannotated energies of all
         computed states (extended over a cluster at the cut), grouped by degeneracy with
@@ -229,6 +243,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         annotated_out.append("")
 
     if kv.get("calc0", "true").lower() == "true":
+        dump_energies(diag, -1)
         annotate(diag, SCALE(0, Lam, disc, z))
         td(-1, diag)
         custom(-1, diag, ops)
@@ -301,6 +316,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             e.nrpost = len(e.values) if (last and lastall) else int(sum(1 for c in e.corr if c <= Emax))
         # after_diag
         total_energy += Egs * scale  # Stats::update (c++/stats.hpp:65-71)
+        dump_energies(new, N)
         annotate(new, scale)
         td(N, new)
         ops_prev = ops

@@ -45,7 +45,7 @@ def main(ref_root: str) -> None:
         dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
         extra = [f for f in sorted(os.listdir(os.path.join(src, "ref")))
-                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm", "annotated.dat")]
+                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm", "annotated.dat", "energies.nrg")]
         for name, rel in [("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")] + \
                 [(f, "ref/" + f) for f in extra]:
             p = os.path.join(src, rel)

@@ -1,14 +1,17 @@
-"""annotated.dat (Annotated::dump, c++/output.hpp:77-125): the lowest `dumpannotated` energies
+"""annotated.dat and energies.nrg.
+annotated.dat (Annotated::dump, c++/output.hpp:77-125): the lowest `dumpannotated` energies
 of every step's computed states (and of the initial subspaces, calc0), extended over a
 degenerate cluster at the cut and grouped by degeneracy, "E (Q SS) ... [multiplicity]".
 The oracle against the reference's files of every regression case that has one; the run driver's formatter
 (nrg_run.annotated_lines) against the oracle on the same cases and on hand-made edge cases;
-the device run against the reference."""
+the device run against the reference. energies.nrg (Output::dump_energies,
+c++/output.hpp:157-161, dumpenergies=true): every computed level of every step by subspace,
+the oracle and the device run against the reference's file, the formatter on a hand-made step."""
 import os
 
 import pytest
 
-from nrgljubljana_b200.nrg_run import RunParams, annotated_lines
+from nrgljubljana_b200.nrg_run import RunParams, annotated_lines, energies_block
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
@@ -97,3 +100,56 @@ def test_gpu_annotated(case):
     from nrgljubljana_b200.nrg_run import run_files
     res = run_files(read(case, "param"), read(case, "data"))
     assert_annotated(res.annotated, read(case, "annotated.dat"), f"{case} (device run)")
+
+
+ENERGY_CASES = sorted(c for c in os.listdir(GOLD) if os.path.exists(os.path.join(GOLD, c, "energies.nrg")))
+
+
+def parse_energies(text):
+    """[(label, [((Q, SS), [levels])])] of an energies.nrg text."""
+    blocks = []
+    for line in text.split("\n"):
+        if line.startswith("===== Iteration number: "):
+            blocks.append((int(line.split(":")[1]), []))
+        elif line.startswith("Subspace: "):
+            q, ss = line.split()[1:3]
+            blocks[-1][1].append(((int(q), int(ss)), None))
+        elif line.strip():
+            I, _ = blocks[-1][1][-1]
+            blocks[-1][1][-1] = (I, [float(x) for x in line.split()])
+    return blocks
+
+
+def assert_energies(got_text, want_text, what):
+    got, want = parse_energies(got_text), parse_energies(want_text)
+    assert [(lab, [I for I, _ in subs]) for lab, subs in got] == [(lab, [I for I, _ in subs]) for lab, subs in want], what
+    for (lab, gs), (_, ws) in zip(got, want):
+        for (I, g), (_, w) in zip(gs, ws):
+            assert len(g) == len(w) and all(abs(a - b) <= 1e-5 * abs(b) + 1e-9 for a, b in zip(g, w)), (what, lab, I)
+
+
+def test_energy_cases_present():
+    assert ENERGY_CASES == ["test62_dumpenergies"]
+
+
+@pytest.mark.parametrize("case", ENERGY_CASES)
+def test_oracle_energies_match_reference(oracle, case):
+    from oracle import nrg_run_cpu
+    out = []
+    nrg_run_cpu.run(read(case, "param"), read(case, "data"), threads=os.cpu_count() or 1, energies_out=out)
+    assert_energies("".join(out), read(case, "energies.nrg"), case)
+
+
+def test_energies_formatter():
+    import numpy as np
+    text = energies_block(3, {(1, 2): np.array([0.25, 1.0 / 3.0]), (-1, 2): np.array([0.0, 1e-5, 12345678.0])})
+    assert text == ("\n===== Iteration number: 3\nSubspace: -1 2\n0 1e-05 1.23457e+07 \n"
+                    "Subspace: 1 2\n0.25 0.333333 \n")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ENERGY_CASES)
+def test_gpu_energies(case):
+    from nrgljubljana_b200.nrg_run import run_files
+    res = run_files(read(case, "param"), read(case, "data"))
+    assert_energies("".join(res.energies), read(case, "energies.nrg"), f"{case} (device run)")
