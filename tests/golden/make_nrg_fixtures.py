@@ -30,7 +30,8 @@ CASES = [
     "test18_dumpscaled", "test19_dumpabs", "test20_dumpgroups", "test24_NN1_Nmax=10", "test24_NN1_Nmax=11",
     "test27_NN2odd", "test2_algorithms_finite", "test30_cosine_band", "test31_flat_band", "test55_gt_ls",
     "test58_dsyev", "test5_disc_y", "test62_dumpenergies", "test67_fixeps", "test68_grouptol", "test8_keep",
-    "test9_keepenergy",
+    "test9_keepenergy", "legacy_sigma_trick_siam_qs", "legacy_substeps_one_siam_std", "test32_arbitrary_DOS",
+    "test47_nrgchain", "test48_adapt_tri=old", "test50_ref1", "test52_ref2", "test54_ref3",
 ]
 # spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)
