@@ -362,6 +362,10 @@ class QSRun:
     def __init__(self, params: RunParams, data: DataFile, device: int = 0, ctx: Optional[Context] = None):
         if data.symtype != "QS" or data.channels not in (1, 2):
             raise ValueError("the driver covers symtype QS with one or two channels")
+        if any(k == "g" for k, _ in data.ops.values()):
+            # global operators gain the added site's part at every step (recalc1_global,
+            # c++/recalc.hpp:111-118) and are listed after the singlets in `custom`; not restated here
+            raise ValueError("global operators (g blocks of the data file) are not supported")
         if data.nmax == 0 and params.algorithms:
             # Params::ZBW (Nmax = 0): the reference bins the initial cluster's spectra with its own
             # window rules (c++/spectrum.hpp:91-95); not restated here
