@@ -1,4 +1,4 @@
-"""CPU restatement of an NRG run for symtype QS, one channel -- TEST INFRASTRUCTURE ONLY.
+"""CPU restatement of an NRG run for symtype QS, one or two channels -- TEST INFRASTRUCTURE ONLY.
 
 The checker of ``nrgljubljana_b200.nrg_run``: the reference's run loop restated on the
 host with LAPACK dsyev and BLAS dgemm through ``oracle.py``. It follows
@@ -22,6 +22,12 @@ host with LAPACK dsyev and BLAS dgemm through ``oracle.py``. It follows
                               Algo_DMNRG c++/algo_DMNRG.hpp:29-52; BaseSpectrum::calc c++/algo.hpp:55-67;
                               mergeNN2half, windowfunction, continuous c++/spectrum.hpp:81-196;
                               Bins c++/bins.hpp:61-185; BR_NEW c++/spectral.hpp:42-70
+  FDM                         c++/dmnrg.hpp:146-217; Algo_FDMgt/ls c++/algo_FDM.hpp:30-151;
+                              calc_ZnD, fdm_thermodynamics c++/measurements.hpp:60-163
+  CFS, FT                     Algo_CFSgt/ls c++/algo_CFS.hpp:28-105; Algo_FT c++/algo_FT.hpp:28-48;
+                              calc_Z c++/measurements.hpp:189-191
+  output                      savebins c++/spectrum.hpp:146-170; Annotated::dump
+                              c++/output.hpp:77-125; dump_energies c++/output.hpp:157-161
 
 Only ``tests/`` and the CPU-baseline leg of ``bench.py`` may import this module.
 """
