@@ -47,7 +47,7 @@ _IGNORED = {
     # model parameters of the generated data and of its discretisation (keys of the data
     # generator, read by nrginit, not by the C++ run: c++/params.hpp has none of them)
     "U1", "U2", "Gamma1", "Gamma2", "eps1", "eps2", "U12", "J12", "tri", "mMAX", "smooth", "dos",
-    "solpath",
+    "solpath", "xmax", "gamma", "options",
 }
 
 

@@ -115,6 +115,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
     disc = kv.get("discretization", "Z")
+    brs = float(kv.get("bandrescale", 1.0))  # Params::SCALE multiplies by bandrescale (c++/params.hpp:632)
     keep = int(kv.get("keep", 100))
     keepenergy = float(kv.get("keepenergy", -1.0))
     keepmin = int(kv.get("keepmin", 0))
@@ -136,11 +137,11 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     O.blas_threads(1)  # one BLAS thread per block, as diagonalisations_OpenMP runs dsyev
 
     def scale_of(trueN):
-        return SCALE(trueN + 1, Lam, disc, z)
+        return SCALE(trueN + 1, Lam, disc, z, brs)
 
     diag: Dict = {}
     for I, e in sorted(d.subspaces):
-        v = e.copy() if rescaled else e / SCALE(0, Lam, disc, z)
+        v = e.copy() if rescaled else e / SCALE(0, Lam, disc, z, brs)
         diag[I] = _Eig(v)
     opch = [dict(d.opch[ch][0]) for ch in range(d.channels)]
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
@@ -250,7 +251,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
 
     if kv.get("calc0", "true").lower() == "true":
         dump_energies(diag, -1)
-        annotate(diag, SCALE(0, Lam, disc, z))
+        annotate(diag, SCALE(0, Lam, disc, z, brs))
         td(-1, diag)
         custom(-1, diag, ops)
 
@@ -540,6 +541,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
     (log-Gaussian broadening). FDM expectation values at step fdmexpvn
     (measure_singlet_fdm, c++/measurements.hpp:31-44)."""
     T = float(kv.get("T", 0.001))
+    brs = float(kv.get("bandrescale", 1.0))
     goodE = float(kv.get("goodE", 2.0))
     bins = int(kv.get("bins", 1000))
     NN1 = kv.get("NN1", "false").lower() == "true"
@@ -559,7 +561,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
     bmin = float(kv.get("broaden_min", -99.0))
     bratio = float(kv.get("broaden_ratio", 1.05))
     fdmexpvn = int(kv.get("fdmexpvn", 0))
-    last_scale = SCALE(Nmax, Lam, disc, z)
+    last_scale = SCALE(Nmax, Lam, disc, z, brs)
     if bmin <= 0.0:
         bmin = float(kv.get("broaden_min_ratio", 3.0)) * last_scale
     Efac = Lam if (combs == 4 and not NN1) else math.sqrt(Lam)  # Params::getEfactor (c++/params.hpp:650-652)
@@ -652,7 +654,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                 fdm_out["customfdm"] = (["T"] + list(singlet_names), row)
     if out is None or not algos:
         return
-    emax = emax_p if emax_p > 0 else SCALE(0, Lam, disc, z) * 100.0
+    emax = emax_p if emax_p > 0 else SCALE(0, Lam, disc, z, brs) * 100.0
     emin = emin_p if emin_p > 0 else last_scale / 100.0
     lmin, lmax = math.floor(math.log10(emin)), math.ceil(math.log10(emax))
     # gf_type and factor of each kind (c++/oprecalc.hpp:160-195; gf_sign, c++/traits.hpp)

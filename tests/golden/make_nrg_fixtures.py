@@ -32,6 +32,7 @@ CASES = [
     "test58_dsyev", "test5_disc_y", "test62_dumpenergies", "test67_fixeps", "test68_grouptol", "test8_keep",
     "test9_keepenergy", "legacy_sigma_trick_siam_qs", "legacy_substeps_one_siam_std", "test32_arbitrary_DOS",
     "test47_nrgchain", "test48_adapt_tri=old", "test50_ref1", "test52_ref2", "test54_ref3",
+    "test33_Delta", "test34_bandrescale", "test49_template1", "test51_template2", "test53_template3",
 ]
 # spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)

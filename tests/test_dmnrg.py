@@ -15,7 +15,8 @@ GOLD = os.path.join(HERE, "golden", "nrg")
 DM_CASES = ["test2_algorithms_dmnrg", "test23_DMNRG", "test24_NN1", "test25_NN2avg", "test26_NN2even", "test27_bins",
             "test24_NN1_Nmax=10", "test24_NN1_Nmax=11", "test27_NN2odd", "test30_cosine_band", "test31_flat_band",
             "test32_arbitrary_DOS", "test47_nrgchain", "test48_adapt_tri=old", "test50_ref1", "test52_ref2",
-            "test54_ref3"]
+            "test54_ref3", "test33_Delta", "test34_bandrescale", "test49_template1", "test51_template2",
+            "test53_template3"]
 SPECTRA = ["spec_DMNRG_dens_A_d-A_d", "corr_DMNRG_dens_n_d-n_d", "spin_DMNRG_dens_sigma_d-sigma_d"]
 SPEC = SPECTRA[0]
 # the refs print 10 significant digits; values far below the peak are compared absolutely
