@@ -94,8 +94,13 @@ def test_formatter_matches_oracle(oracle_annotated, case):
     assert lines == oracle_annotated(case)
 
 
+# the device run's file on a subset: every dump option, one and two channels, the largest case
+GPU_CASES = ["test17_dumpannotated", "test18_dumpscaled", "test19_dumpabs", "test20_dumpgroups", "test68_grouptol",
+             "test56_dsyevr", "test300_QS_ref", "legacy_one_jkondonew"]
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("case", GPU_CASES)
 def test_gpu_annotated(case):
     from nrgljubljana_b200.nrg_run import run_files
     res = run_files(read(case, "param"), read(case, "data"))
