@@ -120,6 +120,7 @@ class RunParams:
     dumpscaled: bool = True
     dumpabs: bool = False
     dumpenergies: bool = False  # energies.nrg: every computed level of every step
+    dumpsubspaces: bool = False  # subspaces.dat: kept and computed states of every subspace
     prec_td: int = 10
     prec_custom: int = 10
     prec_xy: int = 10
@@ -189,6 +190,7 @@ class Result:
     bins: Dict[str, np.ndarray] = field(default_factory=dict)
     annotated: List[str] = field(default_factory=list)  # lines of annotated.dat (dumpannotated > 0)
     energies: List[str] = field(default_factory=list)   # blocks of energies.nrg (dumpenergies)
+    subspaces: List[str] = field(default_factory=list)  # lines of subspaces.dat (dumpsubspaces)
     tdfdm: Optional[Tuple[List[str], List[float]]] = None       # fields, row (fdm_thermodynamics)
     customfdm: Optional[Tuple[List[str], List[float]]] = None   # fields, row (measure_singlet_fdm)
 
@@ -658,6 +660,9 @@ class QSRun:
         keep_all = last and p.keep_all_states_in_last_step
         for s in diag.values():
             s.nkept = len(s.values) if keep_all else int(np.count_nonzero(s.corr <= Emax))
+        if p.dumpsubspaces:  # Store::dump_subspaces (c++/store.hpp:75-84), written after the run
+            res.subspaces += [f"Iteration {N}", f"len_dm={len(diag)}"] + \
+                [f"I={I[0]} {I[1]} kept={diag[I].nkept} total={len(diag[I].values)}" for I in sorted(diag)] + [""]
 
         # after_diag (c++/core.hpp:193-230)
         self._annotate(N, diag)
@@ -1443,6 +1448,9 @@ def write_outputs(out: str, p: RunParams, res: Result) -> None:
                 f.write(f"{e:.{p.prec_xy}g} {v:.{p.prec_xy}g}" + (" 0\n" if p.reim else "\n"))
     for name, rows in res.bins.items():
         write_bins(os.path.join(out, f"{name}.bin"), rows)
+    if p.dumpsubspaces:
+        with open(os.path.join(out, "subspaces.dat"), "w") as f:
+            f.write("".join(line + "\n" for line in res.subspaces))
     if p.dumpenergies:
         with open(os.path.join(out, "energies.nrg"), "w") as f:
             f.write("".join(res.energies))

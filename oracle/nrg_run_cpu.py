@@ -98,7 +98,7 @@ class _Eig:
 
 def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None, fdm_out: dict = None,
         bins_out: dict = None, annotated_out: list = None, annotated_entries: list = None,
-        energies_out: list = None) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
+        energies_out: list = None, subspaces_out: list = None) -> Tuple[List[str], List[List[float]], List[str], List[List[float]]]:
     """td and custom rows of the run; with a `spectra` dict, also the spectra of the specs,
     specd and spect pairs for the algorithms dmnrg, fdm, fdmgt, fdmls that are switched on
     (file stem, e.g. spec_DMNRG_dens_A_d-A_d -> array of (E, A(E)) rows as written to that
@@ -110,7 +110,9 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     `annotated_out` list, the lines of annotated.dat (Annotated::dump, c++/output.hpp:77-125)
     for dumpannotated > 0 (and, in `annotated_entries`, each step's (energy, subspace) pairs
     with its scale and total energy, the formatter's input); with an `energies_out` list and
-    dumpenergies=true, the text of energies.nrg (Output::dump_energies, c++/output.hpp:157-161)."""
+    dumpenergies=true, the text of energies.nrg (Output::dump_energies, c++/output.hpp:157-161);
+    with a `subspaces_out` list and dumpsubspaces=true, the lines of subspaces.dat
+    (Store::dump_subspaces, c++/store.hpp:75-84)."""
     kv = parse_param(param_text)
     Lam = float(kv.get("Lambda", 2.0))
     z = float(kv.get("z", 1.0))
@@ -321,6 +323,12 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         Emax = allc[nrkeep - 1]
         for e in new.values():
             e.nrpost = len(e.values) if (last and lastall) else int(sum(1 for c in e.corr if c <= Emax))
+        if subspaces_out is not None and flag("dumpsubspaces"):  # the Store of the run, dumped after it
+            subspaces_out.append("Iteration %d" % N)
+            subspaces_out.append("len_dm=%d" % len(new))
+            for I in sorted(new):
+                subspaces_out.append("I=%d %d kept=%d total=%d" % (I[0], I[1], new[I].nrpost, len(new[I].values)))
+            subspaces_out.append("")
         # after_diag
         total_energy += Egs * scale  # Stats::update (c++/stats.hpp:65-71)
         dump_energies(new, N)

@@ -33,6 +33,7 @@ CASES = [
     "test9_keepenergy", "legacy_sigma_trick_siam_qs", "legacy_substeps_one_siam_std", "test32_arbitrary_DOS",
     "test47_nrgchain", "test48_adapt_tri=old", "test50_ref1", "test52_ref2", "test54_ref3",
     "test33_Delta", "test34_bandrescale", "test49_template1", "test51_template2", "test53_template3",
+    "test63_dumpsubspaces",
 ]
 # spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)
@@ -47,7 +48,7 @@ def main(ref_root: str) -> None:
         dst = os.path.join(out_root, name)
         os.makedirs(dst, exist_ok=True)
         extra = [f for f in sorted(os.listdir(os.path.join(src, "ref")))
-                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm", "annotated.dat", "energies.nrg")]
+                 if SPECTRUM.match(f) or f in ("tdfdm", "customfdm", "annotated.dat", "energies.nrg", "subspaces.dat")]
         for name, rel in [("param", "param"), ("data", "data"), ("td", "ref/td"), ("custom", "ref/custom")] + \
                 [(f, "ref/" + f) for f in extra]:
             p = os.path.join(src, rel)

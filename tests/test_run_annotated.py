@@ -158,3 +158,28 @@ def test_gpu_energies(case):
     from nrgljubljana_b200.nrg_run import run_files
     res = run_files(read(case, "param"), read(case, "data"))
     assert_energies("".join(res.energies), read(case, "energies.nrg"), f"{case} (device run)")
+
+
+SUBSPACE_CASES = sorted(c for c in os.listdir(GOLD) if os.path.exists(os.path.join(GOLD, c, "subspaces.dat")))
+
+
+def test_subspace_cases_present():
+    assert SUBSPACE_CASES == ["test63_dumpsubspaces"]
+
+
+@pytest.mark.parametrize("case", SUBSPACE_CASES)
+def test_oracle_subspaces_match_reference(oracle, case):
+    """subspaces.dat (Store::dump_subspaces, c++/store.hpp:75-84): per step the number of
+    subspaces and each one's kept and computed states, exactly."""
+    from oracle import nrg_run_cpu
+    out = []
+    nrg_run_cpu.run(read(case, "param"), read(case, "data"), threads=os.cpu_count() or 1, subspaces_out=out)
+    assert "".join(line + "\n" for line in out) == read(case, "subspaces.dat")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", SUBSPACE_CASES)
+def test_gpu_subspaces(case):
+    from nrgljubljana_b200.nrg_run import run_files
+    res = run_files(read(case, "param"), read(case, "data"))
+    assert "".join(line + "\n" for line in res.subspaces) == read(case, "subspaces.dat")
