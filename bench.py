@@ -176,6 +176,14 @@ def sample_blocks_host(torch, sizes, idx, device):
     return out
 
 
+def workload_config(sizes: np.ndarray, args, world: int) -> dict:
+    """The `config` object of both arms (the same keys and values for the same workload)."""
+    return {"workload": WORKLOAD.format(nblk=len(sizes), nmin=args.nmin, nmax=args.nmax), "nblk": int(len(sizes)),
+            "sum_n3": float(np.sum(sizes.astype(float) ** 3)), "flop_per_step": f_eig(sizes),
+            "input_bytes": int(8 * np.sum(sizes.astype(np.int64) ** 2)),
+            "l2": "inputs larger than L2 (30 GB vs 126 MB)", "parallelism": f"replicas x{world}"}
+
+
 def max_over_ranks(dist, x: float, device) -> float:
     """The largest x of all ranks; x itself without a process group. Every rank takes this
     collective step, also after its own failure (pass math.inf there), so that no rank is left
@@ -208,7 +216,7 @@ def reference_arm(args, rank: int) -> None:
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(nblk=args.nblk, nmin=args.nmin, nmax=args.nmax), "nblk": args.nblk, "parallelism": "replicas"},
+            "config": workload_config(sizes, args, args.gpus), "sample": sample,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -225,6 +233,7 @@ def main():
     ap.add_argument("--nmax", type=int, default=NMAX, help="largest block order (profiling cases)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64-peak", action="store_true", help="skip the cuBLAS DGEMM peak measurement")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nrg", action="store_true", help="skip the whole-run NRG measurement")
     ap.add_argument("--no-per-block", action="store_true", help="skip the one-block-per-launch GPU comparator")
@@ -344,10 +353,8 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(nblk=nbk, nmin=args.nmin, nmax=args.nmax), "nblk": nbk, "sum_n3": float(np.sum(sizes.astype(float) ** 3)),
-                       "flop_per_step": flop_step, "input_bytes": 8 * total,
-                       "l2": "inputs larger than L2 (30 GB vs 126 MB); consumed inputs refreshed by a D2D copy inside each step",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(sizes, args, world),
+            "timing": "inputs resident in HBM; the consumed inputs are refreshed by a D2D copy inside each step",
             "steps_per_s": world * args.steps / elapsed, "gpu_launches": launches, "roofline": roof,
             "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items()},
             "clocks": clk.summary()}
@@ -374,10 +381,6 @@ def main():
         line["validation"] = {"error": str(err)[:200]}
     del work, evecs, evals
     torch.cuda.empty_cache()
-    if not args.no_e2e:  # every rank: its own replica through the host API, max over ranks
-        e2e = e2e_arm(torch, ctx, pristine, sizes, offs, voffs, args, dist, dev)
-        if rank == 0:
-            line["e2e"] = e2e
     if not args.no_cpu and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         idx, stride = cpu_sample(sizes, args.cpu_seconds, threads)
@@ -388,7 +391,27 @@ def main():
                                 "sample": f"{len(idx)} of {nbk} blocks (every {stride}th in size order), {t:.1f} s"}
     if not args.no_per_block and rank == 0 and world == 1:
         line["per_block_gpu"] = per_block_arm(torch, pristine, sizes, offs, dev)
-    del pristine
+    if rank == 0 and not args.no_fp64_peak:
+        line["fp64_peak"] = fp64_peak(torch, dev)
+        pk = line["fp64_peak"].get("burst_tflops")
+        if pk:
+            line["fp64_frac"] = {"achieved_tflops": value / world / 1e3, "peak_tflops": pk,
+                                 "frac": value / world / 1e3 / pk,
+                                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run, best of 10"}
+    if not args.no_e2e:  # every rank: its own replica through the host API, max over ranks
+        # The device-resident inputs go to pinned host memory; the device copy and the context's
+        # workspace are given back, so the host path runs within its own bounded ring.
+        hostH = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+        hostH.copy_(pristine)
+        del pristine
+        torch.cuda.empty_cache()
+        ctx.trim()
+        e2e = e2e_arm(torch, ctx, hostH, sizes, offs, voffs, args, dist, dev)
+        del hostH
+        if rank == 0:
+            line["e2e"] = e2e
+    else:
+        del pristine
     torch.cuda.empty_cache()
     if not args.no_nrg and rank == 0:
         line["nrg_run"] = nrg_run_arm(torch, local, args)
@@ -417,6 +440,41 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp64_peak(torch, dev, n: int = 8192, reps: int = 10, sustain_s: float = 4.0) -> dict:
+    """The FP64 denominator of the eigensolver's roofline: a cuBLAS DGEMM of n x n x n
+    (torch.matmul on float64), best of `reps` timed singly with CUDA events (burst), and the
+    mean over a loop of about `sustain_s` seconds (sustained), with the SM clocks sampled
+    during the loop."""
+    a = torch.randn((n, n), dtype=torch.float64, device=dev)
+    b = torch.randn((n, n), dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    flop = 2.0 * n ** 3
+    for _ in range(3):
+        torch.matmul(a, b, out=c)
+    torch.cuda.synchronize()
+    best = math.inf
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    k = max(1, int(sustain_s / best))
+    with ClockSampler(dev.index or 0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+    mean = e0.elapsed_time(e1) / 1e3 / k
+    del a, b, c
+    torch.cuda.empty_cache()
+    return {"gemm": f"cuBLAS DGEMM {n}^3 (torch.matmul, float64)", "burst_tflops": flop / best / 1e12,
+            "sustained_tflops": flop / mean / 1e12, "sustained_loop": k, "clocks": clk.summary()}
 
 
 def per_block_arm(torch, pristine, sizes, offs, dev, target_flop: float = 1.5e12) -> dict:
@@ -503,6 +561,22 @@ C2_WORKLOAD = ("NRG run, QS single-impurity Anderson model U=1, eps_d=-0.5 (delt
                "nrgljubljana_b200.datagen")
 
 
+def per_block_driver(torch):
+    """The same NRG-run driver with the plain GPU eigensolver: one cuSOLVER eigh
+    (torch.linalg.eigh) per block and launch, in place of the batched nrg_diag_batch."""
+    from nrgljubljana_b200.nrg_run import QSRun
+
+    class PerBlock(QSRun):
+        def _diagonalise(self, job):
+            for b, n in enumerate(job.ns):
+                h = job.Hbuf[job.moff[b]:job.moff[b + 1]].view(n, n)
+                w, q = torch.linalg.eigh(h, UPLO="U")
+                job.Ebuf[job.voff[b]:job.voff[b + 1]].copy_(w)
+                job.Vbuf[job.moff[b]:job.moff[b + 1]].view(n, n).copy_(q.T)
+            return np.zeros(len(job.ns), dtype=np.int32)
+    return PerBlock
+
+
 def c2_inputs():
     from nrgljubljana_b200.datagen import siam_qs
     return C2_PARAM, siam_qs(1.0, 0.0, 0.04, 2.0, 60, 1.0, "Z", ops=["n_d", "A_d"])
@@ -519,14 +593,7 @@ def c2_arm(torch, device: int, args) -> dict:
     p, d = RunParams.from_param(parse_param(param)), read_data(data)
     ctx = context(device)
 
-    class PerBlock(QSRun):
-        def _diagonalise(self, job):
-            for b, n in enumerate(job.ns):
-                h = job.Hbuf[job.moff[b]:job.moff[b + 1]].view(n, n)
-                w, q = torch.linalg.eigh(h, UPLO="U")
-                job.Ebuf[job.voff[b]:job.voff[b + 1]].copy_(w)
-                job.Vbuf[job.moff[b]:job.moff[b + 1]].view(n, n).copy_(q.T)
-            return np.zeros(len(job.ns), dtype=np.int32)
+    PerBlock = per_block_driver(torch)
 
     def timed(cls):
         torch.cuda.synchronize()
@@ -725,6 +792,33 @@ def c3_arm(torch, device: int, args) -> dict:
            "peak_device_gib": torch.cuda.max_memory_allocated(device) / 2 ** 30,
            "tdfdm": dict(zip(*res.tdfdm)) if res.tdfdm else None,
            "spectrum": {k: int(len(v)) for k, v in res.spectra.items()}}
+    if not args.no_per_block:
+        # Parity and the plain GPU path: the same run with one cuSOLVER eigh per block and launch.
+        # The comparison covers the steps whose kept states agree (a hard cut at keep inside a
+        # near-degeneracy may keep another multiplet after a round-off difference).
+        td, blk = np.array(res.td), res.block_dims
+        del run, job
+        torch.cuda.empty_cache()
+        PerBlock = per_block_driver(torch)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res_pb = PerBlock(p, d, device, ctx).run()
+        torch.cuda.synchronize()
+        t_pb = time.perf_counter() - t0
+        k = next((j for j, (x, y) in enumerate(zip(blk, res_pb.block_dims)) if sorted(x) != sorted(y)), len(blk))
+        tdp = np.array(res_pb.td)
+        big = np.abs(td[:k]) >= 1e-6
+        name = next(iter(res.spectra))
+        a, b = res.spectra[name][:, 1], res_pb.spectra[name][:, 1]
+        out["per_block_gpu"] = {"steps_per_s": d.nmax / t_pb, "s_per_run": t_pb,
+                                "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch"}
+        out["parity"] = {"against": "the per-block cuSOLVER run of the same driver",
+                         "steps_with_same_kept_states": k, "steps": len(blk),
+                         "td_max_rel_diff": float(np.max(np.abs(tdp[:k][big] - td[:k][big]) / np.abs(td[:k][big]))),
+                         "tdfdm_rel_diff": {f: float(abs(x - y) / max(abs(x), 1e-300))
+                                            for f, x, y in zip(res.tdfdm[0], res.tdfdm[1], res_pb.tdfdm[1])},
+                         "spectrum_max_diff_rel_to_peak": float(np.max(np.abs(a - b)) / np.max(np.abs(a)))
+                         if a.shape == b.shape else None}
     if not args.no_cpu:
         threads = os.cpu_count() or 1
         heavy = max(range(len(res.block_dims)), key=lambda k: sum(float(n) ** 3 for n in res.block_dims[k]))
@@ -800,14 +894,7 @@ def nrg_run_arm(torch, device: int, args) -> dict:
     p, d = RunParams.from_param(parse_param(param)), read_data(data)
     ctx = context(device)
 
-    class PerBlock(QSRun):
-        def _diagonalise(self, job):
-            for b, n in enumerate(job.ns):
-                h = job.Hbuf[job.moff[b]:job.moff[b + 1]].view(n, n)
-                w, q = torch.linalg.eigh(h, UPLO="U")
-                job.Ebuf[job.voff[b]:job.voff[b + 1]].copy_(w)
-                job.Vbuf[job.moff[b]:job.moff[b + 1]].view(n, n).copy_(q.T)
-            return np.zeros(len(job.ns), dtype=np.int32)
+    PerBlock = per_block_driver(torch)
 
     def timed(cls, reps):
         cls(p, d, device).run()  # warm-up
@@ -866,10 +953,11 @@ def nrg_run_arm(torch, device: int, args) -> dict:
     return out
 
 
-def e2e_arm(torch, ctx, pristine, sizes, offs, voffs, args, dist=None, dev=None) -> dict:
-    """Same metric through the host-pointer entry point, from pinned host memory: each step
-    copies the step's blocks in and the eigenpairs out (nrg_diag_batch_host returns when they
-    are in host memory). Timed with CUDA events around the synchronous calls, after a barrier
+def e2e_arm(torch, ctx, hostH, sizes, offs, voffs, args, dist=None, dev=None) -> dict:
+    """Same metric through the host-pointer entry point, from pinned host memory (hostH, the
+    step's blocks): each step copies the blocks in and the eigenpairs out, streamed through
+    the context's bounded device ring (nrg_diag_batch_host returns when they are in host
+    memory). Timed with CUDA events around the synchronous calls, after a barrier
     under torchrun; the whole-job value uses the slowest rank's time. Every rank takes the
     same collective steps whether or not its own calls failed."""
     import ctypes as C
@@ -878,9 +966,7 @@ def e2e_arm(torch, ctx, pristine, sizes, offs, voffs, args, dist=None, dev=None)
     k = max(1, min(args.steps, 3))
     err, dt = None, math.inf
     try:
-        hostH = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
-        hostH.copy_(pristine)
-        hostV = torch.empty(pristine.numel(), dtype=torch.float64, pin_memory=True)
+        hostV = torch.empty(hostH.numel(), dtype=torch.float64, pin_memory=True)
         hostE = torch.empty(int(voffs[-1]), dtype=torch.float64, pin_memory=True)
         n_c = (C.c_int * nbk)(*[int(x) for x in sizes])
         Hp = (C.c_void_p * nbk)(*[hostH.data_ptr() + 8 * int(offs[b]) for b in range(nbk)])

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define NRG_B200_VERSION 1
+#define NRG_B200_VERSION 2
 
 #define NRG_OK 0
 #define NRG_ERR_ARG (-1)    /* invalid argument (sizes, null pointers, shapes) */
@@ -50,9 +50,15 @@ NRG_API const char* nrg_last_error(void);
 
 /* Per-run context: device, device workspace (grown on demand up to workspace_limit bytes,
  * 0 = 90% of the free device memory at creation), descriptor staging. One context may
- * be used from one host thread at a time. */
+ * be used from one host thread at a time. Calls on one context may name different
+ * streams: each call's work is ordered after the previous call's (an event recorded on
+ * the previous call's stream), because all calls share the context's descriptor staging
+ * and workspace. Independent work on several streams at once needs one context each. */
 NRG_API int nrg_create(nrg_ctx** ctx, int device, size_t workspace_limit);
 NRG_API int nrg_destroy(nrg_ctx* ctx);
+/* Gives the context's device memory back (workspace arena, host-block ring, descriptor
+ * staging) after synchronising the device; later calls allocate again as needed. */
+NRG_API int nrg_trim(nrg_ctx* ctx);
 
 /* ------------------------------------------------------------------ diagonalisation
  * Replaces diagonalise() (c++/diag.hpp:261-292) with diag=dsyev|dsyevd|default for real
@@ -71,7 +77,13 @@ NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* 
                    double* const* evecs, int* info, void* stream);
 
 /* Same with host pointers for H[b], evals[b], evecs[b] (the call the reference's
- * diagonalise() makes with its ublas matrix); H[b] is left unchanged. */
+ * diagonalise() makes with its ublas matrix); H[b] is left unchanged. The blocks stream
+ * through a ring of at most three device slots in chunks of consecutive blocks (a chunk
+ * holds about a quarter of the batch, at most 6 GiB): the copy of chunk k+1 to the device
+ * and of chunk k-1 back to the host overlap the solve of chunk k, on two copy streams of
+ * the context. Page-locked host memory lets the copies run asynchronously; pageable
+ * memory works too, with copies that do not overlap. Returns when every result is in host
+ * memory. */
 NRG_API int nrg_diag_batch_host(nrg_ctx* ctx, int nblk, const int* n, const double* const* H, double* const* evals,
                         double* const* evecs, int* info, void* stream);
 
@@ -140,6 +152,9 @@ NRG_API int nrg_gemm3_batch_host(nrg_ctx* ctx, int nterm, const nrg_gemm3* terms
 
 /* One transform term, M (rows x cols) += factor * A (rows x ka) * O (ka x kb) * B^T
  * (B is cols x kb; O = NULL means the identity, ka == kb), that allocates nothing.
+ * Leading dimensions: ldm >= cols, lda >= ka, ldb >= kb and, with O, ldo >= kb (O is
+ * always dense here: the diagonal O of nrg_gemm3 (ldo == 0) is rejected, as are A
+ * transposed and B stored kb x cols; those terms need nrg_gemm3_batch).
  * This entry point has no counterpart in the reference. It is for callers that cannot call
  * cudaMalloc: a host thread that must not stall the device (cudaMalloc/cudaFree may
  * synchronise it), a plugin in a process whose device memory is already reserved by

@@ -22,7 +22,8 @@ NRG_SPEC_FDMGT = 1
 NRG_SPEC_FDMLS = 2
 
 # Every symbol include/nrg_b200.h declares.
-EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_diag_batch", "nrg_diag_batch_host",
+EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_trim", "nrg_diag_batch",
+           "nrg_diag_batch_host",
            "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate", "nrg_profile",
            "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch",
            "nrg_broaden")
@@ -101,6 +102,7 @@ def load() -> C.CDLL:
     L.nrg_last_error.restype = C.c_char_p
     L.nrg_create.argtypes = [C.POINTER(P), C.c_int, C.c_size_t]
     L.nrg_destroy.argtypes = [P]
+    L.nrg_trim.argtypes = [P]
     L.nrg_diag_batch.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                  C.POINTER(C.c_int), P]
     L.nrg_diag_batch_host.argtypes = L.nrg_diag_batch.argtypes

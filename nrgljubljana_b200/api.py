@@ -48,6 +48,10 @@ class Context:
         k = check(self.lib.nrg_profile_read(self.ptr, arr, 32), "nrg_profile_read")
         return {arr[i].name.decode(): (arr[i].ms, int(arr[i].launches)) for i in range(k)}
 
+    def trim(self) -> None:
+        """Give the context's device memory back (nrg_trim); later calls allocate again."""
+        check(self.lib.nrg_trim(self.ptr), "nrg_trim")
+
     def close(self):
         if self.ptr:
             self.lib.nrg_destroy(self.ptr)

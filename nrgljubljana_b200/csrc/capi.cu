@@ -273,6 +273,13 @@ int nrg_destroy(nrg_ctx* c) {
   if (c->fork2_ev) cudaEventDestroy(c->fork2_ev);
   if (c->join2_ev) cudaEventDestroy(c->join2_ev);
   if (c->side2) cudaStreamDestroy(c->side2);
+  if (c->ring) cudaFree(c->ring);
+  if (c->copy_in) cudaStreamDestroy(c->copy_in);
+  if (c->copy_out) cudaStreamDestroy(c->copy_out);
+  for (auto& sl : c->ring_ev)
+    for (auto e : sl)
+      if (e) cudaEventDestroy(e);
+  if (c->order_ev) cudaEventDestroy(c->order_ev);
   delete c;
   return NRG_OK;
 }
@@ -285,6 +292,7 @@ int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double*
   if (nblk < 0 || (nblk > 0 && (!n || !H || !evals || !evecs || !info))) return fail(NRG_ERR_ARG, "bad arguments");
   if (nblk == 0) return NRG_OK;
   auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
   for (int b = 0; b < nblk; b++) {
     if (n[b] < 1 || n[b] > NRG_DIAG_MAX_N) return fail(NRG_ERR_ARG, "block %d: order %d out of range", b, n[b]);
     if (!H[b] || !evals[b] || !evecs[b]) return fail(NRG_ERR_ARG, "block %d: null pointer", b);
@@ -367,44 +375,145 @@ int nrg_diag_batch_host(nrg_ctx* c, int nblk, const int* n, const double* const*
   if (nblk < 0 || (nblk > 0 && (!n || !H || !evals || !evecs || !info))) return fail(NRG_ERR_ARG, "bad arguments");
   if (nblk == 0) return NRG_OK;
   auto s = static_cast<cudaStream_t>(stream);
-  size_t mat = 0, val = 0;
+  nrg::CallOrder call_order(c, s);
+  // Device bytes of one block in a ring slot: H and evecs (n^2 each) and evals.
+  auto slot_bytes = [&](int b) {
+    return 2 * nrg::align_up(sizeof(double) * (size_t)n[b] * n[b], 256) + nrg::align_up(sizeof(double) * n[b], 256);
+  };
+  size_t total = 0;
   for (int b = 0; b < nblk; b++) {
     if (n[b] < 1 || n[b] > NRG_DIAG_MAX_N) return fail(NRG_ERR_ARG, "block %d: order %d out of range", b, n[b]);
-    mat += (size_t)n[b] * n[b];
-    val += n[b];
+    if (!H[b] || !evals[b] || !evecs[b]) return fail(NRG_ERR_ARG, "block %d: null pointer", b);
+    total += slot_bytes(b);
   }
-  // Device copies: H, evecs (n^2 each) and evals; the large path needs its own workspace
-  // on top, so the host variant allocates these buffers separately from the arena.
-  double *dH = nullptr, *dV = nullptr, *dE = nullptr;
-  CK(cudaMalloc(&dH, sizeof(double) * mat));
-  if (cudaMalloc(&dV, sizeof(double) * mat) != cudaSuccess || cudaMalloc(&dE, sizeof(double) * val) != cudaSuccess) {
-    cudaGetLastError();
-    cudaFree(dH);
-    if (dV) cudaFree(dV);
-    return fail(NRG_ERR_OOM, "device buffers for %zu matrix elements", mat);
-  }
-  std::vector<double*> pH(nblk), pV(nblk), pE(nblk);
-  size_t mo = 0, vo = 0;
+  // Chunks of consecutive blocks stream through a ring of up to three device slots: the
+  // host-to-device copy of chunk k+1 and the device-to-host copy of chunk k-1 run on two
+  // copy streams beside the solve of chunk k. A slot holds about a quarter of the batch,
+  // at most 6 GiB, and at most a fifth of the memory this context can use (the solve's own
+  // workspace comes on top of the three slots).
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t usable = std::min(c->ws_limit, fr + c->ring_size + c->ws_size);
+  size_t target = std::min<size_t>(std::max<size_t>(total / 4, (size_t)64 << 20), (size_t)6 << 30);
+  target = std::max<size_t>(std::min(target, usable / 5), (size_t)16 << 20);
+  std::vector<int> first(1, 0);
+  size_t maxchunk = 0, cur = 0;
   for (int b = 0; b < nblk; b++) {
-    pH[b] = dH + mo;
-    pV[b] = dV + mo;
-    pE[b] = dE + vo;
-    cudaMemcpyAsync(pH[b], H[b], sizeof(double) * n[b] * n[b], cudaMemcpyHostToDevice, s);
-    mo += (size_t)n[b] * n[b];
-    vo += n[b];
-  }
-  rc = nrg_diag_batch(c, nblk, n, pH.data(), pE.data(), pV.data(), info, stream);
-  if (rc >= 0) {
-    for (int b = 0; b < nblk; b++) {
-      cudaMemcpyAsync(evals[b], pE[b], sizeof(double) * n[b], cudaMemcpyDeviceToHost, s);
-      cudaMemcpyAsync(evecs[b], pV[b], sizeof(double) * n[b] * n[b], cudaMemcpyDeviceToHost, s);
+    const size_t sb = slot_bytes(b);
+    if (b > first.back() && cur + sb > target) {
+      maxchunk = std::max(maxchunk, cur);
+      first.push_back(b);
+      cur = 0;
     }
-    if (cudaStreamSynchronize(s) != cudaSuccess) rc = fail(NRG_ERR_CUDA, "copy-out failed");
+    cur += sb;
   }
-  cudaFree(dH);
-  cudaFree(dV);
-  cudaFree(dE);
-  return rc;
+  maxchunk = std::max(maxchunk, cur);
+  first.push_back(nblk);
+  const int nchunk = (int)first.size() - 1;
+  const int nslot = std::min(3, nchunk);
+  const size_t slot = nrg::align_up(maxchunk, 1 << 20);
+  if (c->ring_size < slot * nslot) {
+    if (c->ring) {
+      CK(cudaDeviceSynchronize());
+      CK(cudaFree(c->ring));
+      c->ring = nullptr;
+      c->ring_size = 0;
+    }
+    if (cudaMalloc(&c->ring, slot * nslot) != cudaSuccess) {
+      cudaGetLastError();
+      c->ring = nullptr;
+      return fail(NRG_ERR_OOM, "device ring of %d slots of %zu bytes for the host blocks", nslot, slot);
+    }
+    c->ring_size = slot * nslot;
+  }
+  if (!c->copy_in) {
+    CK(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
+    for (auto& sl : c->ring_ev)
+      for (auto& e : sl) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // Device pointers of every block inside its chunk's slot.
+  std::vector<double*> pH(nblk), pV(nblk), pE(nblk);
+  for (int k = 0; k < nchunk; k++) {
+    char* base = static_cast<char*>(c->ring) + (size_t)(k % nslot) * slot;
+    size_t off = 0;
+    for (int b = first[k]; b < first[k + 1]; b++) {
+      const size_t m = nrg::align_up(sizeof(double) * (size_t)n[b] * n[b], 256);
+      pH[b] = reinterpret_cast<double*>(base + off);
+      pV[b] = reinterpret_cast<double*>(base + off + m);
+      pE[b] = reinterpret_cast<double*>(base + off + 2 * m);
+      off += slot_bytes(b);
+    }
+  }
+  auto settle = [&]() {  // no copy may still target the ring or the caller's memory
+    const cudaError_t e1 = cudaStreamSynchronize(c->copy_in);
+    const cudaError_t e2 = cudaStreamSynchronize(c->copy_out);
+    const cudaError_t e3 = cudaStreamSynchronize(s);
+    return e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3;
+  };
+  auto copy_in = [&](int k) -> int {
+    const int sl = k % nslot;
+    if (k >= nslot) CK(cudaStreamWaitEvent(c->copy_in, c->ring_ev[sl][2], 0));  // chunk k - nslot copied out
+    for (int b = first[k]; b < first[k + 1]; b++)
+      CK(cudaMemcpyAsync(pH[b], H[b], sizeof(double) * (size_t)n[b] * n[b], cudaMemcpyHostToDevice, c->copy_in));
+    CK(cudaEventRecord(c->ring_ev[sl][0], c->copy_in));
+    return NRG_OK;
+  };
+  int bad = 0;
+  for (int k = 0; k < nchunk && rc == NRG_OK; k++) {
+    if (k == 0) rc = copy_in(0);
+    if (rc == NRG_OK && k + 1 < nchunk) rc = copy_in(k + 1);
+    if (rc) break;
+    const int sl = k % nslot, b0 = first[k], nb = first[k + 1] - b0;
+    if (cudaStreamWaitEvent(s, c->ring_ev[sl][0], 0) != cudaSuccess) {
+      rc = fail(NRG_ERR_CUDA, "stream wait for the copy of chunk %d", k);
+      break;
+    }
+    const int r = nrg_diag_batch(c, nb, n + b0, pH.data() + b0, pE.data() + b0, pV.data() + b0, info + b0, stream);
+    if (r < 0) {
+      rc = r;
+      break;
+    }
+    bad += r;
+    if (cudaEventRecord(c->ring_ev[sl][1], s) != cudaSuccess ||
+        cudaStreamWaitEvent(c->copy_out, c->ring_ev[sl][1], 0) != cudaSuccess) {
+      rc = fail(NRG_ERR_CUDA, "ordering of the copy-out of chunk %d", k);
+      break;
+    }
+    for (int b = b0; b < b0 + nb && rc == NRG_OK; b++) {
+      if (cudaMemcpyAsync(evals[b], pE[b], sizeof(double) * n[b], cudaMemcpyDeviceToHost, c->copy_out) != cudaSuccess ||
+          cudaMemcpyAsync(evecs[b], pV[b], sizeof(double) * (size_t)n[b] * n[b], cudaMemcpyDeviceToHost,
+                          c->copy_out) != cudaSuccess)
+        rc = fail(NRG_ERR_CUDA, "copy-out of block %d", b);
+    }
+    if (rc == NRG_OK && cudaEventRecord(c->ring_ev[sl][2], c->copy_out) != cudaSuccess)
+      rc = fail(NRG_ERR_CUDA, "event after the copy-out of chunk %d", k);
+  }
+  const cudaError_t se = settle();
+  if (rc == NRG_OK && se != cudaSuccess)
+    rc = fail(NRG_ERR_CUDA, "copies of the host blocks: %s", cudaGetErrorString(se));
+  if (rc) return rc;
+  if (bad) fail(bad, "%d of %d blocks returned a non-zero status", bad, nblk);
+  return bad;
+}
+
+int nrg_trim(nrg_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  if (c->ws) CK(cudaFree(c->ws));
+  c->ws = nullptr;
+  c->ws_size = 0;
+  if (c->ring) CK(cudaFree(c->ring));
+  c->ring = nullptr;
+  c->ring_size = 0;
+  if (c->desc) CK(cudaFree(c->desc));
+  c->desc = nullptr;
+  c->desc_size = 0;
+  if (c->desc_side) CK(cudaFree(c->desc_side));
+  c->desc_side = nullptr;
+  c->desc_side_size = 0;
+  return NRG_OK;
 }
 
 // ---------------------------------------------------------------- GEMM leaves
@@ -415,6 +524,7 @@ int nrg_hamiltonian_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, 
   if (nblk < 0 || npiece < 0 || (nblk > 0 && (!n || !H)) || (npiece > 0 && !pieces))
     return fail(NRG_ERR_ARG, "bad arguments");
   auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
   for (int b = 0; b < nblk; b++) {
     if (n[b] < 0 || n[b] > (1 << 20)) return fail(NRG_ERR_ARG, "block %d: bad order %d", b, n[b]);
     if (n[b] > 0 && !H[b]) return fail(NRG_ERR_ARG, "block %d: null matrix", b);
@@ -474,6 +584,7 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
   if (rc) return rc;
   if (nterm < 0 || (nterm > 0 && !terms)) return fail(NRG_ERR_ARG, "bad arguments");
   auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
   // Group by output pointer, keeping the given order inside a group.
   std::vector<int> live;
   for (int t = 0; t < nterm; t++) {
@@ -568,6 +679,7 @@ int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* st
   if (rc) return rc;
   if (nterm < 0 || (nterm > 0 && !terms)) return fail(NRG_ERR_ARG, "bad arguments");
   auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
   // Copy every referenced host span once (by pointer), compute, copy M spans back.
   struct Span { size_t bytes; double* dev; };
   std::map<const double*, Span> spans;
@@ -632,8 +744,10 @@ int nrg_broaden(nrg_ctx* c, int nspike, const double* e, const double* w, int nm
   if (nspike < 0 || nmesh < 0 || (nspike > 0 && (!e || !w)) || (nmesh > 0 && (!E || !out)))
     return fail(NRG_ERR_ARG, "bad arguments");
   if (!(alpha > 0.0) || !(omega0 > 0.0)) return fail(NRG_ERR_ARG, "alpha and omega0 must be positive");
-  nrg::PhaseScope ps(c, nrg::kPhBroaden, static_cast<cudaStream_t>(stream));
-  CK(nrg::broaden_launch(nspike, e, w, nmesh, E, alpha, omega0, out, static_cast<cudaStream_t>(stream)));
+  auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
+  nrg::PhaseScope ps(c, nrg::kPhBroaden, s);
+  CK(nrg::broaden_launch(nspike, e, w, nmesh, E, alpha, omega0, out, s));
   return NRG_OK;
 }
 
@@ -654,6 +768,7 @@ int nrg_spec_accumulate(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const
   if (bins->nbins < 2 || bins->bins <= 0) return fail(NRG_ERR_ARG, "bad bins");
   if (prm->algo < NRG_SPEC_DMNRG || prm->algo > NRG_SPEC_FDMLS) return fail(NRG_ERR_ARG, "bad algo %d", prm->algo);
   auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
 
   // GEMM-derived matrices in workspace.
   std::vector<size_t> xo(npair, 0), yo(npair, 0);

@@ -44,6 +44,18 @@ struct nrg_ctx {
   // bulk-copy reductions of larger blocks
   cudaStream_t side2 = nullptr;
   cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
+  // Cross-stream order of calls: every entry point records order_ev on its stream when it
+  // leaves; a call on another stream first waits for it, so the descriptor staging buffers
+  // and the workspace arena are never rewritten while an earlier call's kernels read them.
+  cudaEvent_t order_ev = nullptr;
+  cudaStream_t order_stream = nullptr;
+  bool order_set = false;
+  // nrg_diag_batch_host: ring of device slots for streamed chunks of blocks, and the two
+  // copy streams (host to device, device to host) beside the compute stream
+  void* ring = nullptr;
+  size_t ring_size = 0;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ring_ev[3][3] = {};  // per slot: inputs copied, solved, outputs copied
 };
 
 namespace nrg {
@@ -85,6 +97,29 @@ StagedGemm stage_gemm(std::vector<char>& img, const GemmPlan& p);
 int launch_staged_gemm(nrg_ctx* c, const StagedGemm& g, cudaStream_t s, int phase);
 
 int run_gemm_plan(nrg_ctx* c, const GemmPlan& p, cudaStream_t s, int phase);
+
+// Orders an entry point's work on stream s after the previous call on the context (on
+// whatever stream that ran) and records the point the next call waits for.
+struct CallOrder {
+  nrg_ctx* c;
+  cudaStream_t s;
+  CallOrder(nrg_ctx* c_, cudaStream_t s_) : c(c_), s(s_) {
+    if (c->order_set && c->order_stream != s) cudaStreamWaitEvent(s, c->order_ev, 0);
+  }
+  ~CallOrder() {
+    if (!c->order_ev && cudaEventCreateWithFlags(&c->order_ev, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      c->order_ev = nullptr;
+      return;
+    }
+    if (cudaEventRecord(c->order_ev, s) == cudaSuccess) {
+      c->order_stream = s;
+      c->order_set = true;
+    } else {
+      cudaGetLastError();
+    }
+  }
+};
 
 // Counts `nlaunch` kernel launches of `phase` and, when profiling, brackets them with
 // CUDA events recorded on stream s.

@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_version(lib):
-    assert lib.nrg_version() == 1
+    assert lib.nrg_version() == 2
 
 
 def test_no_cpu_fallback_without_device(lib):

@@ -54,6 +54,63 @@ def test_noalloc_matches_batched_entry_point_twice():
     assert torch.allclose(got, ref, rtol=REL, atol=REL)
 
 
+def test_noalloc_at_the_scratch_limit_matches_batched_and_oracle():
+    """ka * cols exactly equal to the scratch size is accepted, and every element of the
+    intermediate is used: the result equals the batched entry point's and the oracle's
+    transform() (c++/numerics_ublas.hpp:119-128)."""
+    import torch
+
+    import nrgljubljana_b200 as nb
+    from oracle import oracle
+    lib = nb.load_library()
+    limit = nb._lib.NRG_NOALLOC_SCRATCH_DOUBLES
+    ka, cols = 1024, limit // 1024
+    assert ka * cols == limit
+    rows, kb, f = 24, 12, 0.375
+    rng = np.random.default_rng(2028)
+    A = torch.tensor(rng.standard_normal((rows, ka)), device="cuda")
+    O = torch.tensor(rng.standard_normal((ka, kb)), device="cuda")
+    B = torch.tensor(rng.standard_normal((cols, kb)), device="cuda")
+    M0 = rng.standard_normal((rows, cols))
+    ref = torch.tensor(M0, device="cuda")
+    nb.gemm3_batch([nb.gemm3(ref, f, A, O, B)], host=False)
+    for _ in range(2):  # two calls in a row on the shared scratch
+        got = torch.tensor(M0, device="cuda")
+        rc = lib.nrg_transform_noalloc(got.data_ptr(), cols, A.data_ptr(), ka, O.data_ptr(), kb, B.data_ptr(), kb,
+                                       rows, cols, ka, kb, f, None)
+        assert rc == 0, nb._lib.last_error()
+        torch.cuda.synchronize()
+        g, r = got.cpu().numpy(), ref.cpu().numpy()
+        scale = max(1.0, np.abs(r).max())
+        assert np.abs(g - r).max() <= REL * scale * ka ** 0.5
+    host = M0.copy()
+    oracle.transform(host, f, A.cpu().numpy(), O.cpu().numpy(), B.cpu().numpy())
+    assert np.abs(g - host).max() <= REL * max(1.0, np.abs(host).max()) * ka ** 0.5
+
+
+def test_noalloc_rejects_bad_leading_dimensions():
+    """ldo = 0 (the batched API's diagonal O) and leading dimensions shorter than a row are
+    rejected, so that no call reads a dense operand with a wrong stride."""
+    import torch
+
+    import nrgljubljana_b200 as nb
+    lib = nb.load_library()
+    rows, cols, ka, kb = 8, 9, 6, 5
+    M = torch.zeros((rows, cols), dtype=torch.float64, device="cuda")
+    A = torch.zeros((rows, ka), dtype=torch.float64, device="cuda")
+    O = torch.zeros((ka, kb), dtype=torch.float64, device="cuda")
+    B = torch.zeros((cols, kb), dtype=torch.float64, device="cuda")
+    good = dict(ldm=cols, lda=ka, ldo=kb, ldb=kb)
+    for key, bad in (("ldo", 0), ("ldo", kb - 1), ("lda", ka - 1), ("ldb", kb - 1), ("ldm", cols - 1)):
+        ld = dict(good, **{key: bad})
+        rc = lib.nrg_transform_noalloc(M.data_ptr(), ld["ldm"], A.data_ptr(), ld["lda"], O.data_ptr(), ld["ldo"],
+                                       B.data_ptr(), ld["ldb"], rows, cols, ka, kb, 1.0, None)
+        assert rc == nb._lib.NRG_ERR_ARG, (key, bad)
+        assert key in nb._lib.last_error()
+    assert lib.nrg_transform_noalloc(M.data_ptr(), cols, A.data_ptr(), ka, O.data_ptr(), kb, B.data_ptr(), kb, rows,
+                                     cols, ka, kb, 1.0, None) == 0
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch():
     import torch
 
