@@ -58,4 +58,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NRG_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: {sys.argv[0]} REFERENCE_DIR (or set NRG_REFERENCE): the NRG Ljubljana source tree")
+    main(ref)
