@@ -60,6 +60,25 @@ NRG_API int nrg_destroy(nrg_ctx* ctx);
  * staging) after synchronising the device; later calls allocate again as needed. */
 NRG_API int nrg_trim(nrg_ctx* ctx);
 
+/* Launch parameters of the batched eigensolver, chosen per device by the autotuner
+ * (nrgljubljana_b200/autotune.py) from timed sweeps; the defaults are its result on B200.
+ *   small_max_n    blocks up to this order are solved whole in the shared memory of one
+ *                  CTA (32..96)
+ *   mid_max_n      larger blocks up to this order are reduced to tridiagonal form in the
+ *                  shared memory of one CTA (small_max_n..236)
+ *   cluster_max_n  larger blocks up to this order are reduced in the distributed shared
+ *                  memory of a thread-block cluster when the clusters fit the SMs at once
+ *                  (mid_max_n..640); larger blocks stream their trailing matrix from HBM
+ *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2) */
+typedef struct nrg_tuning {
+  int small_max_n;
+  int mid_max_n;
+  int cluster_max_n;
+  int reduction_ctas_per_sm;
+} nrg_tuning;
+NRG_API int nrg_get_tuning(nrg_ctx* ctx, nrg_tuning* out);
+NRG_API int nrg_set_tuning(nrg_ctx* ctx, const nrg_tuning* in);
+
 /* ------------------------------------------------------------------ diagonalisation
  * Replaces diagonalise() (c++/diag.hpp:261-292) with diag=dsyev|dsyevd|default for real
  * matrices, and the per-step batch loop diagonalisations() / diagonalisations_OpenMP()

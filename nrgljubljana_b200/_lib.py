@@ -26,7 +26,7 @@ EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_tr
            "nrg_diag_batch_host",
            "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate", "nrg_profile",
            "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch",
-           "nrg_broaden")
+           "nrg_broaden", "nrg_get_tuning", "nrg_set_tuning")
 NRG_NOALLOC_SCRATCH_DOUBLES = 1 << 20
 
 
@@ -81,6 +81,11 @@ class Bins(C.Structure):
                 ("discard_immediately", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("small_max_n", C.c_int), ("mid_max_n", C.c_int), ("cluster_max_n", C.c_int),
+                ("reduction_ctas_per_sm", C.c_int)]
+
+
 class PhaseStat(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("ms", C.c_double), ("launches", C.c_longlong)]
 
@@ -114,6 +119,8 @@ def load() -> C.CDLL:
                                         C.c_int, C.c_int, C.c_double, P]
     L.nrg_hamiltonian_batch.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(P), C.c_int, C.POINTER(HPiece), P]
     L.nrg_broaden.argtypes = [P, C.c_int, P, P, C.c_int, P, C.c_double, C.c_double, P, P]
+    L.nrg_get_tuning.argtypes = [P, C.POINTER(Tuning)]
+    L.nrg_set_tuning.argtypes = [P, C.POINTER(Tuning)]
     L.nrg_profile.argtypes = [P, C.c_int]
     L.nrg_profile_read.argtypes = [P, C.POINTER(PhaseStat), C.c_int]
     _lib = L

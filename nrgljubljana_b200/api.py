@@ -48,6 +48,20 @@ class Context:
         k = check(self.lib.nrg_profile_read(self.ptr, arr, 32), "nrg_profile_read")
         return {arr[i].name.decode(): (arr[i].ms, int(arr[i].launches)) for i in range(k)}
 
+    @property
+    def tuning(self) -> dict:
+        """The eigensolver's launch parameters (nrg_get_tuning)."""
+        t = _lib.Tuning()
+        check(self.lib.nrg_get_tuning(self.ptr, C.byref(t)), "nrg_get_tuning")
+        return {k: getattr(t, k) for k, _ in _lib.Tuning._fields_}
+
+    def set_tuning(self, **kw) -> None:
+        """Change some of the launch parameters (nrg_set_tuning; the library checks ranges)."""
+        cur = self.tuning
+        cur.update(kw)
+        t = _lib.Tuning(**cur)
+        check(self.lib.nrg_set_tuning(self.ptr, C.byref(t)), "nrg_set_tuning")
+
     def trim(self) -> None:
         """Give the context's device memory back (nrg_trim); later calls allocate again."""
         check(self.lib.nrg_trim(self.ptr), "nrg_trim")
@@ -65,8 +79,15 @@ class Context:
 
 
 def context(device: int = 0) -> Context:
+    """The process's context on `device`, created at first use with the autotuned launch
+    parameters of that device model when a table for it is present (autotune.load_table)."""
     if device not in _contexts:
-        _contexts[device] = Context(device)
+        ctx = Context(device)
+        from .autotune import load_table
+        table = load_table(device)
+        if table:
+            ctx.set_tuning(**table)
+        _contexts[device] = ctx
     return _contexts[device]
 
 

@@ -224,6 +224,28 @@ int nrg_create(nrg_ctx** out, int device, size_t workspace_limit) {
   return NRG_OK;
 }
 
+int nrg_get_tuning(nrg_ctx* c, nrg_tuning* out) {
+  if (!c || !out) return fail(NRG_ERR_ARG, "bad arguments");
+  *out = c->tune;
+  return NRG_OK;
+}
+
+int nrg_set_tuning(nrg_ctx* c, const nrg_tuning* in) {
+  if (!c || !in) return fail(NRG_ERR_ARG, "bad arguments");
+  const nrg_tuning t = *in;
+  if (t.small_max_n < 32 || t.small_max_n > nrg::kSmallMaxNLimit)
+    return fail(NRG_ERR_ARG, "small_max_n = %d outside [32, %d]", t.small_max_n, nrg::kSmallMaxNLimit);
+  if (t.mid_max_n < t.small_max_n || t.mid_max_n > nrg::kMidMaxNLimit)
+    return fail(NRG_ERR_ARG, "mid_max_n = %d outside [small_max_n, %d]", t.mid_max_n, nrg::kMidMaxNLimit);
+  if (t.cluster_max_n < t.mid_max_n || t.cluster_max_n > nrg::kClusterMaxNLimit)
+    return fail(NRG_ERR_ARG, "cluster_max_n = %d outside [mid_max_n, %d]", t.cluster_max_n,
+                nrg::kClusterMaxNLimit);
+  if (t.reduction_ctas_per_sm != 1 && t.reduction_ctas_per_sm != 2)
+    return fail(NRG_ERR_ARG, "reduction_ctas_per_sm = %d (1 or 2)", t.reduction_ctas_per_sm);
+  c->tune = t;
+  return NRG_OK;
+}
+
 int nrg_profile(nrg_ctx* c, int enable) {
   if (!c) return fail(NRG_ERR_ARG, "null context");
   CK(cudaSetDevice(c->device));
@@ -306,7 +328,7 @@ int nrg_diag_batch(nrg_ctx* c, int nblk, const int* n, double* const* H, double*
   CK(cudaMemsetAsync(c->info_dev, 0, sizeof(int) * (size_t)nblk, s));
 
   std::vector<int> small, large;
-  for (int b = 0; b < nblk; b++) (n[b] <= nrg::kSmallMaxN ? small : large).push_back(b);
+  for (int b = 0; b < nblk; b++) (n[b] <= c->tune.small_max_n ? small : large).push_back(b);
 
   // With blocks of both kinds the small-block solver runs on the context's side stream,
   // forked from and joined back into s, so that it overlaps the large-block pipeline.

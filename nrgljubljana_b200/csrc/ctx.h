@@ -21,6 +21,7 @@ const char* phase_name(int p);
 
 struct nrg_ctx {
   int device = 0;
+  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 1};  // eigensolver launch parameters
   // profiling: launch counts per phase (always), CUDA-event intervals (when enabled)
   bool prof = false;
   long long launches[nrg::kPhCount] = {};

@@ -746,12 +746,11 @@ __global__ void __launch_bounds__(kTriThreads, 1) tridiag_tcl_kernel(const Large
 }
 
 // ---------------------------------------------------------------- mid-size tridiagonalisation
-// Blocks with kSmallMaxN < n <= kMidMaxN: the whole lower triangle fits in shared memory,
+// Blocks with small_max_n < n <= mid_max_n (nrg_tuning): the whole lower triangle fits in shared memory,
 // packed by columns (column j holds rows j..n-1 at pcol(j)), so the unblocked Householder
 // reduction runs without touching HBM or L2 after the first read of H. Output as
 // tridiag_kernel: d, e, tau, and v_k in row k of W1 (unit at k+1, zeros from the start of
 // its back-transform panel up to k).
-constexpr int kMidMaxN = 224;
 constexpr int kMidThreads = 512;
 
 NRG_DEV int pcol(int j, int n) { return j * n - (j * (j - 1)) / 2; }
@@ -860,7 +859,7 @@ __global__ void __launch_bounds__(kMidThreads) tridiag_smem_kernel(const LargeBl
 }
 
 // ---------------------------------------------------------------- cluster tridiagonalisation
-// Blocks with kMidMaxN < n <= kClusterMaxN: the packed lower triangle is spread over the
+// Blocks with mid_max_n < n <= cluster_max_n (nrg_tuning): the packed lower triangle is spread over the
 // shared memory of a thread-block cluster of C CTAs (column j lives in CTA j mod C) and the
 // unblocked Householder reduction runs there; the CTAs read each other's shared memory
 // (distributed shared memory, plain loads, no bulk copies). Two cluster barriers per column:
@@ -872,7 +871,6 @@ __global__ void __launch_bounds__(kMidThreads) tridiag_smem_kernel(const LargeBl
 //   B  every CTA sums the shares of all CTAs for every row in a fixed order (so all CTAs
 //      hold the same w) and updates its own columns.
 // Output as tridiag_kernel.
-constexpr int kClusterMaxN = 600;
 constexpr int kClThreads = 512;
 
 // Offset of owned column t (global column j = r + t*C) in the local storage of CTA r.
@@ -1551,6 +1549,9 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
                   double* const* evecs, int* info_dev, cudaStream_t s) {
   std::vector<int> ord(which);
   std::stable_sort(ord.begin(), ord.end(), [n](int x, int y) { return n[x] > n[y]; });
+  const int mid_max_n = c->tune.mid_max_n, cluster_max_n = c->tune.cluster_max_n;
+  // at least half an SM's shared memory per reduction CTA keeps one of them per SM
+  const bool one_per_sm = c->tune.reduction_ctas_per_sm == 1;
   for (int b : ord)
     if (n[b] > kMaxLargeN)
       return fail(NRG_ERR_ARG, "block %d: order %d exceeds the supported maximum %d", b, n[b], kMaxLargeN);
@@ -1614,7 +1615,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
       for (int bi = 0; bi < nb; bi++) {
         const LargeBlock& L = blk[bi];
-        if (L.n <= kMidMaxN) continue;  // reduced in the shared memory of one CTA, no bulk copies
+        if (L.n <= mid_max_n) continue;  // reduced in the shared memory of one CTA, no bulk copies
         const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
         const cuuint64_t strides[1] = {(cuuint64_t)L.ldp * sizeof(double)};
         const cuuint32_t box[2] = {(cuuint32_t)kSlabRows, 8u};
@@ -1711,16 +1712,16 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     char* dbase = static_cast<char*>(c->desc);
     const LargeBlock* dblk = reinterpret_cast<const LargeBlock*>(dbase + blk_off);
 
-    // ---- 1. tridiagonalisation: blocks beyond kClusterMaxN (sorted first) stream through
-    //         TMA, blocks beyond kMidMaxN are spread over the shared memory of a cluster,
+    // ---- 1. tridiagonalisation: blocks beyond cluster_max_n (sorted first) stream through
+    //         TMA, blocks beyond mid_max_n are spread over the shared memory of a cluster,
     //         the rest are reduced in the shared memory of one CTA
     {
       int nsm = 148;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
       int nbig = 0;
-      while (nbig < nb && blk[nbig].n > kClusterMaxN) nbig++;
+      while (nbig < nb && blk[nbig].n > cluster_max_n) nbig++;
       int nclu = nbig;
-      while (nclu < nb && blk[nclu].n > kMidMaxN) nclu++;
+      while (nclu < nb && blk[nclu].n > mid_max_n) nclu++;
       // One cluster size for all cluster blocks (one launch): the smallest of 2, 4, 8 that
       // fits the largest of them, raised while the cluster CTAs still fit the SMs once. The
       // clusters serve latency: when they would not all fit the SMs at once (a batch of many
@@ -1798,7 +1799,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         auto tcl_bytes = [&](int st) {
           return std::max(1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)maxn +
                                                    (size_t)kTriWarps * 2 * NB + 4 * NB + 66),
-                          (size_t)smsm / 2 + 1024);
+                          (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
         };
         int stages = 8;
         while (stages > 4 && tcl_bytes(stages) + 256 > (size_t)optin) stages -= 2;
@@ -1844,7 +1845,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           // shared an SM, gave wrong reductions for some blocks (the same alpha race as the
           // cluster kernel, now fixed, pending a confirming run); with one per SM every check
           // passes.
-          const size_t smem1 = std::max(smem, (size_t)smsm / 2 + 1024);
+          const size_t smem1 = std::max(smem, (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
           NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
           tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(dblk, tm);
           NRG_CK(cudaGetLastError());

@@ -66,7 +66,12 @@ struct EigBlock {
   int n, pad_;
 };
 
-constexpr int kSmallMaxN = 64;   // blocks up to this size are solved entirely in shared memory
+constexpr int kSmallMaxN = 64;   // default: blocks up to this size are solved entirely in shared memory
+constexpr int kSmallMaxNLimit = 96;  // the most the one-CTA solver's shared memory holds
+constexpr int kMidMaxN = 224;        // default: one-CTA shared-memory reduction up to this order
+constexpr int kMidMaxNLimit = 236;   // the packed triangle of the most the 227 KB of one CTA holds
+constexpr int kClusterMaxN = 600;    // default: cluster (distributed shared memory) reduction up to here
+constexpr int kClusterMaxNLimit = 640;  // the most an 8-CTA cluster's shared memory holds
 
 cudaError_t eig_small_launch(const EigBlock* d_blocks, int nblk, int maxn, cudaStream_t stream);
 

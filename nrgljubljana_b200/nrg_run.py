@@ -322,7 +322,7 @@ class _Measure:
     every singlet operator over the stored states, and the host Boltzmann weights."""
     T: float
     weights: np.ndarray        # mult(I) * exp(-f * corr) per stored state, subspace order
-    diag: torch.Tensor         # nops x states (device)
+    diag: Optional[torch.Tensor]  # nops x states (device), gathered once the recalculation ran
 
 
 @dataclass
@@ -406,6 +406,34 @@ class QSRun:
         # the steps are kept (eigenvalues, eigenvectors, energy offsets) for the density
         # matrices and the spectral pass after the run
         self.keep_steps = bool(self.specs) or params.fdm_flags
+        # A server merging the per-step recalculation of many runs sets these two lists: the
+        # GEMM terms of end_step are then collected instead of launched, and the reads of
+        # their outputs (the custom diagonals) wait in `deferred_reads` until the server has
+        # launched all runs' terms in one nrg_gemm3_batch call.
+        self.deferred_terms: Optional[List[np.ndarray]] = None
+        self.deferred_reads: Optional[List] = None
+
+    def device_bytes(self) -> int:
+        """Device bytes the run holds between steps: the current eigenvectors, the <||f||>
+        and singlet-operator buffers, and the eigenvectors kept for the density matrices."""
+        seen, total = set(), 0
+        tensors = [getattr(self, "_vecs", None)]
+        for name in ("opch", "ops"):
+            m = getattr(self, name, None)
+            tensors.append(m.buf if m is not None else None)
+        tensors += [st.vecs for st in getattr(self, "dm_steps", [])]
+        for t in tensors:
+            if t is not None and t.data_ptr() not in seen:
+                seen.add(t.data_ptr())
+                total += t.numel() * t.element_size()
+        return total
+
+    def _gemm(self, terms: np.ndarray) -> None:
+        """One batched GEMM call for `terms`, or their collection by a merging server."""
+        if self.deferred_terms is not None:
+            self.deferred_terms.append(terms)
+        else:
+            gemm3_batch_array(terms, self.ctx, self.stream)
 
     # ---- scales (c++/step.hpp:30-39)
     def scale(self, trueN: int) -> float:
@@ -456,8 +484,15 @@ class QSRun:
         idx = np.concatenate(idx) if idx else np.zeros(0, dtype=np.int64)
         full = (np.arange(ops.nops)[:, None] * ops.total + idx[None, :]).ravel()
         g = self._h2d(full.astype(np.int64))
-        dg = torch.index_select(ops.buf, 0, g).view(ops.nops, len(idx))
-        return _Measure(self.scale(trueN) / self.p.betabar, np.concatenate(w) if w else np.zeros(0), dg)
+        m = _Measure(self.scale(trueN) / self.p.betabar, np.concatenate(w) if w else np.zeros(0), None)
+
+        def gather():
+            m.diag = torch.index_select(ops.buf, 0, g).view(ops.nops, len(idx))
+        if self.deferred_reads is not None:
+            self.deferred_reads.append(gather)
+        else:
+            gather()
+        return m
 
     # ---- the run
     def start(self) -> None:
@@ -722,7 +757,7 @@ class QSRun:
                     rows.append((M, sp.nstored, s1.vptr + 8 * s1.offs[i1 - 1], s1.n, 0, 0,
                                  sp.vptr + 8 * sp.offs[ip - 1], sp.n, s1.nstored, sp.nstored, k, k, 0, 1, qs.ieee(fn, Ip[1])))
         if rows:
-            gemm3_batch_array(np.array(rows, dtype=GEMM3_DTYPE), self.ctx, self.stream)
+            self._gemm(np.array(rows, dtype=GEMM3_DTYPE))
         self.opch_keys = [set(out.loc)] * self.T.channels
         return out
 
@@ -752,9 +787,8 @@ class QSRun:
             op = np.repeat(np.arange(cold.nops, dtype=np.uint64), len(b))
             t["M"] += op * np.uint64(8 * out.total)
             t["O"] += op * np.uint64(8 * cold.total)
-            gemm3_batch_array(t, self.ctx, self.stream)
+            self._gemm(t)
         return out
-
 
     def _recalc_tensor(self, diag: Dict[Invar, Sub], cold: MatSet, tables, factor, rows=None) -> MatSet:
         """SymmetryQS::recalc_doublet / recalc_triplet (c++/symmetry/nrg-recalc-QS.hpp:32-117,

@@ -3,10 +3,15 @@
 Requests (a ``param`` + ``data`` pair each, with an arrival time) are admitted while the
 device-memory budget and the slot limit allow; every tick, each active run builds and
 assembles its next step (``QSRun.begin_step``), the blocks of all active runs are solved in
-ONE ``nrg_diag_batch`` call, and each run finishes its step (truncation, thermodynamics,
-recalculation; ``QSRun.end_step``). Runs join and leave the batch between ticks, so a
-request that arrives while others are on the GPU starts at the next tick and overlaps
-their work. Every run's matrices stay resident in device memory for its whole life.
+ONE ``nrg_diag_batch`` call, each run finishes its step on the host (truncation,
+thermodynamics; ``QSRun.end_step``) while its recalculation terms (the <||f||> of the next
+Hamiltonian and the singlet operators, c++/oprecalc.hpp:71-87, 205-221) are collected, and
+the terms of all active runs go to the device in ONE ``nrg_gemm3_batch`` call. Runs join and
+leave the batch between ticks, so a request that arrives while others are on the GPU starts
+at the next tick and overlaps their work. Every run's matrices stay resident in device
+memory for its whole life; a run is charged at admission what it will hold (every step's
+eigenvectors when it computes spectra or FDM quantities) and, once running, the larger of
+that charge and what it actually holds.
 
 Each block is solved by the same kernels whatever else is in the batch, so a run's result
 does not depend on the mix it was served in.
@@ -23,7 +28,7 @@ from typing import List, Optional
 import numpy as np
 import torch
 
-from .api import context, diag_batch_ptrs
+from .api import context, diag_batch_ptrs, gemm3_batch_array
 from .inputs import parse_param, read_data
 from .nrg_run import QSRun, Result, RunParams
 
@@ -52,12 +57,16 @@ class Completed:
         return self.done - self.arrival
 
 
-def run_bytes(p: RunParams, combs: int = 4) -> int:
-    """Device bytes a run is charged at admission: the step's Hamiltonians, eigenvectors and
-    the previous step's eigenvectors, 3 x 8 B x sum of n^2, bounded by the kept states
-    spread over at least four (Q, S) sectors of combs x keep states each."""
-    states = combs * p.keep
-    return 3 * 8 * states * states // 4
+def run_bytes(p: RunParams, nmax: int = 0, channels: int = 1) -> int:
+    """Device bytes a run is charged at admission. One step holds its Hamiltonians, its
+    eigenvectors and the previous step's eigenvectors, 3 x 8 B x sum of n^2, bounded by the
+    kept states spread over at least four (Q, S) sectors of 4^channels x keep states each. A
+    run whose density matrices or spectra need every step's eigenvectors after the forward
+    sweep (any spectral algorithm, or FDM) keeps one more step's worth per step (nmax)."""
+    states = 4 ** channels * p.keep
+    step = 8 * states * states // 4
+    keeps_steps = bool(p.algorithms) or p.fdm_flags
+    return (3 + (nmax if keeps_steps else 0)) * step
 
 
 class Server:
@@ -73,15 +82,19 @@ class Server:
         self.budget = hbm_budget
         self.max_active = max_active
         self.ticks = 0
+        self.recalc_calls = 0  # merged recalculation calls (one per tick with terms)
+        self.max_active_seen = 0
         self.blocks_per_tick: List[int] = []
 
     def serve(self, requests: List[Request], realtime: bool = True) -> List[Completed]:
         """Serve the stream; with realtime=False every request is taken as arrived at once."""
         pending = sorted(requests, key=lambda r: (r.arrival if realtime else 0.0, r.rid))
-        active: List[tuple] = []  # (request, run, charged bytes, admitted time)
+        active: List[list] = []  # [request, run, charged bytes, admitted time]
         out: List[Completed] = []
-        used = 0
         t0 = time.perf_counter()
+
+        def used() -> int:
+            return sum(max(need, run.device_bytes()) for _, run, need, _ in active)
         while pending or active:
             now = time.perf_counter() - t0
             # admission: arrived, a free slot, and room in the budget (a run larger than the
@@ -89,14 +102,15 @@ class Server:
             while pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active:
                 req = pending[0]
                 params = RunParams.from_param(parse_param(req.param))
-                need = run_bytes(params)
-                if active and used + need > self.budget:
+                data = read_data(req.data)
+                need = run_bytes(params, data.nmax, data.channels)
+                if active and used() + need > self.budget:
                     break
                 pending.pop(0)
-                run = QSRun(params, read_data(req.data), self.device, self.ctx)
+                run = QSRun(params, data, self.device, self.ctx)
                 run.start()
-                used += need
-                active.append((req, run, need, now))
+                active.append([req, run, need, now])
+            self.max_active_seen = max(self.max_active_seen, len(active))
             if not active:
                 wait = pending[0].arrival - (time.perf_counter() - t0)
                 if wait > 0:
@@ -113,20 +127,31 @@ class Server:
             info = diag_batch_ptrs(ns, Hp, Ep, Vp, self.ctx, self.stream)
             self.ticks += 1
             self.blocks_per_tick.append(len(ns))
+            terms: List[np.ndarray] = []
+            reads: List = []
             o = 0
             for (_, run, _, _), j in zip(active, jobs):
-                run.end_step(j, info[o:o + len(j.ns)])
+                run.deferred_terms, run.deferred_reads = terms, reads
+                try:
+                    run.end_step(j, info[o:o + len(j.ns)])
+                finally:
+                    run.deferred_terms = run.deferred_reads = None
                 o += len(j.ns)
+            if terms:
+                gemm3_batch_array(np.concatenate(terms), self.ctx, self.stream)
+                self.recalc_calls += 1
+            for gather in reads:
+                gather()
             still = []
-            for req, run, need, adm in active:
+            for item in active:
+                req, run, need, adm = item
                 if run.done:
                     res = run.finish()
                     torch.cuda.synchronize(self.device)
                     out.append(Completed(req.rid, req.tag, res, req.arrival if realtime else 0.0, adm,
                                          time.perf_counter() - t0, run.nmax))
-                    used -= need
                 else:
-                    still.append((req, run, need, adm))
+                    still.append(item)
             active = still
         return out
 

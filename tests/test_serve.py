@@ -23,6 +23,11 @@ def test_poisson_arrivals_and_budget_rule():
     assert np.all(np.diff(a) > 0) and np.array_equal(a, poisson_arrivals(200, 4.0, 7))
     assert abs(200 / a[-1] - 4.0) < 1.0
     assert run_bytes(RunParams(keep=2000)) == 4 * run_bytes(RunParams(keep=1000))
+    # a run that keeps every step's eigenvectors for its spectra is charged for them
+    plain = RunParams(keep=1000)
+    spectral = RunParams(keep=1000, dmnrg=True)
+    assert run_bytes(spectral, nmax=40) == (3 + 40) * run_bytes(plain, nmax=40) // 3
+    assert run_bytes(plain, channels=2) == 16 * run_bytes(plain)
 
 
 @pytest.fixture(scope="module")
@@ -98,3 +103,39 @@ def test_mix_with_large_blocks_within_tolerance():
             big = np.abs(x) >= 1e-6
             assert np.all(np.abs(x[big] - y[big]) <= 1e-10 * np.abs(x[big])), d.rid
             assert np.all(np.abs(x[~big] - y[~big]) <= 1e-12), d.rid
+
+
+@pytest.mark.gpu
+def test_recalculation_merged_per_tick(alone):
+    """Every tick launches the recalculation terms of all active runs in one batched call,
+    and the results stay bit for bit those of the runs alone."""
+    from nrgljubljana_b200.serve import Request, Server
+    reqs = [Request(i, read(c, "param"), read(c, "data"), 0.0, c) for i, c in enumerate(MIX)]
+    srv = Server(max_active=8)
+    done = srv.serve(reqs, realtime=False)
+    assert srv.recalc_calls == srv.ticks
+    for d in done:
+        assert same(d.result, alone[d.tag]), d.tag
+
+
+@pytest.mark.gpu
+def test_spectral_runs_queue_under_a_tight_budget():
+    """DM-NRG runs keep every step's eigenvectors for the density matrices; with a budget
+    that holds one such run they are served one after another (queued, not out of memory),
+    and each result, spectrum included, equals the run alone."""
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import RunParams, run_files
+    from nrgljubljana_b200.serve import Request, Server, run_bytes
+    cases = ["test2_algorithms_dmnrg", "test23_DMNRG", "test2_algorithms_dmnrg"]
+    charges = [run_bytes(RunParams.from_param(parse_param(read(c, "param"))), read_data(read(c, "data")).nmax)
+               for c in cases]
+    reqs = [Request(i, read(c, "param"), read(c, "data"), 0.0, c) for i, c in enumerate(cases)]
+    srv = Server(hbm_budget=max(charges) + min(charges) - 1, max_active=8)
+    done = srv.serve(reqs, realtime=False)
+    assert len(done) == len(cases) and srv.max_active_seen == 1
+    for d in done:
+        a = run_files(read(d.tag, "param"), read(d.tag, "data"))
+        assert same(d.result, a), d.tag
+        assert sorted(a.spectra) == sorted(d.result.spectra)
+        for k in a.spectra:
+            assert np.array_equal(a.spectra[k], d.result.spectra[k]), (d.tag, k)
