@@ -69,12 +69,19 @@ NRG_API int nrg_trim(nrg_ctx* ctx);
  *   cluster_max_n  larger blocks up to this order are reduced in the distributed shared
  *                  memory of a thread-block cluster when the clusters fit the SMs at once
  *                  (mid_max_n..640); larger blocks stream their trailing matrix from HBM
- *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2) */
+ *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2)
+ *   band_min_n     blocks of at least this order, when at most band_max_blocks of them are
+ *                  in a batch, take the two-stage reduction (dense -> band on the FP64
+ *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never
+ *   band_max_blocks  see band_min_n (few large blocks: the regime where the one-stage
+ *                  reduction's per-column chain bounds the step) */
 typedef struct nrg_tuning {
   int small_max_n;
   int mid_max_n;
   int cluster_max_n;
   int reduction_ctas_per_sm;
+  int band_min_n;
+  int band_max_blocks;
 } nrg_tuning;
 NRG_API int nrg_get_tuning(nrg_ctx* ctx, nrg_tuning* out);
 NRG_API int nrg_set_tuning(nrg_ctx* ctx, const nrg_tuning* in);

@@ -83,7 +83,7 @@ class Bins(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("small_max_n", C.c_int), ("mid_max_n", C.c_int), ("cluster_max_n", C.c_int),
-                ("reduction_ctas_per_sm", C.c_int)]
+                ("reduction_ctas_per_sm", C.c_int), ("band_min_n", C.c_int), ("band_max_blocks", C.c_int)]
 
 
 class PhaseStat(C.Structure):

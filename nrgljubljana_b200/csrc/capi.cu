@@ -132,7 +132,8 @@ int stage_desc_side(nrg_ctx* c, const std::vector<char>& img) {
 const char* phase_name(int p) {
   static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
                                         "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
-                                        "gemm3", "spec_gemm", "spec_bin", "assemble", "broaden"};
+                                        "gemm3", "spec_gemm", "spec_bin", "assemble", "broaden",
+                                        "band_reduce", "bulge_chase", "bt_band"};
   return (p >= 0 && p < kPhCount) ? names[p] : "?";
 }
 
@@ -242,6 +243,9 @@ int nrg_set_tuning(nrg_ctx* c, const nrg_tuning* in) {
                 nrg::kClusterMaxNLimit);
   if (t.reduction_ctas_per_sm != 1 && t.reduction_ctas_per_sm != 2)
     return fail(NRG_ERR_ARG, "reduction_ctas_per_sm = %d (1 or 2)", t.reduction_ctas_per_sm);
+  if (t.band_min_n != 0 && (t.band_min_n < 256 || t.band_min_n > NRG_DIAG_MAX_N))
+    return fail(NRG_ERR_ARG, "band_min_n = %d (0, or 256 .. %d)", t.band_min_n, NRG_DIAG_MAX_N);
+  if (t.band_max_blocks < 1) return fail(NRG_ERR_ARG, "band_max_blocks = %d (at least 1)", t.band_max_blocks);
   c->tune = t;
   return NRG_OK;
 }

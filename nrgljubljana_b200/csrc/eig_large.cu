@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "band.h"
 #include "eig_large.h"
 #include "eig_small.cuh"
 
@@ -1537,10 +1538,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-size_t large_block_doubles(int n) {
+size_t large_block_doubles(int n, bool two_stage) {
   const size_t ldp = (size_t)(n + 31) / 32 * 32;
   return (size_t)n * ldp + (size_t)n * n + 8 * (size_t)n + 2 * (size_t)NBT * n + 2 * (size_t)n + 64 * 13 +
-         (prep_layout(n).total > kPrepSmemMax ? (kPrepGlobalB * (size_t)n + 7) / 8 : 0);
+         (prep_layout(n).total > kPrepSmemMax ? (kPrepGlobalB * (size_t)n + 7) / 8 : 0) +
+         (two_stage ? band_extra_doubles(n) + 4 * 64 : 0);
 }
 
 }  // namespace
@@ -1550,6 +1552,12 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
   std::vector<int> ord(which);
   std::stable_sort(ord.begin(), ord.end(), [n](int x, int y) { return n[x] > n[y]; });
   const int mid_max_n = c->tune.mid_max_n, cluster_max_n = c->tune.cluster_max_n;
+  // Two-stage reduction for the largest blocks when they are few (the first nts of `ord`).
+  int nts_all = 0;
+  if (c->tune.band_min_n > 0) {
+    while (nts_all < (int)ord.size() && n[ord[nts_all]] >= c->tune.band_min_n) nts_all++;
+    if (nts_all > c->tune.band_max_blocks) nts_all = 0;
+  }
   // at least half an SM's shared memory per reduction CTA keeps one of them per SM
   const bool one_per_sm = c->tune.reduction_ctas_per_sm == 1;
   for (int b : ord)
@@ -1561,7 +1569,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
   while (pos < ord.size()) {
     size_t bytes = 0, end = pos;
     while (end < ord.size()) {
-      const size_t bb = align_up(sizeof(double) * large_block_doubles(n[ord[end]]), 256);
+      const size_t bb = align_up(sizeof(double) * large_block_doubles(n[ord[end]], (int)end < nts_all), 256);
       if (end > pos && bytes + bb > limit) break;
       bytes += bb;
       end++;
@@ -1570,9 +1578,12 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     if (rc) return rc;
     // ---- per-block descriptors
     std::vector<LargeBlock> blk;
+    std::vector<BandBlock> bblk;  // the chunk's two-stage blocks (its first nts, the largest)
+    std::vector<int> shift;       // row offset of each block's reflectors: 1, or kBand (two-stage)
     char* base = static_cast<char*>(c->ws);
     size_t off = 0;
     int maxn = 0, maxpanel = 0;
+    const int nts = std::max(0, std::min((int)end, nts_all) - (int)pos);
     for (size_t t = pos; t < end; t++) {
       const int b = ord[t], nb_ = n[b];
       LargeBlock L{};
@@ -1603,17 +1614,46 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
                    ? reinterpret_cast<char*>(take((kPrepGlobalB * (size_t)nb_ + 7) / 8)) : nullptr;
       L.info = info_dev + b;
       L.n = nb_;
+      if ((int)(t - pos) < nts) {
+        // two-stage: reflectors of stage 1 at rows k, unit at k + kBand; n - 1 - kBand of them
+        const int K1 = std::max(0, nb_ - 1 - kBand);
+        L.npanel = (K1 + NBT - 1) / NBT;
+        BandBlock Bb{};
+        Bb.S = L.W1;
+        Bb.H = L.H;
+        Bb.lds = L.ldp;
+        Bb.n = nb_;
+        Bb.J = band_nsteps(nb_, 0);
+        int jf = 0;
+        while (nb_ - jf - kBand > 1) jf += kBand;
+        Bb.jfin = jf;
+        Bb.BND = take((size_t)nb_ * kLDB);
+        Bb.V2 = take((size_t)band_nsweeps(nb_) * Bb.J * kBand);
+        Bb.tau2 = take((size_t)band_nsweeps(nb_) * Bb.J);
+        Bb.T2 = take((size_t)band_ngroups(nb_) * Bb.J * kGrp * kGrp);
+        Bb.tau1 = L.tau;
+        Bb.scr = L.W2;
+        Bb.d = L.d;
+        Bb.e = L.e;
+        Bb.evecs = L.evecs;
+        Bb.info = L.info;
+        bblk.push_back(Bb);
+        shift.push_back(kBand);
+      } else {
+        shift.push_back(1);
+      }
       blk.push_back(L);
       maxn = std::max(maxn, nb_);
       maxpanel = std::max(maxpanel, L.npanel);
     }
     const int nb = (int)blk.size();
+    if (off > c->ws_size) return fail(NRG_ERR_ARG, "internal: chunk workspace %zu > %zu", off, c->ws_size);
     // ---- 2-D tensor maps over each block's packed lower triangle (box 64 rows x 8 columns)
     std::vector<CUtensorMap> tmaps(nb);
     {
       auto encode = tensor_map_encoder();
       if (!encode) return fail(NRG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-      for (int bi = 0; bi < nb; bi++) {
+      for (int bi = nts; bi < nb; bi++) {
         const LargeBlock& L = blk[bi];
         if (L.n <= mid_max_n) continue;  // reduced in the shared memory of one CTA, no bulk copies
         const cuuint64_t dims[2] = {(cuuint64_t)L.ldp, (cuuint64_t)L.n};
@@ -1678,13 +1718,16 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       const LargeBlock& L = blk[bi];
       const int nn = L.n;
       size_t vt_off = 0, gt_off = 0;
+      // reflector k has its unit at row k + sh: k + 1 after the one-stage reduction, k + kBand
+      // after the first stage of the two-stage one; nn - 1 - sh reflectors
+      const int sh = shift[bi], nrefl = nn - 1 - sh;
       for (int p = 0; p < L.npanel; p++) {
-        const int k0 = p * NBT, pnb = std::min(NBT, (nn - 2) - k0), K = nn - k0 - 1;
+        const int k0 = p * NBT, pnb = std::min(NBT, nrefl - k0), K = nn - k0 - sh;
         panels.push_back(PanelRef{bi, k0, pnb, 0, (long long)gt_off});
         double* Gp = L.GT + gt_off;                 // pnb x pnb
         double* Tp = Gp + (size_t)pnb * pnb;        // pnb x pnb
         gt_off += 2 * (size_t)pnb * pnb;
-        const double* Vrows = L.W1 + (size_t)k0 * L.ldp + k0 + 1;  // pnb x K, row q = v_{k0+q}
+        const double* Vrows = L.W1 + (size_t)k0 * L.ldp + k0 + sh;  // pnb x K, row q = v_{k0+q}
         gram.add_out(Gp, pnb, pnb, pnb, 0.0);
         gram.add_seg(Vrows, L.ldp, 0, Vrows, L.ldp, 1, K, 1.0);
         double* VTp = L.H + vt_off;  // K x pnb (H is free after the final row permutation)
@@ -1698,12 +1741,56 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         GemmPlan& g2 = bsteps[2 * stp + 1];
         double* Wb = L.W2;  // n x pnb
         g1.add_out(Wb, pnb, nn, pnb, 0.0);
-        g1.add_seg(L.evecs + k0 + 1, nn, 0, Vrows, L.ldp, 1, K, 1.0);
-        g2.add_out(L.evecs + k0 + 1, nn, nn, K, 1.0);
+        g1.add_seg(L.evecs + k0 + sh, nn, 0, Vrows, L.ldp, 1, K, 1.0);
+        g2.add_out(L.evecs + k0 + sh, nn, nn, K, 1.0);
         g2.add_seg(Wb, pnb, 0, VTp, pnb, 1, pnb, -1.0);
       }
     }
     const size_t pan_off = push(img, panels);
+    // two-stage blocks: per stage-1 panel j0 = p kBand, the blocks with more than one row below
+    // the band (a prefix: sorted by order), six GEMMs of the trailing update in compact-WY form
+    //   X = S22 V, Y = X T1, Z = V^T Y, U = T1^T Z, W = Y - V U / 2, S22 -= V W^T + W V^T
+    const size_t bblk_off = push(img, bblk);
+    int npan1 = 0;
+    for (const BandBlock& Bb : bblk) npan1 = std::max(npan1, Bb.jfin / kBand);
+    std::vector<int> pan_active(npan1, 0);
+    std::vector<StagedGemm> s1_g((size_t)npan1 * 6);
+    for (int p = 0; p < npan1; p++) {
+      const int j0 = p * kBand;
+      GemmPlan ga, gb, gc, gd, ge, gf;
+      for (const BandBlock& Bb : bblk) {
+        const int nn = Bb.n, m = nn - j0 - kBand;
+        if (m <= 1) break;
+        pan_active[p]++;
+        const int kb = std::min(kBand, m - 1);
+        double* S22 = Bb.S + (size_t)(j0 + kBand) * Bb.lds + j0 + kBand;
+        const double* Vt = Bb.S + (size_t)j0 * Bb.lds + j0 + kBand;  // kb x m
+        double* X = Bb.scr + band_scr_x(nn);
+        double* Y = Bb.scr + band_scr_y(nn);
+        double* T1 = Bb.scr + band_scr_t(nn);
+        double* Z = Bb.scr + band_scr_z(nn);
+        double* U = Bb.scr + band_scr_u(nn);
+        ga.add_out(X, kBand, m, kb, 0.0);
+        ga.add_seg(S22, Bb.lds, 0, Vt, Bb.lds, 1, m, 1.0);
+        gb.add_out(Y, kBand, m, kb, 0.0);
+        gb.add_seg(X, kBand, 0, T1, kBand, 0, kb, 1.0);
+        gc.add_out(Z, kBand, kb, kb, 0.0);
+        gc.add_seg(Vt, Bb.lds, 0, Y, kBand, 0, m, 1.0);
+        gd.add_out(U, kBand, kb, kb, 0.0);
+        gd.add_seg(T1, kBand, 1, Z, kBand, 0, kb, 1.0);
+        ge.add_out(Y, kBand, m, kb, 1.0);
+        ge.add_seg(Vt, Bb.lds, 1, U, kBand, 0, kb, -0.5);
+        gf.add_out(S22, Bb.lds, m, m, 1.0);
+        gf.add_seg(Vt, Bb.lds, 1, Y, kBand, 1, kb, -1.0);
+        gf.add_seg(Y, kBand, 0, Vt, Bb.lds, 0, kb, -1.0);
+      }
+      s1_g[6 * p + 0] = stage_gemm(img, ga);
+      s1_g[6 * p + 1] = stage_gemm(img, gb);
+      s1_g[6 * p + 2] = stage_gemm(img, gc);
+      s1_g[6 * p + 3] = stage_gemm(img, gd);
+      s1_g[6 * p + 4] = stage_gemm(img, ge);
+      s1_g[6 * p + 5] = stage_gemm(img, gf);
+    }
     const StagedGemm gram_g = stage_gemm(img, gram), vt_g = stage_gemm(img, vt);
     std::vector<StagedGemm> bs_g(bsteps.size());
     for (size_t t = 0; t < bsteps.size(); t++) bs_g[t] = stage_gemm(img, bsteps[t]);
@@ -1711,6 +1798,30 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     if (rc) return rc;
     char* dbase = static_cast<char*>(c->desc);
     const LargeBlock* dblk = reinterpret_cast<const LargeBlock*>(dbase + blk_off);
+    const BandBlock* dbb = reinterpret_cast<const BandBlock*>(dbase + bblk_off);
+
+    // ---- 1a. two-stage reduction of the largest blocks (when few): symmetric copy, stage-1
+    //          panels and their GEMMs, bulge chasing, the T factors of its back-transform
+    if (nts > 0) {
+      {
+        PhaseScope ps(c, kPhBandReduce, s, 1 + 7 * npan1);
+        for (const BandBlock& Bb : bblk)
+          NRG_CK(cudaMemsetAsync(Bb.BND, 0, sizeof(double) * (size_t)Bb.n * kLDB, s));
+        NRG_CK(band_sym_launch(dbb, nts, blk[0].n, s));
+        for (int p = 0; p < npan1; p++) {
+          NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, s));
+          for (int q = 0; q < 6; q++) {
+            rc = launch_staged_gemm(c, s1_g[6 * p + q], s, kPhBandReduce);
+            if (rc) return rc;
+          }
+        }
+      }
+      {
+        PhaseScope ps(c, kPhBulgeChase, s, 2);
+        NRG_CK(band_chase_launch(dbb, nts, s));
+        NRG_CK(band_q2_tfactor_launch(dbb, nts, blk[0].n, s));
+      }
+    }
 
     // ---- 1. tridiagonalisation: blocks beyond cluster_max_n (sorted first) stream through
     //         TMA, blocks beyond mid_max_n are spread over the shared memory of a cluster,
@@ -1718,10 +1829,14 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     {
       int nsm = 148;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+      // the one-stage reductions: the blocks after the two-stage ones
+      const LargeBlock* b1 = blk.data() + nts;
+      const LargeBlock* d1 = dblk + nts;
+      const int nb1 = nb - nts;
       int nbig = 0;
-      while (nbig < nb && blk[nbig].n > cluster_max_n) nbig++;
+      while (nbig < nb1 && b1[nbig].n > cluster_max_n) nbig++;
       int nclu = nbig;
-      while (nclu < nb && blk[nclu].n > mid_max_n) nclu++;
+      while (nclu < nb1 && b1[nclu].n > mid_max_n) nclu++;
       // One cluster size for all cluster blocks (one launch): the smallest of 2, 4, 8 that
       // fits the largest of them, raised while the cluster CTAs still fit the SMs once. The
       // clusters serve latency: when they would not all fit the SMs at once (a batch of many
@@ -1730,8 +1845,8 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       int C = 0;
       if (nclu > nbig) {
         for (int q = 2; q <= 8 && !C; q *= 2)
-          if (sizeof(double) * cl_smem_doubles(blk[nbig].n, q) <= 232448) C = q;
-        if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", blk[nbig].n);
+          if (sizeof(double) * cl_smem_doubles(b1[nbig].n, q) <= 232448) C = q;
+        if (C == 0) return fail(NRG_ERR_ARG, "internal: no cluster size for n=%d", b1[nbig].n);
         if (C * (nclu - nbig) > nsm) {
           nbig = nclu;  // throughput regime
           C = 0;
@@ -1739,30 +1854,30 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           while (C < 8 && 2 * C * (nclu - nbig) <= nsm) C *= 2;
         }
       }
-      const bool fork = nb > nclu && (nbig > 0 || nclu > nbig);
+      const bool fork = nb1 > nclu && (nbig > 0 || nclu > nbig);
       if (fork && !c->side2) {
         NRG_CK(cudaStreamCreateWithFlags(&c->side2, cudaStreamNonBlocking));
         NRG_CK(cudaEventCreateWithFlags(&c->fork2_ev, cudaEventDisableTiming));
         NRG_CK(cudaEventCreateWithFlags(&c->join2_ev, cudaEventDisableTiming));
       }
-      PhaseScope ps(c, kPhTridiag, s, (nbig ? 2 : 0) + (nclu > nbig ? 1 : 0) + (nb > nclu ? 1 : 0));
-      if (nb > nclu) {  // one CTA per block, on the third stream when other launches run beside it
+      PhaseScope ps(c, kPhTridiag, s, (nbig ? 2 : 0) + (nclu > nbig ? 1 : 0) + (nb1 > nclu ? 1 : 0));
+      if (nb1 > nclu) {  // one CTA per block, on the third stream when other launches run beside it
         cudaStream_t ss = s;
         if (fork) {
           NRG_CK(cudaEventRecord(c->fork2_ev, s));
           NRG_CK(cudaStreamWaitEvent(c->side2, c->fork2_ev, 0));
           ss = c->side2;
         }
-        const int mn = blk[nclu].n;
+        const int mn = b1[nclu].n;
         const size_t smem = sizeof(double) * ((size_t)mn * (mn + 1) / 2 + 2 * (size_t)mn + 64);
         NRG_CK(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        tridiag_smem_kernel<<<nb - nclu, kMidThreads, smem, ss>>>(dblk + nclu);
+        tridiag_smem_kernel<<<nb1 - nclu, kMidThreads, smem, ss>>>(d1 + nclu);
         NRG_CK(cudaGetLastError());
         if (fork) NRG_CK(cudaEventRecord(c->join2_ev, ss));
       }
       if (nclu > nbig) {
-        const long long ld0 = cl_smem_doubles(blk[nbig].n, C);  // the largest block sets the layout
-        const int lmax = (int)(ld0 - (4LL * blk[nbig].n + 64));
+        const long long ld0 = cl_smem_doubles(b1[nbig].n, C);  // the largest block sets the layout
+        const int lmax = (int)(ld0 - (4LL * b1[nbig].n + 64));
         const size_t smem = sizeof(double) * (size_t)ld0;
         NRG_CK(cudaFuncSetAttribute(tridiag_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         cudaLaunchConfig_t cfg = {};
@@ -1777,13 +1892,13 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         at[0].val.clusterDim.z = 1;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, dblk + nbig, lmax));
+        NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, d1 + nbig, lmax));
       }
       if (nbig) {
-        const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)maxn +
+        const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)b1[0].n +
                                                      (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
-        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(dbase + tmap_off);
-        pack_lower_kernel<<<dim3((maxn + 7) / 8, nbig), 256, 0, s>>>(dblk);
+        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(dbase + tmap_off) + nts;
+        pack_lower_kernel<<<dim3((b1[0].n + 7) / 8, nbig), 256, 0, s>>>(d1);
         NRG_CK(cudaGetLastError());
         // Few large blocks: one cluster of kTclC CTAs per block, when the clusters fill at most
         // about two waves of the SMs and the device can hold one such cluster at a time.
@@ -1797,7 +1912,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
         auto tcl_bytes = [&](int st) {
-          return std::max(1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)maxn +
+          return std::max(1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)b1[0].n +
                                                    (size_t)kTriWarps * 2 * NB + 4 * NB + 66),
                           (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
         };
@@ -1837,7 +1952,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           }
         }
         if (tcl) {
-          const LargeBlock* db = dblk;
+          const LargeBlock* db = d1;
           void* kargs[] = {(void*)&db, (void*)&tm};
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
@@ -1847,7 +1962,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           // passes.
           const size_t smem1 = std::max(smem, (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
           NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-          tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(dblk, tm);
+          tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(d1, tm);
           NRG_CK(cudaGetLastError());
         }
       }
@@ -1907,6 +2022,11 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       NRG_CK(cudaGetLastError());
       permute_rows_kernel<<<dim3((maxn + 7) / 8, nb), 256, 0, s>>>(dblk);
       NRG_CK(cudaGetLastError());
+    }
+    // ---- 3a. two-stage blocks: the bulge-chasing reflectors applied to the eigenvector rows
+    if (nts > 0) {
+      PhaseScope sc(c, kPhBtBand, s);
+      NRG_CK(band_q2_apply_launch(dbb, nts, blk[0].n, s));
     }
     // ---- 4. back-transform
     rc = launch_staged_gemm(c, gram_g, s, kPhBtGemm);
