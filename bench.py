@@ -879,9 +879,25 @@ def serving_arm(torch, device: int, single: dict) -> dict:
     t0 = time.perf_counter()
     done = srv.serve(stream, realtime=True)
     poi = summary(done, time.perf_counter() - t0)
+    # the plain GPU path on the same 16-run mix: the same driver with one cuSOLVER eigh per block
+    # and launch, runs one after another
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import RunParams
+    PerBlock = per_block_driver(torch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    steps = 0
+    for r in reqs:
+        res = PerBlock(RunParams.from_param(parse_param(r.param)), read_data(r.data), device).run()
+        steps += len(res.block_dims)
+    torch.cuda.synchronize()
+    t_pb = time.perf_counter() - t0
+    pb = {"steps_per_s": steps / t_pb, "wall_s": t_pb, "steps": steps,
+          "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch, the 16 runs one after another"}
     return {"workload": "runs of the reference's regression inputs " + ", ".join(SERVE_MIX),
             "saturation_16_runs": sat, "poisson_4_per_s_32_requests": poi,
-            "single_run_steps_per_s": single["steps_per_s"]}
+            "single_run_steps_per_s": single["steps_per_s"], "per_block_gpu_same_mix": pb,
+            "served_over_per_block": sat["steps_per_s"] / pb["steps_per_s"]}
 
 
 def nrg_run_arm(torch, device: int, args) -> dict:
@@ -918,6 +934,7 @@ def nrg_run_arm(torch, device: int, args) -> dict:
            "ms_per_run": t_b200 * 1e3, "timing": "wall clock of whole runs (host driver included), best of 3",
            "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
            "device_phases_ms_per_run": {k: v[0] / 4 for k, v in phases.items() if v[1]},
+           "kernel_launches_per_step": sum(v[1] for v in phases.values()) / 4 / d.nmax,
            "per_block_gpu": {"steps_per_s": d.nmax / t_pb, "ms_per_run": t_pb * 1e3,
                              "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch"}}
     td = np.array(res.td)
