@@ -69,7 +69,7 @@ NRG_API int nrg_trim(nrg_ctx* ctx);
  *   cluster_max_n  larger blocks up to this order are reduced in the distributed shared
  *                  memory of a thread-block cluster when the clusters fit the SMs at once
  *                  (mid_max_n..640); larger blocks stream their trailing matrix from HBM
- *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2)
+ *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2; default 2)
  *   band_min_n     blocks of at least this order, when at most band_max_blocks of them are
  *                  in a batch, take the two-stage reduction (dense -> band on the FP64
  *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never
@@ -105,7 +105,7 @@ NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* 
 /* Same with host pointers for H[b], evals[b], evecs[b] (the call the reference's
  * diagonalise() makes with its ublas matrix); H[b] is left unchanged. The blocks stream
  * through a ring of at most three device slots in chunks of consecutive blocks (a chunk
- * holds about a quarter of the batch, at most 6 GiB): the copy of chunk k+1 to the device
+ * holds about a third of the batch, at most 16 GiB): the copy of chunk k+1 to the device
  * and of chunk k-1 back to the host overlap the solve of chunk k, on two copy streams of
  * the context. Page-locked host memory lets the copies run asynchronously; pageable
  * memory works too, with copies that do not overlap. Returns when every result is in host

@@ -14,9 +14,12 @@ are diag(2^{-k/2}) plus symmetric N(0, 0.1^2) couplings, as in the benchmark):
   step   8 batches of 40 blocks, orders log-uniform in [8, 480] (the steps of an Anderson-model
          run at keep 1000)
   wide   2 batches of 300 blocks, orders log-uniform in [8, 1024] (many runs served at once)
+  large  12 blocks in [800, 2000] and 4 blocks in [1500, 4096] (the steps of the keep-4000
+         Anderson and keep-5000 two-channel Kondo runs, bound by their largest blocks)
 Each candidate is timed with CUDA events around nrg_diag_batch (the consumed inputs are
-refreshed outside the timed region), best of `reps`, and the objective is the sum over the
-batches. Coordinate descent over the parameters, each from the current best, twice round.
+refreshed outside the timed region), best of `reps`; the objective is the mean over the
+batches of the time relative to the starting parameters. Coordinate descent over the
+parameters, each from the current best, twice round.
 
 The result is written to tuning.json beside this module, keyed by the device name, and
 applied by nrgljubljana_b200.context() to every context it creates on such a device.
@@ -41,7 +44,12 @@ GRID = {
     "small_max_n": [32, 48, 64, 80, 96],
     "mid_max_n": [128, 160, 192, 224, 236],
     "cluster_max_n": [400, 480, 560, 600, 640],
+    "band_min_n": [0, 768, 1024, 1536, 2048, 3072],
+    "band_max_blocks": [4, 8, 16, 32, 64],
 }
+KEYS = ("small_max_n", "mid_max_n", "cluster_max_n", "reduction_ctas_per_sm", "band_min_n", "band_max_blocks")
+# (batches, blocks per batch, smallest and largest order) of the timed workloads
+WORKLOADS = ((8, 40, 8, 480), (2, 300, 8, 1024), (1, 12, 800, 2000), (1, 4, 1500, 4096))
 
 
 def device_name(device: int = 0) -> str:
@@ -64,10 +72,10 @@ def load_table(device: int = 0) -> Optional[Dict[str, int]]:
     return dict(entry["tuning"]) if entry else None
 
 
-def workloads(nmin: int = 8) -> List[np.ndarray]:
+def workloads() -> List[np.ndarray]:
     rng = np.random.Generator(np.random.PCG64(SEED))
     out = []
-    for nb, nmax, k in ((40, 480, 8), (300, 1024, 2)):
+    for k, nb, nmin, nmax in WORKLOADS:
         for _ in range(k):
             u = rng.uniform(math.log(nmin), math.log(nmax), nb)
             out.append(np.clip(np.rint(np.exp(u)), nmin, nmax).astype(np.int64))
@@ -137,32 +145,43 @@ def tune(device: int = 0, reps: int = 3, allow_two_per_sm: bool = False, verbose
     batches = [_Batch(torch, ctx, s, dev, i) for i, s in enumerate(workloads())]
     grid = dict(GRID)
     grid["reduction_ctas_per_sm"] = [1, 2] if allow_two_per_sm else [1]
+    grid["band_max_blocks"] = GRID["band_max_blocks"]
 
-    def objective(t: dict) -> float:
+    base: List[float] = []
+
+    def timed(t: dict) -> List[float]:
         ctx.set_tuning(**t)
-        total = 0.0
+        out = []
         for b in batches:
             b.time_once()  # warm-up: workspace growth, first launch of a kernel
-            total += min(b.time_once() for _ in range(reps))
-        return total
+            out.append(min(b.time_once() for _ in range(reps)))
+        return out
+
+    def objective(ms: List[float]) -> float:
+        """Mean time relative to the starting parameters, so that every workload counts alike."""
+        return float(np.mean([m / b0 for m, b0 in zip(ms, base)]))
 
     best = ctx.tuning
-    best_ms = objective(best)
-    sweep = [{"tuning": dict(best), "ms": best_ms}]
+    base = timed(best)
+    best_obj = objective(base)
+    sweep = [{"tuning": dict(best), "ms": base, "objective": best_obj}]
     t0 = time.perf_counter()
     for _ in range(2):
         changed = False
-        for key in ("small_max_n", "mid_max_n", "cluster_max_n", "reduction_ctas_per_sm"):
+        for key in KEYS:
             for v in grid[key]:
                 cand = dict(best, **{key: v})
                 if cand == best or not (32 <= cand["small_max_n"] <= cand["mid_max_n"] <= cand["cluster_max_n"]):
                     continue
-                ms = objective(cand)
-                sweep.append({"tuning": cand, "ms": ms})
+                if key == "band_max_blocks" and cand["band_min_n"] == 0:
+                    continue
+                ms = timed(cand)
+                obj = objective(ms)
+                sweep.append({"tuning": cand, "ms": ms, "objective": obj})
                 if verbose:
-                    print(f"  {cand} {ms:.3f} ms", flush=True)
-                if ms < best_ms * 0.99:  # a change must win by more than the timing noise
-                    best, best_ms, changed = cand, ms, True
+                    print(f"  {cand} {obj:.4f} {[round(x, 2) for x in ms]}", flush=True)
+                if obj < best_obj * 0.99:  # a change must win by more than the timing noise
+                    best, best_obj, changed = cand, obj, True
         if not changed:
             break
     ctx.set_tuning(**best)
@@ -171,10 +190,11 @@ def tune(device: int = 0, reps: int = 3, allow_two_per_sm: bool = False, verbose
         r = b.max_residual()
         if not r <= 1e-12:
             raise RuntimeError(f"residual {r} with {best}")
-    default = sweep[0]["ms"]
-    return {"tuning": best, "objective_ms": best_ms, "default_ms": default, "speedup_vs_default": default / best_ms,
-            "workloads": "8 x 40 blocks log-uniform in [8, 480], 2 x 300 blocks log-uniform in [8, 1024] "
-                         "(seed 20261203), best of %d, sum over batches" % reps,
+    final = timed(best)
+    return {"tuning": best, "objective": best_obj, "default_ms": base, "tuned_ms": final,
+            "speedup_vs_default": float(np.mean([a / b for a, b in zip(base, final)])),
+            "workloads": "; ".join(f"{k} x {nb} blocks log-uniform in [{lo}, {hi}]" for k, nb, lo, hi in WORKLOADS)
+                         + " (seed 20261203), best of %d per batch; objective: mean time relative to the defaults" % reps,
             "sweep_s": time.perf_counter() - t0, "evaluations": len(sweep), "sweep": sweep}
 
 

@@ -35,14 +35,28 @@ struct BandBlock {
   int n, lds, J, jfin;  // J = band_nsteps(n, 0); jfin: first column of the final diagonal block
 };
 
-// Stage-1 scratch layout inside BandBlock::scr (doubles): X (n x kBand), Y (n x kBand),
-// T1, Z, U (kBand x kBand each).
-__host__ __device__ inline size_t band_scr_x(int) { return 0; }
-__host__ __device__ inline size_t band_scr_y(int n) { return (size_t)n * kBand; }
-__host__ __device__ inline size_t band_scr_t(int n) { return 2 * (size_t)n * kBand; }
-__host__ __device__ inline size_t band_scr_z(int n) { return 2 * (size_t)n * kBand + kBand * kBand; }
-__host__ __device__ inline size_t band_scr_u(int n) { return 2 * (size_t)n * kBand + 2 * kBand * kBand; }
-__host__ __device__ inline size_t band_scr_doubles(int n) { return 2 * (size_t)n * kBand + 3 * kBand * kBand; }
+// Stage-1 GEMMs whose inner dimension is the m rows below the band (X = S22 V and Z = V^T Y,
+// both only kBand wide) are split along it into band_split(m) parts of about kSplitK, summed
+// by the next GEMM as segments, so that they spread over the SMs.
+constexpr int kSplitK = 256;
+constexpr int kSplitMax = 32;
+__host__ __device__ inline int band_split(int m) {
+  const int s = (m + kSplitK - 1) / kSplitK;
+  return s < 1 ? 1 : (s > kSplitMax ? kSplitMax : s);
+}
+// Stage-1 scratch layout inside BandBlock::scr (doubles; the block's n x n W2 buffer): Y
+// (n x kBand), T1 and U (kBand x kBand each), the parts of Z (s0 x kBand x kBand) and of X
+// (s0 x n x kBand), s0 = band_split(n - kBand) the most parts of any panel of the block.
+__host__ __device__ inline size_t band_scr_y(int) { return 0; }
+__host__ __device__ inline size_t band_scr_t(int n) { return (size_t)n * kBand; }
+__host__ __device__ inline size_t band_scr_u(int n) { return (size_t)n * kBand + kBand * kBand; }
+__host__ __device__ inline size_t band_scr_z(int n, int p) {
+  return (size_t)n * kBand + (2 + (size_t)p) * kBand * kBand;
+}
+__host__ __device__ inline size_t band_scr_x(int n, int p) {
+  return (size_t)n * kBand + (2 + (size_t)band_split(n - kBand)) * kBand * kBand + (size_t)p * n * kBand;
+}
+__host__ __device__ inline size_t band_scr_doubles(int n) { return band_scr_x(n, band_split(n - kBand)); }
 
 // Device doubles of the stage-2 arrays of one block: band, reflectors, taus, T factors.
 inline size_t band_extra_doubles(int n) {

@@ -133,7 +133,7 @@ const char* phase_name(int p) {
   static const char* names[kPhCount] = {"eig_small", "tridiag", "dc_leaf", "dc_prep", "dc_secular",
                                         "dc_vectors", "dc_gemm", "sort", "bt_gemm", "bt_tfactor",
                                         "gemm3", "spec_gemm", "spec_bin", "assemble", "broaden",
-                                        "band_reduce", "bulge_chase", "bt_band"};
+                                        "band_reduce", "bulge_chase", "bt_band", "band_panel"};
   return (p >= 0 && p < kPhCount) ? names[p] : "?";
 }
 
@@ -414,13 +414,14 @@ int nrg_diag_batch_host(nrg_ctx* c, int nblk, const int* n, const double* const*
   }
   // Chunks of consecutive blocks stream through a ring of up to three device slots: the
   // host-to-device copy of chunk k+1 and the device-to-host copy of chunk k-1 run on two
-  // copy streams beside the solve of chunk k. A slot holds about a quarter of the batch,
-  // at most 6 GiB, and at most a fifth of the memory this context can use (the solve's own
-  // workspace comes on top of the three slots).
+  // copy streams beside the solve of chunk k. A slot holds about a third of the batch, at
+  // most 16 GiB, and at most a fifth of the memory this context can use (the solve's own
+  // workspace comes on top of the three slots). Few large chunks keep each solve's batch
+  // wide enough to fill the SMs.
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t usable = std::min(c->ws_limit, fr + c->ring_size + c->ws_size);
-  size_t target = std::min<size_t>(std::max<size_t>(total / 4, (size_t)64 << 20), (size_t)6 << 30);
+  size_t target = std::min<size_t>(std::max<size_t>(total / 3, (size_t)64 << 20), (size_t)16 << 30);
   target = std::max<size_t>(std::min(target, usable / 5), (size_t)16 << 20);
   std::vector<int> first(1, 0);
   size_t maxchunk = 0, cur = 0;

@@ -15,14 +15,14 @@ namespace nrg {
 enum Phase : int {
   kPhEigSmall, kPhTridiag, kPhDcLeaf, kPhDcPrep, kPhDcSecular, kPhDcVectors, kPhDcGemm, kPhSort, kPhBtGemm,
   kPhBtTfactor, kPhGemm3, kPhSpecGemm, kPhSpecBin, kPhAssemble, kPhBroaden, kPhBandReduce, kPhBulgeChase,
-  kPhBtBand, kPhCount
+  kPhBtBand, kPhBandPanel, kPhCount
 };
 const char* phase_name(int p);
 }  // namespace nrg
 
 struct nrg_ctx {
   int device = 0;
-  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 1, 0, 64};  // eigensolver launch parameters
+  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 2, 0, 64};  // eigensolver launch parameters
   // profiling: launch counts per phase (always), CUDA-event intervals (when enabled)
   bool prof = false;
   long long launches[nrg::kPhCount] = {};

@@ -183,9 +183,9 @@ __global__ void __launch_bounds__(256) band_panel_kernel(const BandBlock* __rest
 NRG_DEV double bld(const double* band, int c, int t) { return __ldcg(band + (size_t)c * kLDB + t); }
 NRG_DEV void bst(double* band, int c, int t, double x) { band[(size_t)c * kLDB + t] = x; }
 
-NRG_DEV void chase_step(const BandBlock& B, int i, int j, int lane, double* vs, double* ws) {
-  double* band = B.BND;
-  const int n = B.n, r0 = i + 1 + j * kBand, L = min(kBand, n - r0);
+NRG_DEV void chase_step(double* __restrict__ band, double* __restrict__ V2, double* __restrict__ tau2, int n,
+                        int J, int i, int j, int lane, double* vs, double* ws) {
+  const int r0 = i + 1 + j * kBand, L = min(kBand, n - r0);
   const int col = j == 0 ? i : r0 - kBand;
   const double x = lane < L ? bld(band, col, r0 + lane - col) : 0.0;
   const double sigma = warp_sum((lane >= 1 && lane < L) ? x * x : 0.0);
@@ -196,47 +196,55 @@ NRG_DEV void chase_step(const BandBlock& B, int i, int j, int lane, double* vs, 
     tau = (beta - alpha) / beta;
     if (lane >= 1 && lane < L) v = x / (alpha - beta);
   }
-  const size_t ro = (size_t)i * B.J + j;
-  B.V2[ro * kBand + lane] = v;  // zero beyond L
-  if (lane == 0) B.tau2[ro] = tau;
+  const size_t ro = (size_t)i * J + j;
+  V2[ro * kBand + lane] = v;  // zero beyond L
+  if (lane == 0) tau2[ro] = tau;
   if (lane < L) bst(band, col, r0 + lane - col, lane == 0 ? beta : 0.0);
   if (tau == 0.0) return;
   vs[lane] = v;
   __syncwarp();
-  // left: the previous bulge's other columns
-  for (int c = col + 1; c < r0; c++) {
-    const double a = lane < L ? bld(band, c, r0 + lane - c) : 0.0;
-    const double w = warp_sum(v * a);
-    if (lane < L) bst(band, c, r0 + lane - c, a - tau * v * w);
-  }
-  // both sides: the diagonal block D (L x L, symmetric, lower part stored)
-  double p = 0.0;
-  if (lane < L) {
-    for (int s = 0; s < L; s++) {
-      const double dts = s <= lane ? bld(band, r0 + s, lane - s) : bld(band, r0 + lane, s - lane);
-      p += dts * vs[s];
+  // Each phase first loads its operands into registers (all loads in flight at once), then
+  // computes and stores.
+  double a[kBand];
+  // left: the previous bulge's other columns col+1 .. r0-1 (nl <= kBand - 1 of them)
+  const int nl = r0 - col - 1;
+#pragma unroll
+  for (int cc = 0; cc < kBand - 1; cc++)
+    a[cc] = (cc < nl && lane < L) ? bld(band, col + 1 + cc, r0 + lane - col - 1 - cc) : 0.0;
+#pragma unroll
+  for (int cc = 0; cc < kBand - 1; cc++) {
+    if (cc < nl) {
+      const double w = warp_sum(v * a[cc]);
+      if (lane < L) bst(band, col + 1 + cc, r0 + lane - col - 1 - cc, a[cc] - tau * v * w);
     }
-    p *= tau;
   }
+  // both sides: the diagonal block D (L x L, symmetric, lower part stored); lane t holds row t
+#pragma unroll
+  for (int s = 0; s < kBand; s++)
+    a[s] = (lane < L && s < L) ? (s <= lane ? bld(band, r0 + s, lane - s) : bld(band, r0 + lane, s - lane)) : 0.0;
+  double p = 0.0;
+#pragma unroll
+  for (int s = 0; s < kBand; s++) p += a[s] * vs[s];
+  p *= tau;
   const double K = 0.5 * tau * warp_sum(p * v);
   const double w = p - K * v;
   ws[lane] = w;
   __syncwarp();
-  if (lane < L)
-    for (int s = 0; s <= lane; s++) {
-      const double d = bld(band, r0 + s, lane - s);
-      bst(band, r0 + s, lane - s, d - (v * ws[s] + w * vs[s]));
-    }
-  // right: the kBand rows below the block
+#pragma unroll
+  for (int s = 0; s < kBand; s++)
+    if (lane < L && s <= lane) bst(band, r0 + s, lane - s, a[s] - (v * ws[s] + w * vs[s]));
+  // right: the kBand rows below the block (the new bulge); lane u holds row r1+u
   const int r1 = r0 + L, L2 = min(kBand, n - r1);
-  if (L2 > 0 && lane < L2) {
+  if (L2 > 0) {
+#pragma unroll
+    for (int s = 0; s < kBand; s++) a[s] = (lane < L2 && s < L) ? bld(band, r0 + s, r1 + lane - r0 - s) : 0.0;
     double y = 0.0;
-    for (int s = 0; s < L; s++) y += bld(band, r0 + s, r1 + lane - r0 - s) * vs[s];
+#pragma unroll
+    for (int s = 0; s < kBand; s++) y += a[s] * vs[s];
     y *= tau;
-    for (int s = 0; s < L; s++) {
-      const int t = r1 + lane - r0 - s;
-      bst(band, r0 + s, t, bld(band, r0 + s, t) - y * vs[s]);
-    }
+#pragma unroll
+    for (int s = 0; s < kBand; s++)
+      if (lane < L2 && s < L) bst(band, r0 + s, r1 + lane - r0 - s, a[s] - y * vs[s]);
   }
   __syncwarp();
 }
@@ -289,7 +297,7 @@ __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const Band
         }
         __threadfence_block();
       }
-      chase_step(B, i, j, lane, vsh[warp], wsh[warp]);
+      chase_step(B.BND, B.V2, B.tau2, n, J, i, j, lane, vsh[warp], wsh[warp]);
       __syncwarp();
       __threadfence_block();
       if (lane == 0) prog[warp] = i * (J + 1) + (j + 1 == ns ? J : j + 1);
@@ -367,8 +375,13 @@ __global__ void __launch_bounds__(128) band_q2_tfactor_kernel(const BandBlock* _
 
 // The eigenvector rows Zt (evecs, n x n) times Q2^T: for every group, in the order of the
 // product (groups g descending, steps j ascending), Zt[:, R] -= ((Zt[:, R] V) T^T) V^T.
-// Each CTA owns kQ2Rows eigenvector rows and walks all groups; 256 threads.
+// Each CTA owns kQ2Rows eigenvector rows and walks all groups. Per group the three small
+// products run on the FP64 tensor cores (DMMA m8n8k4) from shared memory, zero-padded to
+// 64 x 64 (window), 32 x 64 (V) and 32 x 32 (T); 8 warps.
 constexpr int kQ2Rows = 64;
+static_assert(kGRows <= 64 && kGrp == 32 && kQ2Rows == 64, "the DMMA tiling below assumes these shapes");
+constexpr int kLW = 68;  // row stride (doubles) of the window and of V in shared memory
+constexpr int kLX = 36;  // row stride of X, X2 and T
 
 __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __restrict__ blocks) {
   const BandBlock B = blocks[blockIdx.y];
@@ -377,58 +390,107 @@ __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __r
   if (e0 >= n || J == 0) return;
   const int ne = min(kQ2Rows, n - e0);
   extern __shared__ __align__(16) double q2sm[];
-  double* W = q2sm;                            // kQ2Rows x (kGRows + 1)
-  double* V = W + kQ2Rows * (kGRows + 1);      // kGrp x (kGRows + 1)
-  double* T = V + kGrp * (kGRows + 1);         // kGrp x (kGrp + 1)
-  double* X = T + kGrp * (kGrp + 1);           // kQ2Rows x (kGrp + 1)
-  double* X2 = X + kQ2Rows * (kGrp + 1);       // kQ2Rows x (kGrp + 1)
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int ldw = kGRows + 1, ldx = kGrp + 1;
+  double* W = q2sm;                  // 64 x kLW: the window Zt[e0 .., R]
+  double* V = W + 64 * kLW;          // 32 x kLW: row q = reflector q over the window's columns
+  double* T = V + 32 * kLW;          // 32 x kLX
+  double* X = T + 32 * kLX;          // 64 x kLX
+  double* X2 = X + 64 * kLX;         // 64 x kLX
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int fr = lane >> 2, fc = lane & 3;
   for (int g = band_ngroups(n) - 1; g >= 0; g--) {
     for (int j = 0; j < J; j++) {
       const int nm = group_members(n, g, j);
       if (nm == 0) break;  // members form a prefix in j as well: no later step has any
       const int rs = g * kGrp + 1 + j * kBand;
       const int nr = min(kGRows, n - rs);
-      // load V, T and the window
-      for (int idx = tid; idx < kGrp * kGRows; idx += nt) {
-        const int q = idx / kGRows, r = idx % kGRows;
+      for (int idx = tid; idx < 32 * 64; idx += nt) {
+        const int q = idx >> 6, r = idx & 63;
         double x = 0.0;
         if (q < nm && r >= q && r < q + kBand && r < nr)
           x = B.V2[((size_t)(g * kGrp + q) * J + j) * kBand + (r - q)];
-        V[q * ldw + r] = x;
+        V[q * kLW + r] = x;
       }
       const double* Tg = B.T2 + ((size_t)g * J + j) * kGrp * kGrp;
-      for (int idx = tid; idx < kGrp * kGrp; idx += nt) T[(idx / kGrp) * ldx + idx % kGrp] = Tg[idx];
-      for (int idx = tid; idx < ne * nr; idx += nt) {
-        const int e = idx / nr, r = idx % nr;
-        W[e * ldw + r] = B.evecs[(size_t)(e0 + e) * n + rs + r];
+      for (int idx = tid; idx < kGrp * kGrp; idx += nt) T[(idx / kGrp) * kLX + idx % kGrp] = Tg[idx];
+      for (int idx = tid; idx < 64 * 64; idx += nt) {
+        const int e = idx >> 6, r = idx & 63;
+        W[e * kLW + r] = (e < ne && r < nr) ? B.evecs[(size_t)(e0 + e) * n + rs + r] : 0.0;
       }
       __syncthreads();
-      // X = W V^T-columns: X(e, q) = sum_r W(e, r) V(q, r)
-      for (int idx = tid; idx < ne * nm; idx += nt) {
-        const int e = idx / nm, q = idx % nm;
-        double s = 0.0;
-        const int r1 = min(q + kBand, nr);
-        for (int r = q; r < r1; r++) s += W[e * ldw + r] * V[q * ldw + r];
-        X[e * ldx + q] = s;
+      const int rb = (warp >> 1) * 16;  // the warp's 16 rows
+      // X (64 x 32) = W V^T, K = 64: warp tile 16 x 16
+      {
+        const int cb = (warp & 1) * 16;
+        double acc[2][2][2] = {};
+        for (int k0 = 0; k0 < 64; k0 += 4) {
+          double a[2], bb[2];
+#pragma unroll
+          for (int i = 0; i < 2; i++) a[i] = W[(rb + 8 * i + fr) * kLW + k0 + fc];
+#pragma unroll
+          for (int jj = 0; jj < 2; jj++) bb[jj] = V[(cb + 8 * jj + fr) * kLW + k0 + fc];
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++) dmma884(acc[i][jj][0], acc[i][jj][1], a[i], bb[jj]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) X[(rb + 8 * i + fr) * kLX + cb + 8 * jj + 2 * fc + h] = acc[i][jj][h];
       }
       __syncthreads();
-      // X2 = X T^T: X2(e, q) = sum_{q' >= q} X(e, q') T(q, q')
-      for (int idx = tid; idx < ne * nm; idx += nt) {
-        const int e = idx / nm, q = idx % nm;
-        double s = 0.0;
-        for (int k = q; k < nm; k++) s += X[e * ldx + k] * T[q * ldx + k];
-        X2[e * ldx + q] = s;
+      // X2 (64 x 32) = X T^T, K = 32
+      {
+        const int cb = (warp & 1) * 16;
+        double acc[2][2][2] = {};
+        for (int k0 = 0; k0 < 32; k0 += 4) {
+          double a[2], bb[2];
+#pragma unroll
+          for (int i = 0; i < 2; i++) a[i] = X[(rb + 8 * i + fr) * kLX + k0 + fc];
+#pragma unroll
+          for (int jj = 0; jj < 2; jj++) bb[jj] = T[(cb + 8 * jj + fr) * kLX + k0 + fc];
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++) dmma884(acc[i][jj][0], acc[i][jj][1], a[i], bb[jj]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) X2[(rb + 8 * i + fr) * kLX + cb + 8 * jj + 2 * fc + h] = acc[i][jj][h];
       }
       __syncthreads();
-      // W -= X2 V, written back
-      for (int idx = tid; idx < ne * nr; idx += nt) {
-        const int e = idx / nr, r = idx % nr;
-        double s = 0.0;
-        const int q0 = max(0, r - kBand + 1), q1 = min(nm - 1, r);
-        for (int q = q0; q <= q1; q++) s += X2[e * ldx + q] * V[q * ldw + r];
-        B.evecs[(size_t)(e0 + e) * n + rs + r] = W[e * ldw + r] - s;
+      // W -= X2 V (64 x 64, K = 32): warp tile 16 x 32, written back to the eigenvector rows
+      {
+        const int cb = (warp & 1) * 32;
+        double acc[2][4][2] = {};
+        for (int k0 = 0; k0 < 32; k0 += 4) {
+          double a[2], bb[4];
+#pragma unroll
+          for (int i = 0; i < 2; i++) a[i] = X2[(rb + 8 * i + fr) * kLX + k0 + fc];
+#pragma unroll
+          for (int jj = 0; jj < 4; jj++) bb[jj] = V[(k0 + fc) * kLW + cb + 8 * jj + fr];
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) dmma884(acc[i][jj][0], acc[i][jj][1], a[i], bb[jj]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const int e = rb + 8 * i + fr;
+          if (e >= ne) continue;
+#pragma unroll
+          for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int r = cb + 8 * jj + 2 * fc + h;
+              if (r < nr) B.evecs[(size_t)(e0 + e) * n + rs + r] = W[e * kLW + r] - acc[i][jj][h];
+            }
+        }
       }
       __syncthreads();
     }
@@ -466,8 +528,7 @@ cudaError_t band_q2_tfactor_launch(const BandBlock* d_blocks, int nblk, int maxn
 
 cudaError_t band_q2_apply_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaStream_t s) {
   if (nblk <= 0) return cudaSuccess;
-  const size_t smem = sizeof(double) * ((size_t)kQ2Rows * (kGRows + 1) + (size_t)kGrp * (kGRows + 1) +
-                                        (size_t)kGrp * (kGrp + 1) + 2 * (size_t)kQ2Rows * (kGrp + 1));
+  const size_t smem = sizeof(double) * (64 * kLW + 32 * kLW + 32 * kLX + 2 * 64 * kLX);
   cudaError_t err = cudaFuncSetAttribute(band_q2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (err != cudaSuccess) return err;
   band_q2_apply_kernel<<<dim3((unsigned)((maxn + kQ2Rows - 1) / kQ2Rows), (unsigned)nblk), 256, smem, s>>>(d_blocks);

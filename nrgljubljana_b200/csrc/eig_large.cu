@@ -1765,19 +1765,34 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         const int kb = std::min(kBand, m - 1);
         double* S22 = Bb.S + (size_t)(j0 + kBand) * Bb.lds + j0 + kBand;
         const double* Vt = Bb.S + (size_t)j0 * Bb.lds + j0 + kBand;  // kb x m
-        double* X = Bb.scr + band_scr_x(nn);
         double* Y = Bb.scr + band_scr_y(nn);
         double* T1 = Bb.scr + band_scr_t(nn);
-        double* Z = Bb.scr + band_scr_z(nn);
         double* U = Bb.scr + band_scr_u(nn);
-        ga.add_out(X, kBand, m, kb, 0.0);
-        ga.add_seg(S22, Bb.lds, 0, Vt, Bb.lds, 1, m, 1.0);
+        const int ns = band_split(m), chunk = (m + ns - 1) / ns;
+        // X = S22 V and Z = V^T Y in parts along m (rows k0 .. k1 of V), summed as segments
+        for (int q = 0; q < ns; q++) {
+          const int k0 = q * chunk, k1 = std::min(m, k0 + chunk);
+          if (k1 <= k0) break;
+          double* Xq = Bb.scr + band_scr_x(nn, q);
+          ga.add_out(Xq, kBand, m, kb, 0.0);
+          ga.add_seg(S22 + k0, Bb.lds, 0, Vt + k0, Bb.lds, 1, k1 - k0, 1.0);
+        }
         gb.add_out(Y, kBand, m, kb, 0.0);
-        gb.add_seg(X, kBand, 0, T1, kBand, 0, kb, 1.0);
-        gc.add_out(Z, kBand, kb, kb, 0.0);
-        gc.add_seg(Vt, Bb.lds, 0, Y, kBand, 0, m, 1.0);
+        for (int q = 0; q < ns; q++) {
+          if (q * chunk >= m) break;
+          gb.add_seg(Bb.scr + band_scr_x(nn, q), kBand, 0, T1, kBand, 0, kb, 1.0);
+        }
+        for (int q = 0; q < ns; q++) {
+          const int k0 = q * chunk, k1 = std::min(m, k0 + chunk);
+          if (k1 <= k0) break;
+          gc.add_out(Bb.scr + band_scr_z(nn, q), kBand, kb, kb, 0.0);
+          gc.add_seg(Vt + k0, Bb.lds, 0, Y + (size_t)k0 * kBand, kBand, 0, k1 - k0, 1.0);
+        }
         gd.add_out(U, kBand, kb, kb, 0.0);
-        gd.add_seg(T1, kBand, 1, Z, kBand, 0, kb, 1.0);
+        for (int q = 0; q < ns; q++) {
+          if (q * chunk >= m) break;
+          gd.add_seg(T1, kBand, 1, Bb.scr + band_scr_z(nn, q), kBand, 0, kb, 1.0);
+        }
         ge.add_out(Y, kBand, m, kb, 1.0);
         ge.add_seg(Vt, Bb.lds, 1, U, kBand, 0, kb, -0.5);
         gf.add_out(S22, Bb.lds, m, m, 1.0);
@@ -1804,12 +1819,17 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     //          panels and their GEMMs, bulge chasing, the T factors of its back-transform
     if (nts > 0) {
       {
-        PhaseScope ps(c, kPhBandReduce, s, 1 + 7 * npan1);
         for (const BandBlock& Bb : bblk)
           NRG_CK(cudaMemsetAsync(Bb.BND, 0, sizeof(double) * (size_t)Bb.n * kLDB, s));
-        NRG_CK(band_sym_launch(dbb, nts, blk[0].n, s));
+        {
+          PhaseScope ps(c, kPhBandReduce, s);
+          NRG_CK(band_sym_launch(dbb, nts, blk[0].n, s));
+        }
         for (int p = 0; p < npan1; p++) {
-          NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, s));
+          {
+            PhaseScope ps(c, kPhBandPanel, s);
+            NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, s));
+          }
           for (int q = 0; q < 6; q++) {
             rc = launch_staged_gemm(c, s1_g[6 * p + q], s, kPhBandReduce);
             if (rc) return rc;
@@ -1903,11 +1923,13 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         // Few large blocks: one cluster of kTclC CTAs per block, when the clusters fill at most
         // about two waves of the SMs and the device can hold one such cluster at a time.
         bool tcl = false;
-        // At least half of an SM's shared memory: one CTA of this kernel per SM. With two of its
-        // CTAs on one SM the reductions came out wrong on B200; with one per SM every check
-        // passes. The likely cause, a race on alpha = v[k+1] in the reflector step that grows
-        // with the skew between warps, is fixed; two per SM wait for a run that confirms it. A cluster holds 8 SMs per block either way. The ring gets 8,
-        // 6 or 4 slabs per warp, the most that fit: one CTA per SM leaves the room.
+        // reduction_ctas_per_sm (nrg_tuning) sets how many CTAs of the streaming kernels share an
+        // SM: one, when each requests at least half of an SM's shared memory; two (the default)
+        // otherwise. Two per SM once gave wrong reductions through a race on alpha = v[k+1] in the
+        // reflector step (alpha was read after a barrier that a thread overwriting it could
+        // pass); alpha is now read before that barrier, and batches with more of these CTAs than
+        // SMs pass every check on B200 with two per SM. The ring gets 8, 6 or 4 slabs per warp,
+        // the most that fit.
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
@@ -1956,10 +1978,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           void* kargs[] = {(void*)&db, (void*)&tm};
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
-          // One CTA per SM here too: batches with more of these CTAs than SMs, where two of them
-          // shared an SM, gave wrong reductions for some blocks (the same alpha race as the
-          // cluster kernel, now fixed, pending a confirming run); with one per SM every check
-          // passes.
+          // one or two CTAs per SM as above
           const size_t smem1 = std::max(smem, (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
           NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
           tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(d1, tm);

@@ -428,10 +428,14 @@ class QSRun:
                 total += t.numel() * t.element_size()
         return total
 
-    def _gemm(self, terms: np.ndarray) -> None:
-        """One batched GEMM call for `terms`, or their collection by a merging server."""
+    def _gemm(self, terms: np.ndarray, reads=()) -> None:
+        """One batched GEMM call for `terms`, or their collection by a merging server. `reads`
+        are the matrix sets the terms read besides this step's eigenvectors: collected terms
+        keep them alive until the server's call is on the stream (the run drops its previous
+        operators when the step ends, and the caching allocator may hand their memory to
+        another run's outputs, whose zero fill would come first)."""
         if self.deferred_terms is not None:
-            self.deferred_terms.append(terms)
+            self.deferred_terms.append((terms, reads))
         else:
             gemm3_batch_array(terms, self.ctx, self.stream)
 
@@ -787,7 +791,7 @@ class QSRun:
             op = np.repeat(np.arange(cold.nops, dtype=np.uint64), len(b))
             t["M"] += op * np.uint64(8 * out.total)
             t["O"] += op * np.uint64(8 * cold.total)
-            self._gemm(t)
+            self._gemm(t, (cold,))
         return out
 
     def _recalc_tensor(self, diag: Dict[Invar, Sub], cold: MatSet, tables, factor, rows=None) -> MatSet:

@@ -127,7 +127,7 @@ class Server:
             info = diag_batch_ptrs(ns, Hp, Ep, Vp, self.ctx, self.stream)
             self.ticks += 1
             self.blocks_per_tick.append(len(ns))
-            terms: List[np.ndarray] = []
+            terms: List[tuple] = []  # (GEMM3 terms, matrix sets they read)
             reads: List = []
             o = 0
             for (_, run, _, _), j in zip(active, jobs):
@@ -138,8 +138,9 @@ class Server:
                     run.deferred_terms = run.deferred_reads = None
                 o += len(j.ns)
             if terms:
-                gemm3_batch_array(np.concatenate(terms), self.ctx, self.stream)
+                gemm3_batch_array(np.concatenate([t for t, _ in terms]), self.ctx, self.stream)
                 self.recalc_calls += 1
+            del terms  # the operands they read may be reused from here on (stream-ordered)
             for gather in reads:
                 gather()
             still = []

@@ -23,7 +23,7 @@ from test_dmnrg import ORA_ATOL_REL_TO_MAX, ORA_RTOL, assert_spectrum
 pytestmark = pytest.mark.gpu
 
 TD_RTOL, TD_ATOL = 1e-10, 1e-11  # td of the device run against the oracle (other eigensolver)
-TDFDM_RTOL = 1e-10
+TDFDM_RTOL, TDFDM_ATOL = 1e-10, 1e-11
 
 KONDO_PARAM = """[param]
 symtype=QS
@@ -82,7 +82,8 @@ def test_two_channel_kondo_fdm_reduced(oracle):
     name = "spin_FDM_dens_S_imp-S_imp"
     assert_spectrum(res.spectra[name], spec[name], ORA_RTOL, ORA_ATOL_REL_TO_MAX, f"{name} vs oracle")
     assert res.tdfdm[0] == fo["tdfdm"][0]
-    assert np.allclose(res.tdfdm[1], fo["tdfdm"][1], rtol=TDFDM_RTOL, atol=0), (res.tdfdm[1], fo["tdfdm"][1])
+    # the FDM heat capacity at T = 1e-6 vanishes: round-off noise of order 1e-35 in both runs
+    assert np.allclose(res.tdfdm[1], fo["tdfdm"][1], rtol=TDFDM_RTOL, atol=TDFDM_ATOL), (res.tdfdm[1], fo["tdfdm"][1])
 
 
 def test_anderson_dmnrg_coarse_bins_reduced(oracle):

@@ -14,7 +14,8 @@ from eigcheck import check_eig
 def test_table_lookup_by_device_name(tmp_path, monkeypatch):
     from nrgljubljana_b200 import autotune
     tab = {"NVIDIA B200": {"tuning": {"small_max_n": 48, "mid_max_n": 192, "cluster_max_n": 560,
-                                      "reduction_ctas_per_sm": 1}, "objective_ms": 1.0}}
+                                      "reduction_ctas_per_sm": 1, "band_min_n": 2048, "band_max_blocks": 8},
+                           "objective": 0.9}}
     p = tmp_path / "tuning.json"
     p.write_text(json.dumps(tab))
     monkeypatch.setattr(autotune, "TABLE", str(p))
@@ -27,8 +28,9 @@ def test_table_lookup_by_device_name(tmp_path, monkeypatch):
 def test_workloads_are_seeded():
     from nrgljubljana_b200 import autotune
     a, b = autotune.workloads(), autotune.workloads()
-    assert len(a) == 10 and all(np.array_equal(x, y) for x, y in zip(a, b))
-    assert max(int(x.max()) for x in a[:8]) <= 480 and max(int(x.max()) for x in a[8:]) <= 1024
+    assert len(a) == 12 and all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert max(int(x.max()) for x in a[:8]) <= 480 and max(int(x.max()) for x in a[8:10]) <= 1024
+    assert 800 <= a[10].min() and a[10].max() <= 2000 and 1500 <= a[11].min() and a[11].max() <= 4096
 
 
 @pytest.mark.gpu
