@@ -139,4 +139,8 @@ def test_spectral_runs_queue_under_a_tight_budget():
         assert same(d.result, a), d.tag
         assert sorted(a.spectra) == sorted(d.result.spectra)
         for k in a.spectra:
-            assert np.array_equal(a.spectra[k], d.result.spectra[k]), (d.tag, k)
+            # binning sums with FP64 atomics: equal up to the order of the sums (1e-10 of the
+            # largest bin, the spectral parity bar)
+            x, y = a.spectra[k], d.result.spectra[k]
+            assert x.shape == y.shape and np.array_equal(x[:, 0], y[:, 0]), (d.tag, k)
+            assert np.abs(x[:, 1] - y[:, 1]).max() <= 1e-10 * np.abs(x[:, 1]).max(), (d.tag, k)
