@@ -9,7 +9,8 @@ namespace nrg {
 constexpr int kBand = 32;              // bandwidth after stage 1 = reflector length of stage 2
 constexpr int kGrp = 32;               // bulge-chasing sweeps per compact-WY group of the back-transform
 constexpr int kLDB = 2 * kBand + 1;    // band storage per column: distances 0 .. 2 kBand below the diagonal
-constexpr int kChaseWarps = 16;        // sweeps in flight in one CTA of the bulge chasing
+constexpr int kChaseWarps = 16;        // warps (sweeps in flight) per CTA of the bulge chasing
+constexpr int kChaseCTAs = 4;          // CTAs (a cluster) per block in the bulge chasing
 
 // Steps (reflectors) of bulge-chasing sweep i of an order-n band matrix: step j acts on rows
 // i+1+j*kBand .. +kBand-1 (clipped at n) and exists while it has at least two rows.
@@ -65,7 +66,7 @@ inline size_t band_extra_doubles(int n) {
 }
 
 cudaError_t band_sym_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaStream_t s);
-cudaError_t band_panel_launch(const BandBlock* d_blocks, int nactive, int j0, cudaStream_t s);
+cudaError_t band_panel_launch(const BandBlock* d_blocks, int nactive, int j0, int mmax, cudaStream_t s);
 cudaError_t band_chase_launch(const BandBlock* d_blocks, int nblk, cudaStream_t s);
 cudaError_t band_q2_tfactor_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaStream_t s);
 cudaError_t band_q2_apply_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaStream_t s);

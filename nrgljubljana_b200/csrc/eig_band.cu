@@ -18,6 +18,7 @@
 // Published methods: Householder reflectors as dlarfg (v0 = 1), the compact-WY
 // representation (Schreiber-Van Loan), two-stage tridiagonalisation with bulge chasing
 // (Bischof-Lang-Sun successive band reduction; pipelined sweeps as in Haidar-Ltaief-Dongarra).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "band.h"
@@ -59,116 +60,161 @@ __global__ void __launch_bounds__(256) band_sym_kernel(const BandBlock* __restri
 // ---------------------------------------------------------------- stage 1: panel QR
 // Panel at column j0 of every block with m = n - j0 - kBand > 1 rows below the band. The
 // panel's columns are held transposed in rows j0 .. j0+kBand-1 of the symmetric S:
-// P(q, i) = S[(j0+q)*lds + j0 + kBand + i], i < m. On exit:
+// P(q, i) = S[(j0+q)*lds + j0 + kBand + i], i < m. One thread-block cluster of PC CTAs per
+// block: CTA r keeps P(:, i) for its share of i in shared memory; the Householder QR runs
+// column by column, each column's norm and the dot products of the remaining panel rows with
+// its reflector summed over the cluster through distributed shared memory (every CTA sums the
+// shares in the same order, so all hold the same scalars): two cluster barriers per column.
+// On exit:
 //   - BND holds the lower triangle of the diagonal block (rows/columns j0..j0+kBand-1) and
 //     R, the panel's triangular factor (the band below the diagonal block);
 //   - row k = j0+q of S holds reflector k in the back-transform's form: zeros from the start
 //     of its back-transform panel up to k+kBand, 1 at k+kBand, v beyond -- which is also
 //     exactly the kb x m matrix Vt that the GEMMs of the trailing update read;
 //   - tau1[k], and T1 (kBand x kBand, zero-padded) of H_j0 ... H_j0+kb-1 = I - V T1 V^T.
-__global__ void __launch_bounds__(256) band_panel_kernel(const BandBlock* __restrict__ blocks, int j0) {
-  const BandBlock B = blocks[blockIdx.x];
+constexpr int kPanelThreads = 256;
+constexpr int kPanelPairs = kBand * (kBand - 1) / 2;
+
+__global__ void __launch_bounds__(kPanelThreads) band_panel_kernel(const BandBlock* __restrict__ blocks, int j0,
+                                                                   int chunk_max) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int PC = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const BandBlock B = blocks[blockIdx.x / PC];
   const int n = B.n, ld = B.lds, b = kBand;
   const int m = n - j0 - b;
-  if (m <= 1) return;
-  const int kb = min(b, m - 1);
+  const bool active = m > 1;  // every CTA of the cluster takes every barrier either way
+  const int kb = active ? min(b, m - 1) : 0;
+  const int chunk = active ? (m + PC - 1) / PC : 0;
+  const int c0 = active ? min(m, rank * chunk) : 0, c1 = active ? min(m, c0 + chunk) : 0, nc = c1 - c0;
   double* P = B.S + (size_t)j0 * ld + j0 + b;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5, nt = blockDim.x;
-  __shared__ double red[64];
-  __shared__ double stau[kBand];
-  __shared__ double G[kBand][kBand + 1];
-  __shared__ double T[kBand][kBand + 1];
-  __shared__ double wv[kBand];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = kPanelThreads / 32;
+  extern __shared__ __align__(16) double psm[];
+  const int lp = chunk_max + 1;              // row stride of the slab
+  double* Ps = psm;                          // kBand x lp: P(q, c0 + i)
+  double* sig = Ps + (size_t)b * lp;         // 2: this CTA's share of sigma, and alpha if it owns column q
+  double* dots = sig + 2;                    // kBand: shares of the dot products
+  double* gram = dots + b;                   // kPanelPairs: shares of the Gram matrix
+  double* red = gram + kPanelPairs;          // 64
+  __shared__ double Tsm[kBand][kBand + 1];
+  __shared__ double wv[kBand], stau[kBand];
 
-  // 1. lower triangle of the diagonal block into the band
-  for (int idx = tid; idx < b * b; idx += nt) {
-    const int rr = idx / b, cc = idx % b;
-    if (rr >= cc && j0 + rr < n) B.BND[(size_t)(j0 + cc) * kLDB + (rr - cc)] = B.S[(size_t)(j0 + rr) * ld + j0 + cc];
+  for (int idx = tid; idx < b * nc; idx += kPanelThreads) {
+    const int q = idx / nc, i = idx % nc;
+    Ps[q * lp + i] = P[(size_t)q * ld + c0 + i];
   }
-  // 2. Householder QR, column by column; rows r > q (columns not yet factored) are owned by
-  //    one warp each for the update
-  for (int q = 0; q < kb; q++) {
-    double* pq = P + (size_t)q * ld;
-    double part = 0.0;
-    for (int i = q + 1 + tid; i < m; i += nt) {
-      const double x = pq[i];
-      part += x * x;
+  if (rank == 0 && active)  // lower triangle of the diagonal block into the band
+    for (int idx = tid; idx < b * b; idx += kPanelThreads) {
+      const int rr = idx / b, cc = idx % b;
+      if (rr >= cc && j0 + rr < n)
+        B.BND[(size_t)(j0 + cc) * kLDB + (rr - cc)] = B.S[(size_t)(j0 + rr) * ld + j0 + cc];
     }
-    const double sigma = block_sum(part, red);
-    const double alpha = pq[q];
-    double tau = 0.0, beta = alpha;
+  __syncthreads();
+  for (int q = 0; q < kb; q++) {
+    double* pq = Ps + (size_t)q * lp;
+    // this CTA's share of sigma = sum_{i > q} P(q, i)^2; alpha = P(q, q) from its owner
+    double part = 0.0;
+    for (int i = max(q + 1 - c0, 0) + tid; i < nc; i += kPanelThreads) part += pq[i] * pq[i];
+    part = block_sum(part, red);
+    if (tid == 0) {
+      sig[0] = part;
+      sig[1] = (q >= c0 && q < c1) ? pq[q - c0] : 0.0;
+    }
+    cl.sync();  // (1) shares of sigma and alpha
+    double sigma = 0.0, alpha = 0.0;
+    for (int r = 0; r < PC; r++) {
+      const double* rs = cl.map_shared_rank(sig, r);
+      sigma += rs[0];
+      alpha += rs[1];
+    }
+    double tau = 0.0, beta = alpha, scale = 1.0;
     if (sigma > 0.0) {
       beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
       tau = (beta - alpha) / beta;
-      const double scale = 1.0 / (alpha - beta);
-      for (int i = q + 1 + tid; i < m; i += nt) pq[i] *= scale;
+      scale = 1.0 / (alpha - beta);
+      for (int i = max(q + 1 - c0, 0) + tid; i < nc; i += kPanelThreads) pq[i] *= scale;
     }
     if (tid == 0) stau[q] = tau;
-    __syncthreads();  // v_q complete; every thread has read alpha
+    __syncthreads();
+    // shares of w_r = v . P(r, :) for r > q (v(q) = 1, v(i > q) = the scaled row q)
+    for (int r = q + 1 + warp; r < b; r += nw) {
+      const double* pr = Ps + (size_t)r * lp;
+      double s = 0.0;
+      for (int i = max(q - c0, 0) + lane; i < nc; i += 32) s += pr[i] * (i + c0 == q ? 1.0 : pq[i]);
+      s = warp_sum(s);
+      if (lane == 0) dots[r] = s;
+    }
+    cl.sync();  // (2) shares of the dot products
     if (tau != 0.0) {
       for (int r = q + 1 + warp; r < b; r += nw) {
-        double* pr = P + (size_t)r * ld;
-        double s = 0.0;
-        for (int i = q + 1 + lane; i < m; i += 32) s += pr[i] * pq[i];
-        s = warp_sum(s) + pr[q];
-        const double f = tau * s;
-        __syncwarp();
-        if (lane == 0) pr[q] -= f;
-        for (int i = q + 1 + lane; i < m; i += 32) pr[i] -= f * pq[i];
+        double w = 0.0;
+        for (int k = 0; k < PC; k++) w += cl.map_shared_rank(dots, k)[r];
+        const double f = tau * w;
+        double* pr = Ps + (size_t)r * lp;
+        for (int i = max(q - c0, 0) + lane; i < nc; i += 32) pr[i] -= f * (i + c0 == q ? 1.0 : pq[i]);
       }
     }
-    __syncthreads();
-    if (tid == 0) pq[q] = beta;
+    if (tid == 0 && q >= c0 && q < c1) pq[q - c0] = beta;
     __syncthreads();
   }
-  for (int q = kb + tid; q < b; q += nt) stau[q] = 0.0;
-  __syncthreads();
-  // 3. R into the band: A(j0+b+i, j0+q) = R(i, q) = P(q, i) for i <= q
-  for (int idx = tid; idx < b * b; idx += nt) {
-    const int q = idx / b, i = idx % b;
-    if (i <= q && i < m && j0 + q < n) B.BND[(size_t)(j0 + q) * kLDB + (b + i - q)] = P[(size_t)q * ld + i];
-  }
-  // 4. Gram matrix G(q, r) = v_q . v_r for r < q < kb (v_r(q) = P(r, q)), then T1
-  const int npair = kb * (kb - 1) / 2;
-  for (int p = warp; p < npair; p += nw) {
+  for (int q = kb + tid; q < b; q += kPanelThreads) stau[q] = 0.0;
+  // shares of the Gram matrix G(q, r) = v_q . v_r, r < q < kb
+  for (int p = warp; p < kPanelPairs; p += nw) {
     int q = 1;
     while ((q * (q + 1)) / 2 <= p) q++;
     const int r = p - (q * (q - 1)) / 2;
-    const double* pq = P + (size_t)q * ld;
-    const double* pr = P + (size_t)r * ld;
     double s = 0.0;
-    for (int i = q + 1 + lane; i < m; i += 32) s += pq[i] * pr[i];
-    s = warp_sum(s);
-    if (lane == 0) G[q][r] = s + pr[q];
-  }
-  for (int idx = tid; idx < b * (b + 1); idx += nt) T[idx / (b + 1)][idx % (b + 1)] = 0.0;
-  __syncthreads();
-  for (int q = 0; q < kb; q++) {
-    // T(0:q, q) = -tau_q T(0:q, 0:q) G(q, 0:q)^T
-    if (tid < q) wv[tid] = -stau[q] * G[q][tid];
-    __syncthreads();
-    if (tid < q) {
-      double s = 0.0;
-      for (int r = tid; r < q; r++) s += T[tid][r] * wv[r];
-      T[tid][q] = s;
+    if (q < kb) {
+      const double* pq = Ps + (size_t)q * lp;
+      const double* pr = Ps + (size_t)r * lp;
+      for (int i = max(q - c0, 0) + lane; i < nc; i += 32) s += (i + c0 == q ? 1.0 : pq[i]) * pr[i];
     }
-    if (tid == q) T[q][q] = stau[q];
+    s = warp_sum(s);
+    if (lane == 0) gram[p] = s;
+  }
+  __syncthreads();
+  // the panel rows back in back-transform form (zeros up to the unit), and R into the band
+  for (int idx = tid; idx < b * nc; idx += kPanelThreads) {
+    const int q = idx / nc, i = idx % nc, gi = c0 + i;
+    const double x = Ps[q * lp + i];
+    if (gi <= q && q < b && j0 + q < n) B.BND[(size_t)(j0 + q) * kLDB + (b + gi - q)] = x;  // R(gi, q)
+    P[(size_t)q * ld + gi] = gi < q ? 0.0 : (gi == q ? 1.0 : x);
+  }
+  cl.sync();  // (3) every share of the Gram matrix is complete
+  if (rank == 0 && active) {
+    // zeros left of the panel from the reflector's back-transform panel start (+ kBand)
+    for (int q = 0; q < b; q++) {
+      const int k = j0 + q;
+      if (k >= n) break;
+      double* row = B.S + (size_t)k * ld;
+      const int cz0 = (k / kBtPanel) * kBtPanel + b, cz1 = min(j0 + b, n);
+      for (int c = cz0 + tid; c < cz1; c += kPanelThreads) row[c] = 0.0;
+    }
+    // T1 from the summed Gram matrix
+    for (int idx = tid; idx < b * (b + 1); idx += kPanelThreads) Tsm[idx / (b + 1)][idx % (b + 1)] = 0.0;
     __syncthreads();
+    for (int q = 0; q < kb; q++) {
+      if (tid < q) {
+        const int p = (q * (q - 1)) / 2 + tid;
+        double g = 0.0;
+        for (int k = 0; k < PC; k++) g += cl.map_shared_rank(gram, k)[p];
+        wv[tid] = -stau[q] * g;
+      }
+      __syncthreads();
+      if (tid < q) {
+        double s = 0.0;
+        for (int r = tid; r < q; r++) s += Tsm[tid][r] * wv[r];
+        Tsm[tid][q] = s;
+      }
+      if (tid == q) Tsm[q][q] = stau[q];
+      __syncthreads();
+    }
+    double* T1 = B.scr + band_scr_t(n);
+    for (int idx = tid; idx < b * b; idx += kPanelThreads) T1[idx] = Tsm[idx / b][idx % b];
+    for (int q = tid; q < b; q += kPanelThreads)
+      if (j0 + q < n) B.tau1[j0 + q] = stau[q];
   }
-  double* T1 = B.scr + band_scr_t(n);
-  for (int idx = tid; idx < b * b; idx += nt) T1[idx] = T[idx / b][idx % b];
-  for (int q = tid; q < b; q += nt)
-    if (j0 + q < n) B.tau1[j0 + q] = stau[q];
-  // 5. the rows in back-transform form: zeros from the reflector's back-transform panel start
-  //    (+ kBand) up to k + kBand, the unit at k + kBand
-  for (int q = 0; q < b; q++) {
-    const int k = j0 + q;
-    if (k >= n) break;
-    double* row = B.S + (size_t)k * ld;
-    const int c0 = (k / kBtPanel) * kBtPanel + b, c1 = min(k + b, n);
-    for (int c = c0 + tid; c < c1; c += nt) row[c] = 0.0;
-    if (tid == 0 && k + b < n) row[k + b] = 1.0;
-  }
+  cl.sync();  // (4) no CTA leaves while another may still read its shared memory
 }
 
 // ---------------------------------------------------------------- stage 2: bulge chasing
@@ -184,7 +230,7 @@ NRG_DEV double bld(const double* band, int c, int t) { return __ldcg(band + (siz
 NRG_DEV void bst(double* band, int c, int t, double x) { band[(size_t)c * kLDB + t] = x; }
 
 NRG_DEV void chase_step(double* __restrict__ band, double* __restrict__ V2, double* __restrict__ tau2, int n,
-                        int J, int i, int j, int lane, double* vs, double* ws) {
+                        int J, int i, int j, int lane, double* vs, double* ws, double* lt) {
   const int r0 = i + 1 + j * kBand, L = min(kBand, n - r0);
   const int col = j == 0 ? i : r0 - kBand;
   const double x = lane < L ? bld(band, col, r0 + lane - col) : 0.0;
@@ -208,15 +254,23 @@ NRG_DEV void chase_step(double* __restrict__ band, double* __restrict__ V2, doub
   double a[kBand];
   // left: the previous bulge's other columns col+1 .. r0-1 (nl <= kBand - 1 of them)
   const int nl = r0 - col - 1;
+  if (nl > 0) {
 #pragma unroll
-  for (int cc = 0; cc < kBand - 1; cc++)
-    a[cc] = (cc < nl && lane < L) ? bld(band, col + 1 + cc, r0 + lane - col - 1 - cc) : 0.0;
+    for (int cc = 0; cc < kBand - 1; cc++)
+      a[cc] = (cc < nl && lane < L) ? bld(band, col + 1 + cc, r0 + lane - col - 1 - cc) : 0.0;
+    // w_c = sum_t v_t A(r0+t, c) by lane c, through a transpose in shared memory (lt: 32 x 33)
 #pragma unroll
-  for (int cc = 0; cc < kBand - 1; cc++) {
-    if (cc < nl) {
-      const double w = warp_sum(v * a[cc]);
-      if (lane < L) bst(band, col + 1 + cc, r0 + lane - col - 1 - cc, a[cc] - tau * v * w);
-    }
+    for (int cc = 0; cc < kBand - 1; cc++) lt[lane * (kBand + 1) + cc] = a[cc];
+    __syncwarp();
+    double wc = 0.0;
+    if (lane < nl)
+      for (int t = 0; t < L; t++) wc += vs[t] * lt[t * (kBand + 1) + lane];
+    ws[lane] = wc;
+    __syncwarp();
+#pragma unroll
+    for (int cc = 0; cc < kBand - 1; cc++)
+      if (cc < nl && lane < L) bst(band, col + 1 + cc, r0 + lane - col - 1 - cc, a[cc] - tau * v * ws[cc]);
+    __syncwarp();  // ws is rewritten below
   }
   // both sides: the diagonal block D (L x L, symmetric, lower part stored); lane t holds row t
 #pragma unroll
@@ -249,38 +303,47 @@ NRG_DEV void chase_step(double* __restrict__ band, double* __restrict__ V2, doub
   __syncwarp();
 }
 
-// One CTA per block; warp w runs sweeps w, w + kChaseWarps, ... Step j of sweep i waits until
+// One cluster of kChaseCTAs CTAs per block; warp w of CTA r (global warp g = r*kChaseWarps + w)
+// runs sweeps g, g + G, ... with G = kChaseCTAs * kChaseWarps. Step j of sweep i waits until
 // sweep i-1 has finished step j+3 (from step j+4 on, the two sweeps touch disjoint index
-// ranges). Progress per warp: key(i, c) = i*(J+1) + c after c steps of sweep i (c = J when
-// the sweep is done), monotone. Waits are bounded: if one runs out the CTA stops and marks
-// the block's status word.
+// ranges). Progress per warp, in its CTA's shared memory (read by the other CTAs through
+// distributed shared memory): key(i, c) = i*(J+1) + c after c steps of sweep i (c = J when the
+// sweep is done), monotone; the band stores are fenced (device scope) before the key is
+// published. Waits are bounded: when one runs out, its CTA stops and marks the block.
 __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const BandBlock* __restrict__ blocks) {
-  const BandBlock B = blocks[blockIdx.x];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const BandBlock B = blocks[blockIdx.x / kChaseCTAs];
   const int n = B.n, J = B.J, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int G = kChaseCTAs * kChaseWarps, gw = rank * kChaseWarps + warp;
   __shared__ volatile int prog[kChaseWarps];
   __shared__ volatile int abort_flag;
   __shared__ double vsh[kChaseWarps][kBand], wsh[kChaseWarps][kBand];
+  extern __shared__ __align__(16) double ltsm[];  // kChaseWarps x 32 x 33
+  double* lt = ltsm + (size_t)warp * kBand * (kBand + 1);
   // the final diagonal block [jfin, n) of S into the band (its distances <= kBand)
-  for (int idx = tid; idx < (n - B.jfin) * (kBand + 1); idx += blockDim.x) {
+  const int nfin = (n - B.jfin) * (kBand + 1);
+  for (int idx = rank * blockDim.x + tid; idx < nfin; idx += kChaseCTAs * blockDim.x) {
     const int c = B.jfin + idx / (kBand + 1), t = idx % (kBand + 1);
     if (c + t < n) B.BND[(size_t)c * kLDB + t] = B.S[(size_t)(c + t) * B.lds + c];
   }
   if (tid < kChaseWarps) prog[tid] = -1;
   if (tid == 0) abort_flag = 0;
-  __threadfence_block();
-  __syncthreads();
+  cl.sync();
   const int nsw = band_nsweeps(n);
   bool stop = false;  // warp-uniform
-  for (int i = warp; i < nsw && !stop; i += kChaseWarps) {
+  for (int i = gw; i < nsw && !stop; i += G) {
     const int ns = band_nsteps(n, i);
     for (int j = 0; j < ns; j++) {
       if (i > 0) {
-        const int wp = (i - 1) % kChaseWarps;
+        const int gp = (i - 1) % G;
+        volatile int* pp = cl.map_shared_rank(const_cast<int*>(prog), gp / kChaseWarps) + gp % kChaseWarps;
         const int need = (i - 1) * (J + 1) + min(j + 4, J);
         int ok = 1;
         if (lane == 0) {
           long long it = 0;
-          while (prog[wp] < need) {
+          while (*pp < need) {
             if (abort_flag) break;
             if (++it > (1LL << 24)) {
               abort_flag = 1;
@@ -288,26 +351,24 @@ __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const Band
             }
             __nanosleep(64);
           }
-          ok = prog[wp] >= need;
+          ok = *pp >= need;
         }
         ok = __shfl_sync(kFull, ok, 0);
         if (!ok) {
           stop = true;
           break;
         }
-        __threadfence_block();
+        __threadfence();
       }
-      chase_step(B.BND, B.V2, B.tau2, n, J, i, j, lane, vsh[warp], wsh[warp]);
+      chase_step(B.BND, B.V2, B.tau2, n, J, i, j, lane, vsh[warp], wsh[warp], lt);
       __syncwarp();
-      __threadfence_block();
+      __threadfence();
       if (lane == 0) prog[warp] = i * (J + 1) + (j + 1 == ns ? J : j + 1);
     }
   }
-  __syncthreads();
-  if (abort_flag) {
-    if (tid == 0) *B.info = 1;  // the chase did not finish: not converged, no result
-    return;
-  }
+  cl.sync();  // every sweep is done (or stopped) and no CTA reads another's progress any more
+  if (abort_flag && tid == 0) *B.info = 1;  // the chase did not finish: not converged, no result
+  if (rank != 0) return;
   for (int c = tid; c < n; c += blockDim.x) {
     B.d[c] = bld(B.BND, c, 0);
     B.e[c] = c + 1 < n ? bld(B.BND, c, 1) : 0.0;
@@ -506,16 +567,50 @@ cudaError_t band_sym_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaS
   return cudaGetLastError();
 }
 
-cudaError_t band_panel_launch(const BandBlock* d_blocks, int nactive, int j0, cudaStream_t s) {
+cudaError_t band_panel_launch(const BandBlock* d_blocks, int nactive, int j0, int mmax, cudaStream_t s) {
   if (nactive <= 0) return cudaSuccess;
-  band_panel_kernel<<<nactive, 256, 0, s>>>(d_blocks, j0);
-  return cudaGetLastError();
+  // CTAs per block: enough that a share of the panel (kBand rows) fits 160 KB of shared memory
+  int PC = 2;
+  while (PC < 16 && (size_t)kBand * ((mmax + PC - 1) / PC + 1) * sizeof(double) > 160 * 1024) PC *= 2;
+  const int chunk = (mmax + PC - 1) / PC;
+  const size_t smem = sizeof(double) * ((size_t)kBand * (chunk + 1) + 2 + kBand + kPanelPairs + 64);
+  cudaError_t err = cudaFuncSetAttribute(band_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err == cudaSuccess && PC > 8)
+    err = cudaFuncSetAttribute(band_panel_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (err != cudaSuccess) return err;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nactive * PC));
+  cfg.blockDim = dim3(kPanelThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)PC;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, band_panel_kernel, d_blocks, j0, chunk);
 }
 
 cudaError_t band_chase_launch(const BandBlock* d_blocks, int nblk, cudaStream_t s) {
   if (nblk <= 0) return cudaSuccess;
-  band_chase_kernel<<<nblk, 32 * kChaseWarps, 0, s>>>(d_blocks);
-  return cudaGetLastError();
+  const size_t smem = sizeof(double) * kChaseWarps * kBand * (kBand + 1);
+  cudaError_t err = cudaFuncSetAttribute(band_chase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nblk * kChaseCTAs));
+  cfg.blockDim = dim3(32 * kChaseWarps);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)kChaseCTAs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, band_chase_kernel, d_blocks);
 }
 
 cudaError_t band_q2_tfactor_launch(const BandBlock* d_blocks, int nblk, int maxn, cudaStream_t s) {

@@ -1828,7 +1828,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         for (int p = 0; p < npan1; p++) {
           {
             PhaseScope ps(c, kPhBandPanel, s);
-            NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, s));
+            NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, bblk[0].n - p * kBand - kBand, s));
           }
           for (int q = 0; q < 6; q++) {
             rc = launch_staged_gemm(c, s1_g[6 * p + q], s, kPhBandReduce);
