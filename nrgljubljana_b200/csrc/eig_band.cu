@@ -444,6 +444,16 @@ static_assert(kGRows <= 64 && kGrp == 32 && kQ2Rows == 64, "the DMMA tiling belo
 constexpr int kLW = 68;  // row stride (doubles) of the window and of V in shared memory
 constexpr int kLX = 36;  // row stride of X, X2 and T
 
+// The window of group (g, j) covers rows rs .. rs+62 of the eigenvector components with
+// rs = g*kGrp + 1 + j*kBand, so the windows of steps j and j+1 overlap in 31 columns: the
+// window stays in shared memory along j (its first kBand columns are written back when it
+// moves on), and the loads of the next group (its V, T and the kBand new window columns) are
+// issued into registers before the current group's products, so that their latency overlaps
+// the tensor-core work.
+NRG_DEV double q2_v(const BandBlock& B, int g, int j, int q, int t, int nm) {
+  return q < nm ? B.V2[((size_t)(g * kGrp + q) * B.J + j) * kBand + t] : 0.0;
+}
+
 __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __restrict__ blocks) {
   const BandBlock B = blocks[blockIdx.y];
   const int n = B.n, J = B.J;
@@ -451,34 +461,64 @@ __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __r
   if (e0 >= n || J == 0) return;
   const int ne = min(kQ2Rows, n - e0);
   extern __shared__ __align__(16) double q2sm[];
-  double* W = q2sm;                  // 64 x kLW: the window Zt[e0 .., R]
+  double* W = q2sm;                  // 64 x kLW: the window Zt[e0 .., rs ..]
   double* V = W + 64 * kLW;          // 32 x kLW: row q = reflector q over the window's columns
   double* T = V + 32 * kLW;          // 32 x kLX
   double* X = T + 32 * kLX;          // 64 x kLX
   double* X2 = X + 64 * kLX;         // 64 x kLX
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int fr = lane >> 2, fc = lane & 3;
+  const int rb = (warp >> 1) * 16;  // the warp's 16 rows of the window
+  double* Z = B.evecs + (size_t)e0 * n;
+  for (int idx = tid; idx < 32 * kLW; idx += 256) V[idx] = 0.0;  // off the parallelogram: zero for good
+  // per-thread prefetch registers: 4 reflector entries, 4 T entries, 8 window entries
+  double pv[4], pt[4], pw[8];
+  auto prefetch = [&](int g, int j, int nm, int col0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int idx = tid + 256 * k, q = idx >> 5, t = idx & 31;
+      pv[k] = q2_v(B, g, j, q, t, nm);
+      pt[k] = B.T2[((size_t)g * J + j) * kGrp * kGrp + idx];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int idx = tid + 256 * k, e = idx >> 5, c = idx & 31;
+      const int gc = col0 + c;
+      pw[k] = (e < ne && gc < n) ? Z[(size_t)e * n + gc] : 0.0;
+    }
+  };
+  auto commit = [&](int wcol0) {  // prefetched V, T and window columns wcol0 .. wcol0+31 into place
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int idx = tid + 256 * k, q = idx >> 5, t = idx & 31;
+      V[q * kLW + q + t] = pv[k];
+      T[(idx >> 5) * kLX + (idx & 31)] = pt[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int idx = tid + 256 * k, e = idx >> 5, c = idx & 31;
+      if (wcol0 + c < 64) W[e * kLW + wcol0 + c] = pw[k];
+    }
+  };
   for (int g = band_ngroups(n) - 1; g >= 0; g--) {
+    const int rs0 = g * kGrp + 1;
+    int nm = group_members(n, g, 0);
+    if (nm == 0) continue;
+    // the first window: columns rs0 .. rs0+63 in two halves, V and T of step 0
+    prefetch(g, 0, nm, rs0);
+    __syncthreads();  // the previous pass's window is written back and free
+    commit(0);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int idx = tid + 256 * k, e = idx >> 5, c = idx & 31;
+      const int gc = rs0 + 32 + c;
+      W[e * kLW + 32 + c] = (e < ne && gc < n) ? Z[(size_t)e * n + gc] : 0.0;
+    }
     for (int j = 0; j < J; j++) {
-      const int nm = group_members(n, g, j);
-      if (nm == 0) break;  // members form a prefix in j as well: no later step has any
-      const int rs = g * kGrp + 1 + j * kBand;
-      const int nr = min(kGRows, n - rs);
-      for (int idx = tid; idx < 32 * 64; idx += nt) {
-        const int q = idx >> 6, r = idx & 63;
-        double x = 0.0;
-        if (q < nm && r >= q && r < q + kBand && r < nr)
-          x = B.V2[((size_t)(g * kGrp + q) * J + j) * kBand + (r - q)];
-        V[q * kLW + r] = x;
-      }
-      const double* Tg = B.T2 + ((size_t)g * J + j) * kGrp * kGrp;
-      for (int idx = tid; idx < kGrp * kGrp; idx += nt) T[(idx / kGrp) * kLX + idx % kGrp] = Tg[idx];
-      for (int idx = tid; idx < 64 * 64; idx += nt) {
-        const int e = idx >> 6, r = idx & 63;
-        W[e * kLW + r] = (e < ne && r < nr) ? B.evecs[(size_t)(e0 + e) * n + rs + r] : 0.0;
-      }
-      __syncthreads();
-      const int rb = (warp >> 1) * 16;  // the warp's 16 rows
+      const int rs = rs0 + j * kBand;
+      const int nm_next = (j + 1 < J) ? group_members(n, g, j + 1) : 0;
+      __syncthreads();  // window, V and T of (g, j) in place
+      if (nm_next > 0) prefetch(g, j + 1, nm_next, rs + 64);
       // X (64 x 32) = W V^T, K = 64: warp tile 16 x 16
       {
         const int cb = (warp & 1) * 16;
@@ -525,7 +565,7 @@ __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __r
             for (int h = 0; h < 2; h++) X2[(rb + 8 * i + fr) * kLX + cb + 8 * jj + 2 * fc + h] = acc[i][jj][h];
       }
       __syncthreads();
-      // W -= X2 V (64 x 64, K = 32): warp tile 16 x 32, written back to the eigenvector rows
+      // W -= X2 V (64 x 64, K = 32): warp tile 16 x 32, in place
       {
         const int cb = (warp & 1) * 32;
         double acc[2][4][2] = {};
@@ -541,19 +581,28 @@ __global__ void __launch_bounds__(256) band_q2_apply_kernel(const BandBlock* __r
             for (int jj = 0; jj < 4; jj++) dmma884(acc[i][jj][0], acc[i][jj][1], a[i], bb[jj]);
         }
 #pragma unroll
-        for (int i = 0; i < 2; i++) {
-          const int e = rb + 8 * i + fr;
-          if (e >= ne) continue;
+        for (int i = 0; i < 2; i++)
 #pragma unroll
           for (int jj = 0; jj < 4; jj++)
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int r = cb + 8 * jj + 2 * fc + h;
-              if (r < nr) B.evecs[(size_t)(e0 + e) * n + rs + r] = W[e * kLW + r] - acc[i][jj][h];
-            }
-        }
+            for (int h = 0; h < 2; h++) W[(rb + 8 * i + fr) * kLW + cb + 8 * jj + 2 * fc + h] -= acc[i][jj][h];
       }
       __syncthreads();
+      // the window's first kBand columns are final for this pass; the rest moves to the front
+      const int ncols = nm_next > 0 ? 32 : 64;
+      for (int idx = tid; idx < 64 * ncols; idx += 256) {
+        const int e = idx / ncols, c = idx % ncols;
+        if (e < ne && rs + c < n) Z[(size_t)e * n + rs + c] = W[e * kLW + c];
+      }
+      if (nm_next == 0) break;
+      __syncthreads();
+      for (int idx = tid; idx < 64 * 32; idx += 256) {
+        const int e = idx >> 5, c = idx & 31;
+        W[e * kLW + c] = W[e * kLW + 32 + c];
+      }
+      __syncthreads();  // the shift has read columns 32..63 before they are replaced
+      commit(32);  // columns 32..63 of the next window, its V (zero rows for non-members) and T
+      nm = nm_next;
     }
   }
 }
