@@ -303,13 +303,21 @@ NRG_DEV void chase_step(double* __restrict__ band, double* __restrict__ V2, doub
   __syncwarp();
 }
 
+// Orders this thread's memory accesses at cluster scope: the band is read and written only by
+// the CTAs of one cluster.
+NRG_DEV void fence_cluster() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+
 // One cluster of kChaseCTAs CTAs per block; warp w of CTA r (global warp g = r*kChaseWarps + w)
 // runs sweeps g, g + G, ... with G = kChaseCTAs * kChaseWarps. Step j of sweep i waits until
-// sweep i-1 has finished step j+3 (from step j+4 on, the two sweeps touch disjoint index
-// ranges). Progress per warp, in its CTA's shared memory (read by the other CTAs through
-// distributed shared memory): key(i, c) = i*(J+1) + c after c steps of sweep i (c = J when the
-// sweep is done), monotone; the band stores are fenced (device scope) before the key is
-// published. Waits are bounded: when one runs out, its CTA stops and marks the block.
+// sweep i-1 has finished step j+2: step j of sweep i touches rows i+1+(j-1)kBand ..
+// i+1+(j+2)kBand-1 at most, and every step of sweep i-1 from step j+3 on touches only rows
+// below them (the last row sweep i's step reaches is the column that sweep i-1's step j+3
+// clears, whose entries that step stores in another column). Progress per warp, in its CTA's
+// shared memory (read by the other CTAs through distributed shared memory): key(i, c) =
+// i*(J+1) + c after c steps of sweep i (c = J when the sweep is done), monotone; the band
+// stores are fenced at cluster scope before the key is published, and the reader fences
+// after it sees the key. Waits are bounded: when one runs out, its CTA stops and marks the
+// block.
 __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const BandBlock* __restrict__ blocks) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
@@ -339,7 +347,7 @@ __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const Band
       if (i > 0) {
         const int gp = (i - 1) % G;
         volatile int* pp = cl.map_shared_rank(const_cast<int*>(prog), gp / kChaseWarps) + gp % kChaseWarps;
-        const int need = (i - 1) * (J + 1) + min(j + 4, J);
+        const int need = (i - 1) * (J + 1) + min(j + 3, J);
         int ok = 1;
         if (lane == 0) {
           long long it = 0;
@@ -358,11 +366,11 @@ __global__ void __launch_bounds__(32 * kChaseWarps) band_chase_kernel(const Band
           stop = true;
           break;
         }
-        __threadfence();
+        fence_cluster();
       }
       chase_step(B.BND, B.V2, B.tau2, n, J, i, j, lane, vsh[warp], wsh[warp], lt);
       __syncwarp();
-      __threadfence();
+      fence_cluster();
       if (lane == 0) prog[warp] = i * (J + 1) + (j + 1 == ns ? J : j + 1);
     }
   }

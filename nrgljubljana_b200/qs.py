@@ -35,16 +35,25 @@ def S(ss: int) -> np.float64:
     return np.float64((ss - 1.0) / 2.0)
 
 
+_IEEE_CACHE: dict = {}
+
+
 def ieee(fn, ss: int) -> float:
     """A table factor at SS = ss, evaluated as the reference's C++ evaluates it: in IEEE double
     arithmetic, x/0 is +-inf and the square root of a negative number is nan (the rows where
     that happens are never used, but a factor at S = 0 may still come out finite, e.g.
-    1/sqrt(2 + 2/S) = 0)."""
-    with np.errstate(all="ignore"):
-        try:
-            return float(fn(ss))
-        except ValueError:  # math.sqrt of a negative number
-            return math.nan
+    1/sqrt(2 + 2/S) = 0). The factors are pure functions of (row, SS): each is evaluated
+    once per process and then looked up (a run asks for the same few thousand every step)."""
+    key = (fn, ss)
+    v = _IEEE_CACHE.get(key)
+    if v is None:
+        with np.errstate(all="ignore"):
+            try:
+                v = float(fn(ss))
+            except ValueError:  # math.sqrt of a negative number
+                v = math.nan
+        _IEEE_CACHE[key] = v
+    return v
 
 
 def mult(I: Invar) -> int:
@@ -100,10 +109,18 @@ def correlator_factor(Ip: Invar, I1: Invar) -> float:
     return float(mult(I1))
 
 
+_TRIPLET_CACHE: dict = {}
+
+
 def triplet_factor(fn, ss1: int) -> float:
-    """A triplet-table factor at SS = ss1 in IEEE double arithmetic."""
-    with np.errstate(all="ignore"):
-        v = float(fn(np.float64((ss1 - 1) / 2.0)))
+    """A triplet-table factor at SS = ss1 in IEEE double arithmetic (evaluated once per
+    (row, SS) per process, as ieee)."""
+    key = (fn, ss1)
+    v = _TRIPLET_CACHE.get(key)
+    if v is None:
+        with np.errstate(all="ignore"):
+            v = float(fn(np.float64((ss1 - 1) / 2.0)))
+        _TRIPLET_CACHE[key] = v
     if not math.isfinite(v):
         raise AssertionError(f"triplet recalculation factor is not finite at SS={ss1}")
     return v
