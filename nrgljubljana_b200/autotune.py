@@ -14,8 +14,9 @@ are diag(2^{-k/2}) plus symmetric N(0, 0.1^2) couplings, as in the benchmark):
   step   8 batches of 40 blocks, orders log-uniform in [8, 480] (the steps of an Anderson-model
          run at keep 1000)
   wide   2 batches of 300 blocks, orders log-uniform in [8, 1024] (many runs served at once)
-  large  12 blocks in [800, 2000] and 4 blocks in [1500, 4096] (the steps of the keep-4000
-         Anderson and keep-5000 two-channel Kondo runs, bound by their largest blocks)
+  large  12 blocks in [800, 2000], 4 blocks in [1500, 4096] and 24 blocks in [200, 7049]
+         (the steps of the keep-4000 Anderson and keep-5000 two-channel Kondo runs, bound by
+         their largest blocks)
 Each candidate is timed with CUDA events around nrg_diag_batch (the consumed inputs are
 refreshed outside the timed region), best of `reps`; the objective is the mean over the
 batches of the time relative to the starting parameters. Coordinate descent over the
@@ -49,7 +50,7 @@ GRID = {
 }
 KEYS = ("small_max_n", "mid_max_n", "cluster_max_n", "reduction_ctas_per_sm", "band_min_n", "band_max_blocks")
 # (batches, blocks per batch, smallest and largest order) of the timed workloads
-WORKLOADS = ((8, 40, 8, 480), (2, 300, 8, 1024), (1, 12, 800, 2000), (1, 4, 1500, 4096))
+WORKLOADS = ((8, 40, 8, 480), (2, 300, 8, 1024), (1, 12, 800, 2000), (1, 4, 1500, 4096), (1, 24, 200, 7049))
 
 
 def device_name(device: int = 0) -> str:

@@ -299,6 +299,9 @@ int nrg_destroy(nrg_ctx* c) {
   if (c->fork2_ev) cudaEventDestroy(c->fork2_ev);
   if (c->join2_ev) cudaEventDestroy(c->join2_ev);
   if (c->side2) cudaStreamDestroy(c->side2);
+  if (c->fork3_ev) cudaEventDestroy(c->fork3_ev);
+  if (c->join3_ev) cudaEventDestroy(c->join3_ev);
+  if (c->side3) cudaStreamDestroy(c->side3);
   if (c->ring) cudaFree(c->ring);
   if (c->copy_in) cudaStreamDestroy(c->copy_in);
   if (c->copy_out) cudaStreamDestroy(c->copy_out);

@@ -46,6 +46,9 @@ struct nrg_ctx {
   // bulk-copy reductions of larger blocks
   cudaStream_t side2 = nullptr;
   cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
+  // fourth stream: the two-stage reduction of the largest blocks beside the one-stage ones
+  cudaStream_t side3 = nullptr;
+  cudaEvent_t fork3_ev = nullptr, join3_ev = nullptr;
   // Cross-stream order of calls: every entry point records order_ev on its stream when it
   // leaves; a call on another stream first waits for it, so the descriptor staging buffers
   // and the workspace arena are never rewritten while an earlier call's kernels read them.

@@ -1816,31 +1816,44 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     const BandBlock* dbb = reinterpret_cast<const BandBlock*>(dbase + bblk_off);
 
     // ---- 1a. two-stage reduction of the largest blocks (when few): symmetric copy, stage-1
-    //          panels and their GEMMs, bulge chasing, the T factors of its back-transform
+    //          panels and their GEMMs, bulge chasing, the T factors of its back-transform.
+    //          With one-stage blocks beside them it runs on the context's fourth stream, so
+    //          that the one-stage reductions fill the SMs its clusters leave idle.
+    const bool fork3 = nts > 0 && nts < nb;
+    cudaStream_t s3 = s;
+    if (fork3) {
+      if (!c->side3) {
+        NRG_CK(cudaStreamCreateWithFlags(&c->side3, cudaStreamNonBlocking));
+        NRG_CK(cudaEventCreateWithFlags(&c->fork3_ev, cudaEventDisableTiming));
+        NRG_CK(cudaEventCreateWithFlags(&c->join3_ev, cudaEventDisableTiming));
+      }
+      NRG_CK(cudaEventRecord(c->fork3_ev, s));
+      NRG_CK(cudaStreamWaitEvent(c->side3, c->fork3_ev, 0));
+      s3 = c->side3;
+    }
     if (nts > 0) {
+      for (const BandBlock& Bb : bblk)
+        NRG_CK(cudaMemsetAsync(Bb.BND, 0, sizeof(double) * (size_t)Bb.n * kLDB, s3));
       {
-        for (const BandBlock& Bb : bblk)
-          NRG_CK(cudaMemsetAsync(Bb.BND, 0, sizeof(double) * (size_t)Bb.n * kLDB, s));
+        PhaseScope ps(c, kPhBandReduce, s3);
+        NRG_CK(band_sym_launch(dbb, nts, blk[0].n, s3));
+      }
+      for (int p = 0; p < npan1; p++) {
         {
-          PhaseScope ps(c, kPhBandReduce, s);
-          NRG_CK(band_sym_launch(dbb, nts, blk[0].n, s));
+          PhaseScope ps(c, kPhBandPanel, s3);
+          NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, bblk[0].n - p * kBand - kBand, s3));
         }
-        for (int p = 0; p < npan1; p++) {
-          {
-            PhaseScope ps(c, kPhBandPanel, s);
-            NRG_CK(band_panel_launch(dbb, pan_active[p], p * kBand, bblk[0].n - p * kBand - kBand, s));
-          }
-          for (int q = 0; q < 6; q++) {
-            rc = launch_staged_gemm(c, s1_g[6 * p + q], s, kPhBandReduce);
-            if (rc) return rc;
-          }
+        for (int q = 0; q < 6; q++) {
+          rc = launch_staged_gemm(c, s1_g[6 * p + q], s3, kPhBandReduce);
+          if (rc) return rc;
         }
       }
       {
-        PhaseScope ps(c, kPhBulgeChase, s, 2);
-        NRG_CK(band_chase_launch(dbb, nts, s));
-        NRG_CK(band_q2_tfactor_launch(dbb, nts, blk[0].n, s));
+        PhaseScope ps(c, kPhBulgeChase, s3, 2);
+        NRG_CK(band_chase_launch(dbb, nts, s3));
+        NRG_CK(band_q2_tfactor_launch(dbb, nts, blk[0].n, s3));
       }
+      if (fork3) NRG_CK(cudaEventRecord(c->join3_ev, s3));
     }
 
     // ---- 1. tridiagonalisation: blocks beyond cluster_max_n (sorted first) stream through
@@ -1987,6 +2000,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
       }
       if (fork) NRG_CK(cudaStreamWaitEvent(s, c->join2_ev, 0));
     }
+    if (fork3) NRG_CK(cudaStreamWaitEvent(s, c->join3_ev, 0));  // the two-stage blocks are tridiagonal
     // ---- 2. divide and conquer
     {
       PhaseScope ps(c, kPhDcLeaf, s);

@@ -28,7 +28,8 @@ def test_table_lookup_by_device_name(tmp_path, monkeypatch):
 def test_workloads_are_seeded():
     from nrgljubljana_b200 import autotune
     a, b = autotune.workloads(), autotune.workloads()
-    assert len(a) == 12 and all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert len(a) == 13 and all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert 200 <= a[12].min() and a[12].max() <= 7049
     assert max(int(x.max()) for x in a[:8]) <= 480 and max(int(x.max()) for x in a[8:10]) <= 1024
     assert 800 <= a[10].min() and a[10].max() <= 2000 and 1500 <= a[11].min() and a[11].max() <= 4096
 
