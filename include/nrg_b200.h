@@ -72,9 +72,9 @@ NRG_API int nrg_trim(nrg_ctx* ctx);
  *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2; default 2)
  *   band_min_n     blocks of at least this order, when at most band_max_blocks of them are
  *                  in a batch, take the two-stage reduction (dense -> band on the FP64
- *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never
+ *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never; default 768
  *   band_max_blocks  see band_min_n (few large blocks: the regime where the one-stage
- *                  reduction's per-column chain bounds the step) */
+ *                  reduction's per-column chain bounds the step); default 64 */
 typedef struct nrg_tuning {
   int small_max_n;
   int mid_max_n;
