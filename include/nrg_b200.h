@@ -49,7 +49,9 @@ NRG_API int nrg_version(void);
 NRG_API const char* nrg_last_error(void);
 
 /* Per-run context: device, device workspace (grown on demand up to workspace_limit bytes,
- * 0 = 90% of the free device memory at creation), descriptor staging. One context may
+ * 0 = 90% of the free device memory at creation, and never past the memory free at the
+ * time less a reserve of 2 GiB or 2% of the device: larger batches are solved in chunks),
+ * descriptor staging. One context may
  * be used from one host thread at a time. Calls on one context may name different
  * streams: each call's work is ordered after the previous call's (an event recorded on
  * the previous call's stream), because all calls share the context's descriptor staging
@@ -72,7 +74,7 @@ NRG_API int nrg_trim(nrg_ctx* ctx);
  *   reduction_ctas_per_sm  CTAs of the streaming reduction kernels per SM (1 or 2; default 2)
  *   band_min_n     blocks of at least this order, when at most band_max_blocks of them are
  *                  in a batch, take the two-stage reduction (dense -> band on the FP64
- *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never; default 768
+ *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never; default 3072
  *   band_max_blocks  see band_min_n (few large blocks: the regime where the one-stage
  *                  reduction's per-column chain bounds the step); default 64 */
 typedef struct nrg_tuning {
@@ -105,7 +107,7 @@ NRG_API int nrg_diag_batch(nrg_ctx* ctx, int nblk, const int* n, double* const* 
 /* Same with host pointers for H[b], evals[b], evecs[b] (the call the reference's
  * diagonalise() makes with its ublas matrix); H[b] is left unchanged. The blocks stream
  * through a ring of at most three device slots in chunks of consecutive blocks (a chunk
- * holds about a third of the batch, at most 16 GiB): the copy of chunk k+1 to the device
+ * holds about half of the batch, at most 32 GiB): the copy of chunk k+1 to the device
  * and of chunk k-1 back to the host overlap the solve of chunk k, on two copy streams of
  * the context. Page-locked host memory lets the copies run asynchronously; pageable
  * memory works too, with copies that do not overlap. Returns when every result is in host

@@ -45,7 +45,11 @@ GRID = {
     "small_max_n": [32, 48, 64, 80, 96],
     "mid_max_n": [128, 160, 192, 224, 236],
     "cluster_max_n": [400, 480, 560, 600, 640],
-    "band_min_n": [0, 768, 1024, 1536, 2048, 3072],
+    # The two-stage path's bulge chasing has a critical path of about 3n dependent steps; below
+    # order ~2000 it is as long as the block's one-stage reduction, so lower thresholds only
+    # pay where the other blocks of a batch hide it, and cost 10-15% on keep-4000 Anderson
+    # steps (blocks up to 1622), measured.
+    "band_min_n": [0, 2048, 3072, 4096],
     "band_max_blocks": [4, 8, 16, 32, 64],
 }
 KEYS = ("small_max_n", "mid_max_n", "cluster_max_n", "reduction_ctas_per_sm", "band_min_n", "band_max_blocks")

@@ -33,17 +33,32 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+size_t ws_available(nrg_ctx* c) {
+  // What the arena may grow to now: the context's limit, and no more than the memory free on
+  // the device (plus the arena itself) less a reserve of 2 GiB or 2% of the device, so that the
+  // caller's own allocations (a run's growing set of stored eigenvectors) keep room.
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return std::min(c->ws_limit, c->ws_size);
+  }
+  const size_t reserve = std::max<size_t>((size_t)2 << 30, tot / 50);
+  const size_t have = fr + c->ws_size;
+  return std::min(c->ws_limit, have > reserve ? have - reserve : c->ws_size);
+}
+
 int ensure_ws(nrg_ctx* c, size_t bytes) {
   if (bytes <= c->ws_size) return NRG_OK;
-  if (bytes > c->ws_limit)
-    return fail(NRG_ERR_OOM, "workspace of %zu bytes exceeds the context limit of %zu bytes", bytes, c->ws_limit);
+  const size_t lim = ws_available(c);
+  if (bytes > lim)
+    return fail(NRG_ERR_OOM, "workspace of %zu bytes exceeds the %zu bytes the context can use now", bytes, lim);
   if (c->ws) {
     NRG_CK(cudaDeviceSynchronize());
     NRG_CK(cudaFree(c->ws));
     c->ws = nullptr;
     c->ws_size = 0;
   }
-  const size_t sz = std::max(bytes, std::min(c->ws_limit, align_up(bytes + bytes / 4, 1 << 20)));
+  const size_t sz = std::max(bytes, std::min(lim, align_up(bytes + bytes / 4, 1 << 20)));
   if (cudaMalloc(&c->ws, sz) != cudaSuccess) {
     cudaGetLastError();
     if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
@@ -417,14 +432,14 @@ int nrg_diag_batch_host(nrg_ctx* c, int nblk, const int* n, const double* const*
   }
   // Chunks of consecutive blocks stream through a ring of up to three device slots: the
   // host-to-device copy of chunk k+1 and the device-to-host copy of chunk k-1 run on two
-  // copy streams beside the solve of chunk k. A slot holds about a third of the batch, at
-  // most 16 GiB, and at most a fifth of the memory this context can use (the solve's own
-  // workspace comes on top of the three slots). Few large chunks keep each solve's batch
-  // wide enough to fill the SMs.
+  // copy streams beside the solve of chunk k. A slot holds about half of the batch, at most
+  // 32 GiB, and at most a fifth of the memory this context can use (the solve's own workspace
+  // comes on top of the slots). Few large chunks keep each solve's batch wide enough to fill
+  // the SMs: every chunk ends in a tail where its largest blocks hold few of them.
   size_t fr = 0, tot = 0;
   CK(cudaMemGetInfo(&fr, &tot));
   const size_t usable = std::min(c->ws_limit, fr + c->ring_size + c->ws_size);
-  size_t target = std::min<size_t>(std::max<size_t>(total / 3, (size_t)64 << 20), (size_t)16 << 30);
+  size_t target = std::min<size_t>(std::max<size_t>(total / 2 + 1, (size_t)64 << 20), (size_t)32 << 30);
   target = std::max<size_t>(std::min(target, usable / 5), (size_t)16 << 20);
   std::vector<int> first(1, 0);
   size_t maxchunk = 0, cur = 0;

@@ -22,7 +22,7 @@ const char* phase_name(int p);
 
 struct nrg_ctx {
   int device = 0;
-  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 2, 768, 64};  // the autotuner's B200 values
+  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 2, 3072, 64};  // the autotuner's B200 values
   // profiling: launch counts per phase (always), CUDA-event intervals (when enabled)
   bool prof = false;
   long long launches[nrg::kPhCount] = {};
@@ -68,6 +68,8 @@ namespace nrg {
 int fail(int code, const char* fmt, ...);
 const char* last_error_text();
 int ensure_ws(nrg_ctx* c, size_t bytes);
+// Bytes the workspace arena may hold now (context limit, free device memory, a reserve).
+size_t ws_available(nrg_ctx* c);
 // Copies a host byte image to c->desc (stream-ordered); returns the device base pointer.
 int stage_desc(nrg_ctx* c, const std::vector<char>& img, cudaStream_t s);
 // Same into the side stream's own staging buffer.

@@ -1564,7 +1564,7 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     if (n[b] > kMaxLargeN)
       return fail(NRG_ERR_ARG, "block %d: order %d exceeds the supported maximum %d", b, n[b], kMaxLargeN);
   // Chunk the blocks so that their workspaces fit in the context limit.
-  size_t limit = c->ws_limit;
+  const size_t limit = ws_available(c);  // chunks fit what the arena can grow to now
   size_t pos = 0;
   while (pos < ord.size()) {
     size_t bytes = 0, end = pos;
