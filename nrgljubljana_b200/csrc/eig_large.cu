@@ -1946,10 +1946,12 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        // The cluster kernel serves few blocks (latency): its CTAs keep an SM each, whatever
+        // reduction_ctas_per_sm says for the streaming kernel of the throughput regime.
         auto tcl_bytes = [&](int st) {
           return std::max(1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)b1[0].n +
                                                    (size_t)kTriWarps * 2 * NB + 4 * NB + 66),
-                          (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
+                          (size_t)smsm / 2 + 1024);
         };
         int stages = 8;
         while (stages > 4 && tcl_bytes(stages) + 256 > (size_t)optin) stages -= 2;

@@ -722,9 +722,17 @@ class QSRun:
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
+    # A step whose blocks hold more than this many bytes gives the library's workspace back
+    # after its eigensolve: the workspace arena only grows, and a run that keeps every step's
+    # eigenvectors (spectra, FDM) needs that memory for its own later steps.
+    TRIM_STEP_BYTES = 1 << 30
+
     def _diagonalise(self, job: "StepJob") -> np.ndarray:
         """All blocks of the step in one batched call (diagonalisations, c++/core.hpp:113-120)."""
-        return diag_batch_ptrs(job.ns, job.Hp, job.Ep, job.Vp, self.ctx, self.stream)
+        info = diag_batch_ptrs(job.ns, job.Hp, job.Ep, job.Vp, self.ctx, self.stream)
+        if self.keep_steps and 16 * int(job.moff[-1]) > self.TRIM_STEP_BYTES:
+            self.ctx.trim()
+        return info
 
     def _recalc_irreducible(self, diag: Dict[Invar, Sub]) -> MatSet:
         """SymmetryQS::recalc_irreduc with recalc_f (c++/recalc.hpp:52-76): <I1||f_ch||Ip> of
