@@ -434,7 +434,7 @@ def main():
         try:
             line["c3_run"] = c3_arm(torch, local, args)
         except (RuntimeError, MemoryError) as err:
-            line["c3_run"] = {"workload": C3_WORKLOAD, "error": str(err)[:300]}
+            line["c3_run"] = {"workload": C3_WORKLOAD, "error": str(err)[:600]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -774,13 +774,20 @@ def c3_arm(torch, device: int, args) -> dict:
     run = QSRun(p, d, device, ctx)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    run.start()
-    while not run.done:
-        job = run.begin_step()
-        run.end_step(job, run._diagonalise(job))
-    torch.cuda.synchronize()
-    t_fwd = time.perf_counter() - t0
-    res = run.finish()
+    try:
+        run.start()
+        while not run.done:
+            job = run.begin_step()
+            run.end_step(job, run._diagonalise(job))
+        torch.cuda.synchronize()
+        t_fwd = time.perf_counter() - t0
+        res = run.finish()
+    except Exception as err:  # where the memory went, for the report
+        free, total = torch.cuda.mem_get_info(device)
+        raise RuntimeError(f"step {run.N}: {err}; device: {torch.cuda.memory_allocated(device) / 2 ** 30:.1f} GiB "
+                           f"allocated, {torch.cuda.memory_reserved(device) / 2 ** 30:.1f} reserved by torch, "
+                           f"{free / 2 ** 30:.1f} of {total / 2 ** 30:.1f} free; "
+                           f"{run.spilled_bytes / 2 ** 30:.1f} GiB of eigenvectors in host memory") from err
     torch.cuda.synchronize()
     t_all = time.perf_counter() - t0
     flop = sum(f_eig(np.array(ns)) for ns in res.block_dims)
@@ -790,6 +797,8 @@ def c3_arm(torch, device: int, args) -> dict:
            "eig_flop_per_run": flop, "eig_gflops_forward": flop / t_fwd / 1e9,
            "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
            "peak_device_gib": torch.cuda.max_memory_allocated(device) / 2 ** 30,
+           "eigenvectors_stored_gib": sum(8.0 * sum(n * n for n in ns) for ns in res.block_dims) / 2 ** 30,
+           "eigenvectors_via_host_gib": run.spilled_bytes / 2 ** 30,
            "tdfdm": dict(zip(*res.tdfdm)) if res.tdfdm else None,
            "spectrum": {k: int(len(v)) for k, v in res.spectra.items()}}
     if not args.no_per_block:

@@ -658,65 +658,117 @@ int nrg_gemm3_batch(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream)
     v.push_back(t);
   }
   // Phase 1: T_t = O_t op(B_t) (ka x cols) for every term with an O: a GEMM for a dense O, a
-  // row scaling for a diagonal one (ldo == 0).
+  // row scaling for a diagonal one (ldo == 0). Phase 2: M += sum_t factor_t op(A_t) T_t.
+  // The T_t of all terms share the workspace arena; when they do not fit in what the arena may
+  // hold now, the output groups (and, for a group too large by itself, its terms) go in
+  // consecutive passes on the stream, each adding its terms into M.
+  auto tsize = [&](int t) -> size_t { return terms[t].O ? (size_t)terms[t].ka * terms[t].cols : 0; };
+  std::vector<std::vector<int>> glist;
+  size_t need = 0;
+  for (double* M : order) {
+    glist.push_back(groups[M]);
+    for (int t : glist.back()) need += tsize(t);
+  }
+  std::vector<std::vector<std::vector<int>>> passes;
+  const size_t cap = std::max(c->ws_size, nrg::ws_available(c)) / sizeof(double);
+  if (need <= cap) {
+    passes.push_back(std::move(glist));
+  } else {
+    std::vector<std::vector<int>> cur;
+    size_t used = 0;
+    auto close = [&]() {
+      if (!cur.empty()) passes.push_back(std::move(cur));
+      cur.clear();
+      used = 0;
+    };
+    for (auto& v : glist) {
+      size_t gv = 0;
+      for (int t : v) gv += tsize(t);
+      if (gv <= cap) {
+        if (used + gv > cap) close();
+        cur.push_back(v);
+        used += gv;
+        continue;
+      }
+      std::vector<int> part;
+      for (int t : v) {
+        const size_t x = tsize(t);
+        if (x > cap)
+          return fail(NRG_ERR_OOM, "term %d: workspace of %zu bytes exceeds the %zu bytes the context can use now",
+                      t, sizeof(double) * x, sizeof(double) * cap);
+        if (used + x > cap) {
+          if (!part.empty()) cur.push_back(part);
+          part.clear();
+          close();
+        }
+        part.push_back(t);
+        used += x;
+      }
+      if (!part.empty()) cur.push_back(part);
+    }
+    close();
+  }
   auto dense_O = [&](int t) { return terms[t].O && terms[t].ldo != 0; };
   std::vector<size_t> toff(nterm, 0);
-  size_t need = 0;
-  for (int t : live)
-    if (terms[t].O) {
-      toff[t] = need;
-      need += (size_t)terms[t].ka * terms[t].cols;
-    }
-  rc = ensure_ws(c, sizeof(double) * std::max<size_t>(need, 1));
-  if (rc) return rc;
-  double* T = static_cast<double*>(c->ws);
-  GemmPlan p1, p2;
-  for (int t : live) {
-    const nrg_gemm3& g = terms[t];
-    if (!dense_O(t)) continue;
-    p1.add_out(T + toff[t], g.cols, g.ka, g.cols, 0.0);
-    p1.add_seg(g.O, g.ldo, 0, g.B, g.ldb, g.transB, g.kb, 1.0);
-  }
-  std::vector<nrg::RowScale> rsc;
-  int64_t rtotal = 0;
-  for (int t : live) {
-    const nrg_gemm3& g = terms[t];
-    if (!g.O || dense_O(t)) continue;
-    nrg::RowScale r{};
-    r.T = T + toff[t];
-    r.d = g.O;
-    r.B = g.B;
-    r.ldb = g.ldb;
-    r.off = rtotal;
-    r.rows = g.ka;
-    r.cols = g.cols;
-    r.transB = g.transB;
-    rsc.push_back(r);
-    rtotal += (int64_t)g.ka * g.cols;
-  }
-  // Phase 2: M += sum_t factor_t op(A_t) T_t.
-  for (double* M : order) {
-    const auto& v = groups[M];
-    const nrg_gemm3& f = terms[v[0]];
-    p2.add_out(M, f.ldm, f.rows, f.cols, 1.0);
-    for (int t : v) {
-      const nrg_gemm3& g = terms[t];
-      if (g.O) p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
-      else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
-    }
-  }
-  if (!rsc.empty()) {
-    std::vector<char> img;
-    const size_t ro = push(img, rsc);
-    rc = stage_desc(c, img, s);
+  for (const auto& pass : passes) {
+    size_t pneed = 0;
+    for (const auto& v : pass)
+      for (int t : v)
+        if (terms[t].O) {
+          toff[t] = pneed;
+          pneed += tsize(t);
+        }
+    rc = ensure_ws(c, sizeof(double) * std::max<size_t>(pneed, 1));
     if (rc) return rc;
-    nrg::PhaseScope ps(c, nrg::kPhGemm3, s);
-    CK(nrg::row_scale_launch(reinterpret_cast<const nrg::RowScale*>(static_cast<char*>(c->desc) + ro),
-                             (int)rsc.size(), rtotal, s));
+    double* T = static_cast<double*>(c->ws);
+    GemmPlan p1, p2;
+    std::vector<nrg::RowScale> rsc;
+    int64_t rtotal = 0;
+    for (const auto& v : pass)
+      for (int t : v) {
+        const nrg_gemm3& g = terms[t];
+        if (!g.O) continue;
+        if (dense_O(t)) {
+          p1.add_out(T + toff[t], g.cols, g.ka, g.cols, 0.0);
+          p1.add_seg(g.O, g.ldo, 0, g.B, g.ldb, g.transB, g.kb, 1.0);
+          continue;
+        }
+        nrg::RowScale r{};
+        r.T = T + toff[t];
+        r.d = g.O;
+        r.B = g.B;
+        r.ldb = g.ldb;
+        r.off = rtotal;
+        r.rows = g.ka;
+        r.cols = g.cols;
+        r.transB = g.transB;
+        rsc.push_back(r);
+        rtotal += (int64_t)g.ka * g.cols;
+      }
+    for (const auto& v : pass) {
+      const nrg_gemm3& f = terms[v[0]];
+      p2.add_out(f.M, f.ldm, f.rows, f.cols, 1.0);
+      for (int t : v) {
+        const nrg_gemm3& g = terms[t];
+        if (g.O) p2.add_seg(g.A, g.lda, g.transA, T + toff[t], g.cols, 0, g.ka, g.factor);
+        else p2.add_seg(g.A, g.lda, g.transA, g.B, g.ldb, g.transB, g.ka, g.factor);
+      }
+    }
+    if (!rsc.empty()) {
+      std::vector<char> img;
+      const size_t ro = push(img, rsc);
+      rc = stage_desc(c, img, s);
+      if (rc) return rc;
+      nrg::PhaseScope ps(c, nrg::kPhGemm3, s);
+      CK(nrg::row_scale_launch(reinterpret_cast<const nrg::RowScale*>(static_cast<char*>(c->desc) + ro),
+                               (int)rsc.size(), rtotal, s));
+    }
+    rc = run_gemm_plan(c, p1, s, nrg::kPhGemm3);
+    if (rc) return rc;
+    rc = run_gemm_plan(c, p2, s, nrg::kPhGemm3);
+    if (rc) return rc;
   }
-  rc = run_gemm_plan(c, p1, s, nrg::kPhGemm3);
-  if (rc) return rc;
-  return run_gemm_plan(c, p2, s, nrg::kPhGemm3);
+  return NRG_OK;
 }
 
 int nrg_gemm3_batch_host(nrg_ctx* c, int nterm, const nrg_gemm3* terms, void* stream) {

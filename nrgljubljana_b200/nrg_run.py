@@ -352,8 +352,13 @@ class _StepRecord:
     N: int
     scale: float
     diag: Dict[Invar, "Sub"]
-    vecs: torch.Tensor
+    vecs: Optional[torch.Tensor]
     total_energy: float
+    host: Optional[torch.Tensor] = None  # the eigenvectors while they are held in host memory
+    base: int = 0                        # device address the subspaces' vptr point into
+
+    def __post_init__(self):
+        self.base = self.vecs.data_ptr() if self.vecs is not None else 0
 
 
 class QSRun:
@@ -421,7 +426,7 @@ class QSRun:
         for name in ("opch", "ops"):
             m = getattr(self, name, None)
             tensors.append(m.buf if m is not None else None)
-        tensors += [st.vecs for st in getattr(self, "dm_steps", [])]
+        tensors += [st.vecs for st in getattr(self, "dm_steps", []) if st.vecs is not None]
         for t in tensors:
             if t is not None and t.data_ptr() not in seen:
                 seen.add(t.data_ptr())
@@ -524,6 +529,7 @@ class QSRun:
                           [])
         self.meas: List[_Measure] = []
         self.dm_steps: List[_StepRecord] = []
+        self.spilled_bytes = 0  # eigenvector bytes moved to host memory (and back) in this run
         self.total_energy = float(d.gs_energy)  # Stats::total_energy (c++/stats.hpp:60-71)
         # operators of the spectral pass as read: singlets by subspace, doublets and triplets
         # by subspace pair
@@ -719,6 +725,8 @@ class QSRun:
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
         if self.keep_steps:  # the density matrices and spectra need every step's eigenvectors
             self.dm_steps.append(_StepRecord(N, self.scale(N), diag, job.Vbuf, self.total_energy))
+            self._make_room(self.SPILL_HEADROOM_STEPS * 8 * int(job.moff[-1]),
+                            range(len(self.dm_steps) - 1))
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
@@ -727,10 +735,62 @@ class QSRun:
     # eigenvectors (spectra, FDM) needs that memory for its own later steps.
     TRIM_STEP_BYTES = 1 << 30
 
+    # The kept steps' eigenvectors live on the device while it has room. When, after a step,
+    # the device has less free memory than SPILL_HEADROOM_BYTES or SPILL_HEADROOM_STEPS times
+    # that step's eigenvector bytes (the next step's matrices, eigenvectors and workspace come
+    # out of it), the oldest steps move to pinned host memory; the density-matrix sweeps and
+    # the spectral pass bring each step back when they reach it. This is the device form of
+    # the reference's unitary files, DiagInfo::save / load (c++/eigen.hpp:389-413), which hold
+    # every step's eigenvectors between the NRG run and the density-matrix pass.
+    SPILL_HEADROOM_BYTES = 16 << 30
+    SPILL_HEADROOM_STEPS = 6
+
+    def _free_device_bytes(self) -> int:
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        return free + torch.cuda.memory_reserved(self.dev) - torch.cuda.memory_allocated(self.dev)
+
+    def _make_room(self, need: int, candidates) -> None:
+        """Moves the eigenvectors of the steps in `candidates` (in that order) to host memory
+        until the device has max(need, SPILL_HEADROOM_BYTES) bytes free."""
+        need = max(need, self.SPILL_HEADROOM_BYTES)
+        free = self._free_device_bytes()
+        if free >= need:
+            return
+        for k in candidates:
+            st = self.dm_steps[k]
+            if st.vecs is None:
+                continue
+            host = torch.empty(st.vecs.shape, dtype=st.vecs.dtype, pin_memory=True)
+            host.copy_(st.vecs)  # synchronous: the device buffer is free when this returns
+            free += st.vecs.numel() * st.vecs.element_size()
+            st.host, st.vecs = host, None
+            self.spilled_bytes += host.numel() * host.element_size()
+            if free >= need:
+                break
+        torch.cuda.empty_cache()  # the library's workspace is not allocated through torch
+
+    def _resident(self, k: int, candidates) -> None:
+        """Step k's eigenvectors on the device (moved back from host memory if they were
+        spilled, the subspaces' addresses rebased); `candidates` give way first."""
+        st = self.dm_steps[k]
+        if st.vecs is not None:
+            return
+        nbytes = st.host.numel() * st.host.element_size()
+        self._make_room(nbytes + self.SPILL_HEADROOM_STEPS * nbytes, [j for j in candidates if j != k])
+        vecs = torch.empty(st.host.shape, dtype=st.host.dtype, device=self.dev)
+        vecs.copy_(st.host)
+        delta = vecs.data_ptr() - st.base
+        for sub in st.diag.values():
+            sub.vptr += delta
+        st.vecs, st.base, st.host = vecs, vecs.data_ptr(), None
+
     def _diagonalise(self, job: "StepJob") -> np.ndarray:
         """All blocks of the step in one batched call (diagonalisations, c++/core.hpp:113-120)."""
+        large = self.keep_steps and 16 * int(job.moff[-1]) > self.TRIM_STEP_BYTES
+        if large and torch.cuda.memory_reserved(self.dev) - torch.cuda.memory_allocated(self.dev) > self.TRIM_STEP_BYTES:
+            torch.cuda.empty_cache()  # memory cached by torch is out of the library's reach
         info = diag_batch_ptrs(job.ns, job.Hp, job.Ep, job.Vp, self.ctx, self.stream)
-        if self.keep_steps and 16 * int(job.moff[-1]) > self.TRIM_STEP_BYTES:
+        if large:
             self.ctx.trim()
         return info
 
@@ -870,6 +930,7 @@ class QSRun:
         rhos: List[Optional[MatSet]] = [None] * nst
         rhos[nst - 1] = rho_last
         for k in range(nst - 1, 0, -1):
+            self._resident(k, list(range(nst - 1, k, -1)) + list(range(0, k)))
             cur, prv = steps[k], steps[k - 1]
             out = MatSet(self.dev, {I: (s.nkept, s.nkept) for I, s in prv.diag.items()})
             dsrc = diag_src(k) if diag_src else None
@@ -1070,6 +1131,9 @@ class QSRun:
         expv = None
         for k, st in enumerate(steps):
             last = k == nst - 1
+            if k:  # the pass is the last reader of the previous step's eigenvectors
+                steps[k - 1].vecs = steps[k - 1].host = None
+            self._resident(k, range(nst - 1, k, -1))
             cur = {kind: (self._recalc_singlets(st.diag, m, rows) if kind == "s"
                           else self._recalc_tensor(st.diag, m, *tables[kind], rows)) for kind, m in cur.items()}
             dg = st.diag

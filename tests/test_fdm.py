@@ -90,3 +90,25 @@ def test_gpu_fdm_outputs(oracle_fdm, case):
             got = getattr(res, name)
             assert_row(got[1], rows(case, name)[-1], f"{case} {name} vs reference")
             assert np.allclose(got[1], fo[name][1], rtol=1e-11, atol=0), f"{case} {name} vs oracle"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["test2_algorithms_fdm", "test314_model=ZERO"])
+def test_gpu_fdm_with_eigenvectors_in_host_memory(monkeypatch, case):
+    """The same run with every stored step's eigenvectors moved to host memory after each
+    step (a headroom no device has) and brought back by the FDM sweep and the spectral pass:
+    the FDM thermodynamics are equal and the spectra agree to the binning's round-off."""
+    from nrgljubljana_b200.inputs import parse_param, read_data
+    from nrgljubljana_b200.nrg_run import QSRun, RunParams
+    p, d = RunParams.from_param(parse_param(read(case, "param"))), read_data(read(case, "data"))
+    base = QSRun(p, d, 0).run()
+    monkeypatch.setattr(QSRun, "SPILL_HEADROOM_BYTES", 1 << 60)
+    run = QSRun(p, d, 0)
+    res = run.run()
+    assert run.spilled_bytes > 0
+    assert res.tdfdm == base.tdfdm
+    assert sorted(res.spectra) == sorted(base.spectra)
+    for name, want in base.spectra.items():
+        got = res.spectra[name]
+        assert got.shape == want.shape
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), name

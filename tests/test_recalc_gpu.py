@@ -87,6 +87,43 @@ def test_batched_terms_accumulate_per_output(nb, oracle):
         assert close(dev_M.cpu().numpy(), ref)
 
 
+def test_terms_beyond_the_workspace_run_in_passes(nb, oracle):
+    """A context whose workspace limit holds the intermediates of a few terms only: the batch
+    runs in passes (whole output groups, and the terms of a group too large for one pass), and
+    every output gets the same sums; a single term larger than the limit is refused."""
+    import torch
+    rng = np.random.default_rng(33)
+    ctx = nb.Context(workspace_limit=200 * 64 * 8)  # T of three 64 x 64 terms at most
+    terms, refs, keep = [], [], []
+    for o, nrow in enumerate([1, 2, 7, 3]):  # the 7-term group does not fit in one pass
+        M = rng.standard_normal((48, 64))
+        ref = M.copy()
+        dev_M = torch.tensor(M, device="cuda")
+        for row in range(nrow):
+            A = rng.standard_normal((64, 48))
+            B = rng.standard_normal((64, 64))
+            O = rng.standard_normal((64, 64)) if row % 3 else np.diag(rng.standard_normal(64))
+            f = float(rng.standard_normal())
+            oracle.transform(ref, f, A.T.copy(), O, B)
+            tA, tB, tO = (torch.tensor(x, device="cuda") for x in (A, B, O))
+            if row % 3 == 0:  # a diagonal O (ldo = 0): the row-scale path
+                tO = torch.diagonal(tO).contiguous()
+                t = nb.gemm3(dev_M, f, tA, None, tB, transA=True)
+                t.O, t.ldo = tO.data_ptr(), 0
+            else:
+                t = nb.gemm3(dev_M, f, tA, tO, tB, transA=True)
+            keep.append((tA, tB, tO))
+            terms.append(t)
+        refs.append((dev_M, ref))
+    nb.gemm3_batch(terms, host=False, ctx=ctx)
+    torch.cuda.synchronize()
+    for dev_M, ref in refs:
+        assert close(dev_M.cpu().numpy(), ref)
+    big = torch.zeros((300, 300), dtype=torch.float64, device="cuda")
+    with pytest.raises(nb.NRGError):
+        nb.gemm3_batch([nb.gemm3(big, 1.0, big, big, big)], host=False, ctx=ctx)
+
+
 def test_empty_terms_are_skipped(nb):
     M = np.ones((3, 3))
     nb.transform(M, 2.0, np.zeros((3, 0)), np.zeros((0, 0)), np.zeros((3, 0)))
