@@ -160,7 +160,10 @@ NRG_API int nrg_hamiltonian_batch(nrg_ctx* ctx, int nblk, const int* n, double* 
  * product O op(B) is formed first, as in the reference (for a diagonal O by scaling the
  * rows of op(B)). Terms with the same M are summed in the order given; distinct M regions must
  * not overlap. A term with rows, cols, ka or kb zero is skipped (finite_size checks of the
- * reference). Pointers are device pointers. */
+ * reference). Pointers are device pointers. The intermediates O op(B) (ka x cols each) live
+ * in the context's workspace; when all of them do not fit in what it may hold, the call runs
+ * in passes on the stream (whole groups of one M, or the terms of one group), and fails with
+ * NRG_ERR_OOM only for a single term whose intermediate does not fit. */
 typedef struct nrg_gemm3 {
   double* M;
   int64_t ldm;

@@ -369,10 +369,13 @@ class QSRun:
     def __init__(self, params: RunParams, data: DataFile, device: int = 0, ctx: Optional[Context] = None):
         if data.symtype != "QS" or data.channels not in (1, 2):
             raise ValueError("the driver covers symtype QS with one or two channels")
-        if any(k == "g" for k, _ in data.ops.values()):
-            # global operators gain the added site's part at every step (recalc1_global,
-            # c++/recalc.hpp:111-118) and are listed after the singlets in `custom`; not restated here
-            raise ValueError("global operators (g blocks of the data file) are not supported")
+        gnames = sorted(n for n, (k, _) in data.ops.items() if k == "g")
+        known = qs.tables(data.channels).GLOBAL if data.channels in (1, 2) else {}
+        if any(n not in known for n in gnames):
+            # SymmetryQS::recalc_global knows Qdiff, Q1, Q2, Qtot of two channels and asserts
+            # otherwise (c++/symmetry/nrg-recalc-QS.hpp:680-740)
+            raise ValueError(f"global operators {[n for n in gnames if n not in known]}: QS has "
+                             f"{sorted(known) or 'none'} with {data.channels} channel(s)")
         if data.nmax == 0 and params.algorithms:
             # Params::ZBW (Nmax = 0): the reference bins the initial cluster's spectra with its own
             # window rules (c++/spectrum.hpp:91-95); not restated here
@@ -387,7 +390,10 @@ class QSRun:
         self.stream = torch.cuda.current_stream(self.dev)
         self.nmax = data.nmax
         self.sqrt_lambda = math.sqrt(params.Lambda)  # nrg_step_scale_factor (c++/params.hpp:639-641)
-        self.op_names = sorted(n for n, (k, _) in data.ops.items() if k in "sg")
+        # singlets, then global operators, each by name: the columns of `custom`
+        # (singlet_operators_for_expv_evaluation, c++/output.hpp:121-127)
+        self.gop_names = set(gnames)
+        self.op_names = self._singlet_order(n for n, (k, _) in data.ops.items() if k in "sg")
         # (file prefix, kind, op1, op2) of the spectra (c++/oprecalc.hpp:160-195)
         self.algos = params.algorithms
         self.specs: List[Tuple[str, str, str, str]] = []
@@ -406,8 +412,8 @@ class QSRun:
         self.top_names = sorted({x for sp in self.specs if sp[1] == "t" for x in sp[2:]})
         # singlets of the spectral pass: those of the correlators, and all of them for the FDM
         # expectation values
-        self.sop_names = sorted({x for sp in self.specs if sp[1] == "s" for x in sp[2:]}
-                                | (set(self.op_names) if params.fdmexpv else set()))
+        self.sop_names = self._singlet_order({x for sp in self.specs if sp[1] == "s" for x in sp[2:]}
+                                             | (set(self.op_names) if params.fdmexpv else set()))
         # the steps are kept (eigenvalues, eigenvectors, energy offsets) for the density
         # matrices and the spectral pass after the run
         self.keep_steps = bool(self.specs) or params.fdm_flags
@@ -417,6 +423,10 @@ class QSRun:
         # launched all runs' terms in one nrg_gemm3_batch call.
         self.deferred_terms: Optional[List[np.ndarray]] = None
         self.deferred_reads: Optional[List] = None
+
+    def _singlet_order(self, names) -> List[str]:
+        names = set(names)
+        return sorted(names - self.gop_names) + sorted(names & self.gop_names)
 
     def device_bytes(self) -> int:
         """Device bytes the run holds between steps: the current eigenvectors, the <||f||>
@@ -714,13 +724,13 @@ class QSRun:
         res.td.append(self._td(N, diag))
         new_ops = ops
         if p.strategy == "all":
-            new_ops = self._recalc_singlets(diag, ops)
+            new_ops = self._recalc_singlets(diag, ops, names=self.op_names)
             meas.append(self._measure(N, diag, new_ops))
         for s in diag.values():
             s.nstored = s.nkept  # truncate_perform
         new_opch = opch if last else self._recalc_irreducible(diag)
         if p.strategy == "kept":
-            new_ops = self._recalc_singlets(diag, ops)
+            new_ops = self._recalc_singlets(diag, ops, names=self.op_names)
             meas.append(self._measure(N, diag, new_ops))
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
         if self.keep_steps:  # the density matrices and spectra need every step's eigenvectors
@@ -833,11 +843,15 @@ class QSRun:
         self.opch_keys = [set(out.loc)] * self.T.channels
         return out
 
-    def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet, rows=None) -> MatSet:
+    def _recalc_singlets(self, diag: Dict[Invar, Sub], cold: MatSet, rows=None, names=()) -> MatSet:
         """recalc_singlet (c++/symmetry.hpp:185-200) through recalc_general
         (c++/recalc.hpp:82-108) for every singlet operator of `cold` over the stored states
         (or the first rows(s) states of each subspace): the terms of one operator are built
-        once and replicated over the operators (operator-major)."""
+        once and replicated over the operators (operator-major). `names` are the operators of
+        `cold` in its order; the global ones among them then gain the added site's charge,
+        recalc_global / recalc1_global (c++/symmetry/nrg-recalc-QS.hpp:680-740,
+        c++/recalc.hpp:111-122): <I||Q||I> += value * U_i1 U_ip^T over the same states, in the
+        same batched call after the operator's recalc_general terms."""
         rows = rows or (lambda s: s.nstored)
         out = MatSet(self.dev, {I: (rows(s), rows(s)) for I, s in diag.items()}, cold.nops)
         base = []
@@ -859,6 +873,26 @@ class QSRun:
             op = np.repeat(np.arange(cold.nops, dtype=np.uint64), len(b))
             t["M"] += op * np.uint64(8 * out.total)
             t["O"] += op * np.uint64(8 * cold.total)
+        else:
+            t = np.zeros(0, dtype=GEMM3_DTYPE)
+        glob = []
+        for o, name in enumerate(names):
+            if name not in self.gop_names:
+                continue
+            for I, s in diag.items():
+                k = rows(s)
+                if k == 0:
+                    continue
+                M = out.ptr(I, o)
+                for i1, ip, _, value in self.T.GLOBAL[name]:
+                    w = s.dims[i1 - 1]
+                    if w == 0 or s.dims[ip - 1] == 0:
+                        continue
+                    glob.append((M, k, s.vptr + 8 * s.offs[i1 - 1], s.n, 0, 0, s.vptr + 8 * s.offs[ip - 1], s.n,
+                                 k, k, w, s.dims[ip - 1], 0, 1, float(value)))
+        if glob:
+            t = np.concatenate([t, np.array(glob, dtype=GEMM3_DTYPE)])
+        if len(t):
             self._gemm(t, (cold,))
         return out
 
@@ -1134,7 +1168,7 @@ class QSRun:
             if k:  # the pass is the last reader of the previous step's eigenvectors
                 steps[k - 1].vecs = steps[k - 1].host = None
             self._resident(k, range(nst - 1, k, -1))
-            cur = {kind: (self._recalc_singlets(st.diag, m, rows) if kind == "s"
+            cur = {kind: (self._recalc_singlets(st.diag, m, rows, self.sop_names) if kind == "s"
                           else self._recalc_tensor(st.diag, m, *tables[kind], rows)) for kind, m in cur.items()}
             dg = st.diag
             merge = p.NN1 or p.NN2avg or ((st.N % 2 == 0) if p.NN2even else (st.N % 2 == 1))

@@ -21,7 +21,7 @@ an error when it is used.
 from __future__ import annotations
 
 import math
-from typing import Callable, List, Tuple
+from typing import Callable, Dict, List, Tuple
 
 import numpy as np
 
@@ -141,6 +141,9 @@ class Tables:
                 evaluated by doublet_factor(fn, ss1)
     TRIPLET     (dq, rows (i1, ip, factor(S1))): a triplet operator for Ip = I1 + dq, the factor
                 a function of the spin S1 of I1 (a numpy float64), see triplet_factor
+    GLOBAL      name -> rows (i1, ip, channel, value) of the global charge operators
+                (SymmetryQS::recalc_global, c++/symmetry/nrg-recalc-QS.hpp:680-740): after the
+                singlet recalculation, <I||Q||I> += value * U_i1 U_ip^T for every subspace I
     """
 
     def __init__(self, channels, IN, QN, OFFDIAG, DIAG, DIAG_FIRST, RECALC_F, DOUBLET, TRIPLET,
@@ -151,6 +154,7 @@ class Tables:
         self.OFFDIAG, self.DIAG, self.DIAG_FIRST = OFFDIAG, DIAG, DIAG_FIRST
         self.RECALC_F, self.DOUBLET, self.TRIPLET = RECALC_F, DOUBLET, TRIPLET
         self._doublet_of_spin = doublet_of_spin
+        self.GLOBAL = global_charges(DIAG) if channels == 2 else {}
 
     def doublet_factor(self, fn, ss1: int) -> float:
         """A doublet-table factor at SS = ss1 (rows of the two-channel tables are functions of
@@ -162,6 +166,21 @@ class Tables:
 
     def new_subspaces(self, I: Invar) -> List[Invar]:
         return [(I[0] - d[0], I[1] - d[1]) for d in self.IN]
+
+
+def global_charges(diag) -> Dict[str, List[Tuple[int, int, int, int]]]:
+    """The global operators of two-channel QS: the charge the new site adds in channel 0 (Q1)
+    and in channel 1 (Q2), their difference Q2 - Q1 (Qdiff) and the total charge counted
+    from half filling, sum over the channels of (n_ch - 1) (Qtot). A combination i that adds
+    n electrons in channel ch contributes the row (i, i, ch, value) where value is nonzero,
+    channel 0 rows first, by combination (the reference's qs-2ch-{q1,q2,qdiff,qtot}.dat)."""
+    n = {(i, ch): int(num) for i, ch, num in diag}
+    combs = sorted({i for i, _ in n})
+    rows = {"Q1": [(i, i, 0, n[i, 0]) for i in combs],
+            "Q2": [(i, i, 1, n[i, 1]) for i in combs],
+            "Qdiff": [(i, i, 0, -n[i, 0]) for i in combs] + [(i, i, 1, n[i, 1]) for i in combs],
+            "Qtot": [(i, i, ch, n[i, ch] - 1) for ch in (0, 1) for i in combs]}
+    return {name: [r for r in rs if r[3] != 0] for name, rs in rows.items()}
 
 
 def _one(ss):

@@ -17,6 +17,8 @@ host with LAPACK dsyev and BLAS dgemm through ``oracle.py``. It follows
   measure_singlet             c++/measurements.hpp:18-30
   recalc_irreduc / recalc_f   c++/symmetry/nrg-recalc-QS.hpp:192-330, c++/recalc.hpp:52-76
   recalc_singlet              c++/symmetry.hpp:185-200, c++/recalc.hpp:82-108
+  recalc_global (QS, 2 ch.)   c++/symmetry/nrg-recalc-QS.hpp:680-740, c++/recalc.hpp:111-122,
+                              qs-2ch-{q1,q2,qdiff,qtot}.dat
   recalc_doublet (QS)         c++/symmetry/nrg-recalc-QS.hpp:32-117, qs-1ch-doublet{p,m}.dat
   DM-NRG                      init_rho, cdmI, calc_densitymatrix(_iterN) c++/dmnrg.hpp:43-112;
                               Algo_DMNRG c++/algo_DMNRG.hpp:29-52; BaseSpectrum::calc c++/algo.hpp:55-67;
@@ -148,6 +150,13 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     opch = [dict(d.opch[ch][0]) for ch in range(d.channels)]
     ops = {name: {I1: m for (I1, I2), m in mats.items() if I1 == I2}
            for name, (kind, mats) in d.ops.items() if kind in "sg"}
+    gops = {name for name, (kind, _) in d.ops.items() if kind == "g"}
+    if not gops <= set(T.GLOBAL):
+        raise ValueError(f"global operators {sorted(gops - set(T.GLOBAL))}: not in recalc_global")
+
+    def singlet_order(names):
+        """Singlets, then global operators, each by name (c++/output.hpp:121-127)."""
+        return sorted(set(names) - gops) + sorted(set(names) & gops)
     # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
     algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"),
                             ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls"), ("FT", "finite")) if flag(k)]
@@ -189,7 +198,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         f = betabar
         Z = sum(I[1] * sum(math.exp(-f * c) for c in e.corr[:e.nrstored]) for I, e in diag.items())
         row = [scale_of(trueN) / betabar]
-        for name in sorted(ops):
+        for name in singlet_order(ops):
             tr = 0.0
             for I, e in diag.items():
                 m = ops[name][I]
@@ -356,6 +365,11 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
                         U = np.ascontiguousarray(e.U[i][:k])
                         Oa = np.ascontiguousarray(cold[a][:dims[i], :dims[i]])
                         O.transform(m, 1.0, U, Oa, U)
+                    # recalc_global: the charge of the added site, product(m, value, U_i1, U_ip)
+                    for i1, ip, _, value in (T.GLOBAL[name] if name in gops else ()):
+                        if k and dims[i1 - 1] and dims[ip - 1]:
+                            O.product(m, float(value), np.ascontiguousarray(e.U[i1 - 1][:k]),
+                                      np.ascontiguousarray(e.U[ip - 1][:k]))
                     cn[I] = m
                 out[name] = cn
             return out
@@ -432,9 +446,9 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         diag = new
     if (dm or fdm_needed) and steps:
         _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos if dm else [], spectra, fdm_out if fdm_flags else None,
-                    total_energy, C, sorted(ops), bins_out=bins_out)
+                    total_energy, C, singlet_order(ops), bins_out=bins_out)
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
-    return td_fields, td_rows, ["T"] + sorted(ops), custom_rows
+    return td_fields, td_rows, ["T"] + singlet_order(ops), custom_rows
 
 
 def _exact_sum(values) -> Fraction:

@@ -33,7 +33,7 @@ CASES = [
     "test9_keepenergy", "legacy_sigma_trick_siam_qs", "legacy_substeps_one_siam_std", "test32_arbitrary_DOS",
     "test47_nrgchain", "test48_adapt_tri=old", "test50_ref1", "test52_ref2", "test54_ref3",
     "test33_Delta", "test34_bandrescale", "test49_template1", "test51_template2", "test53_template3",
-    "test63_dumpsubspaces",
+    "test63_dumpsubspaces", "c++sym_all/legacy_globalop_Q1Q2-QS",
 ]
 # spectra of the DM-NRG, FDM, CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)

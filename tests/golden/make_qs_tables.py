@@ -2,7 +2,8 @@
 
 The reference keeps the coefficients of symmetry QS as C++ fragments under
 ``c++/symmetry/coefnew/qs/`` (``qs-{1,2}ch-{offdiag,diag,spinup*,spindown*,doublet*,triplet*}.dat``):
-each row names its combinations and a closed-form factor in the spin S of a subspace. This
+each row names its combinations and a closed-form factor in the spin S of a subspace; the
+two-channel global charge tables (``qs-2ch-{q1,q2,qdiff,qtot}.dat``) hold integers. This
 script evaluates every row's factor for SS = 1..11 (S = 0..5) in IEEE double arithmetic, as
 the C++ evaluates it (so 1/0 is inf and sqrt of a negative number is nan), and writes the
 values in file order. The test tests/test_qs_tables.py compares nrgljubljana_b200/qs.py
@@ -19,7 +20,8 @@ import numpy as np
 
 SS = list(range(1, 12))
 FILES = ["offdiag", "diag", "spinupa", "spindowna", "spinupb", "spindownb", "doubletp", "doubletm",
-         "triplets", "tripletp", "tripletm"]
+         "triplets", "tripletp", "tripletm", "q1", "q2", "qdiff", "qtot"]
+GLOBAL = ("q1", "q2", "qdiff", "qtot")
 
 
 def value(expr: str, s: float) -> float:
@@ -52,13 +54,15 @@ def rows_of(path: str, kind: str):
         line = line.strip()
         if not line:
             continue
-        if kind in ("offdiag", "diag"):
+        if kind in ("offdiag", "diag") + GLOBAL:
             body = line[line.index("(") + 1:line.rindex(")")]
         else:
             body = line.rstrip(",")[1:-1]
         args = split_args(body)
         if kind == "offdiag":      # OFFDIAG(i, j, ch, factor(S(ss)))
             rows.append([int(args[0]), int(args[1]), int(args[2]), [value(args[3], (ss - 1) / 2) for ss in SS]])
+        elif kind in GLOBAL:       # Q1(i1, ip, ch, value) and the like: integer values
+            rows.append([int(args[0]), int(args[1]), int(args[2]), int(args[3])])
         elif kind == "diag":       # DIAG(i, ch, number)
             rows.append([int(args[0]), int(args[1]), float(args[2])])
         elif kind.startswith("spin"):   # { i1, ip, factor(S(ssp)) }

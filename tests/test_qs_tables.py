@@ -76,3 +76,12 @@ def test_table_shapes():
     for ch, T in TABLES:
         assert T.COMBS == len(T.IN) == len(T.QN) == 4 ** ch
     assert np.array_equal(np.array(qs.QS1.IN), np.array([(1, 0), (0, -1), (0, 1), (-1, 0)]))
+
+
+def test_global_charge_tables():
+    """Q1, Q2, Qdiff, Qtot of two-channel QS row by row (qs-2ch-{q1,q2,qdiff,qtot}.dat);
+    one channel has no global operators (recalc_global asserts, nrg-recalc-QS.hpp:680-740)."""
+    assert sorted(qs.QS2.GLOBAL) == ["Q1", "Q2", "Qdiff", "Qtot"]
+    for name, rows in qs.QS2.GLOBAL.items():
+        assert [tuple(r) for r in REF[f"2ch-{name.lower()}"]] == rows, name
+    assert qs.QS1.GLOBAL == {}

@@ -20,7 +20,8 @@ from test_dmnrg import ATOL_REL_TO_MAX, ORA_ATOL_REL_TO_MAX, ORA_RTOL, RTOL, ass
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
 CFS_CASES = ["test2_algorithms_cfs", "test2_algorithms_cfsgtls", "test_cfs_only",
-             "legacy_sigma_trick_siam_qs"]  # keep 5000, four spectra with cross pairs A_d-B_d, B_d-A_d
+             "legacy_sigma_trick_siam_qs",  # keep 5000, four spectra with cross pairs A_d-B_d, B_d-A_d
+             "legacy_globalop_Q1Q2-QS"]  # two channels: correlators of the global charges Q1, Q2, Qdiff
 ALL_CASES = ["test2_algorithms", "test11_T", "test55_gt_ls",  # DMNRG + FDM + CFS + FT (and gt/ls parts)
              "test2_algorithms_finite",  # FT alone
              "legacy_substeps_one_siam_std"]  # DMNRG + FDM + CFS + FT with tdfdm
