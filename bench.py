@@ -921,16 +921,20 @@ def nrg_run_arm(torch, device: int, args) -> dict:
 
     PerBlock = per_block_driver(torch)
 
+    spilled = []
+
     def timed(cls, reps):
         cls(p, d, device).run()  # warm-up
         torch.cuda.synchronize()
         best, res = None, None
         for _ in range(reps):
             t0 = time.perf_counter()
-            res = cls(p, d, device).run()
+            run = cls(p, d, device)
+            res = run.run()
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
             best = dt if best is None else min(best, dt)
+            spilled.append(run.spilled_bytes)
         return best, res
 
     ctx.profile(True)
@@ -944,6 +948,7 @@ def nrg_run_arm(torch, device: int, args) -> dict:
            "blocks_per_step_max": max(res.blocks_per_step), "block_dim_max": max(res.max_dim_per_step),
            "device_phases_ms_per_run": {k: v[0] / 4 for k, v in phases.items() if v[1]},
            "kernel_launches_per_step": sum(v[1] for v in phases.values()) / 4 / d.nmax,
+           "eigenvectors_via_host_bytes": max(spilled),
            "per_block_gpu": {"steps_per_s": d.nmax / t_pb, "ms_per_run": t_pb * 1e3,
                              "impl": "same driver, torch.linalg.eigh (cuSOLVER) one block per launch"}}
     td = np.array(res.td)

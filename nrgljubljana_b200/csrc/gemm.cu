@@ -8,7 +8,7 @@
 //
 // One CTA (4 warps) computes a 64 x 64 tile of one output; each warp owns a 32 x 32
 // sub-tile (4 x 4 DMMA tiles). K is walked in chunks of 16 over all segments of the
-// output, double-buffered through registers into shared memory.
+// output, double-buffered in shared memory by asynchronous copies (cp.async).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -21,13 +21,21 @@ constexpr int BM = kGemmBM, BN = kGemmBN, BK = kGemmBK, NT = kGemmThreads;
 constexpr int PAD = 4;
 constexpr int LDS = BM + PAD;  // shared-memory row stride (doubles) of both operand tiles
 
-struct Stage {
-  double a[8];
-  double b[8];
-};
+// Asynchronous 8-byte copy global -> shared (cp.async, no register staging); with ok false the
+// destination is zero-filled and nothing is read (src must still be a valid address).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = ok ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Load the BK x BM slice of op(A) and the BK x BN slice of op(B) starting at k0 into regs.
-__device__ __forceinline__ void load_stage(Stage& s, const GemmSeg& g, int M, int N, int m0, int n0, int k0) {
+// Copy the BK x BM slice of op(A) and the BK x BN slice of op(B) starting at k0 into the
+// stage's shared-memory tiles As[k][m], Bs[k][n] (zeros outside the matrices). Consecutive
+// threads read consecutive addresses of the contiguous direction of each operand.
+__device__ __forceinline__ void issue_stage(const GemmSeg& g, int M, int N, int m0, int n0, int k0, double* As,
+                                            double* Bs) {
   const int tid = threadIdx.x;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
@@ -35,9 +43,9 @@ __device__ __forceinline__ void load_stage(Stage& s, const GemmSeg& g, int M, in
     int m, k;
     if (!g.transA) { k = e & (BK - 1); m = e >> 4; } else { m = e & (BM - 1); k = e >> 6; }
     const int gm = m0 + m, gk = k0 + k;
-    double v = 0.0;
-    if (gm < M && gk < g.K) v = g.transA ? g.A[(int64_t)gk * g.lda + gm] : g.A[(int64_t)gm * g.lda + gk];
-    s.a[i] = v * g.alpha;
+    const bool ok = gm < M && gk < g.K;
+    const double* src = ok ? (g.transA ? g.A + (int64_t)gk * g.lda + gm : g.A + (int64_t)gm * g.lda + gk) : g.A;
+    cp_async8(As + k * LDS + m, src, ok);
   }
 #pragma unroll
   for (int i = 0; i < 8; i++) {
@@ -45,28 +53,11 @@ __device__ __forceinline__ void load_stage(Stage& s, const GemmSeg& g, int M, in
     int n, k;
     if (!g.transB) { n = e & (BN - 1); k = e >> 6; } else { k = e & (BK - 1); n = e >> 4; }
     const int gn = n0 + n, gk = k0 + k;
-    double v = 0.0;
-    if (gn < N && gk < g.K) v = g.transB ? g.B[(int64_t)gn * g.ldb + gk] : g.B[(int64_t)gk * g.ldb + gn];
-    s.b[i] = v;
+    const bool ok = gn < N && gk < g.K;
+    const double* src = ok ? (g.transB ? g.B + (int64_t)gn * g.ldb + gk : g.B + (int64_t)gk * g.ldb + gn) : g.B;
+    cp_async8(Bs + k * LDS + n, src, ok);
   }
-}
-
-__device__ __forceinline__ void store_stage(const Stage& s, const GemmSeg& g, double* As, double* Bs) {
-  const int tid = threadIdx.x;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int e = tid + NT * i;
-    int m, k;
-    if (!g.transA) { k = e & (BK - 1); m = e >> 4; } else { m = e & (BM - 1); k = e >> 6; }
-    As[k * LDS + m] = s.a[i];
-  }
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int e = tid + NT * i;
-    int n, k;
-    if (!g.transB) { n = e & (BN - 1); k = e >> 6; } else { k = e & (BK - 1); n = e >> 4; }
-    Bs[k * LDS + n] = s.b[i];
-  }
+  cp_async_commit();
 }
 
 // One 64 x 64 output tile `tt` (row-major tile order) of output o, whose segments are
@@ -82,38 +73,51 @@ __device__ __forceinline__ void gemm_tile(const GemmOut& o, const GemmSeg* __res
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   const int fr = lane >> 2, fc = lane & 3;
 
+  // The accumulators start from beta*C: the loads of C go out beside the first operand loads
+  // instead of after the last product, which matters for the short-K updates (K = 128 of the
+  // back-transform), where one exposed load latency is a large part of a tile's time.
   double acc[4][4][2];
+  const bool addc = o.beta != 0.0;
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 4; i++) {
+    const int r = m0 + wm + i * 8 + fr;
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = n0 + wn + j * 8 + 2 * fc + h;
+        acc[i][j][h] = (addc && r < o.M && c < o.N) ? o.beta * o.C[(int64_t)r * o.ldc + c] : 0.0;
+      }
+  }
 
   // Flatten (segment, k-chunk) into one sequence of steps.
   int total = 0;
   for (int s = 0; s < o.nseg; s++) total += (segs[o.seg0 + s].K + BK - 1) / BK;
 
   if (total > 0) {
-    int cs = 0, ck = 0;  // current segment, k offset inside it
+    // Two stages: the copy of chunk step+1 runs while chunk step is multiplied. One barrier per
+    // chunk: after it chunk step has landed for every thread and every thread has finished
+    // reading the other stage (chunk step-1), which the next copy overwrites.
+    int cs = 0, ck = 0;  // segment and k offset of the newest chunk issued
     while (segs[o.seg0 + cs].K <= 0) cs++;
     GemmSeg g = segs[o.seg0 + cs];
-    Stage st;
-    load_stage(st, g, o.M, o.N, m0, n0, 0);
-    store_stage(st, g, As[0], Bs[0]);
-    __syncthreads();
-    int buf = 0;
+    issue_stage(g, o.M, o.N, m0, n0, 0, As[0], Bs[0]);
+    double alpha_next = g.alpha;
     for (int step = 0; step < total; step++) {
-      // advance to the next chunk and prefetch it into registers
-      int ns = cs, nk = ck + BK;
-      GemmSeg gn = g;
-      const bool has_next = step + 1 < total;
-      if (has_next) {
-        if (nk >= g.K) {
-          ns = cs + 1;
-          while (segs[o.seg0 + ns].K <= 0) ns++;
-          nk = 0;
-          gn = segs[o.seg0 + ns];
+      cp_async_wait_all();
+      __syncthreads();
+      const int buf = step & 1;
+      const double alpha = alpha_next;
+      if (step + 1 < total) {
+        ck += BK;
+        if (ck >= g.K) {
+          cs++;
+          while (segs[o.seg0 + cs].K <= 0) cs++;
+          ck = 0;
+          g = segs[o.seg0 + cs];
         }
-        load_stage(st, gn, o.M, o.N, m0, n0, nk);
+        issue_stage(g, o.M, o.N, m0, n0, ck, As[buf ^ 1], Bs[buf ^ 1]);
+        alpha_next = g.alpha;
       }
       const double* as = As[buf];
       const double* bs = Bs[buf];
@@ -121,7 +125,7 @@ __device__ __forceinline__ void gemm_tile(const GemmOut& o, const GemmSeg* __res
       for (int kk = 0; kk < BK; kk += 4) {
         double a[4], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) a[i] = as[(kk + fc) * LDS + wm + i * 8 + fr];
+        for (int i = 0; i < 4; i++) a[i] = as[(kk + fc) * LDS + wm + i * 8 + fr] * alpha;
 #pragma unroll
         for (int j = 0; j < 4; j++) b[j] = bs[(kk + fc) * LDS + wn + j * 8 + fr];
 #pragma unroll
@@ -129,18 +133,10 @@ __device__ __forceinline__ void gemm_tile(const GemmOut& o, const GemmSeg* __res
 #pragma unroll
           for (int j = 0; j < 4; j++) dmma884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
-      if (has_next) {
-        store_stage(st, gn, As[buf ^ 1], Bs[buf ^ 1]);
-        cs = ns;
-        ck = nk;
-        g = gn;
-      }
-      __syncthreads();
-      buf ^= 1;
     }
   }
 
-  // Epilogue: C = beta*C + acc.
+  // Epilogue: C = acc (= beta*C + the products).
 #pragma unroll
   for (int i = 0; i < 4; i++) {
     const int r = m0 + wm + i * 8 + fr;
@@ -150,16 +146,13 @@ __device__ __forceinline__ void gemm_tile(const GemmOut& o, const GemmSeg* __res
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int c = n0 + wn + j * 8 + 2 * fc + h;
-        if (c < o.N) {
-          double* p = o.C + (int64_t)r * o.ldc + c;
-          *p = (o.beta == 0.0) ? acc[i][j][h] : fma(o.beta, *p, acc[i][j][h]);
-        }
+        if (c < o.N) o.C[(int64_t)r * o.ldc + c] = acc[i][j][h];
       }
     }
   }
 }
 
-__global__ void __launch_bounds__(NT) gemm_batch_kernel(const GemmOut* __restrict__ outs,
+__global__ void __launch_bounds__(NT, 5) gemm_batch_kernel(const GemmOut* __restrict__ outs,
                                                          const GemmSeg* __restrict__ segs, int nout) {
   // Locate the output that owns this tile (binary search over tile0).
   const int t = blockIdx.x;
@@ -173,7 +166,7 @@ __global__ void __launch_bounds__(NT) gemm_batch_kernel(const GemmOut* __restric
 }
 
 // Single output with a single segment, both passed by value (no descriptor memory).
-__global__ void __launch_bounds__(NT) gemm_one_kernel(const __grid_constant__ GemmOut o,
+__global__ void __launch_bounds__(NT, 5) gemm_one_kernel(const __grid_constant__ GemmOut o,
                                                        const __grid_constant__ GemmSeg g) {
   gemm_tile(o, &g, blockIdx.x);
 }

@@ -540,6 +540,7 @@ class QSRun:
         self.meas: List[_Measure] = []
         self.dm_steps: List[_StepRecord] = []
         self.spilled_bytes = 0  # eigenvector bytes moved to host memory (and back) in this run
+        self._kept_since_check = 0
         self.total_energy = float(d.gs_energy)  # Stats::total_energy (c++/stats.hpp:60-71)
         # operators of the spectral pass as read: singlets by subspace, doublets and triplets
         # by subspace pair
@@ -735,8 +736,12 @@ class QSRun:
         self._vecs = job.Vbuf  # the step's eigenvectors stay allocated until the next step
         if self.keep_steps:  # the density matrices and spectra need every step's eigenvectors
             self.dm_steps.append(_StepRecord(N, self.scale(N), diag, job.Vbuf, self.total_energy))
-            self._make_room(self.SPILL_HEADROOM_STEPS * 8 * int(job.moff[-1]),
-                            range(len(self.dm_steps) - 1))
+            # the free memory is read (cudaMemGetInfo, milliseconds) once per GiB kept
+            self._kept_since_check += 8 * int(job.moff[-1])
+            if self._kept_since_check >= self.SPILL_CHECK_BYTES:
+                self._kept_since_check = 0
+                self._make_room(self.SPILL_HEADROOM_STEPS * 8 * int(job.moff[-1]),
+                                range(len(self.dm_steps) - 1))
         self.diag, self.opch, self.ops = diag, new_opch, new_ops
         self.N = N + 1
 
@@ -745,24 +750,34 @@ class QSRun:
     # eigenvectors (spectra, FDM) needs that memory for its own later steps.
     TRIM_STEP_BYTES = 1 << 30
 
-    # The kept steps' eigenvectors live on the device while it has room. When, after a step,
-    # the device has less free memory than SPILL_HEADROOM_BYTES or SPILL_HEADROOM_STEPS times
-    # that step's eigenvector bytes (the next step's matrices, eigenvectors and workspace come
+    # The kept steps' eigenvectors live on the device while it has room. When, after a step
+    # (checked each time another SPILL_CHECK_BYTES of eigenvectors have been kept), the device
+    # has less free memory than SPILL_HEADROOM_BYTES or SPILL_HEADROOM_STEPS times that step's
+    # eigenvector bytes (the next step's matrices, eigenvectors and workspace come
     # out of it), the oldest steps move to pinned host memory; the density-matrix sweeps and
     # the spectral pass bring each step back when they reach it. This is the device form of
     # the reference's unitary files, DiagInfo::save / load (c++/eigen.hpp:389-413), which hold
     # every step's eigenvectors between the NRG run and the density-matrix pass.
     SPILL_HEADROOM_BYTES = 16 << 30
     SPILL_HEADROOM_STEPS = 6
+    SPILL_CHECK_BYTES = 1 << 30
 
     def _free_device_bytes(self) -> int:
         free, _ = torch.cuda.mem_get_info(self.dev)
         return free + torch.cuda.memory_reserved(self.dev) - torch.cuda.memory_allocated(self.dev)
 
     def _make_room(self, need: int, candidates) -> None:
-        """Moves the eigenvectors of the steps in `candidates` (in that order) to host memory
-        until the device has max(need, SPILL_HEADROOM_BYTES) bytes free."""
+        """Gives the library's workspace back, then moves the eigenvectors of the steps in
+        `candidates` (in that order) to host memory, until the device has
+        max(need, SPILL_HEADROOM_BYTES) bytes free."""
         need = max(need, self.SPILL_HEADROOM_BYTES)
+        free = self._free_device_bytes()
+        if free >= need:
+            return
+        # first the memory that is only held for reuse: the library's workspace (it grows back
+        # to what the next call needs) and torch's cache
+        self.ctx.trim()
+        torch.cuda.empty_cache()
         free = self._free_device_bytes()
         if free >= need:
             return

@@ -103,6 +103,7 @@ def test_gpu_fdm_with_eigenvectors_in_host_memory(monkeypatch, case):
     p, d = RunParams.from_param(parse_param(read(case, "param"))), read_data(read(case, "data"))
     base = QSRun(p, d, 0).run()
     monkeypatch.setattr(QSRun, "SPILL_HEADROOM_BYTES", 1 << 60)
+    monkeypatch.setattr(QSRun, "SPILL_CHECK_BYTES", 0)
     run = QSRun(p, d, 0)
     res = run.run()
     assert run.spilled_bytes > 0
