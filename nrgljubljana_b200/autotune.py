@@ -4,7 +4,7 @@ The eigensolver sends each block of a step down one of four paths by its order: 
 one-CTA shared-memory solver (n <= small_max_n), the one-CTA shared-memory tridiagonal
 reduction (n <= mid_max_n), the cluster reduction in distributed shared memory
 (n <= cluster_max_n, when the clusters fit the SMs at once) and the streaming reduction
-from HBM, whose CTAs run one or two per SM (reduction_ctas_per_sm). Where the crossovers
+from HBM, whose CTAs run one, two or three per SM (reduction_ctas_per_sm). Where the crossovers
 lie depends on the device, so they are measured, not assumed: the reference's own
 scheduler (c++/core.hpp:98-107, c++/subspaces.hpp:103-123) only orders the blocks largest
 first; on a GPU the choice of path per block is the equivalent decision.
@@ -17,6 +17,7 @@ are diag(2^{-k/2}) plus symmetric N(0, 0.1^2) couplings, as in the benchmark):
   large  12 blocks in [800, 2000], 4 blocks in [1500, 4096] and 24 blocks in [200, 7049]
          (the steps of the keep-4000 Anderson and keep-5000 two-channel Kondo runs, bound by
          their largest blocks)
+  bulk   1500 blocks in [8, 2048] (a seventh of the benchmark's batched-eigensolve step)
 Each candidate is timed with CUDA events around nrg_diag_batch (the consumed inputs are
 refreshed outside the timed region), best of `reps`; the objective is the mean over the
 batches of the time relative to the starting parameters. Coordinate descent over the
@@ -24,7 +25,7 @@ parameters, each from the current best, twice round.
 
 The result is written to tuning.json beside this module, keyed by the device name, and
 applied by nrgljubljana_b200.context() to every context it creates on such a device.
-Run: python -m nrgljubljana_b200.autotune [--reps R] [--allow-two-per-sm]
+Run: python -m nrgljubljana_b200.autotune [--reps R]
 """
 from __future__ import annotations
 
@@ -50,11 +51,13 @@ GRID = {
     # pay where the other blocks of a batch hide it, and cost 10-15% on keep-4000 Anderson
     # steps (blocks up to 1622), measured.
     "band_min_n": [0, 2048, 3072, 4096],
+    "reduction_ctas_per_sm": [1, 2, 3],
     "band_max_blocks": [4, 8, 16, 32, 64],
 }
 KEYS = ("small_max_n", "mid_max_n", "cluster_max_n", "reduction_ctas_per_sm", "band_min_n", "band_max_blocks")
 # (batches, blocks per batch, smallest and largest order) of the timed workloads
-WORKLOADS = ((8, 40, 8, 480), (2, 300, 8, 1024), (1, 12, 800, 2000), (1, 4, 1500, 4096), (1, 24, 200, 7049))
+WORKLOADS = ((8, 40, 8, 480), (2, 300, 8, 1024), (1, 12, 800, 2000), (1, 4, 1500, 4096), (1, 24, 200, 7049),
+             (1, 1500, 8, 2048))
 
 
 def device_name(device: int = 0) -> str:
@@ -140,7 +143,7 @@ class _Batch:
         return worst
 
 
-def tune(device: int = 0, reps: int = 3, allow_two_per_sm: bool = False, verbose: bool = True) -> dict:
+def tune(device: int = 0, reps: int = 3, verbose: bool = True) -> dict:
     import torch
 
     from .api import Context
@@ -149,8 +152,6 @@ def tune(device: int = 0, reps: int = 3, allow_two_per_sm: bool = False, verbose
     dev = torch.device("cuda", device)
     batches = [_Batch(torch, ctx, s, dev, i) for i, s in enumerate(workloads())]
     grid = dict(GRID)
-    grid["reduction_ctas_per_sm"] = [1, 2] if allow_two_per_sm else [1]
-    grid["band_max_blocks"] = GRID["band_max_blocks"]
 
     base: List[float] = []
 
@@ -207,12 +208,10 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--allow-two-per-sm", action="store_true",
-                    help="also try two CTAs per SM for the streaming reductions")
     ap.add_argument("--out", default=TABLE)
     ap.add_argument("--dry-run", action="store_true", help="print the result, do not write the table")
     a = ap.parse_args(argv)
-    res = tune(a.device, a.reps, a.allow_two_per_sm)
+    res = tune(a.device, a.reps)
     name = device_name(a.device)
     print(json.dumps({name: {k: v for k, v in res.items() if k != "sweep"}}, indent=1))
     if not a.dry_run:

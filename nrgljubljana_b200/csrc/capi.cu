@@ -256,8 +256,8 @@ int nrg_set_tuning(nrg_ctx* c, const nrg_tuning* in) {
   if (t.cluster_max_n < t.mid_max_n || t.cluster_max_n > nrg::kClusterMaxNLimit)
     return fail(NRG_ERR_ARG, "cluster_max_n = %d outside [mid_max_n, %d]", t.cluster_max_n,
                 nrg::kClusterMaxNLimit);
-  if (t.reduction_ctas_per_sm != 1 && t.reduction_ctas_per_sm != 2)
-    return fail(NRG_ERR_ARG, "reduction_ctas_per_sm = %d (1 or 2)", t.reduction_ctas_per_sm);
+  if (t.reduction_ctas_per_sm < 1 || t.reduction_ctas_per_sm > 3)
+    return fail(NRG_ERR_ARG, "reduction_ctas_per_sm = %d (1, 2 or 3)", t.reduction_ctas_per_sm);
   if (t.band_min_n != 0 && (t.band_min_n < 256 || t.band_min_n > NRG_DIAG_MAX_N))
     return fail(NRG_ERR_ARG, "band_min_n = %d (0, or 256 .. %d)", t.band_min_n, NRG_DIAG_MAX_N);
   if (t.band_max_blocks < 1) return fail(NRG_ERR_ARG, "band_max_blocks = %d (at least 1)", t.band_max_blocks);

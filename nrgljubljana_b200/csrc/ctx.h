@@ -22,7 +22,7 @@ const char* phase_name(int p);
 
 struct nrg_ctx {
   int device = 0;
-  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 2, 3072, 64};  // the autotuner's B200 values
+  nrg_tuning tune = {nrg::kSmallMaxN, nrg::kMidMaxN, nrg::kClusterMaxN, 3, 3072, 64};  // the autotuner's B200 values
   // profiling: launch counts per phase (always), CUDA-event intervals (when enabled)
   bool prof = false;
   long long launches[nrg::kPhCount] = {};

@@ -402,18 +402,21 @@ __global__ void __launch_bounds__(256) pack_lower_kernel(const LargeBlock* __res
 // One CTA per block: blocked (NB) Householder reduction of the packed lower triangle in W1
 // (leading dimension ldp) to tridiagonal form; d, e, tau out; Householder vector k is left
 // in column k (W1[k*ldp + k+1 ..], with a unit at k+1).
-__global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBlock* __restrict__ blocks,
-                                                                  const CUtensorMap* __restrict__ tmaps) {
+// STAGES slabs in flight per warp; MINB CTAs per SM for the register budget: <4, 2> (two per
+// SM, 255 registers) and <2, 3> (three per SM, 168 registers and a smaller ring).
+template <int STAGES, int MINB>
+__global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeBlock* __restrict__ blocks,
+                                                                    const CUtensorMap* __restrict__ tmaps) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ __align__(8) uint64_t bars[kTriWarps * kStages];
+  __shared__ __align__(8) uint64_t bars[kTriWarps * STAGES];
   const LargeBlock B = blocks[blockIdx.x];
   const int n = B.n, ld = B.ldp, tid = threadIdx.x, nt = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
   double* A = B.W1;
   double* W = B.W2;
-  // TMA destinations: 1024-byte aligned ring of kStages slabs per warp
+  // TMA destinations: 1024-byte aligned ring of STAGES slabs per warp
   double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sm) + 1023) & ~(uintptr_t)1023);
-  double* v = ring + kTriWarps * kStages * kSlabD;     // n
+  double* v = ring + kTriWarps * STAGES * kSlabD;      // n
   double* y = v + n;                                   // n
   double* part = y + n;                                // nwarps * 2NB
   double* cwv = part + nwarps * 2 * NB;                // 2NB
@@ -421,7 +424,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
   int phase = 0;
   unsigned parity = 0;
   if (lane == 0) {
-    for (int st = 0; st < kStages; st++) mbar_init(bars + warp * kStages + st, 1);
+    for (int st = 0; st < STAGES; st++) mbar_init(bars + warp * STAGES + st, 1);
     fence_mbar_init();
     tmap_acquire(tmaps + blockIdx.x);  // lane 0 issues this warp's bulk copies
   }
@@ -484,7 +487,7 @@ __global__ void __launch_bounds__(kTriThreads, 2) tridiag_kernel(const LargeBloc
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        symv_lower(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info, warp, nwarps);
+        symv_lower<STAGES>(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info, warp, nwarps);
         if (j > 0) {
           double pw[NB], pv[NB];
 #pragma unroll
@@ -1558,8 +1561,6 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
     while (nts_all < (int)ord.size() && n[ord[nts_all]] >= c->tune.band_min_n) nts_all++;
     if (nts_all > c->tune.band_max_blocks) nts_all = 0;
   }
-  // at least half an SM's shared memory per reduction CTA keeps one of them per SM
-  const bool one_per_sm = c->tune.reduction_ctas_per_sm == 1;
   for (int b : ord)
     if (n[b] > kMaxLargeN)
       return fail(NRG_ERR_ARG, "block %d: order %d exceeds the supported maximum %d", b, n[b], kMaxLargeN);
@@ -1928,21 +1929,26 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
         NRG_CK(cudaLaunchKernelEx(&cfg, tridiag_cluster_kernel, d1 + nbig, lmax));
       }
       if (nbig) {
-        const size_t smem = 1024 + sizeof(double) * ((size_t)kTriWarps * kStages * kSlabD + 2 * (size_t)b1[0].n +
-                                                     (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
+        auto tri_bytes = [&](int st) {
+          return 1024 + sizeof(double) * ((size_t)kTriWarps * st * kSlabD + 2 * (size_t)b1[0].n +
+                                          (size_t)kTriWarps * 2 * NB + 2 * NB + 64);
+        };
         const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(dbase + tmap_off) + nts;
         pack_lower_kernel<<<dim3((b1[0].n + 7) / 8, nbig), 256, 0, s>>>(d1);
         NRG_CK(cudaGetLastError());
         // Few large blocks: one cluster of kTclC CTAs per block, when the clusters fill at most
         // about two waves of the SMs and the device can hold one such cluster at a time.
         bool tcl = false;
-        // reduction_ctas_per_sm (nrg_tuning) sets how many CTAs of the streaming kernels share an
-        // SM: one, when each requests at least half of an SM's shared memory; two (the default)
-        // otherwise. Two per SM once gave wrong reductions through a race on alpha = v[k+1] in the
-        // reflector step (alpha was read after a barrier that a thread overwriting it could
-        // pass); alpha is now read before that barrier, and batches with more of these CTAs than
-        // SMs pass every check on B200 with two per SM. The ring gets 8, 6 or 4 slabs per warp,
-        // the most that fit.
+        // reduction_ctas_per_sm (nrg_tuning) sets how many CTAs of the streaming kernel share an
+        // SM: one, when each requests at least half of an SM's shared memory; two, with four
+        // slabs in flight per warp; three (the default), with two slabs per warp and at most 168
+        // registers per thread. More CTAs per SM keep the SM's HBM stream going while a CTA is
+        // in the serial part of a column (norm, reflector, block sums); where the blocks' vectors
+        // leave no room for that many, the next smaller count is used. Several per SM once gave
+        // wrong reductions through a race on alpha = v[k+1] in the reflector step (alpha was read
+        // after a barrier that a thread overwriting it could pass); alpha is now read before that
+        // barrier, and batches with more of these CTAs than SMs pass every check on B200. The
+        // cluster kernel's ring gets 8, 6 or 4 slabs per warp, the most that fit.
         int smsm = 0, optin = 0;
         cudaDeviceGetAttribute(&smsm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
@@ -1993,10 +1999,21 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           void* kargs[] = {(void*)&db, (void*)&tm};
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
-          // one or two CTAs per SM as above
-          const size_t smem1 = std::max(smem, (one_per_sm ? (size_t)smsm / 2 + 1024 : (size_t)0));
-          NRG_CK(cudaFuncSetAttribute(tridiag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-          tridiag_kernel<<<nbig, kTriThreads, smem1, s>>>(d1, tm);
+          // one, two or three CTAs per SM as above (1 KB of shared memory is reserved per CTA)
+          int per_sm = c->tune.reduction_ctas_per_sm;
+          if (per_sm == 3 && 3 * (tri_bytes(2) + 1024) > (size_t)smsm) per_sm = 2;
+          if (per_sm == 2 && 2 * (tri_bytes(4) + 1024) > (size_t)smsm) per_sm = 1;
+          if (per_sm == 3) {
+            const size_t smem3 = tri_bytes(2);
+            NRG_CK(cudaFuncSetAttribute(tridiag_kernel<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem3));
+            tridiag_kernel<2, 3><<<nbig, kTriThreads, smem3, s>>>(d1, tm);
+          } else {
+            const size_t smem1 = std::max(tri_bytes(4), (per_sm == 1 ? (size_t)smsm / 2 + 1024 : (size_t)0));
+            NRG_CK(cudaFuncSetAttribute(tridiag_kernel<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem1));
+            tridiag_kernel<4, 2><<<nbig, kTriThreads, smem1, s>>>(d1, tm);
+          }
           NRG_CK(cudaGetLastError());
         }
       }

@@ -28,10 +28,11 @@ def test_table_lookup_by_device_name(tmp_path, monkeypatch):
 def test_workloads_are_seeded():
     from nrgljubljana_b200 import autotune
     a, b = autotune.workloads(), autotune.workloads()
-    assert len(a) == 13 and all(np.array_equal(x, y) for x, y in zip(a, b))
+    assert len(a) == 14 and all(np.array_equal(x, y) for x, y in zip(a, b))
     assert 200 <= a[12].min() and a[12].max() <= 7049
     assert max(int(x.max()) for x in a[:8]) <= 480 and max(int(x.max()) for x in a[8:10]) <= 1024
     assert 800 <= a[10].min() and a[10].max() <= 2000 and 1500 <= a[11].min() and a[11].max() <= 4096
+    assert len(a[13]) == 1500 and 8 <= a[13].min() and a[13].max() <= 2048
 
 
 @pytest.mark.gpu
@@ -40,7 +41,7 @@ def test_set_tuning_checks_ranges():
     ctx = nb.Context()
     t0 = ctx.tuning
     for bad in ({"small_max_n": 31}, {"small_max_n": 97}, {"mid_max_n": 237}, {"cluster_max_n": 641},
-                {"small_max_n": 96, "mid_max_n": 90}, {"reduction_ctas_per_sm": 3}):
+                {"small_max_n": 96, "mid_max_n": 90}, {"reduction_ctas_per_sm": 4}, {"reduction_ctas_per_sm": 0}):
         with pytest.raises(nb.NRGError):
             ctx.set_tuning(**bad)
         assert ctx.tuning == t0
