@@ -71,7 +71,9 @@ NRG_API int nrg_trim(nrg_ctx* ctx);
  *   cluster_max_n  larger blocks up to this order are reduced in the distributed shared
  *                  memory of a thread-block cluster when the clusters fit the SMs at once
  *                  (mid_max_n..640); larger blocks stream their trailing matrix from HBM
- *   reduction_ctas_per_sm  CTAs of the streaming reduction kernel per SM (1, 2 or 3; default 3)
+ *   reduction_ctas_per_sm  most CTAs of the streaming reduction kernel per SM (1, 2 or 3;
+ *                  default 3), used when the batch's streamed blocks fill three waves of them
+ *                  (fewer otherwise: a batch of few large blocks is bound by its largest)
  *   band_min_n     blocks of at least this order, when at most band_max_blocks of them are
  *                  in a batch, take the two-stage reduction (dense -> band on the FP64
  *                  tensor cores, band -> tridiagonal by bulge chasing); 0 = never; default 3072

@@ -21,7 +21,8 @@ are diag(2^{-k/2}) plus symmetric N(0, 0.1^2) couplings, as in the benchmark):
 Each candidate is timed with CUDA events around nrg_diag_batch (the consumed inputs are
 refreshed outside the timed region), best of `reps`; the objective is the mean over the
 batches of the time relative to the starting parameters. Coordinate descent over the
-parameters, each from the current best, twice round.
+parameters, each from the current best, twice round; a change is kept when it wins by more
+than 2% (the batches of small blocks take a few milliseconds and vary by about that much).
 
 The result is written to tuning.json beside this module, keyed by the device name, and
 applied by nrgljubljana_b200.context() to every context it creates on such a device.
@@ -186,7 +187,7 @@ def tune(device: int = 0, reps: int = 3, verbose: bool = True) -> dict:
                 sweep.append({"tuning": cand, "ms": ms, "objective": obj})
                 if verbose:
                     print(f"  {cand} {obj:.4f} {[round(x, 2) for x in ms]}", flush=True)
-                if obj < best_obj * 0.99:  # a change must win by more than the timing noise
+                if obj < best_obj * 0.98:  # a change must win by more than the timing noise
                     best, best_obj, changed = cand, obj, True
         if not changed:
             break

@@ -1999,8 +1999,15 @@ int eig_large_run(nrg_ctx* c, const std::vector<int>& which, const int* n, doubl
           void* kargs[] = {(void*)&db, (void*)&tm};
           NRG_CK(cudaLaunchKernelExC(&cfg, tcl_fn, kargs));
         } else {
-          // one, two or three CTAs per SM as above (1 KB of shared memory is reserved per CTA)
+          // one, two or three CTAs per SM as above (1 KB of shared memory is reserved per CTA);
+          // reduction_ctas_per_sm is the most, used when the batch fills at least three waves of
+          // that many CTAs per SM. A batch of fewer large blocks is bound by its largest ones,
+          // which finish sooner with an SM's bandwidth shared by fewer CTAs (measured on B200:
+          // 1500 blocks of order 8-2048, about 330 of them streamed, take 873 ms with one CTA
+          // per SM, 909 with two, 1015 with three; the benchmark's 10,000 blocks run 6.5% faster
+          // with three than with two).
           int per_sm = c->tune.reduction_ctas_per_sm;
+          while (per_sm > 1 && (long long)nbig < 3LL * per_sm * nsm) per_sm--;
           if (per_sm == 3 && 3 * (tri_bytes(2) + 1024) > (size_t)smsm) per_sm = 2;
           if (per_sm == 2 && 2 * (tri_bytes(4) + 1024) > (size_t)smsm) per_sm = 1;
           if (per_sm == 3) {

@@ -188,6 +188,35 @@ def test_large_orders(nb, n, kind):
     assert (G - torch.diag(torch.diagonal(G))).abs().max().item() < 1e-10
 
 
+@pytest.mark.parametrize("per_sm", [3, 2])
+def test_several_reduction_ctas_per_sm(nb, per_sm):
+    """1400 blocks of order 601-700: enough streamed blocks for three waves of three (or two)
+    CTAs per SM, the launch the benchmark's batch gets (three: two slabs per warp, 168
+    registers). Every block's residual and orthogonality are checked on the device."""
+    import torch
+    ctx = nb.Context()
+    ctx.set_tuning(reduction_ctas_per_sm=per_sm)
+    g = torch.Generator(device="cuda").manual_seed(93)
+    sizes = [601 + (i * 41) % 100 for i in range(1400)]
+    H, E, V, H0 = [], [], [], []
+    for n in sizes:
+        a = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+        h = torch.triu(a + a.T)
+        H0.append(h.clone())
+        H.append(h)
+        E.append(torch.empty(n, dtype=torch.float64, device="cuda"))
+        V.append(torch.empty(n, n, dtype=torch.float64, device="cuda"))
+    info = nb.diag_batch_device(H, E, V, ctx=ctx)
+    torch.cuda.synchronize()
+    assert (info == 0).all()
+    for h, e, v in zip(H0, E, V):
+        n = h.shape[0]
+        Hf = h + torch.triu(h, 1).T
+        nrm = e.abs().max().item()
+        assert torch.linalg.norm(v @ Hf - e[:, None] * v, dim=1).max().item() <= 1e-12 * nrm * math.sqrt(n), n
+        assert (v @ v.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max().item() < 1e-10, n
+
+
 def test_few_large_blocks_batch(nb):
     """A batch like a step of the two-channel Kondo runs: a few large blocks, each reduced by
     its own cluster of CTAs at the same time, beside mid-size and small ones."""
