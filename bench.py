@@ -332,10 +332,11 @@ def main():
     top = max(phases.items(), key=lambda kv: kv[1][0])
     roof = None
     # DRAM bytes per launch of tridiag_kernel relative to its algorithmic bytes, from one ncu
-    # capture of the kernel (two CTAs per SM) on 296 blocks of n = 1024: dram__bytes_read.sum +
-    # dram__bytes_write.sum = 530.8 + 28.7 GB for 474.3 GB algorithmic; the ratio carries over
-    # to larger launches because both grow with the per-column reads of the trailing triangle.
-    tridiag_traffic_ratio = (530.8 + 28.7) / 474.3
+    # capture of the kernel as the benchmark's batch launches it (three CTAs per SM) on 1400
+    # blocks of n = 608: dram__bytes_read.sum + dram__bytes_write.sum = 586.36 + 29.41 GB for
+    # 467.99 GB algorithmic; the ratio carries over to larger launches because both grow with
+    # the per-column reads of the trailing triangle.
+    tridiag_traffic_ratio = (586.36 + 29.41) / 467.99
     if top[0] == "tridiag":
         per_launch_bytes = args.steps * sum(tridiag_bytes(int(n)) for n in sizes if n > 64) / top[1][1]
         avg = top[1][0] / 1e3 / top[1][1]
@@ -343,7 +344,7 @@ def main():
         pk = peaks.get("hbm_gbs", 6650.0)
         roof = {"kernel": "tridiag_kernel", "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
                 "frac": ach / pk, "traffic": per_launch_bytes * tridiag_traffic_ratio,
-                "traffic_source": "ncu dram bytes of tridiag_kernel on 296 x n=1024 (profiles/tridiag_kernel_296x1024.md), scaled by algorithmic bytes",
+                "traffic_source": "ncu dram bytes of tridiag_kernel (three CTAs per SM) on 1400 x n=608 (profiles/tridiag_kernel_1400x608.md), scaled by algorithmic bytes",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg * 1e3}
     else:
