@@ -166,6 +166,23 @@ NRG_DEV void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64
       : "memory");
 }
 
+// The same with an L2 eviction-priority hint (an access policy from createpolicy): the slabs of
+// a trailing triangle that is streamed once per column and does not fit in L2 go first, so
+// that the panel's vectors (read three times per column) stay.
+NRG_DEV void tma_load_2d_hint(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
+      "%3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+NRG_DEV uint64_t l2_evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 constexpr int kStages = 4;                 // slabs in flight per warp
 constexpr int kSlabRows = 64;              // rows of a slab (two per lane)
 constexpr int kSlabD = kSlabRows * 8;      // doubles per slab: 64 rows x 8 columns
@@ -182,7 +199,7 @@ constexpr int kTriWarps = kTriThreads / 32;
 // `parity` holds the warp's mbarrier phase bits across calls.
 // gwarp / gnwarps: this warp's index among the warps that share the product (the warps of
 // one CTA, or of every CTA of a cluster), and their number; y receives this warp's part.
-template <int STAGES = kStages>
+template <int STAGES = kStages, bool EVICT_FIRST = false>
 NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v, double* y, double* ring,
                         uint64_t* bars, unsigned& parity, int* err, int gwarp, int gnwarps) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -202,10 +219,14 @@ NRG_DEV void symv_lower(const CUtensorMap* tmap, int n, int s0, const double* v,
       sl_ = sl0;
     }
   };
+  const uint64_t policy = EVICT_FIRST ? l2_evict_first_policy() : 0;
   auto issue = [&](int I_, int sl_, int st) {
     if (lane == 0) {
       mbar_expect_tx(mybar + st, (unsigned)(kSlabD * sizeof(double)));
-      tma_load_2d(myring + st * kSlabD, tmap, I_ * kSlabRows, sl_ * 8, mybar + st);
+      if (EVICT_FIRST)
+        tma_load_2d_hint(myring + st * kSlabD, tmap, I_ * kSlabRows, sl_ * 8, mybar + st, policy);
+      else
+        tma_load_2d(myring + st * kSlabD, tmap, I_ * kSlabRows, sl_ * 8, mybar + st);
     }
   };
   int I = T0;
@@ -487,7 +508,7 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
       __syncthreads();
       if (tau != 0.0) {
         // (3) y = A_panel_start(k+1:, k+1:) v - V (W^T v) - W (V^T v), W[:, j] = tau y - K v
-        symv_lower<STAGES>(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info, warp, nwarps);
+        symv_lower<STAGES, true>(tmaps + blockIdx.x, n, k + 1, v, y, ring, bars, parity, B.info, warp, nwarps);
         if (j > 0) {
           double pw[NB], pv[NB];
 #pragma unroll
