@@ -333,11 +333,11 @@ def main():
     roof = None
     # DRAM bytes per launch of tridiag_kernel relative to its algorithmic bytes, from one ncu
     # capture of the kernel as the benchmark's batch launches it (three CTAs per SM, the slabs
-    # of the trailing triangle loaded with an L2 evict-first hint) on 1400 blocks of n = 608:
-    # dram__bytes_read.sum + dram__bytes_write.sum = 530.98 + 28.93 GB for 467.99 GB
-    # algorithmic; the ratio carries over to larger launches because both grow with the
-    # per-column reads of the trailing triangle.
-    tridiag_traffic_ratio = (530.98 + 28.93) / 467.99
+    # of the trailing triangle loaded with an L2 evict-first hint, the panel vectors with an
+    # evict-last one) on 1400 blocks of n = 608: dram__bytes_read.sum + dram__bytes_write.sum =
+    # 516.49 + 28.50 GB for 467.99 GB algorithmic; the ratio carries over to larger launches
+    # because both grow with the per-column reads of the trailing triangle.
+    tridiag_traffic_ratio = (516.49 + 28.50) / 467.99
     if top[0] == "tridiag":
         per_launch_bytes = args.steps * sum(tridiag_bytes(int(n)) for n in sizes if n > 64) / top[1][1]
         avg = top[1][0] / 1e3 / top[1][1]

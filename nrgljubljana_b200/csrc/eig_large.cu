@@ -183,6 +183,22 @@ NRG_DEV uint64_t l2_evict_first_policy() {
   return p;
 }
 
+// Loads and stores of the panel's vectors (V and W columns, re-read three times per column of
+// the panel) with an evict-last L2 hint, so that the streamed slabs do not push them out.
+NRG_DEV uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+NRG_DEV double ld_keep(const double* a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+NRG_DEV void st_keep(double* a, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+
 constexpr int kStages = 4;                 // slabs in flight per warp
 constexpr int kSlabRows = 64;              // rows of a slab (two per lane)
 constexpr int kSlabD = kSlabRows * 8;      // doubles per slab: 64 rows x 8 columns
@@ -435,6 +451,7 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
   const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
   double* A = B.W1;
   double* W = B.W2;
+  const uint64_t keep = l2_evict_last_policy();
   // TMA destinations: 1024-byte aligned ring of STAGES slabs per warp
   double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sm) + 1023) & ~(uintptr_t)1023);
   double* v = ring + kTriWarps * STAGES * kSlabD;      // n
@@ -467,7 +484,7 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
           double a = A[(size_t)k * ld + i];
 #pragma unroll
           for (int q = 0; q < NB; q++)
-            if (q < j) a -= A[(size_t)(p0 + q) * ld + i] * wk[q] + W[(size_t)q * n + i] * vk[q];
+            if (q < j) a -= ld_keep(A + (size_t)(p0 + q) * ld + i, keep) * wk[q] + ld_keep(W + (size_t)q * n + i, keep) * vk[q];
           v[i] = a;
           y[i] = 0.0;
         }
@@ -495,7 +512,7 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
       for (int i = k + 2 + tid; i < n; i += nt) {
         const double vi = v[i] * scale;
         v[i] = vi;
-        A[(size_t)k * ld + i] = vi;
+        st_keep(A + (size_t)k * ld + i, vi, keep);
       }
       // column k of W1 now holds v_k below the diagonal; clear its entries above, inside
       // the back-transform panel, so that the panel's V block is exactly unit lower trapezoidal
@@ -518,8 +535,8 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
 #pragma unroll
             for (int q = 0; q < NB; q++)
               if (q < j) {
-                pw[q] = fma(W[(size_t)q * n + i], vi, pw[q]);
-                pv[q] = fma(A[(size_t)(p0 + q) * ld + i], vi, pv[q]);
+                pw[q] = fma(ld_keep(W + (size_t)q * n + i, keep), vi, pw[q]);
+                pv[q] = fma(ld_keep(A + (size_t)(p0 + q) * ld + i, keep), vi, pv[q]);
               }
           }
 #pragma unroll
@@ -552,13 +569,13 @@ __global__ void __launch_bounds__(kTriThreads, MINB) tridiag_kernel(const LargeB
           double yi = y[i];
 #pragma unroll
           for (int q = 0; q < NB; q++)
-            if (q < j) yi -= A[(size_t)(p0 + q) * ld + i] * cw[q] + W[(size_t)q * n + i] * cv[q];
+            if (q < j) yi -= ld_keep(A + (size_t)(p0 + q) * ld + i, keep) * cw[q] + ld_keep(W + (size_t)q * n + i, keep) * cv[q];
           yi *= tau;
           y[i] = yi;
           pp = fma(yi, v[i], pp);
         }
         const double Kc = 0.5 * tau * block_sum_1b(pp, red, phase);
-        for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = y[i] - Kc * v[i];
+        for (int i = k + 1 + tid; i < n; i += nt) st_keep(W + (size_t)j * n + i, y[i] - Kc * v[i], keep);
       } else {
         for (int i = k + 1 + tid; i < n; i += nt) W[(size_t)j * n + i] = 0.0;
       }
