@@ -1061,8 +1061,8 @@ __global__ void __launch_bounds__(kClThreads) tridiag_cluster_kernel(const Large
 __global__ void __launch_bounds__(128) dc_leaf_kernel(const LargeBlock* __restrict__ blocks,
                                                       const DcLeaf* __restrict__ leaves) {
   __shared__ double Z[kLeaf * (kLeaf + 1)];
-  __shared__ double d[kLeaf], e[kLeaf], C[kLeaf], S[kLeaf];
-  __shared__ int ctl[4];
+  __shared__ double d[kLeaf], e[kLeaf], C[2 * kLeaf], S[2 * kLeaf];
+  __shared__ int ctl[8];
   const DcLeaf L = leaves[blockIdx.x];
   const LargeBlock B = blocks[L.blk];
   const int n = B.n, a0 = L.a0, nl = L.a1 - L.a0, ld = kLeaf + 1, tid = threadIdx.x;

@@ -18,7 +18,7 @@ __host__ __device__ inline int small_ld(int n) { return (n & 1) ? n : n + 1; }  
 
 __host__ __device__ inline size_t small_smem_bytes(int n) {
   const int ld = small_ld(n);
-  return sizeof(double) * (2 * (size_t)n * ld + 8 * (size_t)n + 32) + sizeof(int) * ((size_t)n + 8);
+  return sizeof(double) * (2 * (size_t)n * ld + 10 * (size_t)n + 32) + sizeof(int) * ((size_t)n + 8);
 }
 
 __global__ void __launch_bounds__(kThreads) eig_small_kernel(const EigBlock* __restrict__ blocks) {
@@ -31,9 +31,9 @@ __global__ void __launch_bounds__(kThreads) eig_small_kernel(const EigBlock* __r
   double* e = d + n;
   double* taus = e + n;
   double* vw = taus + n;  // 2n
-  double* C = vw + 2 * n;
-  double* S = C + n;
-  double* scr = S + n;  // n
+  double* C = vw + 2 * n;  // 2n: two buffers of QL rotations
+  double* S = C + 2 * n;   // 2n
+  double* scr = S + 2 * n;  // n
   double* red = scr + n;  // 32
   int* ctl = reinterpret_cast<int*>(red + 32);  // 8
   int* perm = ctl + 8;                          // n

@@ -119,79 +119,106 @@ NRG_DEV double chain_hypot(double f, double g) {
 // Implicit-shift QL iteration (Wilkinson-type shift) on the symmetric tridiagonal matrix
 // (d, e), e[i] coupling i and i+1, e[n-1] unused. Rotations are accumulated into the
 // columns of Z (nz rows, row stride ld): on exit column r of Z is the eigenvector of d[r].
-// Eigenvalues are not sorted. C, S: n doubles of scratch; ctl: 4 ints of scratch.
+// Eigenvalues are not sorted. C, S: 2n doubles each of scratch (two buffers of rotations);
+// ctl: 8 ints of scratch. Needs at least 64 threads.
+// The sweeps are pipelined: thread 0 runs the convergence test and the rotation chain of
+// sweep t+1 (a serial recurrence through d and e) while the threads of the other warps apply
+// the rotations of sweep t to the rows of Z. Each row gets every sweep's rotations in the same
+// order as without the overlap, so the results are the same.
 // Returns 0, or l+1 if eigenvalue l failed to converge within 30 sweeps.
 NRG_DEV int smem_ql(double* d, double* e, int n, double* Z, int ld, int nz, double* C, double* S, int* ctl) {
   const int tid = threadIdx.x, nt = blockDim.x;
-  int status = 0;
-  if (tid == 0) e[n - 1] = 0.0;
-  __syncthreads();
-  for (int l = 0; l < n; l++) {
-    int iter = 0;
-    for (;;) {
+  // thread 0's state: current eigenvalue l, sweeps spent on it, status
+  int l = 0, iter = 0, status = 0;
+  // Finds the next sweep and computes its rotations into buffer `buf` (thread 0 only);
+  // returns false when every eigenvalue has converged or one failed to.
+  auto next_sweep = [&](int buf) -> bool {
+    double* Cb = C + (size_t)buf * n;
+    double* Sb = S + (size_t)buf * n;
+    while (l < n) {
       int m = l;
       while (m < n - 1) {
         const double dd = fabs(d[m]) + fabs(d[m + 1]);
         if (fabs(e[m]) <= kEps * dd) break;
         m++;
       }
-      __syncthreads();  // everyone has read d/e before thread 0 updates them
-      if (m == l) break;
-      if (iter++ == 30) { status = l + 1; break; }
-      if (tid == 0) {
-        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-        double r = hypot(g, 1.0);
-        g = d[m] - d[l] + e[l] / (g + copysign(r, g));
-        double s = 1.0, c = 1.0, p = 0.0;
-        int lo = l;
-        bool under = false;
-        for (int i = m - 1; i >= l; i--) {
-          const double f = s * e[i], b = c * e[i];
-          r = chain_hypot(f, g);
-          e[i + 1] = r;
-          if (r == 0.0) {
-            d[i + 1] -= p;
-            e[m] = 0.0;
-            lo = i + 1;
-            under = true;
-            break;
-          }
-          const double ir = 1.0 / r;
-          s = f * ir;
-          c = g * ir;
-          g = d[i + 1] - p;
-          r = (d[i] - g) * s + 2.0 * c * b;
-          p = s * r;
-          d[i + 1] = g + p;
-          g = c * r - b;
-          C[i] = c;
-          S[i] = s;
-        }
-        if (!under) {
-          d[l] -= p;
-          e[l] = g;
-          e[m] = 0.0;
-        }
-        ctl[0] = lo;
-        ctl[1] = m - 1;
+      if (m == l) {
+        l++;
+        iter = 0;
+        continue;
       }
-      __syncthreads();
-      const int lo = ctl[0], hi = ctl[1];
-      for (int row = tid; row < nz; row += nt) {
+      if (iter++ == 30) {
+        status = l + 1;
+        return false;
+      }
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int lo = l;
+      bool under = false;
+      for (int i = m - 1; i >= l; i--) {
+        const double f = s * e[i], b = c * e[i];
+        r = chain_hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          lo = i + 1;
+          under = true;
+          break;
+        }
+        const double ir = 1.0 / r;
+        s = f * ir;
+        c = g * ir;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        Cb[i] = c;
+        Sb[i] = s;
+      }
+      if (!under) {
+        d[l] -= p;
+        e[l] = g;
+        e[m] = 0.0;
+      }
+      ctl[2 * buf] = lo;
+      ctl[2 * buf + 1] = m - 1;
+      return true;
+    }
+    return false;
+  };
+  if (tid == 0) {
+    e[n - 1] = 0.0;
+    ctl[4] = next_sweep(0) ? 1 : 0;
+  }
+  __syncthreads();
+  for (int buf = 0;; buf ^= 1) {
+    const int has = ctl[4], lo = ctl[2 * buf], hi = ctl[2 * buf + 1];
+    __syncthreads();  // every thread has read ctl before thread 0 rewrites it
+    if (!has) break;
+    if (tid == 0) {
+      ctl[4] = next_sweep(buf ^ 1) ? 1 : 0;
+    } else if (tid >= 32) {
+      const double* Cb = C + (size_t)buf * n;
+      const double* Sb = S + (size_t)buf * n;
+      for (int row = tid - 32; row < nz; row += nt - 32) {
         double* z = Z + row * ld;
         for (int i = hi; i >= lo; i--) {
           const double f = z[i + 1];
           const double zi = z[i];
-          z[i + 1] = S[i] * zi + C[i] * f;
-          z[i] = C[i] * zi - S[i] * f;
+          z[i + 1] = Sb[i] * zi + Cb[i] * f;
+          z[i] = Cb[i] * zi - Sb[i] * f;
         }
       }
-      __syncthreads();
     }
-    if (status) break;
+    __syncthreads();
   }
+  if (tid == 0) ctl[5] = status;
   __syncthreads();
-  return status;
+  return ctl[5];
 }
 
 // Stable ascending order of d[0..n) into perm (single thread, small n).
