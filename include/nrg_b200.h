@@ -257,6 +257,19 @@ typedef struct nrg_bins {
 NRG_API int nrg_spec_accumulate(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* params,
                         const nrg_bins* bins, double* pos, double* neg, void* stream);
 
+/* Replaces the per-pair calc() of Algo_FDMmats (c++/algo_FDM.hpp:153-217) with its
+ * ChainMatsubara accumulation (c++/spectrum.hpp:34-42, c++/matsubara.hpp:31-49): the FDM
+ * Green's function on the Matsubara axis. The pairs are given as for NRG_SPEC_FDMGT and
+ * NRG_SPEC_FDMLS together (rho_i = rhoFDM(Ii) with rdi, rho_j = rhoFDM(Ij) with rdj); every
+ * term of both, weight w at energy E = Ej - Ei, adds factor * w / (i w_n - E) to
+ * re[n] + i im[n] for n < mats (ACCUMULATED), w_n = (2n+1) pi T for sign = -1 (fermionic)
+ * and 2n pi T for sign = +1 (bosonic). For a bosonic operator the D x D term of a pair at
+ * n = 0 with |E| <= 1e-8 (WEIGHT_TOL) is -factor * w_gt / T, w_gt its exp(-Ei/T) part
+ * (c++/algo_FDM.hpp:178-188). params->algo is not read; params->T, sign and wnf are.
+ * 1 <= mats <= 6144. */
+NRG_API int nrg_spec_accumulate_mats(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs,
+                                     const nrg_spec_params* params, int mats, double* re, double* im, void* stream);
+
 /* ------------------------------------------------------------------ timing
  * Per-phase device timing in the spirit of the reference's MemTime::time_it sections
  * (c++/time_mem.hpp:97-115): nrg_profile(ctx, 1) resets the counters and brackets every

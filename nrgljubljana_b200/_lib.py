@@ -24,7 +24,8 @@ NRG_SPEC_FDMLS = 2
 # Every symbol include/nrg_b200.h declares.
 EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_trim", "nrg_diag_batch",
            "nrg_diag_batch_host",
-           "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate", "nrg_profile",
+           "nrg_gemm3_batch", "nrg_gemm3_batch_host", "nrg_transform_noalloc", "nrg_spec_accumulate",
+           "nrg_spec_accumulate_mats", "nrg_profile",
            "nrg_profile_read", "nrg_bins_grid", "nrg_hamiltonian_batch",
            "nrg_broaden", "nrg_get_tuning", "nrg_set_tuning")
 NRG_NOALLOC_SCRATCH_DOUBLES = 1 << 20
@@ -114,6 +115,7 @@ def load() -> C.CDLL:
     L.nrg_gemm3_batch.argtypes = [P, C.c_int, C.POINTER(Gemm3), P]
     L.nrg_gemm3_batch_host.argtypes = L.nrg_gemm3_batch.argtypes
     L.nrg_spec_accumulate.argtypes = [P, C.c_int, C.POINTER(SpecPair), C.POINTER(SpecParams), C.POINTER(Bins), P, P, P]
+    L.nrg_spec_accumulate_mats.argtypes = [P, C.c_int, C.POINTER(SpecPair), C.POINTER(SpecParams), C.c_int, P, P, P]
     L.nrg_bins_grid.argtypes = [C.POINTER(Bins), C.POINTER(C.c_double)]
     L.nrg_transform_noalloc.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int64, P, C.c_int64, C.c_int, C.c_int,
                                         C.c_int, C.c_int, C.c_double, P]

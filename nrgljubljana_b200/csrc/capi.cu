@@ -966,4 +966,92 @@ int nrg_spec_accumulate(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const
   return NRG_OK;
 }
 
+int nrg_spec_accumulate_mats(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* prm,
+                             int mats, double* re, double* im, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (npair < 0 || (npair > 0 && (!pairs || !prm || !re || !im))) return fail(NRG_ERR_ARG, "bad arguments");
+  if (npair == 0) return NRG_OK;
+  if (mats < 1 || 2 * sizeof(double) * (size_t)mats > nrg::kSpecSmemMax) return fail(NRG_ERR_ARG, "mats = %d", mats);
+  if (!(prm->T > 0.0) || (prm->sign != 1 && prm->sign != -1)) return fail(NRG_ERR_ARG, "bad T or sign");
+  auto s = static_cast<cudaStream_t>(stream);
+  nrg::CallOrder call_order(c, s);
+  // op2_rho = prod_fit(op2, rhoFDM(Ii)) (nj x rdi) and rho_op2 = prod_fit(rhoFDM(Ij), op2) (rdj x ni)
+  std::vector<size_t> xo(npair, 0), yo(npair, 0);
+  size_t need = 0;
+  for (int p = 0; p < npair; p++) {
+    const nrg_spec_pair& q = pairs[p];
+    if (q.ni < 0 || q.nj < 0 || q.ki < 0 || q.kj < 0 || q.ki > q.ni || q.kj > q.nj)
+      return fail(NRG_ERR_ARG, "pair %d: bad ranges", p);
+    if (q.ki > q.rdi || q.kj > q.rdj) return fail(NRG_ERR_ARG, "pair %d: rdi < ki or rdj < kj", p);
+    xo[p] = need; need += (size_t)q.nj * q.rdi;
+    yo[p] = need; need += (size_t)q.rdj * q.ni;
+  }
+  rc = ensure_ws(c, sizeof(double) * std::max<size_t>(need, 1));
+  if (rc) return rc;
+  double* W = static_cast<double*>(c->ws);
+  GemmPlan gp;
+  std::vector<nrg::SpecRegion> regs;
+  auto region = [&](const nrg_spec_pair& q, int kind, int i0, int i1, int j0, int j1, const double* X, int64_t ldx,
+                    double coef, int special) {
+    if (i1 <= i0 || j1 <= j0) return;
+    nrg::SpecRegion r{};
+    r.Ei = q.Ei; r.Ej = q.Ej; r.op1 = q.op1; r.op2 = q.op2; r.X = X; r.Y = nullptr;
+    r.ld1 = q.ld1; r.ld2 = q.ld2; r.ldx = ldx; r.ldy = 0;
+    r.i0 = i0; r.i1 = i1; r.j0 = j0; r.j1 = j1;
+    r.kind = kind; r.sign = prm->sign; r.mspecial = special; r.coef = coef; r.factor = q.factor; r.T = prm->T;
+    regs.push_back(r);
+  };
+  const double ms = (double)(-prm->sign);
+  for (int p = 0; p < npair; p++) {
+    const nrg_spec_pair& q = pairs[p];
+    double* X = W + xo[p];
+    double* Y = W + yo[p];
+    if (q.rdi > 0 && q.nj > 0) {
+      gp.add_out(X, q.rdi, q.nj, q.rdi, 0.0);
+      gp.add_seg(q.op2, q.ld2, 0, q.rho_i, q.ldri, 0, std::min(q.rdi, q.ni), 1.0);
+    }
+    if (q.rdj > 0 && q.ni > 0) {
+      gp.add_out(Y, q.ni, q.rdj, q.ni, 0.0);
+      gp.add_seg(q.rho_j, q.ldrj, 0, q.op2, q.ld2, 0, std::min(q.rdj, q.nj), 1.0);
+    }
+    // term1 (D x D): weightA (exp(-Ei/T)) + weightB (-sign exp(-Ej/T)); term2 (i in D, j in K):
+    // weightA + (-sign) op1 rho_op2; term3 (i in K, j in D): op1 op2_rho + weightB
+    region(q, nrg::kSpecExpI, q.ki, q.ni, q.kj, q.nj, nullptr, 0, prm->wnf, nrg::kMatsGtDD);
+    region(q, nrg::kSpecExpJ, q.ki, q.ni, q.kj, q.nj, nullptr, 0, ms * prm->wnf, nrg::kMatsLsDD);
+    region(q, nrg::kSpecExpI, q.ki, q.ni, 0, q.kj, nullptr, 0, prm->wnf, nrg::kMatsPlain);
+    region(q, nrg::kSpecGemmX, q.ki, q.ni, 0, q.kj, Y, q.ni, ms, nrg::kMatsPlain);
+    region(q, nrg::kSpecGemmX, 0, q.ki, q.kj, q.nj, X, q.rdi, 1.0, nrg::kMatsPlain);
+    region(q, nrg::kSpecExpJ, 0, q.ki, q.kj, q.nj, nullptr, 0, ms * prm->wnf, nrg::kMatsPlain);
+  }
+  rc = run_gemm_plan(c, gp, s, nrg::kPhSpecGemm);
+  if (rc) return rc;
+  if (regs.empty()) return NRG_OK;
+  std::vector<nrg::SpecTask> tasks;
+  const int64_t chunk = 4096;
+  for (size_t r = 0; r < regs.size(); r++) {
+    const int64_t nt = (int64_t)(regs[r].i1 - regs[r].i0) * (regs[r].j1 - regs[r].j0);
+    for (int64_t t0 = 0; t0 < nt; t0 += chunk) {
+      nrg::SpecTask k{};
+      k.t0 = t0;
+      k.t1 = std::min(nt, t0 + chunk);
+      k.region = (int)r;
+      tasks.push_back(k);
+    }
+  }
+  std::vector<char> img;
+  const size_t ro = push(img, regs), to = push(img, tasks);
+  rc = stage_desc(c, img, s);
+  if (rc) return rc;
+  nrg::MatsParams mp{};
+  mp.mats = mats;
+  mp.bosonic = prm->sign == 1 ? 1 : 0;
+  mp.T = prm->T;
+  const char* base = static_cast<const char*>(c->desc);
+  nrg::PhaseScope ps(c, nrg::kPhSpecBin, s);
+  CK(nrg::spec_mats_launch(reinterpret_cast<const nrg::SpecTask*>(base + to), (int)tasks.size(),
+                           reinterpret_cast<const nrg::SpecRegion*>(base + ro), mp, re, im, s));
+  return NRG_OK;
+}
+
 }  // extern "C"

@@ -1,4 +1,4 @@
-// spec.cu -- fused spectral-weight + log-grid binning kernel.
+// spec.cu -- fused spectral-weight + log-grid binning kernel, and the Matsubara sums.
 //
 // Replaces the per-term loops of Algo_DMNRG::calc (c++/algo_DMNRG.hpp:29-52) and
 // Algo_FDMgt/Algo_FDMls::calc (c++/algo_FDM.hpp:84-114, 30-60) together with
@@ -46,6 +46,31 @@ NRG_DEV void bin_add(const Hist& h, const BinParams& bp, double energy, double w
   }
 }
 
+// The weight of term (i, j) of region r (before `factor`); false for a DM-NRG term outside the
+// energy window.
+NRG_DEV bool term_weight(const SpecRegion& r, int i, int j, double energy, double& w) {
+  const double o1 = r.op1[(int64_t)j * r.ld1 + i];
+  switch (r.kind) {
+    case kSpecDMNRG: {
+      if (fabs(energy) < r.Emin || fabs(energy) > r.Emax) return false;
+      const double o2 = r.op2[(int64_t)j * r.ld2 + i];
+      const double wA = r.X[(int64_t)j * r.ldx + i] * o1;
+      const double wB = r.Y[(int64_t)j * r.ldy + i] * o2;
+      w = wA + (double)(-r.sign) * wB;
+      return true;
+    }
+    case kSpecExpI:
+      w = o1 * r.op2[(int64_t)j * r.ld2 + i] * r.coef * exp(-r.Ei[i] / r.T);
+      return true;
+    case kSpecExpJ:
+      w = o1 * r.op2[(int64_t)j * r.ld2 + i] * r.coef * exp(-r.Ej[j] / r.T);
+      return true;
+    default:  // kSpecGemmX
+      w = o1 * r.X[(int64_t)j * r.ldx + i] * r.coef;
+      return true;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) spec_bin_kernel(const SpecTask* __restrict__ tasks,
                                                             const SpecRegion* __restrict__ regs, BinParams bp,
                                                             double* gpos, double* gneg, int use_smem) {
@@ -64,27 +89,8 @@ __global__ void __launch_bounds__(kThreads) spec_bin_kernel(const SpecTask* __re
     const int j = r.j0 + (int)(t / wi);
     const int i = r.i0 + (int)(t % wi);
     const double energy = r.Ej[j] - r.Ei[i];
-    const double o1 = r.op1[(int64_t)j * r.ld1 + i];
     double w;
-    switch (r.kind) {
-      case kSpecDMNRG: {
-        if (fabs(energy) < r.Emin || fabs(energy) > r.Emax) continue;
-        const double o2 = r.op2[(int64_t)j * r.ld2 + i];
-        const double wA = r.X[(int64_t)j * r.ldx + i] * o1;
-        const double wB = r.Y[(int64_t)j * r.ldy + i] * o2;
-        w = wA + (double)(-r.sign) * wB;
-        break;
-      }
-      case kSpecExpI:
-        w = o1 * r.op2[(int64_t)j * r.ld2 + i] * r.coef * exp(-r.Ei[i] / r.T);
-        break;
-      case kSpecExpJ:
-        w = o1 * r.op2[(int64_t)j * r.ld2 + i] * r.coef * exp(-r.Ej[j] / r.T);
-        break;
-      default:  // kSpecGemmX
-        w = o1 * r.X[(int64_t)j * r.ldx + i] * r.coef;
-        break;
-    }
+    if (!term_weight(r, i, j, energy, w)) continue;
     bin_add(h, bp, energy, r.factor * w);
   }
   if (use_smem) {
@@ -96,7 +102,59 @@ __global__ void __launch_bounds__(kThreads) spec_bin_kernel(const SpecTask* __re
   }
 }
 
+// Algo_FDMmats (c++/algo_FDM.hpp:167-217) into ChainMatsubara (c++/spectrum.hpp:34-42): every
+// term adds factor w / (i w_n - E) = factor w (-E - i w_n) / (E^2 + w_n^2) to point n, for
+// n < mats, into a per-CTA copy of the sums in shared memory, flushed with FP64 atomics.
+__global__ void __launch_bounds__(kThreads) spec_mats_kernel(const SpecTask* __restrict__ tasks,
+                                                             const SpecRegion* __restrict__ regs, MatsParams mp,
+                                                             double* gre, double* gim) {
+  extern __shared__ __align__(16) double sh[];
+  const SpecTask tk = tasks[blockIdx.x];
+  const SpecRegion r = regs[tk.region];
+  double* re = sh;
+  double* im = sh + mp.mats;
+  for (int n = threadIdx.x; n < 2 * mp.mats; n += blockDim.x) sh[n] = 0.0;
+  __syncthreads();
+  const double pt = 3.14159265358979323846 * mp.T;
+  const int wi = r.i1 - r.i0;
+  for (int64_t t = tk.t0 + threadIdx.x; t < tk.t1; t += blockDim.x) {
+    const int j = r.j0 + (int)(t / wi);
+    const int i = r.i0 + (int)(t % wi);
+    const double energy = r.Ej[j] - r.Ei[i];
+    double w;
+    if (!term_weight(r, i, j, energy, w)) continue;
+    w *= r.factor;
+    for (int n = 0; n < mp.mats; n++) {
+      if (n == 0 && mp.bosonic && r.mspecial != kMatsPlain && fabs(energy) <= 1e-8) {
+        if (r.mspecial == kMatsGtDD) atomicAdd(re, -w / mp.T);
+        continue;
+      }
+      const double wn = pt * (double)(mp.bosonic ? 2 * n : 2 * n + 1);
+      const double d = energy * energy + wn * wn;
+      atomicAdd(re + n, -w * energy / d);
+      atomicAdd(im + n, -w * wn / d);
+    }
+  }
+  __syncthreads();
+  for (int n = threadIdx.x; n < mp.mats; n += blockDim.x) {
+    if (re[n] != 0.0) atomicAdd(gre + n, re[n]);
+    if (im[n] != 0.0) atomicAdd(gim + n, im[n]);
+  }
+}
+
 }  // namespace
+
+cudaError_t spec_mats_launch(const SpecTask* d_tasks, int ntask, const SpecRegion* d_regs, const MatsParams& mp,
+                             double* re, double* im, cudaStream_t stream) {
+  if (ntask <= 0 || mp.mats <= 0) return cudaSuccess;
+  const size_t smem = 2 * sizeof(double) * (size_t)mp.mats;
+  if (smem > kSpecSmemMax) return cudaErrorInvalidValue;
+  cudaError_t err =
+      cudaFuncSetAttribute(spec_mats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpecSmemMax);
+  if (err != cudaSuccess) return err;
+  spec_mats_kernel<<<ntask, kThreads, smem, stream>>>(d_tasks, d_regs, mp, re, im);
+  return cudaGetLastError();
+}
 
 cudaError_t spec_bin_launch(const SpecTask* d_tasks, int ntask, const SpecRegion* d_regs, const BinParams& bp,
                             double* pos, double* neg, cudaStream_t stream) {

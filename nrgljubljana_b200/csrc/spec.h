@@ -1,4 +1,4 @@
-// spec.h -- internal descriptors of the spectral-weight binning kernel.
+// spec.h -- internal descriptors of the spectral-weight binning and Matsubara kernels.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -24,7 +24,19 @@ struct SpecRegion {
   int64_t ld1, ld2, ldx, ldy;
   int i0, i1, j0, j1;
   int kind, sign;
+  int mspecial, pad_;  // Matsubara sums: kMatsPlain, kMatsGtDD or kMatsLsDD
   double coef, factor, T, Emin, Emax;
+};
+
+// How a term enters the Matsubara sum at n = 0 for a bosonic operator when |E| <= 1e-8
+// (WEIGHT_TOL, c++/numerics.hpp:318): the D x D term of Algo_FDMmats (c++/algo_FDM.hpp:
+// 178-188) is -weightA / T there, weightA being its exp(-Ei/T) part and weightB dropped.
+enum MatsSpecial : int { kMatsPlain = 0, kMatsGtDD = 1, kMatsLsDD = 2 };
+
+struct MatsParams {
+  int mats;     // points n = 0 .. mats-1
+  int bosonic;  // w_n = 2 n pi T (bosonic) or (2 n + 1) pi T (fermionic)
+  double T;
 };
 
 struct SpecTask {  // a contiguous range [t0, t1) of the terms of one region (t = (j-j0)*(i1-i0) + (i-i0))
@@ -43,5 +55,8 @@ constexpr size_t kSpecSmemMax = 96 * 1024;  // private histograms up to 6144 bin
 
 cudaError_t spec_bin_launch(const SpecTask* d_tasks, int ntask, const SpecRegion* d_regs, const BinParams& bp,
                             double* pos, double* neg, cudaStream_t stream);
+// Matsubara sums: re[n] + i im[n] += factor w / (i w_n - E) for every term (accumulated).
+cudaError_t spec_mats_launch(const SpecTask* d_tasks, int ntask, const SpecRegion* d_regs, const MatsParams& mp,
+                             double* re, double* im, cudaStream_t stream);
 
 }  // namespace nrg

@@ -33,7 +33,7 @@ from . import ddsum, qs
 from ._lib import (GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG, NRG_SPEC_DMNRG, NRG_SPEC_FDMGT,
                    NRG_SPEC_FDMLS, SPECPAIR_DTYPE)
 from .api import (BinGrid, Context, broaden, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch,
-                  spec_accumulate_array)
+                  spec_accumulate_array, spec_accumulate_mats_array)
 from .inputs import DataFile, SCALE, parse_param, read_data
 
 Invar = Tuple[int, int]
@@ -74,6 +74,8 @@ class RunParams:
     fdm: bool = False
     fdmgt: bool = False
     fdmls: bool = False
+    fdmmats: bool = False  # FDM Green's functions on the Matsubara axis (c++/params.hpp:253-254)
+    mats: int = 100
     fdmexpv: bool = False
     fdmexpvn: int = 0
     lastalloverride: bool = False
@@ -153,8 +155,8 @@ class RunParams:
 
     @property
     def fdm_flags(self) -> bool:
-        """Params::fdm_flags (c++/params.hpp:535) without the Matsubara variant."""
-        return self.fdm or self.fdmgt or self.fdmls or self.fdmexpv
+        """Params::fdm_flags (c++/params.hpp:535)."""
+        return self.fdm or self.fdmgt or self.fdmls or self.fdmmats or self.fdmexpv
 
     @property
     def cfs_flags(self) -> bool:
@@ -397,7 +399,7 @@ class QSRun:
         # (file prefix, kind, op1, op2) of the spectra (c++/oprecalc.hpp:160-195)
         self.algos = params.algorithms
         self.specs: List[Tuple[str, str, str, str]] = []
-        if self.algos:
+        if self.algos or params.fdmmats:
             for prefix, kind, text in (("corr", "s", params.specs), ("spec", "d", params.specd),
                                        ("spin", "t", params.spect)):
                 for tok in text.split():
@@ -1172,6 +1174,9 @@ class QSRun:
         zeros = lambda: torch.zeros(nb, dtype=torch.float64, device=self.dev)  # noqa: E731
         dm_acc = {j: (np.zeros(nb), np.zeros(nb)) for j in range(len(self.specs))} if rhos is not None else {}
         fdm_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in fdm_parts}
+        # Algo_FDMmats: one GFMatsubara per spectrum, mats complex points (c++/spectrum.hpp:212-227)
+        zm = lambda: torch.zeros(p.mats, dtype=torch.float64, device=self.dev)  # noqa: E731
+        mats_acc = {j: (zm(), zm()) for j in range(len(self.specs))} if p.fdmmats else {}
         cfs_parts_of = {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}
         cfs_parts = sorted({w for a in self.algos if a in cfs_parts_of for w in cfs_parts_of[a]})
         cfs_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in cfs_parts}
@@ -1225,7 +1230,7 @@ class QSRun:
                     for full, cs in zip(dm_acc[j], (pos.cpu().numpy(), neg.cpu().numpy())):
                         sel = inside & (cs != 0.0)  # mergeNN2half (c++/spectrum.hpp:114-128)
                         full[sel] += f * cs[sel] * win[sel]
-            if fdm_parts and self.specs:
+            if (fdm_parts or p.fdmmats) and self.specs:
                 GS = fdm["GS"]
                 eoff, flat, o = {}, [], 0
                 for I, s in dg.items():  # abs_G energies of all states (c++/eigen.hpp:47)
@@ -1239,7 +1244,7 @@ class QSRun:
                     sign, ff, names = kinds[kind]
                     ops = cur[kind]
                     o1, o2 = names.index(n1), names.index(n2)
-                    gt, ls = [], []
+                    gt, ls, mt = [], [], []
                     for Ii, si in dg.items():
                         for Ij, sj in dg.items():
                             key = Ii if kind == "s" else (Ij, Ii)
@@ -1254,12 +1259,17 @@ class QSRun:
                             base = (eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2), ld)
                             gt.append(base + (ri, max(Ki, 1), 0, 1, ni, Ki, nj, Kj, Ki, 0, ff(Ii, Ij)))
                             ls.append(base + (0, 1, rj, max(Kj, 1), ni, Ki, nj, Kj, 0, Kj, ff(Ii, Ij)))
+                            mt.append(base + (ri, max(Ki, 1), rj, max(Kj, 1), ni, Ki, nj, Kj, Ki, Kj, ff(Ii, Ij)))
                     for w, prs, algo in (("gt", gt, NRG_SPEC_FDMGT), ("ls", ls, NRG_SPEC_FDMLS)):
                         if w in fdm_parts and prs:
                             pos, neg = fdm_acc[(j, w)]
                             spec_accumulate_array(algo, np.array(prs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
                                                   sign=sign, T=p.T, wnf=fdm["wnfactor"][k], ctx=self.ctx,
                                                   stream=self.stream)
+                    if p.fdmmats and mt:  # Algo_FDMmats::calc over the same pairs (c++/algo_FDM.hpp:167-217)
+                        re, im = mats_acc[j]
+                        spec_accumulate_mats_array(np.array(mt, dtype=SPECPAIR_DTYPE), p.mats, re, im, sign, p.T,
+                                                   fdm["wnfactor"][k], ctx=self.ctx, stream=self.stream)
             if "FT" in self.algos and merge and self.specs:
                 self._ft_step(st, cur, kinds, grid, ebins, Efac, ft_acc)
             if cfs_parts and self.specs:
@@ -1268,6 +1278,13 @@ class QSRun:
                 expv = self._fdm_expv(k, st, cur["s"], fdm)
         out: Dict[str, np.ndarray] = {}
         raw: Dict[str, np.ndarray] = {}
+        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+            if p.fdmmats:  # GFMatsubara::save: w_n, Re, Im (outputxy with imagpart, c++/io.hpp:33-38)
+                sign = kinds[kind][0]
+                wn = p.T * math.pi * (2 * np.arange(p.mats) + (0 if sign == 1 else 1))
+                g_re, g_im = (x.cpu().numpy() for x in mats_acc[j])
+                g_im = np.where(np.abs(g_im) > np.abs(g_re) * 1e-10, g_im, 0.0)
+                out[f"{prefix}_FDMmats_dens_{n1}-{n2}"] = np.stack([wn, g_re, g_im], axis=1)
         omega0 = p.omega0 if p.omega0 >= 0.0 else p.omega0_ratio * p.T
         bmin = p.broaden_min if p.broaden_min > 0.0 else p.broaden_min_ratio * last_scale
         mesh = []
@@ -1603,8 +1620,8 @@ def write_outputs(out: str, p: RunParams, res: Result) -> None:
             _write_table(os.path.join(out, name), tab[0], [tab[1]], prec, width)
     for name, rows in res.spectra.items():  # <prefix>_<algo>_dens_<op1>-<op2>.dat
         with open(os.path.join(out, f"{name}.dat"), "w") as f:
-            for e, v in rows:
-                f.write(f"{e:.{p.prec_xy}g} {v:.{p.prec_xy}g}" + (" 0\n" if p.reim else "\n"))
+            for row in rows:  # (E, A(E)), or (w_n, Re G, Im G) on the Matsubara axis
+                f.write(" ".join(f"{x:.{p.prec_xy}g}" for x in row) + (" 0\n" if p.reim and len(row) == 2 else "\n"))
     for name, rows in res.bins.items():
         write_bins(os.path.join(out, f"{name}.bin"), rows)
     if p.dumpsubspaces:

@@ -25,6 +25,8 @@ host with LAPACK dsyev and BLAS dgemm through ``oracle.py``. It follows
                               mergeNN2half, windowfunction, continuous c++/spectrum.hpp:81-196;
                               Bins c++/bins.hpp:61-185; BR_NEW c++/spectral.hpp:42-70
   FDM                         c++/dmnrg.hpp:146-217; Algo_FDMgt/ls c++/algo_FDM.hpp:30-151;
+                              Algo_FDMmats c++/algo_FDM.hpp:153-217, GFMatsubara c++/spectrum.hpp:212-227,
+                              Matsubara c++/matsubara.hpp:19-58;
                               calc_ZnD, fdm_thermodynamics c++/measurements.hpp:60-163
   CFS, FT                     Algo_CFSgt/ls c++/algo_CFS.hpp:28-105; Algo_FT c++/algo_FT.hpp:28-48;
                               calc_Z c++/measurements.hpp:189-191
@@ -131,7 +133,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
     flag = lambda k: kv.get(k, "false").lower() == "true"  # noqa: E731
     # Params::cfs_flags, fdm_flags, keep_all_states_in_last_step (c++/params.hpp:534-539)
     cfs_flags = any(flag(k) for k in ("cfs", "cfsgt", "cfsls"))
-    fdm_flags = any(flag(k) for k in ("fdm", "fdmgt", "fdmls", "fdmexpv"))
+    fdm_flags = any(flag(k) for k in ("fdm", "fdmgt", "fdmls", "fdmmats", "fdmexpv"))
     lastall = flag("lastall") or ((cfs_flags or fdm_flags) and not flag("lastalloverride"))
     rescaled = kv.get("data_has_rescaled_energies", "true").lower() == "true"
     d = read_data(data_text)
@@ -158,7 +160,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         """Singlets, then global operators, each by name (c++/output.hpp:121-127)."""
         return sorted(set(names) - gops) + sorted(set(names) & gops)
     # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
-    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"),
+    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"), ("FDMmats", "fdmmats"),
                             ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls"), ("FT", "finite")) if flag(k)]
     dm = spectra is not None and bool(algos)
     fdm_needed = fdm_flags and (spectra is not None or fdm_out is not None)
@@ -554,6 +556,41 @@ def ft_terms(Ei, Ej, o1, o2, sign, T, Z):
     return E, (o1 * o2 * stat).ravel()
 
 
+def mats_pair(EGi, Ki, EGj, Kj, o1, o2, rho_i, rho_j, factor, sign, T, wnf, w):
+    """Algo_FDMmats::calc (c++/algo_FDM.hpp:167-217) of one subspace pair: the Matsubara
+    values factor * sum (weight / (i w_n - E)), E = Ej - Ei, over the D x D (term1), D x K
+    (term2) and K x D (term3) state pairs, i the states of Ii (columns of op1, op2), j those
+    of Ij (rows); K = the first Ki (Kj) states, D = the rest. For bosonic operators the D x D
+    term at n = 0 with |E| <= WEIGHT_TOL (1e-8, c++/numerics.hpp:318) is -weightA / T."""
+    ni, nj = len(EGi), len(EGj)
+    G = np.zeros(len(w), dtype=complex)
+    if ni == 0 or nj == 0:
+        return G
+    E = EGj[:, None] - EGi[None, :]
+    P = o1 * o2
+    wA = P * wnf * np.exp(-EGi / T)[None, :]           # a[ij] b[ji] exp(-beta e[i])
+    wB = P * (-sign) * wnf * np.exp(-EGj / T)[:, None]  # a[ij] b[ji] sign exp(-beta e[j])
+
+    def add(wt, e, special=None):
+        with np.errstate(invalid="ignore", divide="ignore"):  # the special n = 0 entries are replaced below
+            t = wt[:, :, None] / (1j * w[None, None, :] - e[:, :, None])
+        if special is not None:
+            t[:, :, 0] = np.where(np.abs(e) <= 1e-8, special, t[:, :, 0])
+        return t.sum(axis=(0, 1))
+    if Ki < ni and Kj < nj:  # term1
+        a, b, e = wA[Kj:, Ki:], wB[Kj:, Ki:], E[Kj:, Ki:]
+        G += add(a + b, e, -a / T if sign == 1 else None)
+    if Ki < ni and Kj > 0:  # term2: rho_op2 = prod_fit(rhoFDM(Ij), op2)
+        r = rho_j.shape[0]
+        rho_op2 = rho_j @ o2[:r, :]
+        G += add(wA[:Kj, Ki:] + (-sign) * o1[:Kj, Ki:] * rho_op2[:Kj, Ki:], E[:Kj, Ki:])
+    if Ki > 0 and Kj < nj:  # term3: op2_rho = prod_fit(op2, rhoFDM(Ii))
+        r = rho_i.shape[0]
+        op2_rho = o2[:, :r] @ rho_i
+        G += add(o1[Kj:, :Ki] * op2_rho[Kj:, :Ki] + wB[Kj:, :Ki], E[Kj:, :Ki])
+    return factor * G
+
+
 def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None):
     """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
     calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
@@ -583,6 +620,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
     bmin = float(kv.get("broaden_min", -99.0))
     bratio = float(kv.get("broaden_ratio", 1.05))
     fdmexpvn = int(kv.get("fdmexpvn", 0))
+    nmats = int(kv.get("mats", 100))
     last_scale = SCALE(Nmax, Lam, disc, z, brs)
     if bmin <= 0.0:
         bmin = float(kv.get("broaden_min_ratio", 3.0)) * last_scale
@@ -688,7 +726,10 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
         E /= bratio
     for prefix, kind, name1, name2 in specs:
         sign, ff = kinds[kind]
-        full = {a: O.ChainBinning(lmin, lmax, bins, discard_imm) for a in algos}
+        full = {a: O.ChainBinning(lmin, lmax, bins, discard_imm) for a in algos if a != "FDMmats"}
+        # GFMatsubara of FDMmats (c++/spectrum.hpp:212-227): mats points w_n = ww(n, gt, T)
+        wmats = T * math.pi * (2 * np.arange(nmats) + (0 if sign == 1 else 1))
+        gmats = np.zeros(nmats, dtype=complex)
         for k, (N, scale, diagN, _, opsets, Tshift) in enumerate(steps):
             op1, op2 = opsets[kind][name1], opsets[kind][name2]
             last = k == nst - 1
@@ -752,7 +793,15 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                     for w in {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}[a]:
                         for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
                             getattr(full[a], arr)[:] += getattr(cbs[w], arr)
-            fdm_algos = [a for a in algos if a.startswith("FDM")]
+            if "FDMmats" in algos:
+                for Ii, ei, Ij, ej in pairs:
+                    Ki = 0 if last else ei.nrpost
+                    Kj = 0 if last else ej.nrpost
+                    EGi = ((ei.values - ei.shift) * scale + Tshift) - GS
+                    EGj = ((ej.values - ej.shift) * scale + Tshift) - GS
+                    gmats += mats_pair(EGi, Ki, EGj, Kj, op1[(Ij, Ii)], op2[(Ij, Ii)], fdm[k][Ii], fdm[k][Ij],
+                                       ff(Ii, Ij), sign, T, wnfactor[k], wmats)
+            fdm_algos = [a for a in algos if a.startswith("FDM") and a != "FDMmats"]
             if fdm_algos:
                 cbs = {w: O.ChainBinning(lmin, lmax, bins, discard_imm) for w in ("gt", "ls")}
                 for Ii, ei, Ij, ej in pairs:
@@ -768,7 +817,12 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                     for w in parts:
                         for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
                             getattr(full[a], arr)[:] += getattr(cbs[w], arr)
+        if "FDMmats" in algos:  # Matsubara::save with outputxy(..., imagpart=true) (c++/io.hpp:33-38)
+            out[f"{prefix}_FDMmats_dens_{name1}-{name2}"] = np.array(
+                [(wn, g.real, g.imag if abs(g.imag) > abs(g.real) * 1e-10 else 0.0) for wn, g in zip(wmats, gmats)])
         for a in algos:
+            if a == "FDMmats":
+                continue
             fs = full[a]
 
             def trim(w):
