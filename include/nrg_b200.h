@@ -257,16 +257,25 @@ typedef struct nrg_bins {
 NRG_API int nrg_spec_accumulate(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs, const nrg_spec_params* params,
                         const nrg_bins* bins, double* pos, double* neg, void* stream);
 
-/* Replaces the per-pair calc() of Algo_FDMmats (c++/algo_FDM.hpp:153-217) with its
- * ChainMatsubara accumulation (c++/spectrum.hpp:34-42, c++/matsubara.hpp:31-49): the FDM
- * Green's function on the Matsubara axis. The pairs are given as for NRG_SPEC_FDMGT and
- * NRG_SPEC_FDMLS together (rho_i = rhoFDM(Ii) with rdi, rho_j = rhoFDM(Ij) with rdj); every
- * term of both, weight w at energy E = Ej - Ei, adds factor * w / (i w_n - E) to
- * re[n] + i im[n] for n < mats (ACCUMULATED), w_n = (2n+1) pi T for sign = -1 (fermionic)
- * and 2n pi T for sign = +1 (bosonic). For a bosonic operator the D x D term of a pair at
- * n = 0 with |E| <= 1e-8 (WEIGHT_TOL) is -factor * w_gt / T, w_gt its exp(-Ei/T) part
- * (c++/algo_FDM.hpp:178-188). params->algo is not read; params->T, sign and wnf are.
- * 1 <= mats <= 6144. */
+/* Replaces the per-pair calc() of the Matsubara algorithms with their ChainMatsubara
+ * accumulation (c++/spectrum.hpp:34-42, c++/matsubara.hpp:31-49): every term, weight w at
+ * energy E = Ej - Ei, adds factor * w / (i w_n - E) to re[n] + i im[n] for n < mats
+ * (ACCUMULATED), w_n = (2n+1) pi T for sign = -1 (fermionic) and 2n pi T for sign = +1
+ * (bosonic). params->algo selects the terms:
+ *   NRG_SPEC_FDMMATS  Algo_FDMmats (c++/algo_FDM.hpp:153-217): the terms of NRG_SPEC_FDMGT and
+ *                     NRG_SPEC_FDMLS together (rho_i = rhoFDM(Ii) with rdi, rho_j = rhoFDM(Ij)
+ *                     with rdj; abs_G energies; params->wnf)
+ *   NRG_SPEC_FTMATS   Algo_FTmats (c++/algo_FT.hpp:50-91): over the pair's states (give the
+ *                     kept x kept blocks, abs_zero energies), op1 op2 (e^{-Ei/T} - sign
+ *                     e^{-Ej/T}) * params->wnf, wnf = 1 / Z_ft of the step
+ *   NRG_SPEC_DMNRG    Algo_DMNRGmats (c++/algo_DMNRG.hpp:61-106): the DM-NRG weights of
+ *                     nrg_spec_accumulate over kept x kept, without its energy window
+ * For a bosonic operator the reference replaces the n = 0 term with |E| <= 1e-8 (WEIGHT_TOL)
+ * by its limit, and so does this call: -w_gt / T for the FDM D x D term (w_gt its exp(-Ei/T)
+ * part, c++/algo_FDM.hpp:178-188), -op1 op2 e^{-Ej/T} wnf / T for FT (c++/algo_FT.hpp:66-71),
+ * -X op1 / T for DM-NRG (c++/algo_DMNRG.hpp:88-93). 1 <= mats <= 6144. */
+#define NRG_SPEC_FDMMATS 3
+#define NRG_SPEC_FTMATS 4
 NRG_API int nrg_spec_accumulate_mats(nrg_ctx* ctx, int npair, const nrg_spec_pair* pairs,
                                      const nrg_spec_params* params, int mats, double* re, double* im, void* stream);
 

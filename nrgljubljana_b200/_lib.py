@@ -20,6 +20,8 @@ NRG_DIAG_MAX_N = 10240
 NRG_SPEC_DMNRG = 0
 NRG_SPEC_FDMGT = 1
 NRG_SPEC_FDMLS = 2
+NRG_SPEC_FDMMATS = 3
+NRG_SPEC_FTMATS = 4
 
 # Every symbol include/nrg_b200.h declares.
 EXPORTS = ("nrg_version", "nrg_last_error", "nrg_create", "nrg_destroy", "nrg_trim", "nrg_diag_batch",

@@ -354,14 +354,15 @@ def spec_accumulate_array(algo: int, pairs: np.ndarray, grid: BinGrid, pos, neg,
                                       _stream_ptr(stream)), "nrg_spec_accumulate")
 
 
-def spec_accumulate_mats_array(pairs: np.ndarray, mats: int, re, im, sign: int, T: float, wnf: float, ctx=None,
-                               stream=None) -> None:
-    """nrg_spec_accumulate_mats (FDM on the Matsubara axis) on a numpy record array of
-    SPECPAIR_DTYPE (device pointers); re, im: device tensors of mats doubles, accumulated."""
+def spec_accumulate_mats_array(algo: int, pairs: np.ndarray, mats: int, re, im, sign: int, T: float, wnf: float,
+                               ctx=None, stream=None) -> None:
+    """nrg_spec_accumulate_mats (NRG_SPEC_FDMMATS, NRG_SPEC_FTMATS or NRG_SPEC_DMNRG on the
+    Matsubara axis) on a numpy record array of SPECPAIR_DTYPE (device pointers); re, im: device
+    tensors of mats doubles, accumulated."""
     ctx = ctx or context()
     if pairs.dtype != _lib.SPECPAIR_DTYPE or not pairs.flags.c_contiguous:
         raise ValueError("pairs must be a contiguous SPECPAIR_DTYPE array")
-    prm = SpecParams(0, sign, T, wnf, 0.0, 0.0)
+    prm = SpecParams(algo, sign, T, wnf, 0.0, 0.0)
     check(ctx.lib.nrg_spec_accumulate_mats(ctx.ptr, len(pairs), pairs.ctypes.data_as(C.POINTER(SpecPair)),
                                            C.byref(prm), int(mats), C.c_void_p(re.data_ptr()),
                                            C.c_void_p(im.data_ptr()), _stream_ptr(stream)), "nrg_spec_accumulate_mats")

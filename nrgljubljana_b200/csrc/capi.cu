@@ -974,15 +974,25 @@ int nrg_spec_accumulate_mats(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, 
   if (npair == 0) return NRG_OK;
   if (mats < 1 || 2 * sizeof(double) * (size_t)mats > nrg::kSpecSmemMax) return fail(NRG_ERR_ARG, "mats = %d", mats);
   if (!(prm->T > 0.0) || (prm->sign != 1 && prm->sign != -1)) return fail(NRG_ERR_ARG, "bad T or sign");
+  const int algo = prm->algo;
+  if (algo != NRG_SPEC_DMNRG && algo != NRG_SPEC_FDMMATS && algo != NRG_SPEC_FTMATS)
+    return fail(NRG_ERR_ARG, "bad algo %d for the Matsubara sums", algo);
   auto s = static_cast<cudaStream_t>(stream);
   nrg::CallOrder call_order(c, s);
-  // op2_rho = prod_fit(op2, rhoFDM(Ii)) (nj x rdi) and rho_op2 = prod_fit(rhoFDM(Ij), op2) (rdj x ni)
+  // FDMmats: op2_rho = prod_fit(op2, rhoFDM(Ii)) (nj x rdi) and rho_op2 = prod_fit(rhoFDM(Ij), op2)
+  // (rdj x ni); DMNRGmats: X and Y of the DM-NRG weights (ki x kj... as NRG_SPEC_DMNRG)
   std::vector<size_t> xo(npair, 0), yo(npair, 0);
   size_t need = 0;
   for (int p = 0; p < npair; p++) {
     const nrg_spec_pair& q = pairs[p];
     if (q.ni < 0 || q.nj < 0 || q.ki < 0 || q.kj < 0 || q.ki > q.ni || q.kj > q.nj)
       return fail(NRG_ERR_ARG, "pair %d: bad ranges", p);
+    if (algo == NRG_SPEC_DMNRG) {
+      xo[p] = need; need += (size_t)q.kj * q.ki;
+      yo[p] = need; need += (size_t)q.kj * q.ki;
+      continue;
+    }
+    if (algo == NRG_SPEC_FTMATS) continue;
     if (q.ki > q.rdi || q.kj > q.rdj) return fail(NRG_ERR_ARG, "pair %d: rdi < ki or rdj < kj", p);
     xo[p] = need; need += (size_t)q.nj * q.rdi;
     yo[p] = need; need += (size_t)q.rdj * q.ni;
@@ -1007,6 +1017,26 @@ int nrg_spec_accumulate_mats(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, 
     const nrg_spec_pair& q = pairs[p];
     double* X = W + xo[p];
     double* Y = W + yo[p];
+    if (algo == NRG_SPEC_DMNRG) {  // Algo_DMNRGmats: the DM-NRG weights over kept x kept, no window
+      if (q.ki == 0 || q.kj == 0) continue;
+      gp.add_out(X, q.ki, q.kj, q.ki, 0.0);
+      gp.add_seg(q.op2, q.ld2, 0, q.rho_i, q.ldri, 1, q.ki, 1.0);
+      gp.add_out(Y, q.ki, q.kj, q.ki, 0.0);
+      gp.add_seg(q.rho_j, q.ldrj, 0, q.op1, q.ld1, 0, q.kj, 1.0);
+      nrg::SpecRegion r{};
+      r.Ei = q.Ei; r.Ej = q.Ej; r.op1 = q.op1; r.op2 = q.op2; r.X = X; r.Y = Y;
+      r.ld1 = q.ld1; r.ld2 = q.ld2; r.ldx = q.ki; r.ldy = q.ki;
+      r.i0 = 0; r.i1 = q.ki; r.j0 = 0; r.j1 = q.kj;
+      r.kind = nrg::kSpecDMNRG; r.sign = prm->sign; r.mspecial = nrg::kMatsDmnrgA; r.factor = q.factor;
+      r.T = prm->T; r.Emin = -1.0; r.Emax = 1e300;
+      regs.push_back(r);
+      continue;
+    }
+    if (algo == NRG_SPEC_FTMATS) {  // Algo_FTmats: the two exponentials over the pair's states
+      region(q, nrg::kSpecExpI, 0, q.ni, 0, q.nj, nullptr, 0, prm->wnf, nrg::kMatsZero);
+      region(q, nrg::kSpecExpJ, 0, q.ni, 0, q.nj, nullptr, 0, ms * prm->wnf, nrg::kMatsPlusOverT);
+      continue;
+    }
     if (q.rdi > 0 && q.nj > 0) {
       gp.add_out(X, q.rdi, q.nj, q.rdi, 0.0);
       gp.add_seg(q.op2, q.ld2, 0, q.rho_i, q.ldri, 0, std::min(q.rdi, q.ni), 1.0);
@@ -1017,8 +1047,8 @@ int nrg_spec_accumulate_mats(nrg_ctx* c, int npair, const nrg_spec_pair* pairs, 
     }
     // term1 (D x D): weightA (exp(-Ei/T)) + weightB (-sign exp(-Ej/T)); term2 (i in D, j in K):
     // weightA + (-sign) op1 rho_op2; term3 (i in K, j in D): op1 op2_rho + weightB
-    region(q, nrg::kSpecExpI, q.ki, q.ni, q.kj, q.nj, nullptr, 0, prm->wnf, nrg::kMatsGtDD);
-    region(q, nrg::kSpecExpJ, q.ki, q.ni, q.kj, q.nj, nullptr, 0, ms * prm->wnf, nrg::kMatsLsDD);
+    region(q, nrg::kSpecExpI, q.ki, q.ni, q.kj, q.nj, nullptr, 0, prm->wnf, nrg::kMatsMinusOverT);
+    region(q, nrg::kSpecExpJ, q.ki, q.ni, q.kj, q.nj, nullptr, 0, ms * prm->wnf, nrg::kMatsZero);
     region(q, nrg::kSpecExpI, q.ki, q.ni, 0, q.kj, nullptr, 0, prm->wnf, nrg::kMatsPlain);
     region(q, nrg::kSpecGemmX, q.ki, q.ni, 0, q.kj, Y, q.ni, ms, nrg::kMatsPlain);
     region(q, nrg::kSpecGemmX, 0, q.ki, q.kj, q.nj, X, q.rdi, 1.0, nrg::kMatsPlain);

@@ -102,7 +102,8 @@ __global__ void __launch_bounds__(kThreads) spec_bin_kernel(const SpecTask* __re
   }
 }
 
-// Algo_FDMmats (c++/algo_FDM.hpp:167-217) into ChainMatsubara (c++/spectrum.hpp:34-42): every
+// Algo_FDMmats, Algo_FTmats, Algo_DMNRGmats (c++/algo_FDM.hpp:167-217, c++/algo_FT.hpp:63-85,
+// c++/algo_DMNRG.hpp:76-100) into ChainMatsubara (c++/spectrum.hpp:34-42): every
 // term adds factor w / (i w_n - E) = factor w (-E - i w_n) / (E^2 + w_n^2) to point n, for
 // n < mats, into a per-CTA copy of the sums in shared memory, flushed with FP64 atomics.
 __global__ void __launch_bounds__(kThreads) spec_mats_kernel(const SpecTask* __restrict__ tasks,
@@ -126,7 +127,12 @@ __global__ void __launch_bounds__(kThreads) spec_mats_kernel(const SpecTask* __r
     w *= r.factor;
     for (int n = 0; n < mp.mats; n++) {
       if (n == 0 && mp.bosonic && r.mspecial != kMatsPlain && fabs(energy) <= 1e-8) {
-        if (r.mspecial == kMatsGtDD) atomicAdd(re, -w / mp.T);
+        double v = 0.0;
+        if (r.mspecial == kMatsMinusOverT) v = -w / mp.T;
+        else if (r.mspecial == kMatsPlusOverT) v = w / mp.T;
+        else if (r.mspecial == kMatsDmnrgA)
+          v = -r.factor * r.X[(int64_t)j * r.ldx + i] * r.op1[(int64_t)j * r.ld1 + i] / mp.T;
+        if (v != 0.0) atomicAdd(re, v);
         continue;
       }
       const double wn = pt * (double)(mp.bosonic ? 2 * n : 2 * n + 1);

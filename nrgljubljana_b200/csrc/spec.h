@@ -24,14 +24,18 @@ struct SpecRegion {
   int64_t ld1, ld2, ldx, ldy;
   int i0, i1, j0, j1;
   int kind, sign;
-  int mspecial, pad_;  // Matsubara sums: kMatsPlain, kMatsGtDD or kMatsLsDD
+  int mspecial, pad_;  // Matsubara sums: a MatsSpecial
   double coef, factor, T, Emin, Emax;
 };
 
 // How a term enters the Matsubara sum at n = 0 for a bosonic operator when |E| <= 1e-8
-// (WEIGHT_TOL, c++/numerics.hpp:318): the D x D term of Algo_FDMmats (c++/algo_FDM.hpp:
-// 178-188) is -weightA / T there, weightA being its exp(-Ei/T) part and weightB dropped.
-enum MatsSpecial : int { kMatsPlain = 0, kMatsGtDD = 1, kMatsLsDD = 2 };
+// (WEIGHT_TOL, c++/numerics.hpp:318), where the reference replaces (wA + wB) / (i w_0 - E) by
+// a limit: -wA / T for the D x D term of Algo_FDMmats (c++/algo_FDM.hpp:178-188), wA its
+// exp(-Ei/T) part (kMatsMinusOverT on that part, kMatsZero on the other); -op1 op2
+// exp(-E1/T) / (Z T) for Algo_FTmats (c++/algo_FT.hpp:66-71; kMatsPlusOverT on the
+// (-sign) exp(-Ej/T) part, kMatsZero on the other); -wA / T for Algo_DMNRGmats
+// (c++/algo_DMNRG.hpp:88-93), wA = X(j,i) op1(j,i) (kMatsDmnrgA).
+enum MatsSpecial : int { kMatsPlain = 0, kMatsMinusOverT = 1, kMatsZero = 2, kMatsPlusOverT = 3, kMatsDmnrgA = 4 };
 
 struct MatsParams {
   int mats;     // points n = 0 .. mats-1

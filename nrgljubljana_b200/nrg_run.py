@@ -31,7 +31,7 @@ import torch
 
 from . import ddsum, qs
 from ._lib import (GEMM3_DTYPE, HPIECE_DTYPE, NRG_HP_BLOCK, NRG_HP_DIAG, NRG_SPEC_DMNRG, NRG_SPEC_FDMGT,
-                   NRG_SPEC_FDMLS, SPECPAIR_DTYPE)
+                   NRG_SPEC_FDMLS, NRG_SPEC_FDMMATS, NRG_SPEC_FTMATS, SPECPAIR_DTYPE)
 from .api import (BinGrid, Context, broaden, context, diag_batch_ptrs, gemm3_batch_array, hamiltonian_batch,
                   spec_accumulate_array, spec_accumulate_mats_array)
 from .inputs import DataFile, SCALE, parse_param, read_data
@@ -74,7 +74,9 @@ class RunParams:
     fdm: bool = False
     fdmgt: bool = False
     fdmls: bool = False
-    fdmmats: bool = False  # FDM Green's functions on the Matsubara axis (c++/params.hpp:253-254)
+    fdmmats: bool = False  # Green's functions on the Matsubara axis (c++/params.hpp:251-254)
+    dmnrgmats: bool = False
+    finitemats: bool = False
     mats: int = 100
     fdmexpv: bool = False
     fdmexpvn: int = 0
@@ -169,6 +171,12 @@ class RunParams:
         return [a for a, on in (("DMNRG", self.dmnrg), ("FDM", self.fdm), ("FDMgt", self.fdmgt),
                                 ("FDMls", self.fdmls), ("CFS", self.cfs), ("CFSgt", self.cfsgt),
                                 ("CFSls", self.cfsls), ("FT", self.finite)) if on]
+
+    @property
+    def mats_algorithms(self) -> List[str]:
+        """The Matsubara-axis algorithms switched on (c++/oprecalc.hpp:120-131)."""
+        return [a for a, on in (("DMNRGmats", self.dmnrgmats), ("FDMmats", self.fdmmats),
+                                ("FTmats", self.finitemats)) if on]
 
     @property
     def keep_all_states_in_last_step(self) -> bool:
@@ -399,7 +407,7 @@ class QSRun:
         # (file prefix, kind, op1, op2) of the spectra (c++/oprecalc.hpp:160-195)
         self.algos = params.algorithms
         self.specs: List[Tuple[str, str, str, str]] = []
-        if self.algos or params.fdmmats:
+        if self.algos or params.mats_algorithms:
             for prefix, kind, text in (("corr", "s", params.specs), ("spec", "d", params.specd),
                                        ("spin", "t", params.spect)):
                 for tok in text.split():
@@ -525,6 +533,7 @@ class QSRun:
         for I, e in sorted(d.subspaces):
             v = e.copy() if p.data_has_rescaled_energies else e / scale0
             diag[I] = Sub(I, v, 0.0, v.copy(), len(v), len(v), n=len(v))
+        self.diag0 = diag  # the initial cluster, for the first run's spectra at N = -1 (Algo_FTmats)
         # <||f||> of every channel in one channel-major set; the keys each channel holds are
         # kept, as offdiag_function() needs its channel's matrix to exist
         ocs = [d.opch[ch][0] for ch in range(d.channels)]
@@ -961,7 +970,7 @@ class QSRun:
         matrices with the FDM thermodynamics (calc_rhoFDM), then the spectral pass over the
         kept steps (the second run of the reference without its diagonalisations)."""
         p = self.p
-        rhos = self._rho_dmnrg() if ("DMNRG" in self.algos or p.cfs_flags) else None  # Params::need_rho
+        rhos = self._rho_dmnrg() if ("DMNRG" in self.algos or p.dmnrgmats or p.cfs_flags) else None  # need_rho
         fdm = self._rho_fdm() if p.fdm_flags else None
         if fdm is not None:
             res.tdfdm = (["T", "E_fdm", "C_fdm", "F_fdm", "S_fdm"], fdm["tdrow"])
@@ -1174,9 +1183,12 @@ class QSRun:
         zeros = lambda: torch.zeros(nb, dtype=torch.float64, device=self.dev)  # noqa: E731
         dm_acc = {j: (np.zeros(nb), np.zeros(nb)) for j in range(len(self.specs))} if rhos is not None else {}
         fdm_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in fdm_parts}
-        # Algo_FDMmats: one GFMatsubara per spectrum, mats complex points (c++/spectrum.hpp:212-227)
+        # the Matsubara algorithms: one GFMatsubara per spectrum, mats complex points
+        # (c++/spectrum.hpp:212-227), every step's sums merged whole
         zm = lambda: torch.zeros(p.mats, dtype=torch.float64, device=self.dev)  # noqa: E731
-        mats_acc = {j: (zm(), zm()) for j in range(len(self.specs))} if p.fdmmats else {}
+        mats_acc = {(a, j): (zm(), zm()) for a in p.mats_algorithms for j in range(len(self.specs))}
+        if "FTmats" in p.mats_algorithms and p.calc0 and self.specs:
+            self._ftmats_initial(kinds, mats_acc)
         cfs_parts_of = {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}
         cfs_parts = sorted({w for a in self.algos if a in cfs_parts_of for w in cfs_parts_of[a]})
         cfs_acc = {(j, w): (zeros(), zeros()) for j in range(len(self.specs)) for w in cfs_parts}
@@ -1192,7 +1204,7 @@ class QSRun:
                           else self._recalc_tensor(st.diag, m, *tables[kind], rows)) for kind, m in cur.items()}
             dg = st.diag
             merge = p.NN1 or p.NN2avg or ((st.N % 2 == 0) if p.NN2even else (st.N % 2 == 1))
-            if "DMNRG" in self.algos and merge and self.specs:
+            if ("DMNRG" in self.algos and merge or p.dmnrgmats) and self.specs:
                 rhoN = rhos[k]
                 eoff, flat, o = {}, [], 0
                 for I, s in dg.items():  # abs_zero energies of the kept states (c++/eigen.hpp:45)
@@ -1223,6 +1235,12 @@ class QSRun:
                             pairs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2),
                                           ld, rhoN.ptr(Ii), ki, rhoN.ptr(Ij), kj, ki, ki, kj, kj, ki, kj, ff(Ii, Ij)))
                     if not pairs:
+                        continue
+                    if p.dmnrgmats:  # Algo_DMNRGmats::calc at every step (c++/algo_DMNRG.hpp:76-100)
+                        re, im = mats_acc[("DMNRGmats", j)]
+                        spec_accumulate_mats_array(NRG_SPEC_DMNRG, np.array(pairs, dtype=SPECPAIR_DTYPE), p.mats, re,
+                                                   im, sign, p.T, 0.0, ctx=self.ctx, stream=self.stream)
+                    if not ("DMNRG" in self.algos and merge):
                         continue
                     pos, neg = zeros(), zeros()
                     spec_accumulate_array(NRG_SPEC_DMNRG, np.array(pairs, dtype=SPECPAIR_DTYPE), grid, pos, neg,
@@ -1267,24 +1285,26 @@ class QSRun:
                                                   sign=sign, T=p.T, wnf=fdm["wnfactor"][k], ctx=self.ctx,
                                                   stream=self.stream)
                     if p.fdmmats and mt:  # Algo_FDMmats::calc over the same pairs (c++/algo_FDM.hpp:167-217)
-                        re, im = mats_acc[j]
-                        spec_accumulate_mats_array(np.array(mt, dtype=SPECPAIR_DTYPE), p.mats, re, im, sign, p.T,
-                                                   fdm["wnfactor"][k], ctx=self.ctx, stream=self.stream)
+                        re, im = mats_acc[("FDMmats", j)]
+                        spec_accumulate_mats_array(NRG_SPEC_FDMMATS, np.array(mt, dtype=SPECPAIR_DTYPE), p.mats, re, im,
+                                                   sign, p.T, fdm["wnfactor"][k], ctx=self.ctx, stream=self.stream)
             if "FT" in self.algos and merge and self.specs:
                 self._ft_step(st, cur, kinds, grid, ebins, Efac, ft_acc)
+            if p.finitemats and self.specs:
+                self._ftmats_step(st, cur, kinds, mats_acc)
             if cfs_parts and self.specs:
                 self._cfs_step(st, last, None if last else rhos[k], cur, kinds, grid, cfs_parts, cfs_acc)
             if fdm is not None and p.fdmexpv and st.N == p.fdmexpvn:
                 expv = self._fdm_expv(k, st, cur["s"], fdm)
         out: Dict[str, np.ndarray] = {}
         raw: Dict[str, np.ndarray] = {}
-        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
-            if p.fdmmats:  # GFMatsubara::save: w_n, Re, Im (outputxy with imagpart, c++/io.hpp:33-38)
-                sign = kinds[kind][0]
-                wn = p.T * math.pi * (2 * np.arange(p.mats) + (0 if sign == 1 else 1))
-                g_re, g_im = (x.cpu().numpy() for x in mats_acc[j])
-                g_im = np.where(np.abs(g_im) > np.abs(g_re) * 1e-10, g_im, 0.0)
-                out[f"{prefix}_FDMmats_dens_{n1}-{n2}"] = np.stack([wn, g_re, g_im], axis=1)
+        for (a, j), (g_re, g_im) in mats_acc.items():  # GFMatsubara::save: w_n, Re, Im (c++/io.hpp:33-38)
+            prefix, kind, n1, n2 = self.specs[j]
+            sign = kinds[kind][0]
+            wn = p.T * math.pi * (2 * np.arange(p.mats) + (0 if sign == 1 else 1))
+            g_re, g_im = g_re.cpu().numpy(), g_im.cpu().numpy()
+            g_im = np.where(np.abs(g_im) > np.abs(g_re) * 1e-10, g_im, 0.0)
+            out[f"{prefix}_{a}_dens_{n1}-{n2}"] = np.stack([wn, g_re, g_im], axis=1)
         omega0 = p.omega0 if p.omega0 >= 0.0 else p.omega0_ratio * p.T
         bmin = p.broaden_min if p.broaden_min > 0.0 else p.broaden_min_ratio * last_scale
         mesh = []
@@ -1311,6 +1331,51 @@ class QSRun:
                 if p.savebins:
                     raw[name] = raw_bins(full_pos, full_neg, ebins, p.discard_trim, p.reim)
         return out, raw, expv
+
+    def _ftmats_add(self, dg: Dict[Invar, Sub], scale: float, cur: Dict, kinds: Dict, mats_acc: Dict) -> None:
+        """Algo_FTmats::calc (c++/algo_FT.hpp:63-85) of one step for every spectrum: over
+        kept(Ij) x kept(Ii), op1 op2 ((-sign) e^{-E1/T} + e^{-Ep/T}) / (Z_ft (i w_n - (E1 - Ep)))
+        with the abs_zero energies and stats.Zft of the step (calc_Z, c++/measurements.hpp:
+        189-191), one nrg_spec_accumulate_mats call per spectrum."""
+        p = self.p
+        scT = scale / p.T
+        Z = sum(qs.mult(I) * float(np.sum(np.exp(-s.corr[:s.nkept] * scT))) for I, s in dg.items())
+        eoff, flat, o = {}, [], 0
+        for I, s in dg.items():  # abs_zero energies of the kept states (c++/eigen.hpp:45)
+            eoff[I] = o
+            flat.append((s.values[:s.nkept] - s.shift) * scale)
+            o += s.nkept
+        Edev = self._h2d(np.concatenate(flat) if flat else np.zeros(1))
+        eb = Edev.data_ptr()
+        for j, (prefix, kind, n1, n2) in enumerate(self.specs):
+            sign, ff, names = kinds[kind]
+            ops = cur[kind]
+            o1, o2 = names.index(n1), names.index(n2)
+            prs = []
+            for Ii, si in dg.items():
+                for Ij, sj in dg.items():
+                    key = Ii if kind == "s" else (Ij, Ii)
+                    if (kind == "s" and Ij != Ii) or key not in ops.loc:
+                        continue
+                    ki, kj = si.nkept, sj.nkept
+                    if ki == 0 or kj == 0:
+                        continue
+                    ld = ops.loc[key][2]
+                    prs.append((eb + 8 * eoff[Ii], eb + 8 * eoff[Ij], ops.ptr(key, o1), ld, ops.ptr(key, o2), ld,
+                                0, 1, 0, 1, ki, 0, kj, 0, 0, 0, ff(Ii, Ij)))
+            if prs:
+                re, im = mats_acc[("FTmats", j)]
+                spec_accumulate_mats_array(NRG_SPEC_FTMATS, np.array(prs, dtype=SPECPAIR_DTYPE), p.mats, re, im, sign,
+                                           p.T, 1.0 / Z, ctx=self.ctx, stream=self.stream)
+
+    def _ftmats_step(self, st: "_StepRecord", cur: Dict, kinds: Dict, mats_acc: Dict) -> None:
+        self._ftmats_add(st.diag, st.scale, cur, kinds, mats_acc)
+
+    def _ftmats_initial(self, kinds: Dict, mats_acc: Dict) -> None:
+        """docalc0 runs the first run's spectral algorithms on the initial cluster as well
+        (c++/core.hpp:251-260): the data file's eigenvalues with shift 0 and scale SCALE(Ninit),
+        every state kept, the operators as read (c++/eigen.hpp:219-226, 314)."""
+        self._ftmats_add(self.diag0, self.scale(-1), dict(self.spec_init), kinds, mats_acc)
 
     def _ft_step(self, st: "_StepRecord", cur: Dict, kinds: Dict, grid: BinGrid, ebins: np.ndarray, Efac: float,
                  ft_acc: Dict) -> None:

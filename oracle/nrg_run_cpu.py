@@ -160,7 +160,8 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         """Singlets, then global operators, each by name (c++/output.hpp:121-127)."""
         return sorted(set(names) - gops) + sorted(set(names) & gops)
     # spectral algorithms (c++/oprecalc.hpp:107-132) and the FDM flags (c++/params.hpp:535-541)
-    algos = [a for a, k in (("DMNRG", "dmnrg"), ("FDM", "fdm"), ("FDMgt", "fdmgt"), ("FDMls", "fdmls"), ("FDMmats", "fdmmats"),
+    algos = [a for a, k in (("DMNRG", "dmnrg"), ("DMNRGmats", "dmnrgmats"), ("FDM", "fdm"), ("FDMgt", "fdmgt"),
+                            ("FDMls", "fdmls"), ("FDMmats", "fdmmats"), ("FTmats", "finitemats"),
                             ("CFS", "cfs"), ("CFSgt", "cfsgt"), ("CFSls", "cfsls"), ("FT", "finite")) if flag(k)]
     dm = spectra is not None and bool(algos)
     fdm_needed = fdm_flags and (spectra is not None or fdm_out is not None)
@@ -262,11 +263,18 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
             annotated_out.extend("%s %d %d" % (num(e), I[0], I[1]) for e, I in lst[:n])
         annotated_out.append("")
 
+    init_spec = None
     if kv.get("calc0", "true").lower() == "true":
         dump_energies(diag, -1)
         annotate(diag, SCALE(0, Lam, disc, z, brs))
         td(-1, diag)
         custom(-1, diag, ops)
+        # docalc0 runs the first run's spectral algorithms on the initial cluster too
+        # (c++/core.hpp:251-260): its eigenvalues with shift 0 and scale SCALE(Ninit), every
+        # state kept, the operators as read (c++/eigen.hpp:219-226, 314)
+        init_spec = (SCALE(0, Lam, disc, z, brs), {I: e.values.copy() for I, e in diag.items()},
+                     {"s": {name: {(I, I): m for I, m in ops[name].items()} for name in ops},
+                      "d": {name: dict(m) for name, m in dops.items()}, "t": {name: dict(m) for name, m in tops.items()}})
 
     for N in range(Nmax):
         last = N == Nmax - 1
@@ -448,7 +456,7 @@ def run(param_text: str, data_text: str, threads: int = 1, spectra: dict = None,
         diag = new
     if (dm or fdm_needed) and steps:
         _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos if dm else [], spectra, fdm_out if fdm_flags else None,
-                    total_energy, C, singlet_order(ops), bins_out=bins_out)
+                    total_energy, C, singlet_order(ops), bins_out=bins_out, init_spec=init_spec)
     td_fields = ["T", "<Sz^2>", "<Q>", "<Q^2>", "<E>", "<E^2>", "C", "F", "S"]
     return td_fields, td_rows, ["T"] + singlet_order(ops), custom_rows
 
@@ -591,7 +599,43 @@ def mats_pair(EGi, Ki, EGj, Kj, o1, o2, rho_i, rho_j, factor, sign, T, wnf, w):
     return factor * G
 
 
-def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None):
+def mats_sum(wt, E, w, special=None):
+    """sum over the (j, i) terms of wt / (i w_n - E) for every Matsubara point w_n; `special`
+    replaces the n = 0 terms with |E| <= WEIGHT_TOL (1e-8) when given (bosonic operators)."""
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t = wt[:, :, None] / (1j * w[None, None, :] - E[:, :, None])
+    if special is not None:
+        t[:, :, 0] = np.where(np.abs(E) <= 1e-8, special, t[:, :, 0])
+    return t.sum(axis=(0, 1))
+
+
+def dmnrg_mats_pair(Em, Ej, o1, o2, rho_p, rho_1, factor, sign, T, w):
+    """Algo_DMNRGmats::calc (c++/algo_DMNRG.hpp:76-100) of one pair over kept(Ip) x kept(I1):
+    weightA = (sum_ri op2(rj, ri) rho(Ip)(rm, ri)) op1(rj, rm), weightB = (sum_ri op1(ri, rm)
+    rho(I1)(rj, ri)) op2(rj, rm), term (weightA - sign weightB) / (i w_n - (Ej - Em)); for a
+    bosonic operator at n = 0 and |Ej - Em| <= 1e-8 the term is -weightA / T."""
+    if o1.size == 0:
+        return np.zeros(len(w), dtype=complex)
+    wA = (o2 @ rho_p.T) * o1
+    wB = (rho_1 @ o1) * o2
+    E = Ej[:, None] - Em[None, :]
+    return factor * mats_sum(wA + (-sign) * wB, E, w, -wA / T if sign == 1 else None)
+
+
+def ft_mats_pair(Ep, E1, o1, o2, Z, factor, sign, T, w):
+    """Algo_FTmats::calc (c++/algo_FT.hpp:63-85) of one pair over kept(I1) x kept(Ip):
+    op1 op2 ((-sign) e^{-E1/T} + e^{-Ep/T}) / (Z (i w_n - (E1 - Ep))); for a bosonic operator at
+    n = 0 and |E1 - Ep| <= 1e-8 the term is -op1 op2 e^{-E1/T} / (Z T)."""
+    if o1.size == 0:
+        return np.zeros(len(w), dtype=complex)
+    P = o1 * o2
+    E = E1[:, None] - Ep[None, :]
+    wt = P * ((-sign) * np.exp(-E1 / T)[:, None] + np.exp(-Ep / T)[None, :]) / Z
+    return factor * mats_sum(wt, E, w, -P * np.exp(-E1 / T)[:, None] / (Z * T) if sign == 1 else None)
+
+
+def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, combs, singlet_names, bins_out=None,
+                init_spec=None):
     """The DMNRG run (c++/nrg-general.hpp:139-168): the density matrices (calc_rho +
     calc_densitymatrix for DMNRG, c++/dmnrg.hpp:43-133; calc_rhoFDM for FDM,
     c++/dmnrg.hpp:146-217), then per step the spectra of every algorithm
@@ -664,7 +708,7 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
 
     rhos = fdm = None
     Zft = None
-    if "DMNRG" in algos or any(a.startswith("CFS") for a in algos):  # Params::need_rho
+    if "DMNRG" in algos or "DMNRGmats" in algos or any(a.startswith("CFS") for a in algos):  # Params::need_rho
         # init_rho over the kept states of the last step (c++/dmnrg.hpp:43-50)
         _, scale_last, diag_last, _, _, _ = steps[-1]
         scT = scale_last / T
@@ -726,10 +770,21 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
         E /= bratio
     for prefix, kind, name1, name2 in specs:
         sign, ff = kinds[kind]
-        full = {a: O.ChainBinning(lmin, lmax, bins, discard_imm) for a in algos if a != "FDMmats"}
-        # GFMatsubara of FDMmats (c++/spectrum.hpp:212-227): mats points w_n = ww(n, gt, T)
+        full = {a: O.ChainBinning(lmin, lmax, bins, discard_imm) for a in algos if not a.endswith("mats")}
+        # GFMatsubara of the Matsubara algorithms (c++/spectrum.hpp:212-227): mats points
+        # w_n = ww(n, gt, T), every step's sums merged whole
         wmats = T * math.pi * (2 * np.arange(nmats) + (0 if sign == 1 else 1))
-        gmats = np.zeros(nmats, dtype=complex)
+        gm = {a: np.zeros(nmats, dtype=complex) for a in algos if a.endswith("mats")}
+        if "FTmats" in algos and init_spec is not None:  # the initial cluster (docalc0), all states kept
+            scale0, vals0, opsets0 = init_spec
+            o1s, o2s = opsets0[kind].get(name1, {}), opsets0[kind].get(name2, {})
+            Z0 = sum(I[1] * float(np.sum(np.exp(-v * scale0 / T))) for I, v in vals0.items())
+            for Ii in vals0:
+                for Ij in vals0:
+                    key = (Ij, Ii)
+                    if key in o1s and key in o2s and o1s[key].size:
+                        gm["FTmats"] += ft_mats_pair(vals0[Ii] * scale0, vals0[Ij] * scale0, o1s[key], o2s[key], Z0,
+                                                     ff(Ii, Ij), sign, T, wmats)
         for k, (N, scale, diagN, _, opsets, Tshift) in enumerate(steps):
             op1, op2 = opsets[kind][name1], opsets[kind][name2]
             last = k == nst - 1
@@ -793,7 +848,23 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                     for w in {"CFS": ("gt", "ls"), "CFSgt": ("gt",), "CFSls": ("ls",)}[a]:
                         for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
                             getattr(full[a], arr)[:] += getattr(cbs[w], arr)
+            if "DMNRGmats" in algos:
+                for Ii, ei, Ij, ej in pairs:
+                    ki, kj = ei.nrpost, ej.nrpost
+                    gm["DMNRGmats"] += dmnrg_mats_pair((ei.values[:ki] - ei.shift) * scale,
+                                                       (ej.values[:kj] - ej.shift) * scale, op1[(Ij, Ii)][:kj, :ki],
+                                                       op2[(Ij, Ii)][:kj, :ki], rhos[k][Ii], rhos[k][Ij], ff(Ii, Ij),
+                                                       sign, T, wmats)
+            if "FTmats" in algos:
+                scT = scale / T
+                Zk = sum(I[1] * sum(math.exp(-c * scT) for c in e.corr[:e.nrpost]) for I, e in diagN.items())
+                for Ii, ei, Ij, ej in pairs:
+                    ki, kj = ei.nrpost, ej.nrpost
+                    gm["FTmats"] += ft_mats_pair((ei.values[:ki] - ei.shift) * scale, (ej.values[:kj] - ej.shift) * scale,
+                                                 op1[(Ij, Ii)][:kj, :ki], op2[(Ij, Ii)][:kj, :ki], Zk, ff(Ii, Ij), sign,
+                                                 T, wmats)
             if "FDMmats" in algos:
+                gmats = gm["FDMmats"]
                 for Ii, ei, Ij, ej in pairs:
                     Ki = 0 if last else ei.nrpost
                     Kj = 0 if last else ej.nrpost
@@ -817,11 +888,11 @@ def _dm_outputs(kv, steps, Lam, disc, z, Nmax, specs, algos, out, fdm_out, GS, c
                     for w in parts:
                         for arr in ("pos_re", "pos_im", "neg_re", "neg_im"):
                             getattr(full[a], arr)[:] += getattr(cbs[w], arr)
-        if "FDMmats" in algos:  # Matsubara::save with outputxy(..., imagpart=true) (c++/io.hpp:33-38)
-            out[f"{prefix}_FDMmats_dens_{name1}-{name2}"] = np.array(
-                [(wn, g.real, g.imag if abs(g.imag) > abs(g.real) * 1e-10 else 0.0) for wn, g in zip(wmats, gmats)])
+        for a, g_all in gm.items():  # Matsubara::save with outputxy(..., imagpart=true) (c++/io.hpp:33-38)
+            out[f"{prefix}_{a}_dens_{name1}-{name2}"] = np.array(
+                [(wn, g.real, g.imag if abs(g.imag) > abs(g.real) * 1e-10 else 0.0) for wn, g in zip(wmats, g_all)])
         for a in algos:
-            if a == "FDMmats":
+            if a.endswith("mats"):
                 continue
             fs = full[a]
 

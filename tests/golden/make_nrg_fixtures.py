@@ -35,10 +35,11 @@ CASES = [
     "test33_Delta", "test34_bandrescale", "test49_template1", "test51_template2", "test53_template3",
     "test63_dumpsubspaces", "c++sym_all/legacy_globalop_Q1Q2-QS",
     "test21_mats", "test2_algorithms_fdmmats", "legacy_matsubara_test1-qs",
+    "test_dmnrg_only", "test2_algorithms_finitemats", "test65_algorithms_mats", "test0_clean",
 ]
 # spectra of the DM-NRG, FDM (real frequencies and Matsubara), CFS and FT algorithms, FDM thermodynamics and expectation values,
 # and the annotated eigenvalue lists (annotated.dat)
-SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|FDM|FDMgt|FDMls|FDMmats|CFS|CFSgt|CFSls|FT)_dens_.*\.dat$")
+SPECTRUM = re.compile(r"^(spec|corr|spin)_(DMNRG|DMNRGmats|FDM|FDMgt|FDMls|FDMmats|CFS|CFSgt|CFSls|FT|FTmats)_dens_.*\.dat$")
 
 
 def main(ref_root: str) -> None:

@@ -1,10 +1,12 @@
-"""FDM Green's functions on the Matsubara axis (Algo_FDMmats, c++/algo_FDM.hpp:153-217; saved by
-GFMatsubara, c++/spectrum.hpp:212-227) against the reference's regression outputs
-{spec,corr,spin}_FDMmats_dens_*.dat of test21_mats, test2_algorithms_fdmmats and
-legacy_matsubara_test1-qs (rows w_n, Re G, Im G, printed to 10 significant digits), beside the
-real-frequency FDM spectra of the same runs: the oracle on the CPU, the device run (the FDM terms
-of every subspace pair summed over the Matsubara points by nrg_spec_accumulate_mats) on the
-GPU against both."""
+"""Green's functions on the Matsubara axis -- Algo_FDMmats (c++/algo_FDM.hpp:153-217),
+Algo_DMNRGmats (c++/algo_DMNRG.hpp:61-106) and Algo_FTmats (c++/algo_FT.hpp:50-91, with the
+initial cluster of docalc0, c++/core.hpp:251-260), saved by GFMatsubara (c++/spectrum.hpp:
+212-227) -- against the reference's regression outputs {spec,corr,spin}_*mats_dens_*.dat (rows
+w_n, Re G, Im G, printed to 10 significant digits) of test21_mats, test2_algorithms_fdmmats,
+legacy_matsubara_test1-qs, test_dmnrg_only, test2_algorithms_finitemats, test65_algorithms_mats
+(all six algorithms in one run) and test0_clean, beside the real-frequency spectra of the same
+runs: the oracle on the CPU, the device run (the terms of every subspace pair summed over the
+Matsubara points by nrg_spec_accumulate_mats) on the GPU against both."""
 import os
 
 import numpy as np
@@ -14,7 +16,8 @@ from test_dmnrg import ATOL_REL_TO_MAX, ORA_ATOL_REL_TO_MAX, ORA_RTOL, RTOL, ass
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden", "nrg")
-CASES = ["test21_mats", "test2_algorithms_fdmmats", "legacy_matsubara_test1-qs"]
+CASES = ["test21_mats", "test2_algorithms_fdmmats", "legacy_matsubara_test1-qs", "test_dmnrg_only",
+         "test2_algorithms_finitemats", "test65_algorithms_mats", "test0_clean"]
 MATS_RTOL = 2e-9   # the reference's 10 printed digits
 MATS_ORA_RTOL = 1e-9  # device against the oracle: other eigensolver, other summation order
 
@@ -31,7 +34,7 @@ def rows(case, name):
 
 def files(case, mats):
     return sorted(f[:-4] for f in os.listdir(os.path.join(GOLD, case))
-                  if f.endswith(".dat") and f.startswith(("spec_", "corr_", "spin_")) and ("FDMmats" in f) == mats)
+                  if f.endswith(".dat") and f.startswith(("spec_", "corr_", "spin_")) and ("mats_dens" in f) == mats)
 
 
 def assert_mats(got, want, rtol, what):

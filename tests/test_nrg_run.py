@@ -80,8 +80,7 @@ def test_param_reader_rejects_unsupported():
     from nrgljubljana_b200.nrg_run import RunParams
     p = RunParams.from_param(parse_param(read("test15_safeguard", "param")))
     assert (p.keep, p.safeguard, p.Lambda) == (100, 0.1, 2.0)
-    for bad in ("Ninit=1", "diagratio=0.1", "substeps=true", "absolute=true", "strategy=some", "dmnrgmats=true",
-                "finitemats=true"):
+    for bad in ("Ninit=1", "diagratio=0.1", "substeps=true", "absolute=true", "strategy=some", "specgt=A_d-A_d"):
         with pytest.raises(ValueError):
             RunParams.from_param(parse_param("[param]\n" + bad + "\n"))
 

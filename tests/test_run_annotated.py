@@ -164,7 +164,7 @@ SUBSPACE_CASES = sorted(c for c in os.listdir(GOLD) if os.path.exists(os.path.jo
 
 
 def test_subspace_cases_present():
-    assert SUBSPACE_CASES == ["test63_dumpsubspaces"]
+    assert SUBSPACE_CASES == ["test63_dumpsubspaces", "test_dmnrg_only"]
 
 
 @pytest.mark.parametrize("case", SUBSPACE_CASES)
